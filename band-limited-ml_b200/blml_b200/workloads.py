@@ -1,0 +1,71 @@
+"""Seeded synthetic inputs with the shapes of the binned path's workloads (NumPy on the host, so the GPU path and
+any CPU checker see identical arrays). There is no public dataset on this path; every workload is generated.
+
+  lattice_1d_mixture   1,024-bin histogram of n = 1e5 draws of a 3-component Gaussian mixture (means .3/.5/.7, sd .05,
+                       weights .3/.4/.3), clipped to [0, 1): the 1-D sinc fit.
+  two_disk_field       counts ~ Poisson(N p) on an (M1, M2) torus, p = 0.95 |h|^2 / sum |h|^2 + 0.05 / (M1 M2), h the
+                       inverse DFT of two displaced disks in the band with a random relative phase: the pball fits.
+  cutoff_sweep         64 such fits of uneven size and cut-off with an 80/20 binomial held-out split.
+  points_5d_mixture    n = 2e5 points of an 8-component 5-D Gaussian mixture in the unit cube for the pair path.
+"""
+import numpy as np
+
+SIDES = (64, 96, 128, 192, 256, 384)
+
+
+def lattice_1d_mixture(seed=0, n=100_000, m=1024):
+    rng = np.random.default_rng(seed)
+    comp = rng.choice(3, n, p=[0.3, 0.4, 0.3])
+    x = np.array([0.3, 0.5, 0.7])[comp] + 0.05 * rng.standard_normal(n)
+    x = np.clip(x, 0.0, np.nextafter(1.0, 0.0))
+    return np.bincount(np.floor(x * m).astype(np.int64), minlength=m).astype(np.float64)
+
+
+def two_disk_field(shape=(256, 256), fc=0.33, N=1e6, seed=0, diameter=None, shift=None, bg=0.05):
+    """Counts on an (M1, M2) torus from a field whose spectrum is two disks of diameter `diameter` (cycles/bin,
+    default fc / 2) displaced by +-shift along axis 0 (default fc / 4), so both lie inside the pball band of
+    cut-off fc, with a uniformly random relative phase."""
+    rng = np.random.default_rng(seed)
+    M1, M2 = shape
+    diameter = fc / 2 if diameter is None else diameter
+    shift = fc / 4 if shift is None else shift
+    k1 = np.fft.fftfreq(M1)[:, None]; k2 = np.fft.fftfreq(M2)[None, :]
+    r = diameter / 2
+    A = ((k1 - shift) ** 2 + k2 ** 2 <= r * r).astype(complex)
+    A = A + np.exp(2j * np.pi * rng.uniform()) * ((k1 + shift) ** 2 + k2 ** 2 <= r * r)
+    h = np.fft.ifft2(A)
+    p = (1 - bg) * np.abs(h) ** 2 / np.sum(np.abs(h) ** 2) + bg / (M1 * M2)
+    return rng.poisson(N * p).astype(np.float64)
+
+
+def pball_modes(shape, fc, bg_fc=None):
+    """The signal pball mode over both columns with the lattice as its period, plus an optional background pball."""
+    per = [float(shape[0]), float(shape[1])]
+    modes = [{(0, 1): dict(kind='pball', fc=float(fc), period=per)}]
+    if bg_fc is not None:
+        modes.append({(0, 1): dict(kind='pball', fc=float(bg_fc), period=per)})
+    return modes
+
+
+def cutoff_sweep(seed=0, n_fits=64):
+    """Fit i: sides from SIDES, fc from geomspace(0.05, 0.45, 16), N = 10^U(4, 6), drawn with default_rng(seed + i);
+    train = Binomial(counts, 0.8), held-out = counts - train."""
+    grid = np.geomspace(0.05, 0.45, 16)
+    fits = []
+    for i in range(n_fits):
+        rng = np.random.default_rng(seed + i)
+        M1, M2 = int(rng.choice(SIDES)), int(rng.choice(SIDES))
+        fc = float(rng.choice(grid)); N = float(10 ** rng.uniform(4, 6))
+        counts = two_disk_field((M1, M2), fc=fc, N=N, seed=seed + 1000 + i)
+        train = rng.binomial(counts.astype(np.int64), 0.8).astype(np.float64)
+        fits.append(dict(shape=(M1, M2), fc=fc, N=N, counts=counts, train=train, val=counts - train))
+    return fits
+
+
+def points_5d_mixture(seed=0, n=200_000, d=5, comps=8):
+    rng = np.random.default_rng(seed)
+    means = rng.uniform(0.2, 0.8, (comps, d)); sds = rng.uniform(0.03, 0.1, (comps, d))
+    wts = rng.dirichlet(np.ones(comps))
+    c = rng.choice(comps, n, p=wts)
+    X = means[c] + sds[c] * rng.standard_normal((n, d))
+    return np.clip(X, 0.0, np.nextafter(1.0, 0.0))

@@ -1,0 +1,58 @@
+"""The model specs behind the golden fixtures (shared by tests/golden/make_golden.py and the tests). Modes are plain
+dicts in the reference's modes format, built with the oracle's make_modes restatement."""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, '..', 'oracle'))
+sys.path.insert(0, os.path.join(HERE, '..', 'band-limited-ml_b200'))
+from blml_oracle import make_modes          # noqa: E402
+from blml_b200.workloads import pball_modes  # noqa: E402
+
+# name: (shape, modes, h); the E / U arrays and the complex flag are in matvec.npz
+MATVEC_SPECS = {
+    'd1_sinc40': ((40,), make_modes([0.35], ['sinc']), 1.0),
+    'd1_sinc1024': ((1024,), make_modes([0.05], ['sinc']), 1.0),
+    'd1_slits64': ((64,), make_modes([0.3], ['slits:0.4']), 1.0),
+    'd1_dir_circ32': ((32,), make_modes([0.3], ['dirichlet'], periods=[32.0]), 1.0),
+    'd1_dir_long32': ((32,), make_modes([0.3], ['dirichlet'], periods=[50.0]), 1.0),
+    'd2_pball64': ((64, 64), pball_modes((64, 64), 0.33, 3 / 64), 1.0),
+    'd2_pball_rect': ((48, 80), pball_modes((48, 80), 0.25), 1.0),
+    'd2_pball_linear': ((24, 24), [{(0, 1): dict(kind='pball', fc=0.33, period=[31.0, 31.0])}], 1.0),
+    'd2_sinc_dir': ((24, 24), make_modes([0.4, 0.3], ['sinc', 'dirichlet'], periods=[None, 24.0]), 1.0),
+    'd2_ball': ((24, 24), make_modes([0.4, 0.4], ['ball', 'ball']), 1.0),
+    'd2_ball_h': ((24, 24), make_modes([0.8, 0.8], ['ball', 'ball']), 0.5),
+    'd3_sinc': ((10, 10, 10), make_modes([0.5] * 3, ['sinc'] * 3), 1.0),
+}
+MATVEC_COMPLEX = {'d1_slits64', 'd1_dir_circ32', 'd2_pball64', 'd2_pball_rect', 'd2_pball_linear', 'd2_sinc_dir',
+                  'd2_ball_h'}
+
+UPDATE_MODES = {
+    'real1': pball_modes((16, 16), 0.4),
+    'psd_eq': make_modes([0.4, 0.4], ['sinc', 'sinc'], rank=2),
+    'psd_sec': pball_modes((16, 16), 0.4, 0.2),
+}
+
+# name: (modes, fit kwargs, constructor kwargs); counts are in fits.npz
+FIT_SPECS = {
+    'd1_sinc_real': (make_modes([0.35], ['sinc']), {}, dict(tol=1e-9)),
+    'd1_sinc_complex': (make_modes([0.35], ['sinc']), dict(complex_g=True), dict(tol=1e-9)),
+    'd1_sinc_rank2_real': (make_modes([0.35], ['sinc'], rank=2), {}, dict(tol=1e-8)),
+    'd1_sinc_rank2_permode': (make_modes([[0.35], [0.12]], ['sinc']), dict(complex_g=True), dict(tol=1e-8)),
+    'd1_dir_circ_real': (make_modes([0.3], ['dirichlet'], periods=[32.0]), {}, dict(tol=1e-9)),
+    'd2_sinc_sinc_real': (make_modes([0.4, 0.3], ['sinc', 'sinc']), {}, dict(tol=1e-9)),
+    'd2_ball_real': (make_modes([0.4, 0.4], ['ball', 'ball']), {}, dict(tol=1e-9)),
+    'd2_pball_lbfgs': (pball_modes((32, 32), 0.33), dict(complex_g=True), dict(tol=1e-8, solver='lbfgs', max_sweeps=3000)),
+    'd2_pball_bg_lbfgs': (pball_modes((32, 32), 0.33, 3 / 32), dict(complex_g=True),
+                          dict(tol=1e-8, solver='lbfgs', max_sweeps=3000)),
+    'd2_pball_cd': (pball_modes((32, 32), 0.33), dict(complex_g=True), dict(tol=1e-7, max_sweeps=3000)),
+    'c1_sinc1024': (make_modes([0.05], ['sinc']), {}, dict(tol=1e-7)),
+}
+
+
+def hist(rng, shape, n, f):
+    g = np.meshgrid(*[np.arange(m, dtype=float) for m in shape], indexing='ij')
+    p = f(*g); p = p / p.sum()
+    return rng.multinomial(n, p.ravel()).reshape(shape).astype(float)
