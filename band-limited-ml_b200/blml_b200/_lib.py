@@ -1,0 +1,106 @@
+"""ctypes binding of libblml_b200.so (the C ABI declared in include/blml_b200.h).
+
+The library is the only compute path: there is no CPU fallback. Loading fails loudly when the shared library is
+missing, and every call raises BLMLError when the library returns an error status."""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libblml_b200.so')
+
+F64, F32 = 0, 1
+ENGINE_SIMT, ENGINE_TC = 0, 1
+
+
+class BLMLError(RuntimeError):
+    pass
+
+
+class Tables(C.Structure):
+    """blml_tables: the pair kernels' value tables (device pointers)."""
+    _fields_ = [('d', C.c_int), ('U', C.c_int), ('G', C.c_int), ('nW', C.c_int), ('LR', C.c_int), ('f32', C.c_int),
+                ('nT', C.c_int64), ('ndT', C.c_int64),
+                ('T', C.c_void_p), ('base', C.c_void_p), ('Jk', C.c_void_p), ('mk', C.c_void_p),
+                ('kinds', C.c_void_p), ('nbins', C.c_void_p), ('grp', C.c_void_p), ('RT', C.c_void_p),
+                ('dim_unit', C.c_void_p), ('grp_unit', C.c_void_p), ('dT', C.c_void_p), ('dbase', C.c_void_p),
+                ('dR', C.c_void_p), ('wunit', C.c_void_p), ('wcol', C.c_void_p), ('wgrp', C.c_void_p),
+                ('T32', C.c_void_p), ('RT32', C.c_void_p), ('dT32', C.c_void_p), ('dR32', C.c_void_p)]
+
+
+_P, _I, _L, _D = C.c_void_p, C.c_int, C.c_int64, C.c_double
+_SIGS = {
+    'blml_last_error': (C.c_char_p, []),
+    'blml_abi_version': (_I, []),
+    'blml_reduce_blocks': (_I, []),
+    'blml_launch_count': (_L, []),
+    'blml_plan_create': (_I, [_I, _P, _P, _P, _P, _I, _I, C.POINTER(_P)]),
+    'blml_plan_destroy': (_I, [_P]),
+    'blml_plan_status': (_I, [_P]),
+    'blml_matvec_workspace': (_L, [_P, _I]),
+    'blml_matvec': (_I, [_P, _P, _P, _I, _I, _P, _L, _P]),
+    'blml_jacobi_update': (_I, [_I, _I, _L, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_merit_terms': (_I, [_I, _I, _L, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_resid': (_I, [_I, _I, _L, _I, _P, _P, _P, _D, _P, _P, _P]),
+    'blml_dots': (_I, [_I, _L, _I, _P, _P, _P, _P, _P]),
+    'blml_lincomb': (_I, [_I, _L, _P, _I, _P, _P, _P]),
+    'blml_mul_bins': (_I, [_I, _I, _L, _I, _P, _P, _P, _P]),
+    'blml_lgrad_weights': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
+    'blml_lgrad_finish': (_I, [_I, _I, _L, _I, _P, _P, _P, _D, _P, _P]),
+    'blml_lbfgs_trial': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
+    'blml_finish': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
+    'blml_log_score': (_I, [_I, _I, _L, _I, _P, _P, _D, _D, _P, _P, _P]),
+    'blml_start_root': (_I, [_I, _L, _P, _P, _D, _P, _P]),
+    'blml_fill_modes': (_I, [_I, _I, _L, _I, _I, _I, _D, _P, _P, _P]),
+    'blml_cert_weights': (_I, [_I, _I, _L, _I, _P, _P, _P, _P]),
+    'blml_rows': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P, _P, _P]),
+    'blml_cols': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P]),
+}
+EXPORTS = tuple(_SIGS)
+
+_lib = None
+
+
+def lib():
+    """The loaded library (raises when it was not built: python -m blml_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BLMLError(f'{LIB_PATH} is missing: build it with `python -m blml_b200.build` (no CPU fallback)')
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = lib().blml_last_error().decode(errors='replace')
+        raise BLMLError(f'{what} failed ({rc}): {msg}')
+
+
+def call(name, *args):
+    check(getattr(lib(), name)(*args), name)
+
+
+def ptrs(arrs):
+    """A ctypes array of device pointers from tensors (or raw ints)."""
+    vals = [a if isinstance(a, int) else a.data_ptr() for a in arrs]
+    return (C.c_void_p * max(len(vals), 1))(*vals)
+
+
+def dbl(vals):
+    vals = [float(v) for v in vals]
+    return (C.c_double * max(len(vals), 1))(*vals)
+
+
+def host_ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def i64(vals):
+    return np.ascontiguousarray(vals, np.int64)

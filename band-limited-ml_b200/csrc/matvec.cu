@@ -1,0 +1,252 @@
+// The per-mode Gram mat-vec S e as restricted transforms.
+//
+// A mode's kernel is a weighted sum of plane waves over a product grid of per-axis frequencies:
+//     S e = sum_q W_q v_q v_q^H e,   v_q(j) = exp(2 pi i sum_a nu_{a, q_a} j_a).
+// Exact for periodic bands (the harmonics of dirichlet / pball), Gauss-Legendre quadrature for interval bands (sinc,
+// slits), and the padded lattice's own DFT for any other kernel. The transform runs as 2d "stages": each contracts
+// the LAST axis of the current (nb, R, M) tensor against an (M x N) matrix and writes the result as (nb, N, R),
+// i.e. the new axis moves to the front. After d forward stages the spectrum sits in natural order (q_1 .. q_d),
+// where the weight W is applied in the last forward stage's epilogue; d inverse stages bring the lattice back in
+// natural order. Every stage is one batched GEMM-shaped launch.
+#include <vector>
+#include <algorithm>
+#include "plan.cuh"
+
+namespace blml {
+
+constexpr int TR = 64, TN = 64, TK = 16;
+
+// Y[b, n, r] = (sum_m X[b, r, m] T[m, n]) * (W[n R + r] if WEIGHT); X real or complex, Y complex or (YREAL) its real
+// part. grid (ceil(R / TR), ceil(N / TN), nb), 256 threads, 4 x 4 outputs per thread.
+template <typename T, bool XREAL, bool WEIGHT, bool YREAL>
+__global__ void __launch_bounds__(256) k_contract(const void* __restrict__ X_, const cpx<T>* __restrict__ Tw,
+                                                  const T* __restrict__ W, void* __restrict__ Y_, int64_t R, int M,
+                                                  int N) {
+  __shared__ cpx<T> Xs[TK][TR + 1];
+  __shared__ cpx<T> Ts[TK][TN + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int64_t r0 = (int64_t)blockIdx.x * TR;
+  const int n0 = blockIdx.y * TN;
+  const int64_t b = blockIdx.z;
+  const int64_t xoff = b * R * (int64_t)M;
+  cpx<T> acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = {T(0), T(0)};
+  for (int m0 = 0; m0 < M; m0 += TK) {
+    // X tile: TR rows (r) x TK (m); thread loads m = tid % 16, r = tid / 16 + 16 i
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int rr = (tid >> 4) + 16 * i, mm = tid & 15;
+      const int64_t r = r0 + rr; const int m = m0 + mm;
+      cpx<T> v = {T(0), T(0)};
+      if (r < R && m < M) {
+        if (XREAL) v.re = reinterpret_cast<const T*>(X_)[xoff + r * M + m];
+        else v = reinterpret_cast<const cpx<T>*>(X_)[xoff + r * M + m];
+      }
+      Xs[mm][rr] = v;
+    }
+    // T tile: TK (m) x TN (n); thread loads n = tid % 64, m = tid / 64 + 4 i
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int nn = tid & 63, mm = (tid >> 6) + 4 * i;
+      const int n = n0 + nn, m = m0 + mm;
+      Ts[mm][nn] = (n < N && m < M) ? Tw[(int64_t)m * N + n] : cpx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TK; kk++) {
+      cpx<T> a[4], bb[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = Xs[kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) bb[j] = Ts[kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = cfma(a[i], bb[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  const int64_t yoff = b * (int64_t)N * R;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int n = n0 + ty + 16 * j;
+    if (n >= N) continue;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int64_t r = r0 + tx + 16 * i;
+      if (r >= R) continue;
+      cpx<T> v = acc[i][j];
+      if (WEIGHT) { const T wv = W[(int64_t)n * R + r]; v.re *= wv; v.im *= wv; }
+      if (YREAL) reinterpret_cast<T*>(Y_)[yoff + (int64_t)n * R + r] = v.re;
+      else reinterpret_cast<cpx<T>*>(Y_)[yoff + (int64_t)n * R + r] = v;
+    }
+  }
+}
+
+template <typename T>
+static int launch_stage(const void* X, bool xreal, const void* Tw, const void* W, void* Y, bool yreal, int64_t R,
+                        int M, int N, int nb, cudaStream_t st) {
+  dim3 grid((unsigned)((R + TR - 1) / TR), (unsigned)((N + TN - 1) / TN), (unsigned)nb);
+  const cpx<T>* t = reinterpret_cast<const cpx<T>*>(Tw);
+  const T* w = reinterpret_cast<const T*>(W);
+  // the combinations the stage schedule uses: first stage (real or complex input), last forward (weights),
+  // last inverse (real output when the input was real), and plain complex stages
+  if (xreal && W) k_contract<T, true, true, false><<<grid, 256, 0, st>>>(X, t, w, Y, R, M, N);
+  else if (xreal) k_contract<T, true, false, false><<<grid, 256, 0, st>>>(X, t, w, Y, R, M, N);
+  else if (W) k_contract<T, false, true, false><<<grid, 256, 0, st>>>(X, t, w, Y, R, M, N);
+  else if (yreal) k_contract<T, false, false, true><<<grid, 256, 0, st>>>(X, t, w, Y, R, M, N);
+  else k_contract<T, false, false, false><<<grid, 256, 0, st>>>(X, t, w, Y, R, M, N);
+  BLML_CHECK_LAUNCH("matvec stage");
+  return BLML_OK;
+}
+
+template <typename T>
+static int simt_matvec(blml_plan_s* p, const void* x, void* y, int nb, int xc, void* ws, cudaStream_t st) {
+  const int d = p->d;
+  std::vector<int64_t> dims(p->shape, p->shape + d);   // current axis order, natural at the start
+  const size_t esz = sizeof(cpx<T>);
+  char* buf[2] = {reinterpret_cast<char*>(ws), reinterpret_cast<char*>(ws) + (size_t)nb * p->max_elems * esz};
+  const void* cur = x; bool cur_real = !xc; int which = 0;
+  for (int s = 0; s < 2 * d; s++) {
+    const bool fwd = s < d;
+    const int a = d - 1 - (s % d);
+    const int64_t M = dims.back();
+    int64_t tot = 1; for (auto v : dims) tot *= v;
+    const int64_t R = tot / M;
+    const int64_t N = fwd ? p->nfreq[a] : p->shape[a];
+    const bool last = s == 2 * d - 1;
+    void* out = last ? y : buf[which];
+    const void* Tw = fwd ? p->tf[a] : p->ti[a];
+    const void* W = (s == d - 1) ? p->W : nullptr;
+    int rc = launch_stage<T>(cur, cur_real, Tw, W, out, last && !xc, R, (int)M, (int)N, nb, st);
+    if (rc) return rc;
+    dims.pop_back(); dims.insert(dims.begin(), N);
+    cur = out; cur_real = false; which ^= 1;
+  }
+  return BLML_OK;
+}
+
+}  // namespace blml
+
+using namespace blml;
+
+extern "C" {
+
+int blml_plan_create(int d, const int64_t* shape, const int32_t* nfreq, const double* freqs, const double* weights,
+                     int dtype, int engine, blml_plan* plan) {
+  if (!plan || d < 1 || d > 8 || !shape || !nfreq || !freqs || !weights) {
+    set_error("blml_plan_create: bad arguments"); return BLML_ERR_ARG;
+  }
+  if (dtype != BLML_F64 && dtype != BLML_F32) { set_error("blml_plan_create: dtype"); return BLML_ERR_ARG; }
+  if (engine == BLML_ENGINE_TC && (dtype != BLML_F32 || d != 2)) {
+    set_error("blml_plan_create: the tensor-core engine takes 2-D lattices in float32"); return BLML_ERR_UNSUPPORTED;
+  }
+  blml_plan_s* p = new blml_plan_s();
+  p->d = d; p->dtype = dtype; p->engine = engine;
+  int64_t nf_tot = 1, m_tot = 1;
+  for (int a = 0; a < d; a++) {
+    if (shape[a] < 1 || nfreq[a] < 1) { delete p; set_error("blml_plan_create: empty axis"); return BLML_ERR_ARG; }
+    p->shape[a] = shape[a]; p->nfreq[a] = nfreq[a]; nf_tot *= nfreq[a]; m_tot *= shape[a];
+  }
+  // largest intermediate: after s forward stages the tensor holds the frequencies of axes >= d - s and the lattice
+  // of the others; after s inverse stages the lattice of axes >= d - s and the frequencies of the others
+  int64_t mx = 0;
+  for (int s = 0; s <= d; s++) {
+    int64_t ef = 1, ei = 1;
+    for (int a = 0; a < d; a++) {
+      ef *= (a >= d - s) ? nfreq[a] : shape[a];
+      ei *= (a >= d - s) ? shape[a] : nfreq[a];
+    }
+    mx = std::max(mx, std::max(ef, ei));
+  }
+  p->max_elems = mx;
+  const bool f64 = dtype == BLML_F64;
+  const size_t esz = f64 ? 16 : 8;
+  const double* fq = freqs;
+  int rc = BLML_OK;
+  std::vector<std::vector<double>> fwd_all(d), inv_all(d);
+  for (int a = 0; a < d && rc == BLML_OK; a++) {
+    const int64_t M = shape[a]; const int H = nfreq[a];
+    std::vector<double>& fr = fwd_all[a];
+    std::vector<double>& iv = inv_all[a];
+    fr.resize(2 * M * H); iv.resize(2 * M * H);
+    for (int64_t j = 0; j < M; j++)
+      for (int q = 0; q < H; q++) {
+        // phase in cycles, reduced before scaling by 2 pi
+        double ph = fq[q] * (double)j; ph -= floor(ph);
+        const double cs = cos(2.0 * M_PI * ph), sn = sin(2.0 * M_PI * ph);
+        fr[2 * (j * H + q)] = cs; fr[2 * (j * H + q) + 1] = -sn;     // conj(v): forward (M x H)
+        iv[2 * (q * M + j)] = cs; iv[2 * (q * M + j) + 1] = sn;      // v^T: inverse (H x M)
+      }
+    fq += H;
+    for (int w = 0; w < 2; w++) {
+      std::vector<double>& src = w ? iv : fr;
+      void* dst = nullptr;
+      if (cudaMalloc(&dst, M * H * esz) != cudaSuccess) { rc = BLML_ERR_CUDA; break; }
+      if (f64) {
+        rc = cuda_status(cudaMemcpy(dst, src.data(), M * H * esz, cudaMemcpyHostToDevice), "plan twiddles");
+      } else {
+        std::vector<float> s32(src.begin(), src.end());
+        rc = cuda_status(cudaMemcpy(dst, s32.data(), M * H * esz, cudaMemcpyHostToDevice), "plan twiddles");
+      }
+      (w ? p->ti[a] : p->tf[a]) = dst;
+    }
+  }
+  if (rc == BLML_OK) {
+    if (cudaMalloc(&p->W, nf_tot * (f64 ? 8 : 4)) != cudaSuccess) rc = BLML_ERR_CUDA;
+    else if (f64) rc = cuda_status(cudaMemcpy(p->W, weights, nf_tot * 8, cudaMemcpyHostToDevice), "plan weights");
+    else {
+      std::vector<float> w32(weights, weights + nf_tot);
+      rc = cuda_status(cudaMemcpy(p->W, w32.data(), nf_tot * 4, cudaMemcpyHostToDevice), "plan weights");
+    }
+  }
+  if (rc == BLML_OK && engine == BLML_ENGINE_TC) rc = tc_plan_init(p, fwd_all, inv_all);
+  if (rc != BLML_OK) {
+    if (rc == BLML_ERR_CUDA && blml_last_error()[0] == 0) set_error("blml_plan_create: device allocation failed");
+    blml_plan_destroy(p);
+    return rc;
+  }
+  *plan = p;
+  return BLML_OK;
+}
+
+int blml_plan_destroy(blml_plan p) {
+  if (!p) return BLML_OK;
+  for (int a = 0; a < p->d; a++) { cudaFree(p->tf[a]); cudaFree(p->ti[a]); }
+  cudaFree(p->W);
+  if (p->tc) tc_plan_free(p);
+  delete p;
+  return BLML_OK;
+}
+
+int blml_plan_status(blml_plan p) {
+  if (!p) { set_error("blml_plan_status: null plan"); return BLML_ERR_ARG; }
+  int e = cuda_status(cudaDeviceSynchronize(), "blml_plan_status");
+  if (e) return e;
+  if (p->tc && tc_error(p)) { set_error("tensor-core mat-vec: a bounded wait timed out"); return BLML_ERR_TIMEOUT; }
+  return BLML_OK;
+}
+
+int64_t blml_matvec_workspace(blml_plan p, int nb) {
+  if (!p || nb < 1) return -1;
+  if (p->engine == BLML_ENGINE_TC) return tc_workspace(p, nb);
+  return 2 * (int64_t)nb * p->max_elems * (p->dtype == BLML_F64 ? 16 : 8);
+}
+
+int blml_matvec(blml_plan p, const void* x, void* y, int nb, int xc, void* ws, int64_t wsb, void* stream) {
+  if (!p || !x || !y || nb < 1) { set_error("blml_matvec: bad arguments"); return BLML_ERR_ARG; }
+  const int64_t need = blml_matvec_workspace(p, nb);
+  if (wsb < need || (need > 0 && !ws)) {
+    set_error("blml_matvec: workspace of %lld bytes, need %lld", (long long)wsb, (long long)need);
+    return BLML_ERR_WORKSPACE;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (p->engine == BLML_ENGINE_TC) return tc_matvec(p, x, y, nb, xc, ws, wsb, st);
+  return p->dtype == BLML_F64 ? simt_matvec<double>(p, x, y, nb, xc, ws, st)
+                              : simt_matvec<float>(p, x, y, nb, xc, ws, st);
+}
+
+}

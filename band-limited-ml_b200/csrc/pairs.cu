@@ -1,0 +1,435 @@
+// Pair accumulation over occupied lattice bins from the product kernel's value tables:
+//     rows:  s_r = sum_j w_j prod_u T_u[idx_u(ZA_r, ZB_j)]   (+ d/dtheta rows with grad)
+//     cols:  out[r, j] = prod_u T_u[idx_u(ZA_r, ZB_j)]
+// Every CTA keeps the value tables in shared memory and streams the columns j in chunks (coordinates and weights
+// staged in shared memory, read as warp broadcasts). Each thread owns rows; products are in REAL (float or
+// double, the reference's f32 flag), sums in float64. Column slices of one row block are reduced in a fixed order
+// by a second kernel, so results are deterministic (the reference combines slices with float64 atomics).
+// Before any launch the coordinates are checked against the tables' extents on the device, so a stale table is an
+// error, never an out-of-range read.
+#include "common.cuh"
+
+namespace blml {
+
+constexpr int RQ = 4;               // radial rows: grid points per lattice step (linear interpolation)
+constexpr int PR_THREADS = 128;     // rows per CTA (one per thread)
+constexpr int PR_CHUNK = 256;       // columns staged per shared-memory chunk
+constexpr int MAXD = 8, MAXU = 8, MAXG = 4, MAXW = 8;
+
+struct ColMeta {
+  int d, U, G, nW, LR;
+  int code[MAXD], grp[MAXD], dim_unit[MAXD];
+  int64_t base[MAXD], J[MAXD], mk[MAXD], nb[MAXD];
+  int grp_unit[MAXG];
+  int wunit[MAXW], wcol[MAXW], wgrp[MAXW];
+  int64_t dbase[MAXW];
+  int64_t Tn, dTn;
+};
+
+template <typename REAL>
+__device__ __forceinline__ REAL col_value(const ColMeta& cm, const REAL* T, int k, int64_t za, int64_t zb) {
+  const int code = cm.code[k];
+  int64_t idx;
+  if (code == 0) idx = cm.base[k] + za - zb + cm.J[k];
+  else if (code == 3) idx = cm.base[k] + za * cm.mk[k] + zb;
+  else {                                     // circular distance, |za - zb| < nb
+    const int64_t nb = cm.nb[k];
+    int64_t m = za - zb;
+    if (m < 0) m += nb; else if (m >= nb) m -= nb;
+    if (m > nb - m) m = nb - m;
+    idx = cm.base[k] + m;
+  }
+  return T[idx];
+}
+
+// One pair's unit factors (fac[u]) and the group indices (r2 / torus index per group).
+template <typename REAL>
+__device__ __forceinline__ void pair_factors(const ColMeta& cm, const REAL* T, const REAL* RT, const int64_t* za,
+                                             const int64_t* zb, REAL* fac, int64_t* r2, bool* tor) {
+  for (int g = 0; g < cm.G; g++) { r2[g] = 0; tor[g] = false; }
+  for (int k = 0; k < cm.d; k++) {
+    const int code = cm.code[k];
+    const int64_t off = za[k] - zb[k];
+    if (code == 2) { r2[cm.grp[k]] += off * off; continue; }
+    if (code == 4) {
+      const int g = cm.grp[k]; const int64_t nb = cm.nb[k];
+      const int64_t m = off < 0 ? off + nb : off;
+      r2[g] = r2[g] * nb + m; tor[g] = true; continue;
+    }
+    fac[cm.dim_unit[k]] = col_value(cm, T, k, za[k], zb[k]);
+  }
+  for (int g = 0; g < cm.G; g++) {
+    const REAL* row = RT + (int64_t)g * cm.LR;
+    if (tor[g]) { fac[cm.grp_unit[g]] = row[r2[g]]; continue; }
+    const double t = sqrt((double)r2[g]) * RQ; const int i0 = (int)t; const REAL f = (REAL)(t - i0);
+    fac[cm.grp_unit[g]] = row[i0] * (REAL(1) - f) + row[i0 + 1] * f;
+  }
+}
+
+// derivative entry q of a pair (the reference's dval): a column's derivative row (raw offsets, rank tables), a
+// group's torus row, or a radial row on the r grid times the offset of column wcol[q] for a shift entry
+template <typename REAL>
+__device__ __forceinline__ REAL dval(const ColMeta& cm, const REAL* dT, const REAL* dR, int q, const int64_t* za,
+                                     const int64_t* zb, const int64_t* r2, const bool* tor) {
+  const int g = cm.wgrp[q], k = cm.wcol[q];
+  if (g >= 0 && tor[g]) return dR[(int64_t)q * cm.LR + r2[g]];
+  if (g < 0) {
+    const int64_t idx = cm.code[k] == 3 ? za[k] * cm.mk[k] + zb[k] : za[k] - zb[k] + cm.J[k];
+    return dT[cm.dbase[q] + idx];
+  }
+  const double t = sqrt((double)r2[g]) * RQ; const int i0 = (int)t; const REAL f = (REAL)(t - i0);
+  REAL v = dR[(int64_t)q * cm.LR + i0] * (REAL(1) - f) + dR[(int64_t)q * cm.LR + i0 + 1] * f;
+  if (k >= 0) v *= (REAL)(za[k] - zb[k]);
+  return v;
+}
+
+// General rows kernel: any column codes, groups and derivative entries. grid (row blocks, column slices).
+// part[slice][r] (and dpart[slice][r][q]) are the slice sums.
+template <typename REAL, bool GRAD>
+__global__ void __launch_bounds__(PR_THREADS) k_rows_general(ColMeta cm, const REAL* Tg, const REAL* RTg,
+                                                             const REAL* dTg, const REAL* dRg, const int64_t* ZA,
+                                                             int64_t R, const int64_t* ZB, const double* w,
+                                                             int64_t j0s, int64_t slice, int64_t M, double* part,
+                                                             double* dpart) {
+  extern __shared__ unsigned char smem_raw[];
+  REAL* Ts = reinterpret_cast<REAL*>(smem_raw);
+  REAL* RTs = Ts + cm.Tn;
+  const int64_t nRT = (int64_t)cm.G * cm.LR;
+  for (int64_t i = threadIdx.x; i < cm.Tn; i += blockDim.x) Ts[i] = Tg[i];
+  for (int64_t i = threadIdx.x; i < nRT; i += blockDim.x) RTs[i] = RTg[i];
+  __syncthreads();
+  const int64_t r = (int64_t)blockIdx.x * PR_THREADS + threadIdx.x;
+  const int64_t j0 = j0s + (int64_t)blockIdx.y * slice, j1 = min(M, j0 + slice);
+  int64_t za[MAXD];
+  const bool live = r < R;
+  for (int k = 0; k < cm.d; k++) za[k] = live ? ZA[r * cm.d + k] : 0;
+  double acc = 0.0, dacc[MAXW];
+  for (int q = 0; q < MAXW; q++) dacc[q] = 0.0;
+  REAL fac[MAXU + 1];
+  for (int u = 0; u < MAXU; u++) fac[u] = REAL(1);
+  int64_t r2[MAXG]; bool tor[MAXG];
+  for (int64_t j = j0; j < j1 && live; j++) {
+    const double wj = w[j];
+    if (wj == 0.0) continue;
+    int64_t zb[MAXD];
+    for (int k = 0; k < cm.d; k++) zb[k] = ZB[j * cm.d + k];
+    pair_factors<REAL>(cm, Ts, RTs, za, zb, fac, r2, tor);
+    REAL pre[MAXU + 1];
+    pre[0] = REAL(1);
+    for (int u = 0; u < cm.U; u++) pre[u + 1] = pre[u] * fac[u];
+    acc += (double)pre[cm.U] * wj;
+    if (GRAD) {
+      REAL suf[MAXU + 1];
+      suf[cm.U] = REAL(1);
+      for (int u = cm.U - 1; u >= 0; u--) suf[u] = suf[u + 1] * fac[u];
+      for (int q = 0; q < cm.nW; q++) {
+        const int u = cm.wunit[q];
+        const REAL dv = dval<REAL>(cm, dTg, dRg, q, za, zb, r2, tor);
+        dacc[q] += (double)(dv * pre[u] * suf[u + 1]) * wj;
+      }
+    }
+  }
+  if (!live) return;
+  part[(int64_t)blockIdx.y * R + r] = acc;
+  if (GRAD)
+    for (int q = 0; q < cm.nW; q++) dpart[((int64_t)blockIdx.y * R + r) * cm.nW + q] = dacc[q];
+}
+
+// shared-memory layout of k_rows_offset (the host sizes the launch with the same functions): the table, then the
+// chunk's column coordinates (int32, D per column), then its weights, each part 16-byte aligned
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+template <typename REAL> __host__ __device__ constexpr size_t offset_smem_zb(int64_t Tn) {
+  return align16((size_t)Tn * sizeof(REAL));
+}
+template <typename REAL> __host__ __device__ constexpr size_t offset_smem_w(int64_t Tn, int D) {
+  return offset_smem_zb<REAL>(Tn) + align16((size_t)PR_CHUNK * D * sizeof(int));
+}
+template <typename REAL> __host__ __device__ constexpr size_t offset_smem_bytes(int64_t Tn, int D) {
+  return offset_smem_w<REAL>(Tn, D) + (size_t)PR_CHUNK * sizeof(double);
+}
+
+// Fast rows kernel for product kernels whose columns are all offset rows (sinc / slits / raw dirichlet): each
+// thread keeps one pointer per column into the shared-memory table (T_k + base_k + J_k + za_k), so a pair costs
+// D shared-memory gathers, D - 1 multiplies and one float64 FMA; column coordinates (int32) and weights are staged
+// per chunk and read as broadcasts.
+template <typename REAL, int D>
+__global__ void __launch_bounds__(PR_THREADS) k_rows_offset(ColMeta cm, const REAL* Tg, const int64_t* ZA, int64_t R,
+                                                            const int64_t* ZB, const double* w, int64_t slice,
+                                                            int64_t M, double* part) {
+  extern __shared__ unsigned char smem_raw[];
+  REAL* Ts = reinterpret_cast<REAL*>(smem_raw);
+  int* zbs = reinterpret_cast<int*>(smem_raw + offset_smem_zb<REAL>(cm.Tn));
+  double* ws = reinterpret_cast<double*>(smem_raw + offset_smem_w<REAL>(cm.Tn, D));
+  for (int64_t i = threadIdx.x; i < cm.Tn; i += blockDim.x) Ts[i] = Tg[i];
+  const int64_t r = (int64_t)blockIdx.x * PR_THREADS + threadIdx.x;
+  const bool live = r < R;
+  const REAL* ptr[D];
+#pragma unroll
+  for (int k = 0; k < D; k++) ptr[k] = Ts + cm.base[k] + cm.J[k] + (live ? ZA[r * D + k] : 0);
+  const int64_t j0 = (int64_t)blockIdx.y * slice, j1 = min(M, j0 + slice);
+  double acc = 0.0;
+  for (int64_t c0 = j0; c0 < j1; c0 += PR_CHUNK) {
+    const int n = (int)(j1 - c0 < PR_CHUNK ? j1 - c0 : PR_CHUNK);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n * D; i += blockDim.x) zbs[i] = (int)ZB[c0 * D + i];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) ws[i] = w[c0 + i];
+    __syncthreads();
+    if (live) {
+#pragma unroll 4
+      for (int jj = 0; jj < n; jj++) {
+        REAL p = ptr[0][-zbs[jj * D]];
+#pragma unroll
+        for (int k = 1; k < D; k++) p *= ptr[k][-zbs[jj * D + k]];
+        acc = fma((double)p, ws[jj], acc);
+      }
+    }
+  }
+  if (live) part[(int64_t)blockIdx.y * R + r] = acc;
+}
+
+__global__ void k_sum_slices(const double* part, int nsl, int64_t n, double* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int y = 0; y < nsl; y++) s += part[(int64_t)y * n + i];
+    out[i] = s;
+  }
+}
+
+template <typename REAL, typename OUT>
+__global__ void k_cols(ColMeta cm, const REAL* T, const REAL* RT, const int64_t* ZA, int64_t R, const int64_t* ZB,
+                       int64_t M, OUT* out) {
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < R * M;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx / M, j = idx % M;
+    int64_t za[MAXD], zb[MAXD], r2[MAXG]; bool tor[MAXG];
+    REAL fac[MAXU];
+    for (int u = 0; u < MAXU; u++) fac[u] = REAL(1);
+    for (int k = 0; k < cm.d; k++) { za[k] = ZA[r * cm.d + k]; zb[k] = ZB[j * cm.d + k]; }
+    pair_factors<REAL>(cm, T, RT, za, zb, fac, r2, tor);
+    REAL v = REAL(1);
+    for (int u = 0; u < cm.U; u++) v *= fac[u];
+    out[idx] = (OUT)v;
+  }
+}
+
+// per column: min and max of ZA and ZB (for the extent check); out[4 * k + {0,1,2,3}] = minA, maxA, minB, maxB
+__global__ void k_coord_range(const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, int d, long long* out) {
+  const int k = blockIdx.x;
+  long long mnA = LLONG_MAX, mxA = LLONG_MIN, mnB = LLONG_MAX, mxB = LLONG_MIN;
+  for (int64_t i = threadIdx.x; i < R; i += blockDim.x) { long long v = ZA[i * d + k]; mnA = min(mnA, v); mxA = max(mxA, v); }
+  for (int64_t i = threadIdx.x; i < M; i += blockDim.x) { long long v = ZB[i * d + k]; mnB = min(mnB, v); mxB = max(mxB, v); }
+  __shared__ long long sh[4][256];
+  sh[0][threadIdx.x] = mnA; sh[1][threadIdx.x] = mxA; sh[2][threadIdx.x] = mnB; sh[3][threadIdx.x] = mxB;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      sh[0][threadIdx.x] = min(sh[0][threadIdx.x], sh[0][threadIdx.x + s]);
+      sh[1][threadIdx.x] = max(sh[1][threadIdx.x], sh[1][threadIdx.x + s]);
+      sh[2][threadIdx.x] = min(sh[2][threadIdx.x], sh[2][threadIdx.x + s]);
+      sh[3][threadIdx.x] = max(sh[3][threadIdx.x], sh[3][threadIdx.x + s]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) for (int q = 0; q < 4; q++) out[4 * k + q] = sh[q][0];
+}
+
+}  // namespace blml
+
+using namespace blml;
+
+static int read_meta(const blml_tables* tb, ColMeta& cm, cudaStream_t st) {
+  if (!tb || tb->d < 1 || tb->d > MAXD || tb->U < 1 || tb->U > MAXU || tb->G < 0 || tb->G > MAXG || tb->nW < 0 ||
+      tb->nW > MAXW) {
+    set_error("pair tables: d <= %d, units <= %d, groups <= %d, derivative entries <= %d", MAXD, MAXU, MAXG, MAXW);
+    return BLML_ERR_ARG;
+  }
+  const int d = tb->d;
+  cm.d = d; cm.U = tb->U; cm.G = tb->G; cm.nW = tb->nW; cm.LR = tb->LR;
+  cm.Tn = tb->nT; cm.dTn = tb->ndT;
+  auto fetch = [&](const int64_t* src, int n, int64_t* dst) -> int {
+    if (n == 0) return BLML_OK;
+    return cuda_status(cudaMemcpyAsync(dst, src, n * sizeof(int64_t), cudaMemcpyDeviceToHost, st), "pair tables");
+  };
+  int64_t base[MAXD], J[MAXD], mk[MAXD], nb[MAXD], grp[MAXD], du[MAXD], gu[MAXG], wu[MAXW], wc[MAXW], wg[MAXW], db[MAXW];
+  int64_t codes[MAXD];
+  struct { const int64_t* s; int n; int64_t* d; } req[] = {
+      {tb->kinds, d, codes}, {tb->base, d, base}, {tb->Jk, d, J}, {tb->mk, d, mk}, {tb->nbins, d, nb},
+      {tb->grp, d, grp}, {tb->dim_unit, d, du}, {tb->grp_unit, tb->G, gu}, {tb->wunit, tb->nW, wu},
+      {tb->wcol, tb->nW, wc}, {tb->wgrp, tb->nW, wg}, {tb->dbase, tb->nW, db}};
+  for (auto& q : req) {
+    if (q.n && !q.s) { set_error("pair tables: a metadata array is missing"); return BLML_ERR_ARG; }
+    int e = fetch(q.s, q.n, q.d);
+    if (e) return e;
+  }
+  int e = cuda_status(cudaStreamSynchronize(st), "pair tables");
+  if (e) return e;
+  for (int k = 0; k < d; k++) {
+    cm.code[k] = (int)codes[k]; cm.base[k] = base[k]; cm.J[k] = J[k]; cm.mk[k] = mk[k]; cm.nb[k] = nb[k];
+    cm.grp[k] = (int)grp[k]; cm.dim_unit[k] = (int)du[k];
+    if (codes[k] < 0 || codes[k] > 4) { set_error("pair tables: column %d has kind code %lld", k, (long long)codes[k]); return BLML_ERR_ARG; }
+    if ((codes[k] == 2 || codes[k] == 4) && (grp[k] < 0 || grp[k] >= tb->G)) { set_error("pair tables: column %d group", k); return BLML_ERR_ARG; }
+    if (!(codes[k] == 2 || codes[k] == 4) && (du[k] < 0 || du[k] >= tb->U)) { set_error("pair tables: column %d unit", k); return BLML_ERR_ARG; }
+  }
+  for (int k = 0; k < d; k++) {              // every column block lies inside the flat value array
+    int64_t len = 0;
+    if (cm.code[k] == 0) len = 2 * cm.J[k] + 1;
+    else if (cm.code[k] == 3) len = cm.mk[k] * cm.mk[k];
+    else if (cm.code[k] == 1) len = cm.nb[k] / 2 + 1;
+    if (cm.base[k] < 0 || cm.base[k] + len > cm.Tn || cm.J[k] < 0 || cm.mk[k] < 0 || cm.nb[k] < 0) {
+      set_error("pair tables: column %d block outside the value array of %lld", k, (long long)cm.Tn);
+      return BLML_ERR_ARG;
+    }
+  }
+  for (int g = 0; g < tb->G; g++) {
+    cm.grp_unit[g] = (int)gu[g];
+    if (gu[g] < 0 || gu[g] >= tb->U) { set_error("pair tables: group %d unit", g); return BLML_ERR_ARG; }
+  }
+  for (int q = 0; q < tb->nW; q++) {
+    cm.wunit[q] = (int)wu[q]; cm.wcol[q] = (int)wc[q]; cm.wgrp[q] = (int)wg[q]; cm.dbase[q] = db[q];
+    bool ok = wu[q] >= 0 && wu[q] < tb->U && wg[q] < tb->G && wc[q] < d;
+    if (ok && wg[q] < 0) {                   // a column's derivative row: inside dT, with the column's block length
+      const int k = (int)wc[q];
+      ok = k >= 0 && (cm.code[k] == 0 || cm.code[k] == 3) && db[q] >= 0 &&
+           db[q] + (cm.code[k] == 3 ? cm.mk[k] * cm.mk[k] : 2 * cm.J[k] + 1) <= cm.dTn;
+    }
+    if (!ok) { set_error("pair tables: derivative entry %d outside its tables", q); return BLML_ERR_ARG; }
+  }
+  return BLML_OK;
+}
+
+// the coordinates must lie in the tables' extents: offsets within +-J (offset rows), ranks within the rank table,
+// folded coordinates within the period (circular / torus), radii within the radial row
+static int check_extents(const ColMeta& cm, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                         cudaStream_t st) {
+  if (R == 0 || M == 0) return BLML_OK;
+  long long* dr = nullptr;
+  long long hr[4 * MAXD];
+  int e = cuda_status(cudaMallocAsync((void**)&dr, 4 * cm.d * sizeof(long long), st), "pair extents");
+  if (e) return e;
+  k_coord_range<<<cm.d, 256, 0, st>>>(ZA, R, ZB, M, cm.d, dr);
+  count_launches(1);
+  e = cuda_status(cudaMemcpyAsync(hr, dr, 4 * cm.d * sizeof(long long), cudaMemcpyDeviceToHost, st), "pair extents");
+  cudaFreeAsync(dr, st);
+  if (!e) e = cuda_status(cudaStreamSynchronize(st), "pair extents");
+  if (e) return e;
+  double rad[MAXG] = {0, 0, 0, 0};
+  for (int k = 0; k < cm.d; k++) {
+    const long long mnA = hr[4 * k], mxA = hr[4 * k + 1], mnB = hr[4 * k + 2], mxB = hr[4 * k + 3];
+    const long long span = std::max(mxA - mnB, mxB - mnA);
+    bool ok = true;
+    switch (cm.code[k]) {
+      case 0: ok = span <= cm.J[k]; break;
+      case 3: ok = mnA >= 0 && mnB >= 0 && mxA < cm.mk[k] && mxB < cm.mk[k]; break;
+      case 1: case 4: ok = mnA >= 0 && mnB >= 0 && mxA < cm.nb[k] && mxB < cm.nb[k]; break;
+      case 2: rad[cm.grp[k]] += (double)span * (double)span; break;
+    }
+    if (!ok) {
+      set_error("pair tables: column %d coordinates outside the tables' span (stale tables)", k);
+      return BLML_ERR_ARG;
+    }
+  }
+  for (int k = 0; k < cm.d; k++)
+    if (cm.code[k] == 2 && sqrt(rad[cm.grp[k]]) * RQ + 1 >= cm.LR) {
+      set_error("pair tables: radial group %d radius outside its row (stale tables)", cm.grp[k]);
+      return BLML_ERR_ARG;
+    }
+  return BLML_OK;
+}
+
+template <typename REAL>
+static int rows_impl(const blml_tables* tb, const ColMeta& cm, const REAL* T, const REAL* RT, const REAL* dT,
+                     const REAL* dR, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
+                     int grad, double* s, double* ds, cudaStream_t st) {
+  const int64_t rblocks = (R + PR_THREADS - 1) / PR_THREADS;
+  // column slices so that the grid covers the GPU about four times
+  int64_t nsl = std::max<int64_t>(1, std::min<int64_t>((4 * 148 + rblocks - 1) / rblocks, (M + 1023) / 1024));
+  nsl = std::min<int64_t>(nsl, 65535);
+  const int64_t slice = (M + nsl - 1) / nsl;
+  nsl = (M + slice - 1) / slice;
+  const int nW = grad ? cm.nW : 0;
+  double* part = nullptr;
+  const size_t pbytes = (size_t)nsl * R * (1 + nW) * sizeof(double);
+  int e = cuda_status(cudaMallocAsync((void**)&part, std::max<size_t>(pbytes, 8), st), "blml_rows workspace");
+  if (e) return e;
+  double* dpart = part + (size_t)nsl * R;
+  bool offset_only = cm.G == 0 && !grad;
+  for (int k = 0; k < cm.d; k++) offset_only = offset_only && cm.code[k] == 0;
+  const size_t tsz = (size_t)cm.Tn * sizeof(REAL);
+  dim3 grid((unsigned)rblocks, (unsigned)nsl);
+  if (offset_only) {
+    const size_t sm = offset_smem_bytes<REAL>(cm.Tn, cm.d);
+    if (sm > 200 * 1024) { cudaFreeAsync(part, st); set_error("blml_rows: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+#define ROWS_OFF(DD) case DD: \
+      cudaFuncSetAttribute(k_rows_offset<REAL, DD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+      k_rows_offset<REAL, DD><<<grid, PR_THREADS, sm, st>>>(cm, T, ZA, R, ZB, w, slice, M, part); break;
+    switch (cm.d) { ROWS_OFF(1) ROWS_OFF(2) ROWS_OFF(3) ROWS_OFF(4) ROWS_OFF(5) ROWS_OFF(6) ROWS_OFF(7) ROWS_OFF(8) }
+#undef ROWS_OFF
+  } else {
+    const size_t sm = tsz + (size_t)cm.G * cm.LR * sizeof(REAL);
+    if (sm > 200 * 1024) { cudaFreeAsync(part, st); set_error("blml_rows: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+    if (grad) {
+      cudaFuncSetAttribute(k_rows_general<REAL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_rows_general<REAL, true><<<grid, PR_THREADS, sm, st>>>(cm, T, RT, dT, dR, ZA, R, ZB, w, 0, slice, M, part, dpart);
+    } else {
+      cudaFuncSetAttribute(k_rows_general<REAL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      k_rows_general<REAL, false><<<grid, PR_THREADS, sm, st>>>(cm, T, RT, dT, dR, ZA, R, ZB, w, 0, slice, M, part, dpart);
+    }
+  }
+  e = cuda_status(cudaGetLastError(), "blml_rows");
+  if (!e) {
+    count_launches(2);                       // the rows kernel and the slice sum
+    k_sum_slices<<<std::min<int64_t>((R + 255) / 256, 4096), 256, 0, st>>>(part, (int)nsl, R, s);
+    if (grad && nW) {
+      k_sum_slices<<<std::min<int64_t>((R * nW + 255) / 256, 4096), 256, 0, st>>>(dpart, (int)nsl, R * nW, ds);
+      count_launches(1);
+    }
+    e = cuda_status(cudaGetLastError(), "blml_rows finish");
+  }
+  cudaFreeAsync(part, st);
+  return e;
+}
+
+extern "C" {
+
+int blml_rows(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
+              int grad, double* s, double* ds, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  ColMeta cm;
+  int e = read_meta(tb, cm, st);
+  if (e) return e;
+  if (grad && cm.nW == 0) grad = 0;
+  if (R == 0) return BLML_OK;
+  if (M == 0) return cuda_status(cudaMemsetAsync(s, 0, R * sizeof(double), st), "blml_rows");
+  e = check_extents(cm, ZA, R, ZB, M, st);
+  if (e) return e;
+  if (tb->f32) {
+    if (!tb->T32 || (cm.G && !tb->RT32) || (grad && (!tb->dT32 || !tb->dR32))) { set_error("blml_rows: float32 tables missing"); return BLML_ERR_ARG; }
+    return rows_impl<float>(tb, cm, tb->T32, tb->RT32, tb->dT32, tb->dR32, ZA, R, ZB, M, w, grad, s, ds, st);
+  }
+  if (!tb->T || (cm.G && !tb->RT) || (grad && (!tb->dT || !tb->dR))) { set_error("blml_rows: tables missing"); return BLML_ERR_ARG; }
+  return rows_impl<double>(tb, cm, tb->T, tb->RT, tb->dT, tb->dR, ZA, R, ZB, M, w, grad, s, ds, st);
+}
+
+int blml_cols(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
+              int out_f32, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  ColMeta cm;
+  int e = read_meta(tb, cm, st);
+  if (e) return e;
+  if (R == 0 || M == 0) return BLML_OK;
+  e = check_extents(cm, ZA, R, ZB, M, st);
+  if (e) return e;
+  const int64_t n = R * M;
+  const int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 32);
+  if (tb->f32) {
+    if (out_f32) k_cols<float, float><<<g, 256, 0, st>>>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, (float*)out);
+    else k_cols<float, double><<<g, 256, 0, st>>>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, (double*)out);
+  } else {
+    if (out_f32) k_cols<double, float><<<g, 256, 0, st>>>(cm, tb->T, tb->RT, ZA, R, ZB, M, (float*)out);
+    else k_cols<double, double><<<g, 256, 0, st>>>(cm, tb->T, tb->RT, ZA, R, ZB, M, (double*)out);
+  }
+  count_launches(1);
+  return cuda_status(cudaGetLastError(), "blml_cols");
+}
+
+}

@@ -1,0 +1,146 @@
+/* libblml_b200 -- the C ABI of the B200 engine for BLML's binned fitting path.
+ *
+ * Every entry point takes plain device pointers (e.g. torch tensors' data_ptr()), sizes and a CUDA stream
+ * (cudaStream_t passed as void*), and returns 0 on success or a negative BLML_ERR_* code (blml_last_error() gives
+ * the message). Arrays of modes are (K, B) row-major, B = the number of lattice bins; complex arrays are
+ * interleaved (re, im) pairs (torch complex64 / complex128). `dtype` selects float64 (BLML_F64) or float32
+ * (BLML_F32) storage; every reduction accumulates in float64 and is deterministic (fixed-order block partials:
+ * `part` holds nq * blml_reduce_blocks() doubles, `out` receives nq doubles, both on the device).
+ *
+ * The reference (rahuljhu/band-limited-ml) is Python over NumPy/CuPy; each entry point below names the method
+ * whose arithmetic it replaces (file:line in the reference).
+ */
+#ifndef BLML_B200_H
+#define BLML_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { BLML_OK = 0, BLML_ERR_ARG = -1, BLML_ERR_CUDA = -2, BLML_ERR_WORKSPACE = -3, BLML_ERR_UNSUPPORTED = -4,
+       BLML_ERR_TIMEOUT = -5 };
+enum { BLML_F64 = 0, BLML_F32 = 1 };
+/* mat-vec engines: SIMT contraction (float64 or float32), or tcgen05 tensor cores with split-TF32 operands
+   (float32 storage, three products per term, FP32 accumulation in TMEM) */
+enum { BLML_ENGINE_SIMT = 0, BLML_ENGINE_TC = 1 };
+
+typedef struct blml_plan_s* blml_plan;
+
+const char* blml_last_error(void);
+int blml_abi_version(void);
+/* blocks of every reduction grid: `part` buffers hold nq * blml_reduce_blocks() doubles */
+int blml_reduce_blocks(void);
+/* cumulative number of kernels the library has launched in this process (for launch accounting) */
+int64_t blml_launch_count(void);
+
+/* ---- the per-mode Gram mat-vec S_k e (replaces _ModeKernel + BLMLBinned._S, blml_binned.py:49-101, 156-168) ----
+ * The mode's kernel on a d-dim lattice of `shape`, given as restricted transforms: per axis a nfreq[a] frequencies
+ * (cycles per lattice index, concatenated over axes in `freqs`) and a weight tensor over the product frequency grid
+ * (prod nfreq doubles, row-major): S e = sum_q W_q v_q v_q^H e, v_q(j) = exp(2 pi i sum_a nu_{a,q_a} j_a). */
+int blml_plan_create(int d, const int64_t* shape, const int32_t* nfreq, const double* freqs, const double* weights,
+                     int dtype, int engine, blml_plan* plan);
+int blml_plan_destroy(blml_plan plan);
+/* bytes of workspace one blml_matvec call over nbatch lattices needs */
+int64_t blml_matvec_workspace(blml_plan plan, int nbatch);
+/* y[b] = S x[b] for b < nbatch lattices; x real (x_complex = 0: y real) or complex */
+int blml_matvec(blml_plan plan, const void* x, void* y, int nbatch, int x_complex, void* ws, int64_t ws_bytes,
+                void* stream);
+/* synchronises the device and reports whether a tensor-core mat-vec gave up on a bounded wait since the plan was
+   made (BLML_ERR_TIMEOUT; the results of that call are invalid) or BLML_OK */
+int blml_plan_status(blml_plan plan);
+
+/* ---- coordinate (Jacobi) update of every bin (BLMLBinned._update / _secular / _cd_root,
+ *      blml_binned.py:184-206, 1549-1573; cd_root blml_trivial.py:84-89) ----
+ * psd = 0: real rank 1, out = sg * cd_root(sg * (U - s0 E), c, s0) on occupied bins (c > 0), 0 elsewhere.
+ * psd = 1: complex and/or rank K; the closed form when every s_k is equal, else the safeguarded secular root.
+ * s: K host doubles (K(0) of each mode). */
+int blml_jacobi_update(int dtype, int K, int64_t B, int cplx, int psd, const double* s, const void* E, const void* U,
+                       const void* c, const void* sg, void* out, void* stream);
+
+/* ---- merit terms (BLMLBinned._merit, blml_binned.py:171-182) ----
+ * psd: out[0] = sum_b c_b log max(F_b, 1e-30), F_b = sum_k |U_kb|^2; out[1] = Q = Re sum conj(E) U; out[2] = 0.
+ * real rank 1: out[0] = sum e u, out[1] = sum_occ c log|e|, out[2] = #occupied bins with sg e <= 0. nq = 3. */
+int blml_merit_terms(int dtype, int K, int64_t B, int cplx, int psd, const void* E, const void* U, const void* c,
+                     const void* sg, double* part, double* out, void* stream);
+
+/* ---- stationarity residual max_b rho_b of (scale E, scale U) (BLMLBinned._resid, blml_binned.py:216-220);
+ *      out[0] = the largest finite rho_b, out[1] = the number of bins whose rho_b is NaN; nq = 2 */
+int blml_resid(int dtype, int K, int64_t B, int cplx, const void* E, const void* U, const void* c, double scale,
+               double* part, double* out, void* stream);
+
+/* ---- real inner products Re sum conj(a_i) b_i over n scalars (complex arrays: 2n reals) in float64, npairs <= 64
+ *      pairs (32 per pass) (_rdot, _anderson_mix, the L-BFGS dots; blml_binned.py:1463-1482, 290-335) ----
+ * a, b: host arrays of device pointers. nq = npairs. */
+int blml_dots(int dtype, int64_t n, int npairs, const void* const* a, const void* const* b, double* part,
+              double* out, void* stream);
+
+/* ---- out = sum_i coef_i v_i over n scalars, nterms <= 64 (out may alias any v_i): Anderson mixing, damping, L-BFGS
+ *      directions and steps (blml_binned.py:243-258, 307-321, 1475-1478) ---- */
+int blml_lincomb(int dtype, int64_t n, void* out, int nterms, const double* coef, const void* const* v, void* stream);
+
+/* ---- out[k, b] = x[k, b] * r[b] (r real, same dtype as x): masks and diagonal scalings ---- */
+int blml_mul_bins(int dtype, int K, int64_t B, int cplx, const void* x, const void* r, void* out, void* stream);
+
+/* ---- likelihood gradient pieces (BLMLBinned._lgrad, blml_binned.py:278-288; canonical form :345-349) ----
+ * weights: F = sum_k |U_k|^2; V = vscale * w / F * U on occupied bins (0 elsewhere); out[0] = sum_occ w log F. nq = 1
+ * finish:  g = 2 (SV - nq U) on occupied bins, 0 elsewhere. */
+int blml_lgrad_weights(int dtype, int K, int64_t B, int cplx, const void* U, const void* w, double vscale, void* V,
+                       double* part, double* out, void* stream);
+int blml_lgrad_finish(int dtype, int K, int64_t B, int cplx, const void* SV, const void* U, const void* w, double nq,
+                      void* g, void* stream);
+
+/* ---- one Armijo trial of the L-BFGS line search (BLMLBinned._solve_lbfgs, blml_binned.py:316-321) ----
+ * En = E + t q and Un = U + t Sq (S linear: U + t S q = S(E + t q)), both written; out[0] = sum_occ w log F(Un),
+ * out[1] = Re <En, Un>, from which L(En) = out[0] - n log out[1]. nq = 2. */
+int blml_lbfgs_trial(int dtype, int K, int64_t B, int cplx, const void* E, const void* q, const void* U,
+                     const void* Sq, const void* w, double t, void* En, void* Un, double* part, double* out,
+                     void* stream);
+
+/* ---- fit outputs (BLMLBinned._finish, blml_binned.py:438-445): density = F / n^2; out[0] = sum_occ w log density */
+int blml_finish(int dtype, int K, int64_t B, int cplx, const void* U, const void* w, double inv_n2, void* density,
+                double* part, double* out, void* stream);
+
+/* ---- lattice score (BLMLBinned.log_density / _val_score, blml_binned.py:630-645): out[0] = sum over m_b > 0 of
+ *      m_b log max(F_b inv_z + eps, 1e-300), out[1] = sum m_b; m (B) in the fit dtype. nq = 2 ---- */
+int blml_log_score(int dtype, int K, int64_t B, int cplx, const void* U, const void* m, double inv_z, double eps,
+                   double* part, double* out, void* stream);
+
+/* ---- start (BLMLBinned._start / _fill_modes, blml_binned.py:415-436) ----
+ * start_root: e0 = sg sqrt(c / s0) on occupied bins, 0 elsewhere (real, dtype).
+ * fill_modes: with phases, E[0] *= exp(i pn z); modes k >= kk: E[k] = pn |E[0]| z_k (complex: (zr + i zi) / sqrt 2).
+ * z: float64 normals on the device in the order the reference draws them (phases first, then per mode re, im). */
+int blml_start_root(int dtype, int64_t B, const void* c, const void* sg, double s0, void* e0, void* stream);
+int blml_fill_modes(int dtype, int K, int64_t B, int cplx, int kk, int phases, double pn, const double* z, void* E,
+                    void* stream);
+
+/* ---- certificate weights (BLMLBinned.certificate, blml_binned.py:506-507): dh = sqrt(sum_k |E_k|^2 / w) on
+ *      occupied bins, 0 elsewhere, float64 output whatever the fit dtype ---- */
+int blml_cert_weights(int dtype, int K, int64_t B, int cplx, const void* E, const void* w, double* dh, void* stream);
+
+/* ---- pair accumulation over lattice bins from the row-kernel value tables (blml_local_gpu.rows / cols,
+ *      blml_local_gpu.py:42-105, 320-361, 408-455; numba twins blml_local.py:117-191) ----
+ * ZA (R, d), ZB (M, d): int64 lattice coordinates as the tables read them (rank columns: ranks). Table arrays are
+ * the ProductKernel layout (blml_kernels.py:133-200): T flat values, base / Jk / mk / kinds / nbins / grp per column,
+ * RT (G, LR) group rows, dim_unit / grp_unit, and for grad the derivative rows dT / dbase / dR / wunit / wcol /
+ * wgrp (nW entries). rows: s (R) float64 = sum_j w_j S(ZA_r, ZB_j); ds (R, nW) with grad.
+ * f32 = 1: table values and products in float32 (sums in float64), as the reference's f32 flag. */
+typedef struct {
+  int d, U, G, nW, LR, f32;
+  int64_t nT, ndT;                    /* lengths of the flat value arrays T and dT */
+  const double* T; const int64_t* base; const int64_t* Jk; const int64_t* mk; const int64_t* kinds;
+  const int64_t* nbins; const int64_t* grp; const double* RT; const int64_t* dim_unit; const int64_t* grp_unit;
+  const double* dT; const int64_t* dbase; const double* dR; const int64_t* wunit; const int64_t* wcol;
+  const int64_t* wgrp;
+  const float* T32; const float* RT32; const float* dT32; const float* dR32;   /* float32 copies when f32 = 1 */
+} blml_tables;
+int blml_rows(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
+              int grad, double* s, double* ds, void* stream);
+/* out (R, M) row-major = S(ZA_r, ZB_j), float64 (out_f32 = 0) or float32 */
+int blml_cols(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
+              int out_f32, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -228,9 +228,10 @@ def mode_table(spec, shape, h, pad):
 class Operator:
     """S_k for every mode: rFFT of each mode's table (modes with one kernel share it)."""
 
-    def __init__(self, specs, shape, h):
+    def __init__(self, specs, shape, h, workers=None):
         import scipy.fft as sfft
         self.fft = sfft
+        self.kw = {} if workers is None else dict(workers=workers)
         self.shape = tuple(shape); self.h = np.asarray(h, float)
         self.pad = pad_rule(self.shape, self.h, specs)
         key = lambda sp: (tuple(sp['fc']), tuple(sp['kinds']), tuple(sp['periods']))
@@ -246,12 +247,12 @@ class Operator:
 
     def S(self, k, e):
         sl = tuple(slice(0, m) for m in self.shape)
-        f = self.fft
+        f, kw = self.fft, self.kw
         if np.iscomplexobj(e):
-            re = f.irfftn(f.rfftn(e.real, s=self.pad) * self.Kf[k], s=self.pad)[sl]
-            im = f.irfftn(f.rfftn(e.imag, s=self.pad) * self.Kf[k], s=self.pad)[sl]
+            re = f.irfftn(f.rfftn(e.real, s=self.pad, **kw) * self.Kf[k], s=self.pad, **kw)[sl]
+            im = f.irfftn(f.rfftn(e.imag, s=self.pad, **kw) * self.Kf[k], s=self.pad, **kw)[sl]
             return re + 1j * im
-        return f.irfftn(f.rfftn(e, s=self.pad) * self.Kf[k], s=self.pad)[sl]
+        return f.irfftn(f.rfftn(e, s=self.pad, **kw) * self.Kf[k], s=self.pad, **kw)[sl]
 
     def Sall(self, E):
         return np.stack([self.S(k, E[k]) for k in range(len(self.Kf))])
@@ -508,7 +509,7 @@ class BinnedFit:
         self.d = counts.ndim; self.shape = counts.shape
         self.specs = parse_modes(modes, self.d)
         self.h = np.broadcast_to(np.asarray(h, float), (self.d,)).copy()
-        self.op = Operator(self.specs, self.shape, self.h)
+        self.op = Operator(self.specs, self.shape, self.h, getattr(self, 'workers', None))
         self.s = self.op.s.copy(); self.K = len(self.specs); self.shared = self.op.shared
         w = np.asarray(counts, float)
         self.w = w; self.n = float(w.sum())

@@ -1,0 +1,189 @@
+"""GPU parity of the binned path against the reference's golden outputs and the CPU oracle.
+
+Tolerances: float64 pieces to 1e-11 relative (round-off of a different summation order); whole float64 fits to the
+parity bar, density_ within 1e-5 relative L-inf on occupied bins and loglik_ within 1e-7 relative. float32 state
+(float64 reductions): loglik_ within 1e-7 relative and density_ within 1e-5 of the largest density -- per-bin
+relative error at near-empty bins is bounded below by float32 storage (eps * max|S e| / |S e|), for the reference's
+own complex64 engine as for this one. Non-convex (complex) fits whose reference endpoint stopped on ll_tol are
+compared at the convergence level of that endpoint (density 1e-4 relative), loglik to 1e-7."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from golden_cases import MATVEC_SPECS, MATVEC_COMPLEX, UPDATE_MODES, FIT_SPECS
+
+pytestmark = pytest.mark.gpu
+
+DENS_TOL, LL_TOL = 1e-5, 1e-7
+
+
+def _plan(shape, spec, h, dtype):
+    from blml_b200 import operator as op_mod, _lib
+    d = len(shape)
+    hv = np.full(d, h)
+    return op_mod.Plan(*op_mod.mode_transform(spec, shape, hv, op_mod.pad_rule(shape, hv, [spec])), shape,
+                       dtype, _lib.ENGINE_SIMT)
+
+
+@pytest.mark.parametrize('dt', ['f64', 'f32'])
+@pytest.mark.parametrize('name', list(MATVEC_SPECS))
+def test_matvec_matches_reference(cuda_device, name, dt):
+    from blml_b200 import operator as op_mod, _lib
+    from blml_b200.spec import parse_modes
+    g = golden('matvec.npz')[name]
+    shape, modes, h = MATVEC_SPECS[name]
+    specs, _ = parse_modes(modes, len(shape))
+    hv = np.full(len(shape), h)
+    pad = op_mod.pad_rule(shape, hv, specs)
+    code = _lib.F64 if dt == 'f64' else _lib.F32
+    cplx = name in MATVEC_COMPLEX
+    tdt = {('f64', True): torch.complex128, ('f64', False): torch.float64,
+           ('f32', True): torch.complex64, ('f32', False): torch.float32}[(dt, cplx)]
+    st = torch.cuda.current_stream().cuda_stream
+    for k, sp in enumerate(specs):
+        plan = op_mod.Plan(*op_mod.mode_transform(sp, shape, hv, pad), shape, code, _lib.ENGINE_SIMT)
+        x = torch.as_tensor(g['E'][k]).to(cuda_device, tdt).contiguous()
+        y = torch.empty_like(x)
+        plan.apply(x, y, 1, cplx, st)
+        ref = g['U'][k]
+        err = np.abs(y.cpu().numpy().astype(ref.dtype) - ref).max() / np.abs(ref).max()
+        assert err <= (1e-12 if dt == 'f64' else 1e-5), (name, k, err)
+
+
+def test_matvec_batched_modes(cuda_device):
+    """Several lattices in one call give the same results as one call each."""
+    from blml_b200 import _lib
+    from blml_b200.spec import parse_modes
+    specs, _ = parse_modes(MATVEC_SPECS['d2_pball64'][1], 2)
+    plan = _plan((64, 64), specs[0], 1.0, _lib.F64)
+    x = torch.randn(3, 64, 64, dtype=torch.complex128, device=cuda_device)
+    y = torch.empty_like(x); y1 = torch.empty_like(x)
+    st = torch.cuda.current_stream().cuda_stream
+    plan.apply(x, y, 3, True, st)
+    for b in range(3):
+        plan.apply(x[b], y1[b], 1, True, st)
+    assert torch.equal(y, y1)
+
+
+def _fit_state(name, dt):
+    from blml_b200.binned import BLMLBinned
+    g = golden('updates.npz')[name]
+    w = g['w']
+    m = BLMLBinned(dtype=np.float64 if dt == 'f64' else np.float32)
+    m._setup(w, UPDATE_MODES[name], 1.0, 0.0)
+    m.n_ = float(w.sum())
+    m.w_t_ = torch.as_tensor(w.ravel(), dtype=m._rt).cuda()
+    m.c_t_ = torch.as_tensor(m.n_ * w.ravel(), dtype=m._rt).cuda()
+    m.sg_t_ = torch.ones(w.size, dtype=m._rt, device='cuda')
+    m.complex_g_ = name != 'real1'; m.psd_ = m.complex_g_ or m.K_ > 1
+    et = m._ct if m.complex_g_ else m._rt
+    E = torch.as_tensor(g['E'].reshape(m.K_, -1)).to('cuda', et).contiguous()
+    U = torch.as_tensor(g['U'].reshape(m.K_, -1)).to('cuda', et).contiguous()
+    return m, g, E, U
+
+
+@pytest.mark.parametrize('name', ['real1', 'psd_eq', 'psd_sec'])
+def test_bin_kernels_match_reference(cuda_device, name):
+    m, g, E, U = _fit_state(name, 'f64')
+    upd = m._update(E, U).cpu().numpy().reshape(g['update'].shape)
+    np.testing.assert_allclose(upd, g['update'], rtol=1e-11, atol=1e-11 * np.abs(g['update']).max())
+    assert abs(m._merit(E, U) - float(g['merit'])) <= 1e-11 * abs(float(g['merit']))
+    assert abs(m._resid(E, U) - float(g['resid'])) <= 1e-11
+    E2, U2 = E.clone(), U.clone()
+    m._rescale(E2, U2)
+    np.testing.assert_allclose(E2.cpu().numpy().reshape(g['rescaled_E'].shape), g['rescaled_E'], rtol=1e-12)
+    if m.psd_:
+        L, gr, Q = m._lgrad(E, U)
+        assert abs(L - float(g['lgrad_L'])) <= 1e-11 * abs(L)
+        ref = g['lgrad_g']
+        np.testing.assert_allclose(gr.cpu().numpy().reshape(ref.shape), ref, rtol=1e-9, atol=1e-11 * np.abs(ref).max())
+
+
+FITS_F64 = ['d1_sinc_real', 'd1_sinc_rank2_real', 'd1_dir_circ_real', 'd2_sinc_sinc_real', 'd2_ball_real',
+            'c1_sinc1024', 'd2_pball_cd']
+
+
+def _fit(name, dtype, **over):
+    from blml_b200.binned import BLMLBinned
+    g = golden('fits.npz')[name]
+    modes, fkw, ckw = FIT_SPECS[name]
+    ckw = dict(ckw, **over)
+    return g, BLMLBinned(dtype=dtype, **ckw).fit(g['counts'], modes, **fkw)
+
+
+def _check(g, m, dens_tol=DENS_TOL, ll_tol=LL_TOL, of_max=False):
+    occ = g['counts'] > 0
+    dens = m.density_
+    ref = g['density'][occ]
+    rel = np.max(np.abs(dens[occ] - ref) / (ref.max() if of_max else ref))
+    dll = abs(m.loglik_ - float(g['loglik'])) / abs(float(g['loglik']))
+    assert rel <= dens_tol and dll <= ll_tol, (rel, dll)
+    return rel, dll
+
+
+@pytest.mark.parametrize('name', FITS_F64)
+def test_fit_float64_matches_reference(cuda_device, name):
+    g, m = _fit(name, np.float64)
+    _check(g, m)
+    assert m.converged_ or m.stop_reason_ == str(g['stop'])
+    if 'cert' in g and name != 'd2_pball_cd':
+        assert abs(m.certificate() - float(g['cert'])) <= 1e-5 * max(1.0, abs(float(g['cert'])))
+
+
+@pytest.mark.parametrize('name', ['c1_sinc1024', 'd2_sinc_sinc_real', 'd1_dir_circ_real'])
+def test_fit_float32_matches_reference(cuda_device, name):
+    """float32 state (float64 reductions) on the convex fits: same optimum within the parity bar."""
+    g, m = _fit(name, np.float32, tol=1e-5)
+    _check(g, m, of_max=True)
+
+
+@pytest.mark.parametrize('name', ['d2_pball_lbfgs', 'd2_pball_bg_lbfgs'])
+def test_lbfgs_polish_of_reference_optimum(cuda_device, name):
+    """Complex fits are non-convex: started at the reference's optimum (init=), the GPU L-BFGS stays there
+    (the reference's own polish test, results/pball_parity.py:108-118), within the parity bar."""
+    from blml_b200.binned import BLMLBinned
+    g = golden('fits.npz')[name]
+    modes, fkw, ckw = FIT_SPECS[name]
+
+    class Init:
+        e_hat_ = g['e_hat']; shape_ = g['counts'].shape
+    m = BLMLBinned(dtype=np.float64, **ckw).fit(g['counts'], modes, init=Init(), **fkw)
+    _check(g, m, dens_tol=1e-4)
+    assert m.loglik_ >= float(g['loglik']) - 1e-12 * abs(float(g['loglik']))    # polishing never loses likelihood
+
+
+@pytest.mark.parametrize('name', ['d2_pball_lbfgs', 'd2_pball_bg_lbfgs'])
+def test_lbfgs_same_start_same_optimum(cuda_device, name):
+    """From the same seeded start, the GPU L-BFGS reaches the reference's optimum (loglik to 1e-7)."""
+    g, m = _fit(name, np.float64)
+    _check(g, m, dens_tol=1e-4)
+
+
+def test_certificate_matches_dense(cuda_device):
+    """certificate() equals the dense eigvalsh of D^1/2 S D^1/2 / n (results/binned_checks.py:50-53)."""
+    import blml_oracle as bo
+    g, m = _fit('d2_sinc_sinc_real', np.float64)
+    f = bo.BinnedFit(**FIT_SPECS['d2_sinc_sinc_real'][2]).fit(g['counts'], FIT_SPECS['d2_sinc_sinc_real'][0])
+    assert abs(m.certificate(tol=1e-10) - f.certificate_dense()) < 1e-7
+
+
+def test_errors_like_reference(cuda_device):
+    from blml_b200.binned import BLMLBinned
+    from blml_b200 import make_modes
+    with pytest.raises(ValueError):
+        BLMLBinned(solver='newton')
+    with pytest.raises(ValueError):
+        BLMLBinned().fit(-np.ones(8), make_modes([0.3], ['sinc']))
+    with pytest.raises(ValueError):
+        BLMLBinned().fit(np.zeros(8), make_modes([0.3], ['sinc']))
+    with pytest.raises(ValueError):
+        BLMLBinned().fit(np.ones(8), make_modes([0.3], ['sinc'], rank=2), signs=np.ones(8))
+    m = BLMLBinned().fit(np.arange(16.0), make_modes([[0.3], [0.1]], ['sinc']), complex_g=True)
+    with pytest.raises(ValueError):
+        m.certificate()
+
+
+def test_log_density_is_loglik(cuda_device):
+    g, m = _fit('c1_sinc1024', np.float64)
+    assert abs(m.log_density(g['counts']) - m.loglik_) < 1e-10

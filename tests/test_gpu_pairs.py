@@ -1,0 +1,73 @@
+"""GPU pair accumulation (rows / cols) against the reference's golden outputs: binning and pair indices bit-exact,
+float64 sums to 1e-12 of the largest entry, float32 tables to 2e-4 (the reference's own f32 bar,
+results/gpu_kernels_check.py)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_rows_cols_5d(cuda_device):
+    from blml_b200.local_gpu import ProductKernel, rows, cols, rank_coords
+    p = golden('pairs.npz')['p5']
+    u, cnt = p['bins'], p['counts']
+    pk = ProductKernel(['sinc'] * 5, [None] * 5)
+    tab = pk.tables(p['fc'], [None] * 5, p['h'], u)
+    s, _ = rows(u, u, cnt, tab)
+    scale = np.abs(p['rows']).max()
+    assert np.abs(s - p['rows']).max() <= 1e-12 * scale
+    s32, _ = rows(u, u, cnt, tab, f32=True)
+    assert np.abs(s32 - p['rows']).max() <= 2e-4 * scale
+    A = torch.as_tensor(rank_coords(u[:300], tab)).cuda(); B = torch.as_tensor(rank_coords(u[:200], tab)).cuda()
+    out = torch.empty((300, 200), dtype=torch.float64, device='cuda')
+    cols(A, B, tab, out)
+    assert np.abs(out.cpu().numpy() - p['cols']).max() <= 1e-14
+    assert np.abs(out.cpu().numpy() - p['gram']).max() <= 1e-13
+
+
+def test_rows_torus_with_derivatives(cuda_device):
+    from blml_b200.local_gpu import ProductKernel, rows, cols, rank_coords
+    t = golden('pairs.npz')['pt']
+    kinds, per = ['pball:0-1', 'pball:0-1', 'sinc'], [31.0, 31.0, None]
+    fc, h = np.array([0.33, 0.33, 0.2]), np.array([1.0, 1.0, 0.7])
+    pk = ProductKernel(kinds, per, fold=[True] * 3)
+    want = [(1, ('shift', 0)), (1, ('shift', 1)), (0, 'fc')]
+    tab = pk.tables(fc, per, h, np.r_[t['ZA'], t['ZB']], want=want)
+    s, ds = rows(t['ZA'], t['ZB'], t['w'], tab, grad=True)
+    assert np.abs(s - t['rows']).max() <= 1e-12
+    assert np.abs(ds - t['drows']).max() <= 1e-12
+    A = torch.as_tensor(rank_coords(t['ZA'], tab)).cuda(); B = torch.as_tensor(rank_coords(t['ZB'], tab)).cuda()
+    out = torch.empty((len(t['ZA']), len(t['ZB'])), dtype=torch.float64, device='cuda')
+    cols(A, B, tab, out)
+    assert np.abs(out.cpu().numpy() - t['cols']).max() <= 1e-12
+
+
+def test_stale_tables_are_an_error(cuda_device):
+    """Coordinates outside the tables' span raise instead of reading out of range."""
+    from blml_b200.local_gpu import ProductKernel, rows
+    from blml_b200._lib import BLMLError
+    Z = np.array([[0, 0], [3, 4], [6, 1]], np.int64)
+    pk = ProductKernel(['sinc', 'sinc'])
+    tab = pk.tables([0.3, 0.3], [None, None], [1.0, 1.0], Z)
+    far = np.array([[40, 0]], np.int64)
+    with pytest.raises(RuntimeError):                 # a rank column: the host rank lookup refuses it
+        rows(far, Z, np.ones(3), tab)
+    Zw = np.array([[0, 0], [3, 4], [6, 1], [1, 1], [2, 5]], np.int64)
+    tab = ProductKernel(['sinc', 'sinc']).tables([0.3, 0.3], [None, None], [1.0, 1.0], Zw, )
+    assert all(v is None for v in tab['vals'])        # offset rows only
+    far_dev = torch.as_tensor([[400, 0]], dtype=torch.int64, device='cuda')
+    with pytest.raises(BLMLError):                    # offset rows: the device extent check refuses it
+        rows(far_dev, torch.as_tensor(Zw).cuda(), np.ones(5), tab)
+
+
+def test_empty_inputs(cuda_device):
+    from blml_b200.local_gpu import ProductKernel, rows
+    Z = np.array([[0, 0], [3, 4]], np.int64)
+    tab = ProductKernel(['sinc', 'sinc']).tables([0.3, 0.3], [None, None], [1.0, 1.0], Z)
+    s, _ = rows(Z, Z[:0], np.zeros(0), tab)
+    assert np.array_equal(s, np.zeros(2))
+    s, _ = rows(Z[:0], Z, np.ones(2), tab)
+    assert s.shape == (0,)
