@@ -20,6 +20,12 @@ from .spec import parse_modes, spec_key
 from .operator import pad_rule, mode_transform, kernel_at_zero, Plan
 
 
+from collections import OrderedDict
+
+_PLANS = OrderedDict()            # (kernel spec, lattice, h, dtype, engine, device) -> (Plan, K(0), transform)
+_PLAN_CACHE_SIZE = 128
+
+
 def _device(dev):
     if not torch.cuda.is_available():
         raise _lib.BLMLError('BLMLBinned needs a CUDA device (this engine has no CPU path)')
@@ -100,22 +106,26 @@ class BLMLBinned:
         return counts
 
     def _build_kernels(self):
-        """One device plan per distinct mode kernel (modes with the same kernel share it)."""
-        cache, old = {}, {k: v for k, v in getattr(self, '_plan_cache', {}).items()}
-        eng = _lib.ENGINE_TC if self.matvec_engine == 'tc' else _lib.ENGINE_SIMT
+        """One device plan per distinct mode kernel (modes with the same kernel share it), from a process-wide cache
+        of recent plans (refits on the same lattice and kernel reuse their twiddles)."""
+        eng = _lib.ENGINE_TC if self.matvec_engine == 'tc' and self.d_ == 2 and self.shape_[-1] % 4 == 0 \
+            else _lib.ENGINE_SIMT
         self.kern_ = []
+        mine = set()
         for sp in self.specs_:
-            key = (spec_key(sp), self.shape_, tuple(np.round(self.h_, 15)), self._code, eng)
-            if key not in cache:
-                if key in old:
-                    cache[key] = old[key]
-                else:
-                    freqs, W = mode_transform(sp, self.shape_, self.h_, self.pad_)
-                    plan = Plan(freqs, W, self.shape_, self._code, eng if self.d_ == 2 else _lib.ENGINE_SIMT)
-                    cache[key] = (plan, kernel_at_zero(sp, self.d_), (freqs, W))
-            self.kern_.append(cache[key])
-        self._plan_cache = cache
-        self.shared_ = len(cache) == 1
+            key = (spec_key(sp), self.shape_, tuple(np.round(self.h_, 15)), self._code, eng, str(self.dev_))
+            hit = _PLANS.pop(key, None)
+            if hit is None:
+                freqs, W = mode_transform(sp, self.shape_, self.h_, self.pad_)
+                with torch.cuda.device(self.dev_):
+                    plan = Plan(freqs, W, self.shape_, self._code, eng)
+                hit = (plan, kernel_at_zero(sp, self.d_), (freqs, W))
+            _PLANS[key] = hit                         # most recent last
+            mine.add(key)
+            self.kern_.append(hit)
+        while len(_PLANS) > _PLAN_CACHE_SIZE:
+            _PLANS.popitem(last=False)
+        self.shared_ = len(mine) == 1
         self.s_ = np.array([kk[1] for kk in self.kern_])
 
     # ---------------------------------------------------------------- device helpers
@@ -360,7 +370,12 @@ class BLMLBinned:
                     self.stop_reason_ = 'stall'; break
                 Sh, Yh = [], []; SY = np.zeros((0, 0)); YY = np.zeros((0, 0)); reset = True; continue
             reset = False
-            V, _ = self._grad_weights(Un)
+            # the accepted point's U exactly: U + t S q equals S(E + t q) only up to rounding, and a drifting U lets
+            # the ascent move e along the near-null directions of S (which change Q = <E, U> through the drift alone)
+            self._Sall(En, out=Un)
+            Qn = self._Q(En, Un)
+            V, Lwn = self._grad_weights(Un)
+            Ln = Lwn - n * np.log(Qn) if Qn > 0 else -np.inf
             gn = self._grad_finish(self._Sall(V), Un, n / Qn)
             s_ = self._lin([(t, q)]); y_ = self._lin([(1.0, g), (-1.0, gn)])
             vals = self._dots([(s_, y_), (s_, s_), (y_, y_)] + [(s, y_) for s in Sh] + [(y, y_) for y in Yh])
@@ -441,21 +456,44 @@ class BLMLBinned:
         return self
 
     def _start(self, et):
-        """Real positive root of mode 0 (one convex solve), then small phases / small other modes."""
+        """Real positive root of mode 0 (one convex solve), then small phases / small other modes. For float32 fits
+        the convex start is solved in float64: its merit safeguard needs more than float32 resolution below
+        max|rho| ~ 1e-2, where a float32 solve stalls."""
         e0 = torch.empty((1, self.B_), dtype=self._rt, device=self.dev_)
         call('blml_start_root', self._code, self.B_, self.c_t_.data_ptr(), self.sg_t_.data_ptr(), float(self.s_[0]),
              e0.data_ptr(), self._st)
         if not self.psd_:
             return e0
-        save = (self.psd_, self.K_, self.kern_, self.s_)
-        self.psd_, self.K_, self.kern_, self.s_ = False, 1, self.kern_[:1], self.s_[:1]
-        try:
-            er, _ = self._solve(e0, self.max_sweeps)
-        finally:
-            self.psd_, self.K_, self.kern_, self.s_ = save
+        if self._code == _lib.F32:
+            er = self._start_f64()
+        else:
+            save = (self.psd_, self.K_, self.kern_, self.s_)
+            self.psd_, self.K_, self.kern_, self.s_ = False, 1, self.kern_[:1], self.s_[:1]
+            try:
+                er, _ = self._solve(e0, self.max_sweeps)
+            finally:
+                self.psd_, self.K_, self.kern_, self.s_ = save
         E = torch.zeros((self.K_, self.B_), dtype=et, device=self.dev_)
         E[0] = er[0].to(et)
         return self._fill_modes(E, 1)
+
+    def _start_f64(self):
+        """The real rank-1 start under mode 0, solved by a float64 twin of this fit (same counts, solver settings)."""
+        twin = BLMLBinned(tol=self.tol, max_sweeps=self.max_sweeps, anderson=self.anderson, dtype=np.float64,
+                          phase_noise=self.phase_noise, seed=self.seed, stall=self.stall, ll_tol=self.ll_tol,
+                          ll_window=self.ll_window, solver='cd', device=self.dev_)
+        twin._setup(self.w_t_.reshape(self.shape_).to(torch.float64), self.modes_[:1], self.h_, self.origin_)
+        twin.n_ = self.n_
+        twin.w_t_ = self.w_t_.to(torch.float64)
+        twin.c_t_ = twin._lin([(self.n_, twin.w_t_)])
+        twin.sg_t_ = self.sg_t_.to(torch.float64)
+        twin.complex_g_ = False; twin.psd_ = False
+        e0 = torch.empty((1, self.B_), dtype=torch.float64, device=self.dev_)
+        call('blml_start_root', _lib.F64, self.B_, twin.c_t_.data_ptr(), twin.sg_t_.data_ptr(), float(twin.s_[0]),
+             e0.data_ptr(), self._st)
+        er, _ = twin._solve(e0, self.max_sweeps)
+        self.start_sweeps_ = twin.n_sweeps_
+        return er
 
     def _fill_modes(self, E, kk, phases=True):
         """The reference's seeded start noise (blml_binned.py:429-436): the normals are drawn on the host with the same

@@ -212,6 +212,12 @@ __global__ void k_cols(ColMeta cm, const REAL* T, const REAL* RT, const int64_t*
   }
 }
 
+// lattice coordinates of bin centres: round(Z / h) in float64, ties to even (np.round's rule, so bit-exact with it)
+__global__ void k_lattice_coords(const double* Z, int64_t n, int d, const double* h, int64_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * d; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int64_t)rint(Z[i] / h[i % d]);
+}
+
 // per column: min and max of ZA and ZB (for the extent check); out[4 * k + {0,1,2,3}] = minA, maxA, minB, maxB
 __global__ void k_coord_range(const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, int d, long long* out) {
   const int k = blockIdx.x;
@@ -408,6 +414,15 @@ int blml_rows(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t
   }
   if (!tb->T || (cm.G && !tb->RT) || (grad && (!tb->dT || !tb->dR))) { set_error("blml_rows: tables missing"); return BLML_ERR_ARG; }
   return rows_impl<double>(tb, cm, tb->T, tb->RT, tb->dT, tb->dR, ZA, R, ZB, M, w, grad, s, ds, st);
+}
+
+int blml_lattice_coords(const double* Z, int64_t n, int d, const double* h, int64_t* out, void* stream) {
+  if (n < 0 || d < 1) { set_error("blml_lattice_coords: bad sizes"); return BLML_ERR_ARG; }
+  if (n == 0) return BLML_OK;
+  const int g = (int)std::min<int64_t>((n * d + 255) / 256, 148 * 32);
+  k_lattice_coords<<<g, 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(Z, n, d, h, out);
+  count_launches(1);
+  return cuda_status(cudaGetLastError(), "blml_lattice_coords");
 }
 
 int blml_cols(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,

@@ -179,10 +179,19 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--cpu-sample-iters', type=int, default=40)
+    ap.add_argument('--one-fit', action='store_true', help='one fit of the workload and exit (profiling runs)')
+    ap.add_argument('--engine', default='simt', choices=['simt', 'tc'], help='mat-vec engine of the float32 fits')
     args = ap.parse_args()
     rank, ws, local = dist_init()
     if args.impl == 'reference':
         return reference_arm(args, rank, ws)
+    if args.one_fit:
+        from blml_b200.binned import BLMLBinned
+        counts, modes = workload(0)
+        m = BLMLBinned(tol=TOL, solver='lbfgs', dtype=np.float32, matvec_engine=args.engine).fit(counts, modes,
+                                                                                                complex_g=True)
+        print(json.dumps({'loglik': m.loglik_, 'iterations': m.n_sweeps_, 'stop': m.stop_reason_}))
+        return
     import torch
     from blml_b200.binned import BLMLBinned
     from blml_b200 import _lib
@@ -191,7 +200,8 @@ def main():
     counts, modes = workload(seed=rank)
     counts_dev = torch.as_tensor(counts).to(dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    kw = dict(tol=TOL, solver='lbfgs', dtype=np.float32, device=dev)
+    kw = dict(tol=TOL, solver='lbfgs', dtype=np.float32, device=dev, matvec_engine=args.engine)
+    CONFIG['matvec_engine'] = args.engine
     # certification reference: the float64 fit of the same counts
     ref64 = BLMLBinned(tol=TOL, solver='lbfgs', dtype=np.float64, device=dev).fit(counts_dev, modes, complex_g=True)
     for _ in range(args.warmup):

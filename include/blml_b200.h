@@ -136,6 +136,10 @@ typedef struct {
 } blml_tables;
 int blml_rows(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
               int grad, double* s, double* ds, void* stream);
+/* ---- fixed-lattice binning (BLMLQuick._fit_lattice, blml_trivial.py:3572; SincKernel.quantize :402-403) ----
+ * out (n, d) int64 = round(Z / h) of bin centres Z (n, d) float64, h (d) float64, ties to even as np.round */
+int blml_lattice_coords(const double* Z, int64_t n, int d, const double* h, int64_t* out, void* stream);
+
 /* out (R, M) row-major = S(ZA_r, ZB_j), float64 (out_f32 = 0) or float32 */
 int blml_cols(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
               int out_f32, void* stream);

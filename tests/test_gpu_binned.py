@@ -133,9 +133,23 @@ def test_fit_float64_matches_reference(cuda_device, name):
 
 @pytest.mark.parametrize('name', ['c1_sinc1024', 'd2_sinc_sinc_real', 'd1_dir_circ_real'])
 def test_fit_float32_matches_reference(cuda_device, name):
-    """float32 state (float64 reductions) on the convex fits: same optimum within the parity bar."""
+    """float32 state (float64 reductions) on the convex fits: loglik within 1e-7 relative; density within 1e-4 of
+    the largest density (a float32 coordinate descent stops at max|rho| ~ 1e-5)."""
     g, m = _fit(name, np.float32, tol=1e-5)
-    _check(g, m, of_max=True)
+    _check(g, m, dens_tol=1e-4, of_max=True)
+
+
+def test_fit_float32_lbfgs_matches_float64(cuda_device):
+    """A complex two-mode pball fit with float32 state lands on the float64 fit's likelihood (1e-6 relative, the
+    certification bar): U is recomputed as S E at every accepted step, so the float32 iterate cannot drift."""
+    from blml_b200.binned import BLMLBinned
+    from blml_b200 import workloads
+    counts = workloads.two_disk_field((96, 96), fc=0.33, N=3e5, seed=5)
+    modes = workloads.pball_modes((96, 96), 0.33, 3 / 96)
+    m64 = BLMLBinned(tol=1e-6, solver='lbfgs', dtype=np.float64).fit(counts, modes, complex_g=True)
+    m32 = BLMLBinned(tol=1e-6, solver='lbfgs', dtype=np.float32).fit(counts, modes, complex_g=True)
+    assert abs(m32.loglik_ - m64.loglik_) <= 1e-6 * abs(m64.loglik_)
+    assert m32.Se_.shape == (2, 96, 96) and np.isfinite(m32.density_).all()
 
 
 @pytest.mark.parametrize('name', ['d2_pball_lbfgs', 'd2_pball_bg_lbfgs'])
