@@ -40,6 +40,24 @@ _SIGS = {
     'blml_plan_status': (_I, [_P]),
     'blml_matvec_workspace': (_L, [_P, _I]),
     'blml_matvec': (_I, [_P, _P, _P, _I, _I, _P, _L, _P]),
+    'blml_group_create': (_I, [_I, _P, _P, _I, _P, _P, _P, _P, C.POINTER(_P)]),
+    'blml_group_matvec': (_I, [_P, _P]),
+    'blml_group_destroy': (_I, [_P]),
+    'blml_seg_blocks': (_I, []),
+    'blml_seg_start_root': (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_update_real1': (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_merit': (_I, [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_resid': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_dots': (_I, [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P]),
+    'blml_seg_lincomb': (_I, [_I, _I, _P, _I, _P, _I, _P, _P, _P]),
+    'blml_seg_lgrad_weights': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_lgrad_finish': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_trials': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_axpy2': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_finish': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_log_score': (_I, [_I, _I, _P, _I, _P, _P, _P, _D, _P, _P, _P]),
+    'blml_seg_phases': (_I, [_I, _I, _P, _D, _P, _P, _P]),
+    'blml_seg_real_to_complex': (_I, [_I, _I, _P, _P, _P, _P, _P]),
     'blml_jacobi_update': (_I, [_I, _I, _L, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_merit_terms': (_I, [_I, _I, _L, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_resid': (_I, [_I, _I, _L, _I, _P, _P, _P, _D, _P, _P, _P]),

@@ -1,0 +1,484 @@
+"""Many BLMLBinned fits in lockstep on one GPU: the cut-off sweep (selector._search, selector.py:488-553; the binned
+sweeps of dslit_job.py:158-171 and results/p3_window_pball.py:27-30) and rolling windows run their fits one after
+another through the reference's single-fit solver (blml_binned.py:223-355); here F fits of uneven lattice size and
+cut-off advance together, every phase one launch over all fits (csrc/batched.cu, grouped mat-vecs in
+csrc/matvec.cu), and the per-fit scalar control (Anderson weights, the L-BFGS direction, Armijo choices, stop rules)
+runs vectorised on the host with a fixed number of host syncs per iteration, whatever F is.
+
+    fits = BLMLBinnedBatch(tol=1e-6, dtype=np.float32).fit(counts_list, modes_list)   # complex_g, L-BFGS
+    fits[i].loglik_, fits[i].density_, fits[i].n_sweeps_, fits[i].stop_reason_
+    scores = batch.log_density(val_counts_list)                                       # held-out scores
+
+Each fit is the reference's algorithm: the real rank-1 start under the fit's kernel by Jacobi coordinate updates
+with Anderson mixing and the merit safeguard (in float64, see BLMLBinned._start), the seeded phases, L-BFGS ascent
+of L = sum w log F - n log Q with Armijo backtracking (the first of t = 1, 1/2, ..., 2^-39 that passes; all forty
+trials in one pass), memory 20, the canonical form at the end. One mode per fit (shared kernel), complex_g."""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call, ptrs
+from .spec import parse_modes, spec_key
+from .operator import pad_rule, mode_transform, kernel_at_zero, Plan
+
+NT = 40
+
+
+class _Seg(C.Structure):
+    _fields_ = [('off', C.c_int64), ('boff', C.c_int64), ('B', C.c_int64), ('K', C.c_int32), ('pad', C.c_int32)]
+
+
+class FitResult:
+    """One fit of a batch: the attributes of a BLMLBinned fit (host NumPy)."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def density_(self):
+        return self._batch.density(self._f)
+
+
+class _Group:
+    def __init__(self, plans, x, x_off, y, y_off, x_complex):
+        G = len(plans)
+        arr = (C.c_void_p * G)(*[p._h.value for p in plans])
+        nb = np.ones(G, np.int32)
+        xo = np.ascontiguousarray(x_off, np.int64); yo = np.ascontiguousarray(y_off, np.int64)
+        h = C.c_void_p()
+        call('blml_group_create', G, C.cast(arr, C.c_void_p), nb.ctypes.data_as(C.c_void_p), int(x_complex),
+             x.data_ptr(), xo.ctypes.data_as(C.c_void_p), y.data_ptr(), yo.ctypes.data_as(C.c_void_p), C.byref(h))
+        self._h = h; self._keep = (plans, x, y)
+
+    def __call__(self, stream):
+        call('blml_group_matvec', self._h, stream)
+
+    def __del__(self):
+        if getattr(self, '_h', None) is not None and self._h.value and _lib._lib is not None:
+            _lib.lib().blml_group_destroy(self._h)
+
+
+class BLMLBinnedBatch:
+    """F independent complex one-mode BLMLBinned fits (L-BFGS) in lockstep; see the module docstring."""
+
+    def __init__(self, tol=1e-5, max_sweeps=None, anderson=5, dtype=np.float32, phase_noise=0.1, seed=0, stall=1000,
+                 ll_tol=None, ll_window=100, lbfgs_m=20, device=None, verbose=False):
+        self.tol, self.max_sweeps, self.anderson = tol, max_sweeps, anderson
+        self.dtype = np.dtype(dtype); self.phase_noise, self.seed, self.stall = phase_noise, seed, stall
+        self.ll_tol, self.ll_window, self.lbfgs_m = ll_tol, ll_window, int(lbfgs_m)
+        self.device = torch.device(device or 'cuda'); self.verbose = verbose
+        if self.lbfgs_m > 20:
+            raise ValueError("lbfgs_m: at most 20")
+
+    # ---------------------------------------------------------------- set-up
+    def _prepare(self, counts_list, modes_list):
+        if not torch.cuda.is_available():
+            raise _lib.BLMLError('BLMLBinnedBatch needs a CUDA device (no CPU path)')
+        dev = self.device
+        F = len(counts_list)
+        if F < 1 or len(modes_list) != F:
+            raise ValueError("one modes list per counts array")
+        self.F = F
+        f32 = self.dtype == np.float32
+        self.code = _lib.F32 if f32 else _lib.F64
+        self.rt = torch.float32 if f32 else torch.float64
+        self.ct = torch.complex64 if f32 else torch.complex128
+        shapes, specs, ws, ns, Bs = [], [], [], [], []
+        for counts, modes in zip(counts_list, modes_list):
+            counts = np.asarray(counts, float)
+            if counts.ndim != 2 or np.any(counts < 0) or not np.all(np.isfinite(counts)):
+                raise ValueError("counts: non-negative finite 2-D arrays")
+            sp, dep = parse_modes(modes, 2)
+            if dep is not None or len(sp) != 1:
+                raise ValueError("BLMLBinnedBatch fits one mode per lattice (shared kernel)")
+            n = float(counts.sum())
+            if not n > 0:
+                raise ValueError("counts: no observations")
+            shapes.append(counts.shape); specs.append(sp[0]); ws.append(counts.ravel()); ns.append(n)
+            Bs.append(counts.size)
+        self.shapes, self.specs, self.n = shapes, specs, np.array(ns)
+        self.B = np.array(Bs, np.int64)
+        boff = np.concatenate([[0], np.cumsum(self.B)])
+        self.boff = boff
+        segs = (_Seg * F)(*[_Seg(int(boff[f]), int(boff[f]), int(self.B[f]), 1, 0) for f in range(F)])
+        self.segs_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
+        Btot = int(boff[-1])
+        self.Btot = Btot
+        w = np.concatenate(ws)
+        self.w64 = torch.as_tensor(w, dtype=torch.float64).to(dev)
+        self.w = self.w64.to(self.rt)
+        self.c64 = (self.w64 * torch.as_tensor(np.repeat(self.n, self.B), dtype=torch.float64).to(dev))
+        self.c = self.c64.to(self.rt)
+        self.sg64 = torch.ones(Btot, dtype=torch.float64, device=dev); self.sg = self.sg64.to(self.rt)
+        nb = _lib.lib().blml_seg_blocks()
+        self.part = torch.empty(48 * F * nb + 64, dtype=torch.float64, device=dev)
+        self.out = torch.empty(48 * F + 64, dtype=torch.float64, device=dev)
+        self.host = torch.empty(48 * F + 64, dtype=torch.float64, pin_memory=True)
+        # plans: float64 for the start, the fit dtype for the L-BFGS
+        self.p64, self.pfit, self.s = [], [], []
+        for shape, sp in zip(shapes, specs):
+            h = np.ones(2)
+            pad = pad_rule(shape, h, [sp])
+            freqs, W = mode_transform(sp, shape, h, pad)
+            self.p64.append(Plan(freqs, W, shape, _lib.F64, _lib.ENGINE_SIMT))
+            self.pfit.append(self.p64[-1] if not f32 else Plan(freqs, W, shape, _lib.F32, _lib.ENGINE_SIMT))
+            self.s.append(kernel_at_zero(sp, 2))
+        self.s = np.array(self.s)
+        self.s_t = torch.as_tensor(self.s, dtype=torch.float64).to(dev)
+        self.st = torch.cuda.current_stream(dev).cuda_stream
+
+    # ---------------------------------------------------------------- device helpers
+    def _read(self, nq):
+        self.host[:nq * self.F].copy_(self.out[:nq * self.F], non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        return self.host[:nq * self.F].numpy().reshape(self.F, nq).copy()
+
+    def _dots(self, code, cplx, pairs):
+        call('blml_seg_dots', code, self.F, self.segs_t.data_ptr(), int(cplx), len(pairs), ptrs([p[0] for p in pairs]),
+             ptrs([p[1] for p in pairs]), self.part.data_ptr(), self.out.data_ptr(), self.st)
+        return self._read(len(pairs))
+
+    def _lin(self, code, cplx, out, coef, vecs):
+        """out = sum_i coef[:, i] v_i per fit (coef (F, nterms))."""
+        cf = torch.as_tensor(np.ascontiguousarray(coef, np.float64)).to(self.device, non_blocking=True)
+        call('blml_seg_lincomb', code, self.F, self.segs_t.data_ptr(), int(cplx), out.data_ptr(), len(vecs),
+             cf.data_ptr(), ptrs(vecs), self.st)
+        return out
+
+    def _dev(self, a):
+        return torch.as_tensor(np.ascontiguousarray(a, np.float64)).to(self.device, non_blocking=True)
+
+    # ---------------------------------------------------------------- the real rank-1 start (float64)
+    def _start(self):
+        """Jacobi updates + Anderson (m = anderson) + the merit safeguard (blml_binned.py:223-276 with psd False),
+        float64, every fit at once; returns the real roots E (flat float64)."""
+        F, code, dev = self.F, _lib.F64, self.device
+        E = torch.empty(self.Btot, dtype=torch.float64, device=dev)
+        call('blml_seg_start_root', code, F, self.segs_t.data_ptr(), self.c64.data_ptr(), self.sg64.data_ptr(),
+             self.s_t.data_ptr(), E.data_ptr(), self.st)
+        U = torch.zeros_like(E)
+        EJ, UJ, EA, UA, ET, UT, f = (torch.zeros_like(E) for _ in range(7))
+        mA = self.anderson
+        DX = [torch.zeros_like(E) for _ in range(mA)]; DF = [torch.zeros_like(E) for _ in range(mA)]
+        pX, pF = torch.zeros_like(E), torch.zeros_like(E)
+        g_EU = _Group(self.p64, E, self.boff[:-1], U, self.boff[:-1], False)
+        g_J = _Group(self.p64, EJ, self.boff[:-1], UJ, self.boff[:-1], False)
+        g_A = _Group(self.p64, EA, self.boff[:-1], UA, self.boff[:-1], False)
+        n = self.n
+        g_EU(self.st)
+
+        def rescale(E_, U_, where=None):
+            Q = self._dots(code, False, [(E_, U_)])[:, 0]
+            sc = np.where(Q > 0, n / np.sqrt(np.maximum(Q, 1e-300)), 1.0)
+            if where is not None:
+                sc = np.where(where, sc, 1.0)
+            self._lin(code, False, E_, sc[:, None], [E_]); self._lin(code, False, U_, sc[:, None], [U_])
+
+        def merit(E_, U_):
+            call('blml_seg_merit', code, F, self.segs_t.data_ptr(), 0, 0, E_.data_ptr(), U_.data_ptr(),
+                 self.c64.data_ptr(), self.sg64.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+            r = self._read(3)
+            m = -(0.5 * r[:, 0] - r[:, 1]) / n
+            return np.where(r[:, 2] > 0, -np.inf, m)
+
+        def resid(E_, U_):
+            call('blml_seg_resid', code, F, self.segs_t.data_ptr(), 0, E_.data_ptr(), U_.data_ptr(),
+                 self.c64.data_ptr(), self._dev(np.ones(F)).data_ptr(), self.part.data_ptr(), self.out.data_ptr(),
+                 self.st)
+            r = self._read(2)
+            return np.where(r[:, 1] > 0, np.nan, r[:, 0])
+
+        rescale(E, U)
+        cur = merit(E, U); res = resid(E, U)
+        active = res >= self.tol
+        it = np.zeros(F, np.int64); best_res = res.copy(); best_it = np.zeros(F, np.int64); best_m = cur.copy()
+        cap = np.inf if self.max_sweeps is None else self.max_sweeps
+        valid = np.zeros((F, mA), bool); has_prev = np.zeros(F, bool)
+        G = np.zeros((F, mA, mA))
+        sweep = 0
+        while active.any():
+            stalled = active & (it - best_it >= self.stall)
+            active &= ~stalled & (it < cap)
+            if not active.any():
+                break
+            it += active
+            call('blml_seg_update_real1', code, F, self.segs_t.data_ptr(), E.data_ptr(), U.data_ptr(),
+                 self.c64.data_ptr(), self.sg64.data_ptr(), self.s_t.data_ptr(), EJ.data_ptr(), self.st)
+            g_J(self.st)
+            mJ = merit(EJ, UJ)
+            take_A = np.zeros(F, bool)
+            if mA:
+                self._lin(code, False, f, np.tile([1.0, -1.0], (F, 1)), [EJ, E])
+                p = sweep % mA
+                # the new differences go to slot p for every fit (slots written before a fit's last reset are
+                # invalid for it); the Anderson solve is invariant to the order of its columns
+                self._lin(code, False, DX[p], np.tile([1.0, -1.0], (F, 1)), [E, pX])
+                self._lin(code, False, DF[p], np.tile([1.0, -1.0], (F, 1)), [f, pF])
+                valid[:, p] = has_prev & active
+                vals = self._dots(code, False, [(DF[p], DF[q]) for q in range(mA)] + [(DF[q], f) for q in range(mA)])
+                G[:, p, :] = vals[:, :mA]; G[:, :, p] = vals[:, :mA]
+                rhs = vals[:, mA:]
+                self._lin(code, False, pX, np.ones((F, 1)), [E]); self._lin(code, False, pF, np.ones((F, 1)), [f])
+                has_prev |= active
+                k = valid.sum(1)
+                use = active & (k >= 2)
+                gam = np.zeros((F, mA))
+                for fi in np.where(use)[0]:
+                    vv = np.where(valid[fi])[0]
+                    Gs = G[fi][np.ix_(vv, vv)]
+                    try:
+                        gg = np.linalg.solve(Gs + 1e-12 * np.trace(Gs) * np.eye(len(vv)), rhs[fi, vv])
+                        if not np.all(np.isfinite(gg)):
+                            raise np.linalg.LinAlgError
+                        gam[fi, vv] = gg
+                    except np.linalg.LinAlgError:
+                        valid[fi] = False; has_prev[fi] = False; use[fi] = False
+                if use.any():
+                    coef = np.concatenate([np.ones((F, 2)), -gam, -gam], 1)
+                    coef[~use] = 0.0; coef[~use, 0] = 1.0          # fits without a mix: EA = E (unused)
+                    self._lin(code, False, EA, coef, [E, f] + DX + DF)
+                    g_A(self.st)
+                    mAc = merit(EA, UA)
+                    take_A = use & (mAc > mJ)
+                    mJ = np.where(take_A, mAc, mJ)
+            # candidate: the Anderson point where it won, else the Jacobi point
+            ta = take_A.astype(float)
+            self._lin(code, False, ET, np.stack([ta, 1 - ta], 1), [EA, EJ])
+            self._lin(code, False, UT, np.stack([ta, 1 - ta], 1), [UA, UJ])
+            damp = active & (mJ < cur - 1e-12 * np.abs(cur))
+            if damp.any():                                   # no ascent: damp the Jacobi step, a = 0.5, 0.25, ...
+                valid[damp] = False; has_prev[damp] = False
+                a = np.where(damp, 0.5, 0.0); searching = damp.copy(); found = np.zeros(F, bool)
+                while searching.any():
+                    am = np.where(searching, a, 0.0)
+                    self._lin(code, False, EA, np.stack([1 - am, am], 1), [E, EJ])
+                    self._lin(code, False, UA, np.stack([1 - am, am], 1), [U, UJ])
+                    mt = merit(EA, UA)
+                    ok = searching & (mt >= cur)
+                    sel = ok.astype(float)[:, None]
+                    self._lin(code, False, ET, np.concatenate([sel, 1 - sel], 1), [EA, ET])
+                    self._lin(code, False, UT, np.concatenate([sel, 1 - sel], 1), [UA, UT])
+                    mJ = np.where(ok, mt, mJ); found |= ok
+                    searching &= ~ok
+                    a = a * 0.5
+                    searching &= a > 1e-8
+                stay = damp & ~found                         # no step found: the iterate stays (psd False: no gradient)
+                st = stay.astype(float)[:, None]
+                self._lin(code, False, ET, np.concatenate([st, 1 - st], 1), [E, ET])
+                self._lin(code, False, UT, np.concatenate([st, 1 - st], 1), [U, UT])
+                mJ = np.where(stay, cur, mJ)
+            act = active.astype(float)[:, None]
+            self._lin(code, False, E, np.concatenate([act, 1 - act], 1), [ET, E])
+            self._lin(code, False, U, np.concatenate([act, 1 - act], 1), [UT, U])
+            rescale(E, U, active)
+            cur = np.where(active, merit(E, U), cur)
+            r = resid(E, U)
+            res = np.where(active, r, res)
+            improved = active & ((res < 0.9 * best_res) | (cur > best_m + 1e-13 * np.abs(best_m)))
+            best_res = np.where(improved, np.minimum(res, best_res), best_res)
+            best_it = np.where(improved, it, best_it); best_m = np.where(improved, np.maximum(cur, best_m), best_m)
+            active &= res >= self.tol
+            sweep += 1
+        self.start_sweeps_ = it
+        return E
+
+    # ---------------------------------------------------------------- fit
+    def fit(self, counts_list, modes_list):
+        self._prepare(counts_list, modes_list)
+        F, code, dev = self.F, self.code, self.device
+        n = self.n
+        er = self._start()
+        # complex start: the real root with the seeded phases exp(i pn N(0,1)) (blml_binned.py:429-436)
+        E = torch.zeros(self.Btot, dtype=self.ct, device=dev)
+        er_fit = er.to(self.rt)
+        call('blml_seg_real_to_complex', code, F, self.segs_t.data_ptr(), self.segs_t.data_ptr(), er_fit.data_ptr(),
+             E.data_ptr(), self.st)
+        z = np.concatenate([np.random.default_rng(self.seed).standard_normal(shape).ravel() for shape in self.shapes])
+        zt = torch.as_tensor(z, dtype=torch.float64).to(dev)
+        call('blml_seg_phases', code, F, self.segs_t.data_ptr(), float(self.phase_noise), zt.data_ptr(), E.data_ptr(),
+             self.st)
+        self._lbfgs(E)
+        return self.results_
+
+    def _lbfgs(self, E):
+        F, code, dev, n, m_ = self.F, self.code, self.device, self.n, self.lbfgs_m
+        U, g, gn, q, Sq, V, SV, tmp = (torch.zeros_like(E) for _ in range(8))
+        Sh = [torch.zeros_like(E) for _ in range(m_)]; Yh = [torch.zeros_like(E) for _ in range(m_)]
+        off = self.boff[:-1]
+        g_EU = _Group(self.pfit, E, off, U, off, True)
+        g_q = _Group(self.pfit, q, off, Sq, off, True)
+        g_V = _Group(self.pfit, V, off, SV, off, True)
+        segs = self.segs_t.data_ptr()
+
+        def Qdot(E_, U_):
+            return self._dots(code, True, [(E_, U_)])[:, 0]
+
+        def grad(Qv):
+            """V = w / F U, S V, g = 2 (S V - n U / Q) for every fit; returns sum w log F per fit."""
+            call('blml_seg_lgrad_weights', code, F, segs, 1, U.data_ptr(), self.w.data_ptr(),
+                 self._dev(np.ones(F)).data_ptr(), V.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+            Lw = self._read(1)[:, 0]
+            g_V(self.st)
+            call('blml_seg_lgrad_finish', code, F, segs, 1, SV.data_ptr(), U.data_ptr(), self.w.data_ptr(),
+                 self._dev(n / Qv).data_ptr(), gn.data_ptr(), self.st)
+            return Lw
+
+        def resid(Qv):
+            call('blml_seg_resid', code, F, segs, 1, E.data_ptr(), U.data_ptr(), self.c.data_ptr(),
+                 self._dev(np.where(Qv > 0, n / np.sqrt(np.maximum(Qv, 1e-300)), 1.0)).data_ptr(),
+                 self.part.data_ptr(), self.out.data_ptr(), self.st)
+            r = self._read(2)
+            return np.where(r[:, 1] > 0, np.nan, r[:, 0])
+
+        g_EU(self.st)
+        Q = Qdot(E, U)
+        sc = np.where(Q > 0, n / np.sqrt(np.maximum(Q, 1e-300)), 1.0)
+        self._lin(code, True, E, sc[:, None], [E]); self._lin(code, True, U, sc[:, None], [U])
+        Q = Q * sc * sc
+        Lw = grad(Q)
+        self._lin(code, True, g, np.ones((F, 1)), [gn])
+        L = Lw - n * np.log(Q)
+        res = resid(Q)
+        stamp = np.full((F, m_), -1, np.int64)             # iteration at which each slot's pair entered (-1: empty)
+        SY = np.zeros((F, m_, m_)); YY = np.zeros((F, m_, m_))
+        it = np.zeros(F, np.int64); active = res >= self.tol
+        reset = np.zeros(F, bool); stop = np.array(['tol'] * F, dtype=object)
+        ftol, fwin = (self.ll_tol if self.ll_tol is not None else 1e-11), 10
+        mhist = [L / n]
+        cap = np.inf if self.max_sweeps is None else self.max_sweeps
+        step = 0
+        while active.any():
+            if len(mhist) > fwin:
+                lt = active & (mhist[-1] - mhist[-1 - fwin] < ftol)
+                stop[lt] = 'll_tol'; active &= ~lt
+            active &= it < cap
+            if not active.any():
+                break
+            it += active
+            # ---- direction (compact L-BFGS over each fit's chronologically ordered pairs)
+            vals = self._dots(code, True, [(s, g) for s in Sh] + [(y, g) for y in Yh] + [(g, g), (E, E)])
+            a_all, b_all = vals[:, :m_], vals[:, m_:2 * m_]; gg, ee = vals[:, 2 * m_], vals[:, 2 * m_ + 1]
+            first = 1e-3 * np.sqrt(ee / np.maximum(gg, 1e-300))
+            coef = np.zeros((F, 1 + 2 * m_)); slope = np.zeros(F)
+            for fi in range(F):
+                if not active[fi]:
+                    continue
+                occ = np.where(stamp[fi] >= 0)[0]
+                if len(occ):
+                    order = occ[np.argsort(stamp[fi, occ])]
+                    R = np.triu(SY[fi][np.ix_(order, order)]); Yy = YY[fi][np.ix_(order, order)]
+                    last = order[-1]
+                    gam = SY[fi, last, last] / YY[fi, last, last]
+                    a_, b_ = a_all[fi, order], b_all[fi, order]
+                    try:
+                        import scipy.linalg as sl
+                        t_ = sl.solve_triangular(R, a_, lower=False)
+                        p_ = sl.solve_triangular(R.T, (np.diag(np.diag(R)) + gam * Yy) @ t_ - gam * b_, lower=True)
+                        coef[fi, 0] = gam; coef[fi, 1 + order] = p_; coef[fi, 1 + m_ + order] = -gam * t_
+                        slope[fi] = gam * gg[fi] + a_ @ p_ - gam * b_ @ t_
+                    except (np.linalg.LinAlgError, ValueError):
+                        slope[fi] = -1.0
+                if not len(occ) or not slope[fi] > 0:
+                    if len(occ):
+                        stamp[fi] = -1
+                    coef[fi] = 0.0; coef[fi, 0] = first[fi]; slope[fi] = first[fi] * gg[fi]
+            self._lin(code, True, q, coef, [g] + Sh + Yh)
+            g_q(self.st)
+            # ---- every fit's Armijo search in one pass
+            call('blml_seg_trials', code, F, segs, 1, E.data_ptr(), q.data_ptr(), U.data_ptr(), Sq.data_ptr(),
+                 self.w.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+            tr = self._read(NT + 3)
+            ts = 0.5 ** np.arange(NT)
+            Qt = Q[:, None] + ts[None, :] * (tr[:, NT] + tr[:, NT + 1])[:, None] + ts[None, :] ** 2 * tr[:, NT + 2][:, None]
+            with np.errstate(invalid='ignore', divide='ignore'):
+                Lt = np.where(Qt > 0, tr[:, :NT] - n[:, None] * np.log(np.where(Qt > 0, Qt, 1.0)), -np.inf)
+            okt = Lt >= L[:, None] + 1e-4 * ts[None, :] * slope[:, None]
+            ok = okt.any(1) & active
+            j = np.argmax(okt, 1)
+            t = np.where(ok, ts[j], 0.0)
+            fail = active & ~ok
+            stall = fail & (reset | (stamp < 0).all(1))
+            stop[stall] = 'stall'; active &= ~stall
+            retry = fail & ~stall
+            stamp[retry] = -1; reset = np.where(retry, True, np.where(ok, False, reset))
+            # ---- the accepted steps: E += t q, then U = S E exactly
+            call('blml_seg_axpy2', code, F, segs, 1, E.data_ptr(), q.data_ptr(), U.data_ptr(), Sq.data_ptr(),
+                 self._dev(t).data_ptr(), self.st)
+            g_EU(self.st)
+            Qn = Qdot(E, U)
+            Lwn = grad(np.where(ok, Qn, Q))
+            Ln = np.where(Qn > 0, Lwn - n * np.log(np.where(Qn > 0, Qn, 1.0)), -np.inf)
+            # ---- the new pair (s, y) = (t q, g - g_new) into slot p of the fits that stepped
+            p = step % m_
+            okf = ok.astype(float)
+            self._lin(code, True, Sh[p], np.stack([t, 1 - okf], 1), [q, Sh[p]])
+            self._lin(code, True, Yh[p], np.stack([okf, -okf, 1 - okf], 1), [g, gn, Yh[p]])
+            vals = self._dots(code, True, [(Sh[p], Yh[p]), (Sh[p], Sh[p]), (Yh[p], Yh[p])] +
+                              [(s, Yh[p]) for s in Sh] + [(y, Yh[p]) for y in Yh])
+            sy, ss, yy = vals[:, 0], vals[:, 1], vals[:, 2]
+            enter = ok & (sy > 1e-12 * np.sqrt(np.maximum(ss * yy, 0.0)))
+            stamp[ok, p] = -1
+            stamp[enter, p] = step
+            full = enter & ((stamp >= 0).sum(1) > m_)
+            SY[enter, :, p] = vals[enter, 3:3 + m_]; SY[enter, p, p] = sy[enter]
+            YY[enter, :, p] = vals[enter, 3 + m_:3 + 2 * m_]; YY[enter, p, :] = YY[enter, :, p]; YY[enter, p, p] = yy[enter]
+            for fi in np.where(full)[0]:                   # more than m pairs: the oldest leaves
+                live = np.where(stamp[fi] >= 0)[0]
+                stamp[fi, live[np.argmin(stamp[fi, live])]] = -1
+            # g = g_new on the fits that stepped
+            self._lin(code, True, g, np.stack([okf, 1 - okf], 1), [gn, g])
+            L = np.where(ok, Ln, L); Q = np.where(ok, Qn, Q)
+            r = resid(Q)
+            res = np.where(ok, r, res)
+            mhist.append(np.where(active, L / n, mhist[-1]))
+            conv = active & (res < self.tol)
+            active &= ~conv
+            step += 1
+            if self.verbose and step % 100 == 0:
+                print(f'  batch lbfgs {step}: active {int(active.sum())}/{F} max rho {np.nanmax(res):.2e}', flush=True)
+        stop[(stop == 'tol') & (res >= self.tol)] = 'max_sweeps'
+        # canonical form per fit (kept unless it loses likelihood), then the outputs
+        Qc = Qdot(E, U)
+        call('blml_seg_lgrad_weights', code, F, segs, 1, U.data_ptr(), self.w.data_ptr(), self._dev(Qc / n).data_ptr(),
+             V.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+        self._read(1)
+        g_V(self.st)                                       # SV = S Ec
+        Qcc = self._dots(code, True, [(V, SV)])[:, 0]
+        call('blml_seg_lgrad_weights', code, F, segs, 1, SV.data_ptr(), self.w.data_ptr(), self._dev(np.ones(F)).data_ptr(),
+             tmp.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+        Lwc = self._read(1)[:, 0]
+        Lc = np.where(Qcc > 0, Lwc - n * np.log(np.where(Qcc > 0, Qcc, 1.0)), -np.inf)
+        keep = (Lc >= L - 1e-9 * n).astype(float)[:, None]
+        self._lin(code, True, E, np.concatenate([keep, 1 - keep], 1), [V, E])
+        self._lin(code, True, U, np.concatenate([keep, 1 - keep], 1), [SV, U])
+        Q = Qdot(E, U)
+        sc = np.where(Q > 0, n / np.sqrt(np.maximum(Q, 1e-300)), 1.0)
+        self._lin(code, True, E, sc[:, None], [E]); self._lin(code, True, U, sc[:, None], [U])
+        res = resid(np.full(F, 1.0) * n * n)
+        dens = torch.empty(self.Btot, dtype=self.rt, device=dev)
+        call('blml_seg_finish', code, F, segs, 1, U.data_ptr(), self.w.data_ptr(), self._dev(1.0 / n ** 2).data_ptr(),
+             dens.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+        ll = self._read(1)[:, 0] / n
+        self.E_t, self.U_t, self.dens_t = E, U, dens
+        conv = (res < self.tol) | (stop == 'll_tol')
+        self.results_ = [FitResult(loglik_=float(ll[f]), n_sweeps_=int(it[f]), stop_reason_=str(stop[f]),
+                                   residual_=float(res[f]), converged_=bool(conv[f]), n_=float(n[f]),
+                                   shape_=self.shapes[f], start_sweeps_=int(self.start_sweeps_[f]), _batch=self, _f=f)
+                         for f in range(F)]
+        return self.results_
+
+    def density(self, f):
+        a, b = self.boff[f], self.boff[f + 1]
+        return self.dens_t[a:b].cpu().numpy().reshape(self.shapes[f])
+
+    def log_density(self, counts_list, eps=0.0):
+        """Per fit: mean over the counts of log(f_b + eps), f = F / Q (blml_binned.py:630-645), one launch for all."""
+        m = torch.as_tensor(np.concatenate([np.asarray(c, float).ravel() for c in counts_list]),
+                            dtype=self.rt).to(self.device)
+        Q = self._dots(self.code, True, [(self.E_t, self.U_t)])[:, 0]
+        call('blml_seg_log_score', self.code, self.F, self.segs_t.data_ptr(), 1, self.U_t.data_ptr(), m.data_ptr(),
+             self._dev(1.0 / Q).data_ptr(), float(eps), self.part.data_ptr(), self.out.data_ptr(), self.st)
+        r = self._read(2)
+        return r[:, 0] / r[:, 1]

@@ -1,0 +1,576 @@
+// Segmented kernels of the batched engine: many independent fits of uneven lattice size advance in lockstep, each
+// phase one launch over all fits. Fit f owns the slice [off_f, off_f + K_f B_f) of every flat mode array (K_f modes of
+// B_f bins, the (K, B) layout of one fit) and [boff_f, boff_f + B_f) of every flat bin array (counts, signs);
+// blockIdx.y is the fit, blockIdx.x strides over its bins. Per-fit scalars (step sizes, scales, linear-combination
+// coefficients) come from device arrays, so a whole phase needs no host round trip. Reductions are per-fit float64
+// block partials summed in a fixed order by blml_seg_finish.
+#include "common.cuh"
+#include "plan.cuh"
+
+namespace blml {
+
+struct SegView { const blml_seg* s; };
+
+template <typename T, bool CPLX>
+struct SAcc {
+  static __device__ __forceinline__ void get(const void* p, int64_t i, double& re, double& im) {
+    if (CPLX) { const cpx<T> v = reinterpret_cast<const cpx<T>*>(p)[i]; re = (double)v.re; im = (double)v.im; }
+    else { re = (double)reinterpret_cast<const T*>(p)[i]; im = 0.0; }
+  }
+  static __device__ __forceinline__ void put(void* p, int64_t i, double re, double im) {
+    if (CPLX) reinterpret_cast<cpx<T>*>(p)[i] = cpx<T>{(T)re, (T)im};
+    else reinterpret_cast<T*>(p)[i] = (T)re;
+  }
+};
+
+#define SEG_LOOP(b, sg) for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < (sg).B; \
+                             b += (int64_t)gridDim.x * blockDim.x)
+
+// partials layout: part[((f * NQ) + q) * gridDim.x + blockIdx.x]
+template <int NQ>
+__device__ __forceinline__ void seg_partials(double (&v)[NQ], double* part, unsigned maxmask = 0u) {
+  __shared__ double sh[NQ][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    double x = ((maxmask >> q) & 1u) ? warp_max(v[q]) : warp_sum(v[q]);
+    if (lane == 0) sh[q][wid] = x;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      const bool mx = (maxmask >> q) & 1u;
+      double x = lane < nw ? sh[q][lane] : (mx ? -INFINITY : 0.0);
+      x = mx ? warp_max(x) : warp_sum(x);
+      if (lane == 0) part[((int64_t)blockIdx.y * NQ + q) * gridDim.x + blockIdx.x] = x;
+    }
+  }
+}
+
+// one block per (fit, quantity): out[f * nq + q] = fixed-order reduction of its partials
+__global__ void k_seg_finish(const double* part, int nq, int nblk, unsigned maxmask, double* out) {
+  const int f = blockIdx.x;
+  for (int q = 0; q < nq; q++) {
+    const bool mx = (maxmask >> q) & 1u;
+    double acc = mx ? -INFINITY : 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
+      const double v = part[((int64_t)f * nq + q) * nblk + i];
+      acc = mx ? fmax(acc, v) : acc + v;
+    }
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double x = mx ? warp_max(acc) : warp_sum(acc);
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      x = lane < nw ? sh[lane] : (mx ? -INFINITY : 0.0);
+      x = mx ? warp_max(x) : warp_sum(x);
+      if (lane == 0) out[(int64_t)f * nq + q] = x;
+    }
+    __syncthreads();
+  }
+}
+
+// the same with the results of fit f at out[f * stride + q] (several passes fill one fit-major table)
+__global__ void k_seg_finish_strided(const double* part, int nq, int nblk, double* out, int stride) {
+  const int f = blockIdx.x;
+  for (int q = 0; q < nq; q++) {
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += part[((int64_t)f * nq + q) * nblk + i];
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double x = warp_sum(acc);
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      x = lane < nw ? sh[lane] : 0.0;
+      x = warp_sum(x);
+      if (lane == 0) out[(int64_t)f * stride + q] = x;
+    }
+    __syncthreads();
+  }
+}
+
+constexpr int SEG_BLOCKS = 16;        // blocks per fit (x); 64 fits x 16 blocks x 256 threads covers a B200 ~2 times
+
+template <typename T>
+__global__ void k_seg_start_root(const blml_seg* segs, const T* c, const T* sg, const double* s0, T* e0) {
+  const blml_seg S = segs[blockIdx.y];
+  SEG_LOOP(b, S) {
+    const double cb = (double)c[S.boff + b];
+    e0[S.off + b] = (T)(cb > 0 ? sqrt(cb / s0[blockIdx.y]) * (double)sg[S.boff + b] : 0.0);
+  }
+}
+
+__device__ __forceinline__ double cd_root_s(double b, double c, double s) {
+  const double disc = sqrt(b * b + 4.0 * s * c);
+  return b >= 0 ? 2.0 * c / fmax(b + disc, 1e-300) : (-b + disc) / (2.0 * s);
+}
+
+template <typename T>
+__global__ void k_seg_update_real1(const blml_seg* segs, const T* E, const T* U, const T* c, const T* sg,
+                                   const double* s0, T* out) {
+  const blml_seg S = segs[blockIdx.y];
+  const double s = s0[blockIdx.y];
+  SEG_LOOP(b, S) {
+    const double cb = (double)c[S.boff + b], sgb = (double)sg[S.boff + b];
+    double t = 0.0;
+    if (cb > 0) t = cd_root_s(sgb * ((double)U[S.off + b] - s * (double)E[S.off + b]), cb, s);
+    out[S.off + b] = (T)(sgb * t);
+  }
+}
+
+// merit terms per fit: psd [sum c log max(F, 1e-30), Q, 0]; real rank 1 [sum e u, sum_occ c log|e|, #(sg e <= 0)]
+template <typename T, bool CPLX>
+__global__ void k_seg_merit(const blml_seg* segs, int psd, const void* E, const void* U, const T* c, const T* sg,
+                            double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  double v[3] = {0.0, 0.0, 0.0};
+  SEG_LOOP(b, S) {
+    const double cb = (double)c[S.boff + b];
+    if (psd) {
+      double F = 0.0, Q = 0.0;
+      for (int k = 0; k < S.K; k++) {
+        double er, ei, ur, ui;
+        const int64_t i = S.off + (int64_t)k * S.B + b;
+        SAcc<T, CPLX>::get(E, i, er, ei); SAcc<T, CPLX>::get(U, i, ur, ui);
+        F += ur * ur + ui * ui; Q += er * ur + ei * ui;
+      }
+      if (cb != 0.0) v[0] += cb * log(fmax(F, 1e-30));
+      v[1] += Q;
+    } else {
+      double e, im, u;
+      SAcc<T, CPLX>::get(E, S.off + b, e, im); SAcc<T, CPLX>::get(U, S.off + b, u, im);
+      v[0] += e * u;
+      if (cb > 0) { v[1] += cb * log(fabs(e)); if ((double)sg[S.boff + b] * e <= 0) v[2] += 1.0; }
+    }
+  }
+  seg_partials<3>(v, part);
+}
+
+template <typename T, bool CPLX>
+__global__ void k_seg_resid(const blml_seg* segs, const void* E, const void* U, const T* c, const double* scale,
+                            double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const double sc = scale[blockIdx.y];
+  double v[2] = {0.0, 0.0};
+  SEG_LOOP(b, S) {
+    const double cb = (double)c[S.boff + b];
+    if (!(cb > 0)) continue;
+    double nrm2 = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      double er, ei; SAcc<T, CPLX>::get(E, S.off + (int64_t)k * S.B + b, er, ei);
+      er *= sc; ei *= sc; nrm2 += er * er + ei * ei;
+    }
+    const double f = nrm2 / cb;
+    double r2 = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      double er, ei, ur, ui;
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      SAcc<T, CPLX>::get(E, i, er, ei); SAcc<T, CPLX>::get(U, i, ur, ui);
+      const double dr = ur * sc * f - er * sc, di = ui * sc * f - ei * sc;
+      r2 += dr * dr + di * di;
+    }
+    const double r = sqrt(r2) / sqrt(fmax(nrm2, 1e-300));
+    if (r != r) v[1] += 1.0; else v[0] = fmax(v[0], r);
+  }
+  seg_partials<2>(v, part, 1u);
+}
+
+struct SegPairs { const void* a[16]; const void* b[16]; };
+
+// per-fit real inner products over the fit's K B elements (complex: 2 K B reals)
+template <typename T, int NP>
+__global__ void k_seg_dots(const blml_seg* segs, int cplx, int np, SegPairs pp, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const int64_t w = cplx ? 2 : 1;
+  const int64_t o = S.off * w, n = (int64_t)S.K * S.B * w;
+  double v[NP];
+#pragma unroll
+  for (int q = 0; q < NP; q++) v[q] = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NP; q++)
+      if (q < np) v[q] += (double)reinterpret_cast<const T*>(pp.a[q])[o + i] *
+                          (double)reinterpret_cast<const T*>(pp.b[q])[o + i];
+  }
+  seg_partials<NP>(v, part);
+}
+
+struct SegTerms { const void* v[48]; };
+
+// out = sum_i coef[f * nt + i] v_i over each fit's slice
+template <typename T>
+__global__ void k_seg_lincomb(const blml_seg* segs, int cplx, T* out, int nt, const double* coef, SegTerms t) {
+  const blml_seg S = segs[blockIdx.y];
+  const int64_t w = cplx ? 2 : 1;
+  const int64_t o = S.off * w, n = (int64_t)S.K * S.B * w;
+  const double* cf = coef + (int64_t)blockIdx.y * nt;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int q = 0; q < nt; q++) {
+      const double c = cf[q];
+      if (c != 0.0) acc += c * (double)reinterpret_cast<const T*>(t.v[q])[o + i];
+    }
+    out[o + i] = (T)acc;
+  }
+}
+
+template <typename T, bool CPLX>
+__global__ void k_seg_lgrad_weights(const blml_seg* segs, const void* U, const T* w, const double* vs, void* V,
+                                    double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const double vsc = vs[blockIdx.y];
+  double v[1] = {0.0};
+  SEG_LOOP(b, S) {
+    double F = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      double ur, ui; SAcc<T, CPLX>::get(U, S.off + (int64_t)k * S.B + b, ur, ui); F += ur * ur + ui * ui;
+    }
+    const double wb = (double)w[S.boff + b];
+    const bool occ = wb > 0;
+    if (occ) v[0] += wb * log(F);
+    const double f = occ ? vsc * wb / F : 0.0;
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double ur, ui; SAcc<T, CPLX>::get(U, i, ur, ui);
+      SAcc<T, CPLX>::put(V, i, occ ? ur * f : 0.0, occ ? ui * f : 0.0);
+    }
+  }
+  seg_partials<1>(v, part);
+}
+
+template <typename T, bool CPLX>
+__global__ void k_seg_lgrad_finish(const blml_seg* segs, const void* SV, const void* U, const T* w, const double* nq,
+                                   void* g) {
+  const blml_seg S = segs[blockIdx.y];
+  const double q = nq[blockIdx.y];
+  SEG_LOOP(b, S) {
+    const bool occ = (double)w[S.boff + b] > 0;
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double sr, si, ur, ui;
+      SAcc<T, CPLX>::get(SV, i, sr, si); SAcc<T, CPLX>::get(U, i, ur, ui);
+      SAcc<T, CPLX>::put(g, i, occ ? 2.0 * (sr - q * ur) : 0.0, occ ? 2.0 * (si - q * ui) : 0.0);
+    }
+  }
+}
+
+// the Armijo search of every fit in one pass: for t_j = 2^-j, j < NT, sum_occ w log F(U + t_j S q); and the three
+// inner products <q, U>, <E, S q>, <q, S q> from which Q(t) = Q + t (<q, U> + <E, S q>) + t^2 <q, S q>
+constexpr int NT = 40;
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(256) k_seg_trials(const blml_seg* segs, const void* E, const void* q, const void* U,
+                                                    const void* Sq, const T* w, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  double v[NT + 3];
+#pragma unroll
+  for (int j = 0; j < NT + 3; j++) v[j] = 0.0;
+  SEG_LOOP(b, S) {
+    const double wb = (double)w[S.boff + b];
+    double a = 0.0, bb = 0.0, cc = 0.0;        // F(t) = a + 2 t b + t^2 c
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double er, ei, qr, qi, ur, ui, sr, si;
+      SAcc<T, CPLX>::get(E, i, er, ei); SAcc<T, CPLX>::get(q, i, qr, qi);
+      SAcc<T, CPLX>::get(U, i, ur, ui); SAcc<T, CPLX>::get(Sq, i, sr, si);
+      a += ur * ur + ui * ui; bb += ur * sr + ui * si; cc += sr * sr + si * si;
+      v[NT] += qr * ur + qi * ui; v[NT + 1] += er * sr + ei * si; v[NT + 2] += qr * sr + qi * si;
+    }
+    if (wb > 0) {
+      double t = 1.0;
+#pragma unroll
+      for (int j = 0; j < NT; j++) { v[j] += wb * log(a + t * (2.0 * bb + t * cc)); t *= 0.5; }
+    }
+  }
+  seg_partials<NT + 3>(v, part);
+}
+
+// the accepted step of every fit: E += t_f q, U += t_f S q (t_f = 0 leaves a fit unchanged)
+template <typename T, bool CPLX>
+__global__ void k_seg_axpy2(const blml_seg* segs, void* E, const void* q, void* U, const void* Sq, const double* t) {
+  const blml_seg S = segs[blockIdx.y];
+  const double tf = t[blockIdx.y];
+  if (tf == 0.0) return;
+  SEG_LOOP(b, S) {
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double er, ei, qr, qi, ur, ui, sr, si;
+      SAcc<T, CPLX>::get(E, i, er, ei); SAcc<T, CPLX>::get(q, i, qr, qi);
+      SAcc<T, CPLX>::get(U, i, ur, ui); SAcc<T, CPLX>::get(Sq, i, sr, si);
+      SAcc<T, CPLX>::put(E, i, er + tf * qr, ei + tf * qi); SAcc<T, CPLX>::put(U, i, ur + tf * sr, ui + tf * si);
+    }
+  }
+}
+
+template <typename T, bool CPLX>
+__global__ void k_seg_finish_fit(const blml_seg* segs, const void* U, const T* w, const double* inv_n2, T* dens,
+                                 double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const double s = inv_n2[blockIdx.y];
+  double v[1] = {0.0};
+  SEG_LOOP(b, S) {
+    double F = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      double ur, ui; SAcc<T, CPLX>::get(U, S.off + (int64_t)k * S.B + b, ur, ui); F += ur * ur + ui * ui;
+    }
+    const T dv = (T)(F * s);
+    dens[S.boff + b] = dv;
+    const double wb = (double)w[S.boff + b];
+    if (wb > 0) v[0] += wb * log((double)dv);
+  }
+  seg_partials<1>(v, part);
+}
+
+// held-out score per fit: [sum_{m > 0} m log max(F inv_z + eps, 1e-300), sum m]
+template <typename T, bool CPLX>
+__global__ void k_seg_log_score(const blml_seg* segs, const void* U, const T* m, const double* inv_z, double eps,
+                                double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const double iz = inv_z[blockIdx.y];
+  double v[2] = {0.0, 0.0};
+  SEG_LOOP(b, S) {
+    const double mb = (double)m[S.boff + b];
+    if (!(mb > 0)) continue;
+    double F = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      double ur, ui; SAcc<T, CPLX>::get(U, S.off + (int64_t)k * S.B + b, ur, ui); F += ur * ur + ui * ui;
+    }
+    v[0] += mb * log(fmax(F * iz + eps, 1e-300)); v[1] += mb;
+  }
+  seg_partials<2>(v, part);
+}
+
+// start noise of every fit (the phases of mode 0; complex fits of one mode): E[0] *= exp(i pn z), z per fit at boff
+template <typename T>
+__global__ void k_seg_phases(const blml_seg* segs, double pn, const double* z, void* E) {
+  const blml_seg S = segs[blockIdx.y];
+  SEG_LOOP(b, S) {
+    double er, ei; SAcc<T, true>::get(E, S.off + b, er, ei);
+    double sn, cs; sincos(pn * z[S.boff + b], &sn, &cs);
+    SAcc<T, true>::put(E, S.off + b, er * cs - ei * sn, er * sn + ei * cs);
+  }
+}
+
+template <typename T>
+__global__ void k_seg_real_to_complex(const blml_seg* real_segs, const blml_seg* cplx_segs, const T* er, void* E) {
+  const blml_seg S = real_segs[blockIdx.y], C = cplx_segs[blockIdx.y];
+  SEG_LOOP(b, S) SAcc<T, true>::put(E, C.off + b, (double)er[S.off + b], 0.0);
+}
+
+static int seg_finish(const double* part, int F, int nq, unsigned maxmask, double* out, cudaStream_t st) {
+  k_seg_finish<<<F, 256, 0, st>>>(part, nq, SEG_BLOCKS, maxmask, out);
+  BLML_CHECK_LAUNCH("seg finish");
+  return BLML_OK;
+}
+
+template <typename T>
+static void seg_dots_launch(dim3 g, const blml_seg* s, int cplx, int np, const SegPairs& pp, double* part,
+                            cudaStream_t st) {
+  if (np <= 1) k_seg_dots<T, 1><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else if (np <= 2) k_seg_dots<T, 2><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else if (np <= 4) k_seg_dots<T, 4><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else if (np <= 8) k_seg_dots<T, 8><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else k_seg_dots<T, 16><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+}
+
+}  // namespace blml
+
+using namespace blml;
+#define SST reinterpret_cast<cudaStream_t>(stream)
+#define SGRID(F) dim3(SEG_BLOCKS, (unsigned)(F))
+#define TYPED(dtype, cplx, K, ...)                                          \
+  do {                                                                      \
+    if (dtype == BLML_F64) { if (cplx) K<double, true>__VA_ARGS__; else K<double, false>__VA_ARGS__; } \
+    else { if (cplx) K<float, true>__VA_ARGS__; else K<float, false>__VA_ARGS__; }                   \
+  } while (0)
+
+static int seg_args(int dtype, int F, const blml_seg* segs, const char* who) {
+  if ((dtype != BLML_F64 && dtype != BLML_F32) || F < 1 || F > 65535 || !segs) {
+    set_error("%s: dtype, 1 <= F <= 65535 fits and a segment table", who); return BLML_ERR_ARG;
+  }
+  return BLML_OK;
+}
+
+extern "C" {
+
+int blml_seg_blocks(void) { return SEG_BLOCKS; }
+
+int blml_seg_start_root(int dtype, int F, const blml_seg* segs, const void* c, const void* sg, const double* s0,
+                        void* e0, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_start_root")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) k_seg_start_root<double><<<SGRID(F), 256, 0, SST>>>(segs, (const double*)c, (const double*)sg, s0, (double*)e0);
+  else k_seg_start_root<float><<<SGRID(F), 256, 0, SST>>>(segs, (const float*)c, (const float*)sg, s0, (float*)e0);
+  BLML_CHECK_LAUNCH("blml_seg_start_root");
+  return BLML_OK;
+}
+
+int blml_seg_update_real1(int dtype, int F, const blml_seg* segs, const void* E, const void* U, const void* c,
+                          const void* sg, const double* s0, void* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_update_real1")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64)
+    k_seg_update_real1<double><<<SGRID(F), 256, 0, SST>>>(segs, (const double*)E, (const double*)U, (const double*)c,
+                                                          (const double*)sg, s0, (double*)out);
+  else
+    k_seg_update_real1<float><<<SGRID(F), 256, 0, SST>>>(segs, (const float*)E, (const float*)U, (const float*)c,
+                                                         (const float*)sg, s0, (float*)out);
+  BLML_CHECK_LAUNCH("blml_seg_update_real1");
+  return BLML_OK;
+}
+
+int blml_seg_merit(int dtype, int F, const blml_seg* segs, int cplx, int psd, const void* E, const void* U,
+                   const void* c, const void* sg, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_merit")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_merit<double, true><<<SGRID(F), 256, 0, SST>>>(segs, psd, E, U, (const double*)c, (const double*)sg, part);
+    else k_seg_merit<double, false><<<SGRID(F), 256, 0, SST>>>(segs, psd, E, U, (const double*)c, (const double*)sg, part);
+  } else {
+    if (cplx) k_seg_merit<float, true><<<SGRID(F), 256, 0, SST>>>(segs, psd, E, U, (const float*)c, (const float*)sg, part);
+    else k_seg_merit<float, false><<<SGRID(F), 256, 0, SST>>>(segs, psd, E, U, (const float*)c, (const float*)sg, part);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_merit");
+  return seg_finish(part, F, 3, 0u, out, SST);
+}
+
+int blml_seg_resid(int dtype, int F, const blml_seg* segs, int cplx, const void* E, const void* U, const void* c,
+                   const double* scale, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_resid")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_resid<double, true><<<SGRID(F), 256, 0, SST>>>(segs, E, U, (const double*)c, scale, part);
+    else k_seg_resid<double, false><<<SGRID(F), 256, 0, SST>>>(segs, E, U, (const double*)c, scale, part);
+  } else {
+    if (cplx) k_seg_resid<float, true><<<SGRID(F), 256, 0, SST>>>(segs, E, U, (const float*)c, scale, part);
+    else k_seg_resid<float, false><<<SGRID(F), 256, 0, SST>>>(segs, E, U, (const float*)c, scale, part);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_resid");
+  return seg_finish(part, F, 2, 1u, out, SST);
+}
+
+int blml_seg_dots(int dtype, int F, const blml_seg* segs, int cplx, int npairs, const void* const* a,
+                  const void* const* b, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_dots")) return BLML_ERR_ARG;
+  if (npairs < 1 || npairs > 48) { set_error("blml_seg_dots: 1..48 pairs"); return BLML_ERR_ARG; }
+  // 16 accumulators per pass; the passes write fit-major slices out[f * npairs + q0 ...] via a strided finish
+  for (int q0 = 0; q0 < npairs; q0 += 16) {
+    const int np = std::min(16, npairs - q0);
+    SegPairs pp;
+    for (int q = 0; q < 16; q++) { pp.a[q] = q < np ? a[q0 + q] : nullptr; pp.b[q] = q < np ? b[q0 + q] : nullptr; }
+    double* pt = part + (size_t)q0 * F * SEG_BLOCKS;
+    if (dtype == BLML_F64) seg_dots_launch<double>(SGRID(F), segs, cplx, np, pp, pt, SST);
+    else seg_dots_launch<float>(SGRID(F), segs, cplx, np, pp, pt, SST);
+    BLML_CHECK_LAUNCH("blml_seg_dots");
+    k_seg_finish_strided<<<F, 256, 0, SST>>>(pt, np, SEG_BLOCKS, out + q0, npairs);
+    BLML_CHECK_LAUNCH("blml_seg_dots finish");
+  }
+  return BLML_OK;
+}
+
+int blml_seg_lincomb(int dtype, int F, const blml_seg* segs, int cplx, void* out, int nterms, const double* coef,
+                     const void* const* v, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_lincomb")) return BLML_ERR_ARG;
+  if (nterms < 1 || nterms > 48) { set_error("blml_seg_lincomb: 1..48 terms"); return BLML_ERR_ARG; }
+  SegTerms t;
+  for (int q = 0; q < 48; q++) t.v[q] = q < nterms ? v[q] : nullptr;
+  if (dtype == BLML_F64) k_seg_lincomb<double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (double*)out, nterms, coef, t);
+  else k_seg_lincomb<float><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (float*)out, nterms, coef, t);
+  BLML_CHECK_LAUNCH("blml_seg_lincomb");
+  return BLML_OK;
+}
+
+int blml_seg_lgrad_weights(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* w,
+                           const double* vscale, void* V, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_lgrad_weights")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_lgrad_weights<double, true><<<SGRID(F), 256, 0, SST>>>(segs, U, (const double*)w, vscale, V, part);
+    else k_seg_lgrad_weights<double, false><<<SGRID(F), 256, 0, SST>>>(segs, U, (const double*)w, vscale, V, part);
+  } else {
+    if (cplx) k_seg_lgrad_weights<float, true><<<SGRID(F), 256, 0, SST>>>(segs, U, (const float*)w, vscale, V, part);
+    else k_seg_lgrad_weights<float, false><<<SGRID(F), 256, 0, SST>>>(segs, U, (const float*)w, vscale, V, part);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_lgrad_weights");
+  return seg_finish(part, F, 1, 0u, out, SST);
+}
+
+int blml_seg_lgrad_finish(int dtype, int F, const blml_seg* segs, int cplx, const void* SV, const void* U,
+                          const void* w, const double* nq, void* g, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_lgrad_finish")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_lgrad_finish<double, true><<<SGRID(F), 256, 0, SST>>>(segs, SV, U, (const double*)w, nq, g);
+    else k_seg_lgrad_finish<double, false><<<SGRID(F), 256, 0, SST>>>(segs, SV, U, (const double*)w, nq, g);
+  } else {
+    if (cplx) k_seg_lgrad_finish<float, true><<<SGRID(F), 256, 0, SST>>>(segs, SV, U, (const float*)w, nq, g);
+    else k_seg_lgrad_finish<float, false><<<SGRID(F), 256, 0, SST>>>(segs, SV, U, (const float*)w, nq, g);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_lgrad_finish");
+  return BLML_OK;
+}
+
+int blml_seg_trials(int dtype, int F, const blml_seg* segs, int cplx, const void* E, const void* q, const void* U,
+                    const void* Sq, const void* w, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_trials")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_trials<double, true><<<SGRID(F), 256, 0, SST>>>(segs, E, q, U, Sq, (const double*)w, part);
+    else k_seg_trials<double, false><<<SGRID(F), 256, 0, SST>>>(segs, E, q, U, Sq, (const double*)w, part);
+  } else {
+    if (cplx) k_seg_trials<float, true><<<SGRID(F), 256, 0, SST>>>(segs, E, q, U, Sq, (const float*)w, part);
+    else k_seg_trials<float, false><<<SGRID(F), 256, 0, SST>>>(segs, E, q, U, Sq, (const float*)w, part);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_trials");
+  return seg_finish(part, F, NT + 3, 0u, out, SST);
+}
+
+int blml_seg_axpy2(int dtype, int F, const blml_seg* segs, int cplx, void* E, const void* q, void* U, const void* Sq,
+                   const double* t, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_axpy2")) return BLML_ERR_ARG;
+  TYPED(dtype, cplx, k_seg_axpy2, <<<SGRID(F), 256, 0, SST>>>(segs, E, q, U, Sq, t));
+  BLML_CHECK_LAUNCH("blml_seg_axpy2");
+  return BLML_OK;
+}
+
+int blml_seg_finish(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* w,
+                    const double* inv_n2, void* density, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_finish")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_finish_fit<double, true><<<SGRID(F), 256, 0, SST>>>(segs, U, (const double*)w, inv_n2, (double*)density, part);
+    else k_seg_finish_fit<double, false><<<SGRID(F), 256, 0, SST>>>(segs, U, (const double*)w, inv_n2, (double*)density, part);
+  } else {
+    if (cplx) k_seg_finish_fit<float, true><<<SGRID(F), 256, 0, SST>>>(segs, U, (const float*)w, inv_n2, (float*)density, part);
+    else k_seg_finish_fit<float, false><<<SGRID(F), 256, 0, SST>>>(segs, U, (const float*)w, inv_n2, (float*)density, part);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_finish");
+  return seg_finish(part, F, 1, 0u, out, SST);
+}
+
+int blml_seg_log_score(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* m,
+                       const double* inv_z, double eps, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_log_score")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) {
+    if (cplx) k_seg_log_score<double, true><<<SGRID(F), 256, 0, SST>>>(segs, U, (const double*)m, inv_z, eps, part);
+    else k_seg_log_score<double, false><<<SGRID(F), 256, 0, SST>>>(segs, U, (const double*)m, inv_z, eps, part);
+  } else {
+    if (cplx) k_seg_log_score<float, true><<<SGRID(F), 256, 0, SST>>>(segs, U, (const float*)m, inv_z, eps, part);
+    else k_seg_log_score<float, false><<<SGRID(F), 256, 0, SST>>>(segs, U, (const float*)m, inv_z, eps, part);
+  }
+  BLML_CHECK_LAUNCH("blml_seg_log_score");
+  return seg_finish(part, F, 2, 0u, out, SST);
+}
+
+int blml_seg_phases(int dtype, int F, const blml_seg* segs, double pn, const double* z, void* E, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_phases")) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) k_seg_phases<double><<<SGRID(F), 256, 0, SST>>>(segs, pn, z, E);
+  else k_seg_phases<float><<<SGRID(F), 256, 0, SST>>>(segs, pn, z, E);
+  BLML_CHECK_LAUNCH("blml_seg_phases");
+  return BLML_OK;
+}
+
+int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const blml_seg* cplx_segs, const void* er,
+                             void* E, void* stream) {
+  if (seg_args(dtype, F, real_segs, "blml_seg_real_to_complex") || !cplx_segs) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) k_seg_real_to_complex<double><<<SGRID(F), 256, 0, SST>>>(real_segs, cplx_segs, (const double*)er, E);
+  else k_seg_real_to_complex<float><<<SGRID(F), 256, 0, SST>>>(real_segs, cplx_segs, (const float*)er, E);
+  BLML_CHECK_LAUNCH("blml_seg_real_to_complex");
+  return BLML_OK;
+}
+
+}

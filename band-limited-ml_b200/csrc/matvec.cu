@@ -86,12 +86,70 @@ __global__ void __launch_bounds__(256) k_contract(const void* __restrict__ X_, c
   }
 }
 
+// The same stage for small problems (one lattice of a few hundred bins per axis), where 64 x 64 tiles leave most
+// SMs idle: 16 x 16 output tiles, one output per thread, K staged 32 deep. grid (ceil(R / 16), ceil(N / 16), nb).
+constexpr int SR = 16, SN = 16, SK = 32;
+template <typename T, bool XREAL, bool WEIGHT, bool YREAL>
+__global__ void __launch_bounds__(256) k_contract_small(const void* __restrict__ X_, const cpx<T>* __restrict__ Tw,
+                                                        const T* __restrict__ W, void* __restrict__ Y_, int64_t R,
+                                                        int M, int N) {
+  __shared__ cpx<T> Xs[SK][SR + 1];
+  __shared__ cpx<T> Ts[SK][SN + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int64_t r0 = (int64_t)blockIdx.x * SR;
+  const int n0 = blockIdx.y * SN;
+  const int64_t b = blockIdx.z;
+  const int64_t xoff = b * R * (int64_t)M;
+  cpx<T> acc = {T(0), T(0)};
+  for (int m0 = 0; m0 < M; m0 += SK) {
+#pragma unroll
+    for (int i = 0; i < 2; i++) {              // X tile: SR rows x SK (m), thread loads m = tid % 32, r = tid / 32 + 8 i
+      const int mm = tid & 31, rr = (tid >> 5) + 8 * i;
+      const int64_t r = r0 + rr; const int m = m0 + mm;
+      cpx<T> v = {T(0), T(0)};
+      if (r < R && m < M) {
+        if (XREAL) v.re = reinterpret_cast<const T*>(X_)[xoff + r * M + m];
+        else v = reinterpret_cast<const cpx<T>*>(X_)[xoff + r * M + m];
+      }
+      Xs[mm][rr] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {              // T tile: SK (m) x SN (n), thread loads n = tid % 16, m = tid / 16 + 16 i
+      const int nn = tid & 15, mm = (tid >> 4) + 16 * i;
+      const int n = n0 + nn, m = m0 + mm;
+      Ts[mm][nn] = (n < N && m < M) ? Tw[(int64_t)m * N + n] : cpx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int kk = 0; kk < SK; kk++) acc = cfma(Xs[kk][tx], Ts[kk][ty], acc);
+    __syncthreads();
+  }
+  const int n = n0 + ty;
+  const int64_t r = r0 + tx;
+  if (n < N && r < R) {
+    const int64_t o = b * (int64_t)N * R + (int64_t)n * R + r;
+    if (WEIGHT) { const T wv = W[(int64_t)n * R + r]; acc.re *= wv; acc.im *= wv; }
+    if (YREAL) reinterpret_cast<T*>(Y_)[o] = acc.re;
+    else reinterpret_cast<cpx<T>*>(Y_)[o] = acc;
+  }
+}
+
 template <typename T>
 static int launch_stage(const void* X, bool xreal, const void* Tw, const void* W, void* Y, bool yreal, int64_t R,
                         int M, int N, int nb, cudaStream_t st) {
   dim3 grid((unsigned)((R + TR - 1) / TR), (unsigned)((N + TN - 1) / TN), (unsigned)nb);
   const cpx<T>* t = reinterpret_cast<const cpx<T>*>(Tw);
   const T* w = reinterpret_cast<const T*>(W);
+  if ((int64_t)grid.x * grid.y * grid.z < 2 * 148) {     // too few big tiles to fill the GPU: small tiles
+    dim3 gs((unsigned)((R + SR - 1) / SR), (unsigned)((N + SN - 1) / SN), (unsigned)nb);
+    if (xreal && W) k_contract_small<T, true, true, false><<<gs, 256, 0, st>>>(X, t, w, Y, R, M, N);
+    else if (xreal) k_contract_small<T, true, false, false><<<gs, 256, 0, st>>>(X, t, w, Y, R, M, N);
+    else if (W) k_contract_small<T, false, true, false><<<gs, 256, 0, st>>>(X, t, w, Y, R, M, N);
+    else if (yreal) k_contract_small<T, false, false, true><<<gs, 256, 0, st>>>(X, t, w, Y, R, M, N);
+    else k_contract_small<T, false, false, false><<<gs, 256, 0, st>>>(X, t, w, Y, R, M, N);
+    BLML_CHECK_LAUNCH("matvec stage");
+    return BLML_OK;
+  }
   // the combinations the stage schedule uses: first stage (real or complex input), last forward (weights),
   // last inverse (real output when the input was real), and plain complex stages
   if (xreal && W) k_contract<T, true, true, false><<<grid, 256, 0, st>>>(X, t, w, Y, R, M, N);
@@ -129,7 +187,80 @@ static int simt_matvec(blml_plan_s* p, const void* x, void* y, int nb, int xc, v
   return BLML_OK;
 }
 
+// ---------------------------------------------------------------------------------------------- grouped stages
+// One stage of many mat-vecs (different plans, lattice sizes and buffers) in one launch: problem g = blockIdx.z reads
+// its descriptor; rows rho = b R + r of its nb lattices; 32 x 32 output tiles, 2 x 2 outputs per thread.
+struct StageDesc {
+  const void* X; const void* T; const void* W; void* Y;
+  int64_t R; int M, N, nb, flags;      // flags: 1 real input, 2 weight epilogue, 4 real output
+};
+constexpr int GR = 32, GN = 32, GK = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_contract_grouped(const StageDesc* __restrict__ descs) {
+  __shared__ cpx<T> Xs[GK][GR + 1];
+  __shared__ cpx<T> Ts[GK][GN + 1];
+  const StageDesc D = descs[blockIdx.z];
+  const int64_t rows = D.R * D.nb;
+  const int64_t r0 = (int64_t)blockIdx.x * GR;
+  const int n0 = blockIdx.y * GN;
+  if (r0 >= rows || n0 >= D.N) return;                 // uniform per CTA: past this problem's tiles
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const bool xreal = D.flags & 1;
+  const cpx<T>* Tw = reinterpret_cast<const cpx<T>*>(D.T);
+  const int M = D.M, N = D.N;
+  cpx<T> acc[2][2] = {{{T(0), T(0)}, {T(0), T(0)}}, {{T(0), T(0)}, {T(0), T(0)}}};
+  for (int m0 = 0; m0 < M; m0 += GK) {
+#pragma unroll
+    for (int i = 0; i < 2; i++) {              // X tile GR x GK: m = tid % 16, row = tid / 16 + 16 i
+      const int mm = tid & 15, rr = (tid >> 4) + 16 * i;
+      const int64_t rho = r0 + rr; const int m = m0 + mm;
+      cpx<T> v = {T(0), T(0)};
+      if (rho < rows && m < M) {               // rows of all nb lattices are contiguous, M apart
+        if (xreal) v.re = reinterpret_cast<const T*>(D.X)[rho * M + m];
+        else v = reinterpret_cast<const cpx<T>*>(D.X)[rho * M + m];
+      }
+      Xs[mm][rr] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++) {              // T tile GK x GN: n = tid % 32, m = tid / 32 + 8 i
+      const int nn = tid & 31, mm = (tid >> 5) + 8 * i;
+      const int n = n0 + nn, m = m0 + mm;
+      Ts[mm][nn] = (n < N && m < M) ? Tw[(int64_t)m * N + n] : cpx<T>{T(0), T(0)};
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GK; kk++) {
+      const cpx<T> a0 = Xs[kk][tx], a1 = Xs[kk][tx + 16], b0 = Ts[kk][ty], b1 = Ts[kk][ty + 16];
+      acc[0][0] = cfma(a0, b0, acc[0][0]); acc[0][1] = cfma(a0, b1, acc[0][1]);
+      acc[1][0] = cfma(a1, b0, acc[1][0]); acc[1][1] = cfma(a1, b1, acc[1][1]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const int64_t rho = r0 + tx + 16 * i; const int n = n0 + ty + 16 * j;
+      if (rho >= rows || n >= N) continue;
+      const int64_t b = rho / D.R, r = rho - b * D.R;
+      const int64_t o = b * (int64_t)N * D.R + (int64_t)n * D.R + r;
+      cpx<T> v = acc[i][j];
+      if (D.flags & 2) { const T wv = reinterpret_cast<const T*>(D.W)[(int64_t)n * D.R + r]; v.re *= wv; v.im *= wv; }
+      if (D.flags & 4) reinterpret_cast<T*>(D.Y)[o] = v.re;
+      else reinterpret_cast<cpx<T>*>(D.Y)[o] = v;
+    }
+}
+
 }  // namespace blml
+
+// a set of mat-vecs applied together: per stage a device array of descriptors and the grid that covers them
+struct blml_group_s {
+  int G, d_max, dtype, nstages;
+  std::vector<blml::StageDesc*> dev;    // one descriptor array per stage index
+  std::vector<dim3> grids;
+  void* ws;                             // the group's own intermediate buffers
+};
 
 using namespace blml;
 
@@ -219,6 +350,80 @@ int blml_plan_destroy(blml_plan p) {
   cudaFree(p->W);
   if (p->tc) tc_plan_free(p);
   delete p;
+  return BLML_OK;
+}
+
+int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_complex, const void* x_base,
+                      const int64_t* x_off, void* y_base, const int64_t* y_off, blml_group* out) {
+  if (G < 1 || G > 65535 || !plans || !nbatch || !x_off || !y_off || !out) {
+    set_error("blml_group_create: bad arguments"); return BLML_ERR_ARG;
+  }
+  const int d = plans[0]->d, dtype = plans[0]->dtype;
+  for (int g = 0; g < G; g++)
+    if (!plans[g] || plans[g]->d != d || plans[g]->dtype != dtype || nbatch[g] < 1) {
+      set_error("blml_group_create: every plan of a group has one dimension count and dtype"); return BLML_ERR_ARG;
+    }
+  const size_t esz = dtype == BLML_F64 ? 16 : 8, rsz = dtype == BLML_F64 ? 8 : 4;
+  const size_t xsz = x_complex ? esz : rsz, ysz = x_complex ? esz : rsz;
+  std::vector<size_t> wso(G + 1, 0);
+  for (int g = 0; g < G; g++) wso[g + 1] = wso[g] + 2 * (size_t)nbatch[g] * plans[g]->max_elems * esz;
+  blml_group_s* grp = new blml_group_s();
+  grp->G = G; grp->d_max = d; grp->dtype = dtype; grp->nstages = 2 * d; grp->ws = nullptr;
+  if (cudaMalloc(&grp->ws, std::max<size_t>(wso[G], 16)) != cudaSuccess) {
+    delete grp; set_error("blml_group_create: workspace allocation"); return BLML_ERR_CUDA;
+  }
+  std::vector<std::vector<StageDesc>> host(2 * d, std::vector<StageDesc>(G));
+  std::vector<int64_t> maxr(2 * d, 0), maxn(2 * d, 0);
+  for (int g = 0; g < G; g++) {
+    const blml_plan_s* p = plans[g];
+    std::vector<int64_t> dims(p->shape, p->shape + d);
+    char* buf[2] = {reinterpret_cast<char*>(grp->ws) + wso[g],
+                    reinterpret_cast<char*>(grp->ws) + wso[g] + (size_t)nbatch[g] * p->max_elems * esz};
+    const void* cur = reinterpret_cast<const char*>(x_base) + x_off[g] * xsz;
+    for (int s = 0; s < 2 * d; s++) {
+      const bool fwd = s < d, last = s == 2 * d - 1;
+      const int a = d - 1 - (s % d);
+      const int64_t M = dims.back();
+      int64_t tot = 1; for (auto v : dims) tot *= v;
+      const int64_t R = tot / M, N = fwd ? p->nfreq[a] : p->shape[a];
+      void* outp = last ? reinterpret_cast<char*>(y_base) + y_off[g] * ysz : buf[s & 1];
+      StageDesc& D = host[s][g];
+      D.X = cur; D.T = fwd ? p->tf[a] : p->ti[a]; D.W = (s == d - 1) ? p->W : nullptr; D.Y = outp;
+      D.R = R; D.M = (int)M; D.N = (int)N; D.nb = nbatch[g];
+      D.flags = ((s == 0 && !x_complex) ? 1 : 0) | ((s == d - 1) ? 2 : 0) | ((last && !x_complex) ? 4 : 0);
+      maxr[s] = std::max(maxr[s], R * nbatch[g]); maxn[s] = std::max<int64_t>(maxn[s], N);
+      dims.pop_back(); dims.insert(dims.begin(), N);
+      cur = outp;
+    }
+  }
+  int e = BLML_OK;
+  grp->dev.assign(2 * d, nullptr);
+  for (int s = 0; s < 2 * d && !e; s++) {
+    if (cudaMalloc(&grp->dev[s], G * sizeof(StageDesc)) != cudaSuccess) { set_error("blml_group_create: allocation"); e = BLML_ERR_CUDA; break; }
+    e = cuda_status(cudaMemcpy(grp->dev[s], host[s].data(), G * sizeof(StageDesc), cudaMemcpyHostToDevice), "blml_group_create");
+    grp->grids.push_back(dim3((unsigned)((maxr[s] + GR - 1) / GR), (unsigned)((maxn[s] + GN - 1) / GN), (unsigned)G));
+  }
+  if (e) { blml_group_destroy(grp); return e; }
+  *out = grp;
+  return BLML_OK;
+}
+
+int blml_group_matvec(blml_group grp, void* stream) {
+  if (!grp) { set_error("blml_group_matvec: null group"); return BLML_ERR_ARG; }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  for (int s = 0; s < grp->nstages; s++) {
+    if (grp->dtype == BLML_F64) k_contract_grouped<double><<<grp->grids[s], 256, 0, st>>>(grp->dev[s]);
+    else k_contract_grouped<float><<<grp->grids[s], 256, 0, st>>>(grp->dev[s]);
+    BLML_CHECK_LAUNCH("blml_group_matvec");
+  }
+  return BLML_OK;
+}
+
+int blml_group_destroy(blml_group grp) {
+  if (!grp) return BLML_OK;
+  for (auto p : grp->dev) cudaFree(p);
+  cudaFree(grp->ws);
+  delete grp;
   return BLML_OK;
 }
 

@@ -50,6 +50,17 @@ int blml_matvec(blml_plan plan, const void* x, void* y, int nbatch, int x_comple
    made (BLML_ERR_TIMEOUT; the results of that call are invalid) or BLML_OK */
 int blml_plan_status(blml_plan plan);
 
+/* ---- grouped mat-vecs: many plans (fits of uneven lattice size and band) applied in one launch per stage ----
+ * Problem g: y_base[y_off[g] ...] = S_g x_base[x_off[g] ...] over nbatch[g] lattices of plan g (SIMT engine); every
+ * plan of a group has the same dimension count and dtype; offsets count elements (complex elements when
+ * x_complex). The group owns its intermediate buffers and the per-stage descriptor arrays. Replaces the reference's
+ * sequential per-fit _Sall calls of a cut-off sweep (selector.py:488-553 calling blml_binned.py:156-168). */
+typedef struct blml_group_s* blml_group;
+int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_complex, const void* x_base,
+                      const int64_t* x_off, void* y_base, const int64_t* y_off, blml_group* group);
+int blml_group_matvec(blml_group group, void* stream);
+int blml_group_destroy(blml_group group);
+
 /* ---- coordinate (Jacobi) update of every bin (BLMLBinned._update / _secular / _cd_root,
  *      blml_binned.py:184-206, 1549-1573; cd_root blml_trivial.py:84-89) ----
  * psd = 0: real rank 1, out = sg * cd_root(sg * (U - s0 E), c, s0) on occupied bins (c > 0), 0 elsewhere.
@@ -117,6 +128,44 @@ int blml_fill_modes(int dtype, int K, int64_t B, int cplx, int kk, int phases, d
 /* ---- certificate weights (BLMLBinned.certificate, blml_binned.py:506-507): dh = sqrt(sum_k |E_k|^2 / w) on
  *      occupied bins, 0 elsewhere, float64 output whatever the fit dtype ---- */
 int blml_cert_weights(int dtype, int K, int64_t B, int cplx, const void* E, const void* w, double* dh, void* stream);
+
+/* ---- segmented (batched) solver kernels: F independent fits in lockstep, one launch per phase ----
+ * Fit f owns elements [off, off + K B) of every flat mode array (its (K, B) block) and [boff, boff + B) of every flat
+ * bin array (counts, signs); `segs` is a device array of F entries. Per-fit scalars are device arrays of F doubles
+ * (coefficient tables: F x nterms). Reductions give out[f * nq + q] (part: F * nq * blml_seg_blocks() doubles).
+ * These are the reference's single-fit operations (blml_binned.py:171-220, 278-355, 415-445, 630-645) applied to a
+ * sweep of fits at once, as selector._search / the cut-off sweeps run them one after another. */
+typedef struct { int64_t off; int64_t boff; int64_t B; int32_t K; int32_t pad; } blml_seg;
+int blml_seg_blocks(void);
+int blml_seg_start_root(int dtype, int F, const blml_seg* segs, const void* c, const void* sg, const double* s0,
+                        void* e0, void* stream);
+int blml_seg_update_real1(int dtype, int F, const blml_seg* segs, const void* E, const void* U, const void* c,
+                          const void* sg, const double* s0, void* out, void* stream);
+int blml_seg_merit(int dtype, int F, const blml_seg* segs, int cplx, int psd, const void* E, const void* U,
+                   const void* c, const void* sg, double* part, double* out, void* stream);        /* nq = 3 */
+int blml_seg_resid(int dtype, int F, const blml_seg* segs, int cplx, const void* E, const void* U, const void* c,
+                   const double* scale, double* part, double* out, void* stream);                   /* nq = 2 */
+int blml_seg_dots(int dtype, int F, const blml_seg* segs, int cplx, int npairs, const void* const* a,
+                  const void* const* b, double* part, double* out, void* stream);                   /* npairs <= 48 */
+int blml_seg_lincomb(int dtype, int F, const blml_seg* segs, int cplx, void* out, int nterms, const double* coef,
+                     const void* const* v, void* stream);                                           /* nterms <= 48 */
+int blml_seg_lgrad_weights(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* w,
+                           const double* vscale, void* V, double* part, double* out, void* stream);  /* nq = 1 */
+int blml_seg_lgrad_finish(int dtype, int F, const blml_seg* segs, int cplx, const void* SV, const void* U,
+                          const void* w, const double* nq, void* g, void* stream);
+/* every fit's Armijo search in one pass: out[f * 43 + j] = sum_occ w log F(U + 2^-j S q) for j < 40, then
+   <q, U>, <E, S q>, <q, S q> (blml_binned.py:316-321 evaluates the same trials one at a time) */
+int blml_seg_trials(int dtype, int F, const blml_seg* segs, int cplx, const void* E, const void* q, const void* U,
+                    const void* Sq, const void* w, double* part, double* out, void* stream);
+int blml_seg_axpy2(int dtype, int F, const blml_seg* segs, int cplx, void* E, const void* q, void* U, const void* Sq,
+                   const double* t, void* stream);
+int blml_seg_finish(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* w,
+                    const double* inv_n2, void* density, double* part, double* out, void* stream);  /* nq = 1 */
+int blml_seg_log_score(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* m,
+                       const double* inv_z, double eps, double* part, double* out, void* stream);   /* nq = 2 */
+int blml_seg_phases(int dtype, int F, const blml_seg* segs, double pn, const double* z, void* E, void* stream);
+int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const blml_seg* cplx_segs, const void* er,
+                             void* E, void* stream);
 
 /* ---- pair accumulation over lattice bins from the row-kernel value tables (blml_local_gpu.rows / cols,
  *      blml_local_gpu.py:42-105, 320-361, 408-455; numba twins blml_local.py:117-191) ----
