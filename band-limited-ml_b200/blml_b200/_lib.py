@@ -75,6 +75,7 @@ _SIGS = {
     'blml_rows': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P, _P, _P]),
     'blml_cols': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P]),
     'blml_lattice_coords': (_I, [_P, _L, _I, _P, _P, _P]),
+    'blml_rows_noalloc': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _P, _P]),
 }
 EXPORTS = tuple(_SIGS)
 

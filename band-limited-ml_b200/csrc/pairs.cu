@@ -7,6 +7,7 @@
 // by a second kernel, so results are deterministic (the reference combines slices with float64 atomics).
 // Before any launch the coordinates are checked against the tables' extents on the device, so a stale table is an
 // error, never an out-of-range read.
+#include <mutex>
 #include "common.cuh"
 
 namespace blml {
@@ -414,6 +415,128 @@ int blml_rows(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t
   }
   if (!tb->T || (cm.G && !tb->RT) || (grad && (!tb->dT || !tb->dR))) { set_error("blml_rows: tables missing"); return BLML_ERR_ARG; }
   return rows_impl<double>(tb, cm, tb->T, tb->RT, tb->dT, tb->dR, ZA, R, ZB, M, w, grad, s, ds, st);
+}
+
+}  // extern "C"
+
+// ---- blml_rows_noalloc: the value rows with a fixed scratch array instead of any device allocation ----
+// Its scratch (the per-column coordinate ranges of the extent check, then the column-slice partial sums) lives in
+// this file-scope device array: 4 MiB on every GPU that loads the library, held until the process exits. Host code
+// must not pass the symbol itself to a kernel (on the host it names a stand-in, not device memory): the device
+// address comes from cudaGetSymbolAddress, taken once per device with that device current, on the first call.
+constexpr int64_t kRowsScratchDoubles = (int64_t)1 << 19;       // 4 MiB
+constexpr int64_t kRowsScratchRangeSlots = 64;                   // 4 * d <= 32 range words, padded to 512 bytes
+constexpr int64_t kRowsNoAllocMaxR = kRowsScratchDoubles - kRowsScratchRangeSlots;
+static __device__ __align__(256) double g_rows_scratch[kRowsScratchDoubles];
+
+static int rows_scratch(double** out) {
+  int dev = 0;
+  int e = cuda_status(cudaGetDevice(&dev), "blml_rows_noalloc");
+  if (e) return e;
+  if (dev < 0 || dev >= 64) { set_error("blml_rows_noalloc: device ordinal %d above 63", dev); return BLML_ERR_ARG; }
+  static std::mutex mu;
+  static double* ptrs[64] = {nullptr};
+  std::lock_guard<std::mutex> lock(mu);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    e = cuda_status(cudaGetSymbolAddress(&p, g_rows_scratch), "blml_rows_noalloc scratch address");
+    if (e) return e;
+    ptrs[dev] = reinterpret_cast<double*>(p);
+  }
+  *out = ptrs[dev];
+  return BLML_OK;
+}
+
+template <typename REAL>
+static int rows_noalloc_launch(const ColMeta& cm, const REAL* T, const REAL* RT, const int64_t* ZA, int64_t R,
+                               const int64_t* ZB, int64_t M, const double* w, double* part, double* s,
+                               cudaStream_t st) {
+  const int64_t rblocks = (R + PR_THREADS - 1) / PR_THREADS;
+  int64_t nsl = std::max<int64_t>(1, std::min<int64_t>((4 * 148 + rblocks - 1) / rblocks, (M + 1023) / 1024));
+  nsl = std::min<int64_t>(std::min<int64_t>(nsl, 65535), std::max<int64_t>(1, kRowsNoAllocMaxR / R));
+  const int64_t slice = (M + nsl - 1) / nsl;
+  nsl = (M + slice - 1) / slice;
+  bool offset_only = cm.G == 0;
+  for (int k = 0; k < cm.d; k++) offset_only = offset_only && cm.code[k] == 0;
+  dim3 grid((unsigned)rblocks, (unsigned)nsl);
+  if (offset_only) {
+    const size_t sm = offset_smem_bytes<REAL>(cm.Tn, cm.d);
+    if (sm > 200 * 1024) { set_error("blml_rows_noalloc: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+#define ROWS_OFF_NA(DD) case DD: \
+      cudaFuncSetAttribute(k_rows_offset<REAL, DD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
+      k_rows_offset<REAL, DD><<<grid, PR_THREADS, sm, st>>>(cm, T, ZA, R, ZB, w, slice, M, part); break;
+    switch (cm.d) { ROWS_OFF_NA(1) ROWS_OFF_NA(2) ROWS_OFF_NA(3) ROWS_OFF_NA(4) ROWS_OFF_NA(5) ROWS_OFF_NA(6) ROWS_OFF_NA(7) ROWS_OFF_NA(8) }
+#undef ROWS_OFF_NA
+  } else {
+    const size_t sm = (size_t)cm.Tn * sizeof(REAL) + (size_t)cm.G * cm.LR * sizeof(REAL);
+    if (sm > 200 * 1024) { set_error("blml_rows_noalloc: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+    cudaFuncSetAttribute(k_rows_general<REAL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_rows_general<REAL, false><<<grid, PR_THREADS, sm, st>>>(cm, T, RT, nullptr, nullptr, ZA, R, ZB, w, 0, slice, M,
+                                                              part, nullptr);
+  }
+  int e = cuda_status(cudaGetLastError(), "blml_rows_noalloc");
+  if (e) return e;
+  k_sum_slices<<<std::min<int64_t>((R + 255) / 256, 4096), 256, 0, st>>>(part, (int)nsl, R, s);
+  count_launches(2);
+  return cuda_status(cudaGetLastError(), "blml_rows_noalloc finish");
+}
+
+extern "C" {
+
+int blml_rows_noalloc(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                      const double* w, double* s, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  ColMeta cm;
+  int e = read_meta(tb, cm, st);
+  if (e) return e;
+  if (R < 0 || M < 0) { set_error("blml_rows_noalloc: negative sizes"); return BLML_ERR_ARG; }
+  if (R > kRowsNoAllocMaxR) {
+    set_error("blml_rows_noalloc: %lld rows exceed the fixed scratch (at most %lld rows)", (long long)R,
+              (long long)kRowsNoAllocMaxR);
+    return BLML_ERR_ARG;
+  }
+  if (R == 0) return BLML_OK;
+  if (M == 0) return cuda_status(cudaMemsetAsync(s, 0, R * sizeof(double), st), "blml_rows_noalloc");
+  double* scratch = nullptr;
+  e = rows_scratch(&scratch);
+  if (e) return e;
+  // extent check: per-column coordinate ranges into the scratch head, read back, compared with the tables
+  long long* ranges = reinterpret_cast<long long*>(scratch);
+  k_coord_range<<<cm.d, 256, 0, st>>>(ZA, R, ZB, M, cm.d, ranges);
+  count_launches(1);
+  long long hr[4 * MAXD];
+  e = cuda_status(cudaMemcpyAsync(hr, ranges, 4 * cm.d * sizeof(long long), cudaMemcpyDeviceToHost, st),
+                  "blml_rows_noalloc extents");
+  if (!e) e = cuda_status(cudaStreamSynchronize(st), "blml_rows_noalloc extents");
+  if (e) return e;
+  double rad[MAXG] = {0, 0, 0, 0};
+  for (int k = 0; k < cm.d; k++) {
+    const long long mnA = hr[4 * k], mxA = hr[4 * k + 1], mnB = hr[4 * k + 2], mxB = hr[4 * k + 3];
+    const long long span = std::max(mxA - mnB, mxB - mnA);
+    bool ok = true;
+    switch (cm.code[k]) {
+      case 0: ok = span <= cm.J[k]; break;
+      case 3: ok = mnA >= 0 && mnB >= 0 && mxA < cm.mk[k] && mxB < cm.mk[k]; break;
+      case 1: case 4: ok = mnA >= 0 && mnB >= 0 && mxA < cm.nb[k] && mxB < cm.nb[k]; break;
+      case 2: rad[cm.grp[k]] += (double)span * (double)span; break;
+    }
+    if (!ok) {
+      set_error("pair tables: column %d coordinates outside the tables' span (stale tables)", k);
+      return BLML_ERR_ARG;
+    }
+  }
+  for (int k = 0; k < cm.d; k++)
+    if (cm.code[k] == 2 && sqrt(rad[cm.grp[k]]) * RQ + 1 >= cm.LR) {
+      set_error("pair tables: radial group %d radius outside its row (stale tables)", cm.grp[k]);
+      return BLML_ERR_ARG;
+    }
+  double* part = scratch + kRowsScratchRangeSlots;
+  if (tb->f32) {
+    if (!tb->T32 || (cm.G && !tb->RT32)) { set_error("blml_rows_noalloc: float32 tables missing"); return BLML_ERR_ARG; }
+    return rows_noalloc_launch<float>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, w, part, s, st);
+  }
+  if (!tb->T || (cm.G && !tb->RT)) { set_error("blml_rows_noalloc: tables missing"); return BLML_ERR_ARG; }
+  return rows_noalloc_launch<double>(cm, tb->T, tb->RT, ZA, R, ZB, M, w, part, s, st);
 }
 
 int blml_lattice_coords(const double* Z, int64_t n, int d, const double* h, int64_t* out, void* stream) {

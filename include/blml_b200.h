@@ -185,6 +185,21 @@ typedef struct {
 } blml_tables;
 int blml_rows(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
               int grad, double* s, double* ds, void* stream);
+/* ---- blml_rows without any allocation: no counterpart in the reference ----
+ * For callers that cannot allocate device memory themselves or let the library do it: code that runs while a
+ * stream is being captured into a CUDA graph (where cudaMalloc breaks the capture), processes whose device memory
+ * is reserved up front by another allocator, and embedded hosts that forbid allocation after start-up.
+ * blml_rows allocates its column-slice partial sums and its extent-check buffer stream-ordered on every call; this
+ * entry point keeps them in a fixed 4 MiB device array inside the library instead (every GPU that loads the library
+ * holds it until the process exits), so it takes at most 524,224 rows (R), and larger R is rejected with
+ * BLML_ERR_ARG. Value rows only (no derivative rows); same tables, inputs, outputs and results as blml_rows.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) and must come before any
+ * stream capture on that device. Every call shares the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and give wrong sums, so serialise them. Every scratch entry is written before it is
+ * read, so nothing needs clearing between calls. */
+int blml_rows_noalloc(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                      const double* w, double* s, void* stream);
+
 /* ---- fixed-lattice binning (BLMLQuick._fit_lattice, blml_trivial.py:3572; SincKernel.quantize :402-403) ----
  * out (n, d) int64 = round(Z / h) of bin centres Z (n, d) float64, h (d) float64, ties to even as np.round */
 int blml_lattice_coords(const double* Z, int64_t n, int d, const double* h, int64_t* out, void* stream);
