@@ -26,7 +26,8 @@ struct SAcc {
 #define SEG_LOOP(b, sg) for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < (sg).B; \
                              b += (int64_t)gridDim.x * blockDim.x)
 
-// partials layout: part[((f * NQ) + q) * gridDim.x + blockIdx.x]
+// partials layout, quantity-major so it does not depend on how many accumulators a kernel carries:
+// part[((q * F) + f) * gridDim.x + blockIdx.x], F = gridDim.y fits
 template <int NQ>
 __device__ __forceinline__ void seg_partials(double (&v)[NQ], double* part, unsigned maxmask = 0u) {
   __shared__ double sh[NQ][32];
@@ -43,19 +44,19 @@ __device__ __forceinline__ void seg_partials(double (&v)[NQ], double* part, unsi
       const bool mx = (maxmask >> q) & 1u;
       double x = lane < nw ? sh[q][lane] : (mx ? -INFINITY : 0.0);
       x = mx ? warp_max(x) : warp_sum(x);
-      if (lane == 0) part[((int64_t)blockIdx.y * NQ + q) * gridDim.x + blockIdx.x] = x;
+      if (lane == 0) part[((int64_t)q * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = x;
     }
   }
 }
 
-// one block per (fit, quantity): out[f * nq + q] = fixed-order reduction of its partials
+// one block per fit: out[f * nq + q] = fixed-order reduction of its partials (F = gridDim.x fits)
 __global__ void k_seg_finish(const double* part, int nq, int nblk, unsigned maxmask, double* out) {
   const int f = blockIdx.x;
   for (int q = 0; q < nq; q++) {
     const bool mx = (maxmask >> q) & 1u;
     double acc = mx ? -INFINITY : 0.0;
     for (int i = threadIdx.x; i < nblk; i += blockDim.x) {
-      const double v = part[((int64_t)f * nq + q) * nblk + i];
+      const double v = part[((int64_t)q * gridDim.x + f) * nblk + i];
       acc = mx ? fmax(acc, v) : acc + v;
     }
     __shared__ double sh[32];
@@ -77,7 +78,7 @@ __global__ void k_seg_finish_strided(const double* part, int nq, int nblk, doubl
   const int f = blockIdx.x;
   for (int q = 0; q < nq; q++) {
     double acc = 0.0;
-    for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += part[((int64_t)f * nq + q) * nblk + i];
+    for (int i = threadIdx.x; i < nblk; i += blockDim.x) acc += part[((int64_t)q * gridDim.x + f) * nblk + i];
     __shared__ double sh[32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     double x = warp_sum(acc);

@@ -49,9 +49,10 @@ def test_batch_matches_single_fits(cuda_device, dt):
     fits = _sweep(4)
     batch = BLMLBinnedBatch(tol=1e-6, dtype=dt)
     res = batch.fit([c for c, _ in fits], [m for _, m in fits])
+    bar = 1e-6 if dt == np.float64 else 5e-5        # float32 state stops ~1e-5 short (test_gpu_binned)
     for (counts, modes), r in zip(fits, res):
         one = BLMLBinned(tol=1e-6, solver='lbfgs', dtype=np.float64).fit(counts, modes, complex_g=True)
-        assert abs(r.loglik_ - one.loglik_) <= 1e-6 * abs(one.loglik_), (r.loglik_, one.loglik_, r.stop_reason_)
+        assert abs(r.loglik_ - one.loglik_) <= bar * abs(one.loglik_), (r.loglik_, one.loglik_, r.stop_reason_)
         assert r.density_.shape == counts.shape and np.all(np.isfinite(r.density_))
 
 
