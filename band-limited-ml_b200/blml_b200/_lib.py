@@ -58,6 +58,17 @@ _SIGS = {
     'blml_seg_log_score': (_I, [_I, _I, _P, _I, _P, _P, _P, _D, _P, _P, _P]),
     'blml_seg_phases': (_I, [_I, _I, _P, _D, _P, _P, _P]),
     'blml_seg_real_to_complex': (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    'blml_group_matvec_masked': (_I, [_P, _P, _I, _P, _P]),
+    'blml_lbfgs_batch_create': (_I, [_I, _I, _P, _P, _I, _D, _D, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    'blml_lbfgs_batch_run': (_I, [_P, _P]),
+    'blml_lbfgs_batch_result': (_I, [_P, _P, _P, _P, _P, _P]),
+    'blml_lbfgs_batch_stats': (_I, [_P, _P]),
+    'blml_lbfgs_batch_destroy': (_I, [_P]),
+    'blml_start_batch_create': (_I, [_I, _P, _P, _I, _D, _L, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    'blml_start_batch_run': (_I, [_P, _P]),
+    'blml_start_batch_result': (_I, [_P, _P, _P]),
+    'blml_start_batch_stats': (_I, [_P, _P]),
+    'blml_start_batch_destroy': (_I, [_P]),
     'blml_jacobi_update': (_I, [_I, _I, _L, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_merit_terms': (_I, [_I, _I, _L, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_resid': (_I, [_I, _I, _L, _I, _P, _P, _P, _D, _P, _P, _P]),

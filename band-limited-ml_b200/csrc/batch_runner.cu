@@ -1,0 +1,1024 @@
+// Device-side control of the batched engine. The per-fit scalar logic of the two solver phases -- the real rank-1
+// start (Jacobi updates, Anderson mixing, the merit safeguard; blml_binned.py:223-276) and L-BFGS (compact
+// direction, Armijo choice, pair update, stop rules; blml_trivial.py:2590-2645 as blml_binned.py runs it) -- runs as
+// small kernels over the fits, so one iteration is a fixed sequence of launches with no host decision in it. A ring
+// of iterations (one per memory slot) is captured once as a CUDA graph and replayed until every fit has stopped;
+// the host reads one active mask per replay, and when the active set has shrunk it captures the graph again over
+// the fits still iterating (compact index j -> fit f = fid[j]; per-fit state is indexed by f, per-launch scalar
+// tables by j). A fit that stops inside a replay gets an empty segment (B = 0) and a cleared live flag, which every
+// later launch of the replay reads, so it does no more work.
+#include <vector>
+#include <algorithm>
+#include <limits.h>
+#include "common.cuh"
+#include "plan.cuh"
+#include "segmented.cuh"
+
+namespace blml {
+
+constexpr int LB_MMAX = 20, LB_FWIN = 10, LB_NT = 40, AA_MMAX = 8, DAMP_NT = 26;
+enum { STOP_TOL = 0, STOP_LLTOL = 1, STOP_STALL = 2 };
+
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// the start's merit from its three terms [sum e u, sum_occ c log|e|, #(sg e <= 0)] (blml_binned.py:208-220)
+__device__ __forceinline__ double merit_value(const double* r, double n) {
+  const double m = -(0.5 * r[0] - r[1]) / n;
+  return r[2] > 0 ? -INFINITY : m;
+}
+
+__device__ __forceinline__ void set_live(int j, int f, int on, int* live, const blml_seg* segs_c, blml_seg* segs_eff) {
+  live[f] = on;
+  blml_seg s = segs_c[j];
+  if (!on) s.B = 0;
+  segs_eff[j] = s;
+}
+
+__global__ void k_fill_int(int* a, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+__global__ void k_fill_double(double* a, int64_t n, double v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// one warp per quantity: out[j * nq + q] = the fixed-order sum of the fit's SEG_BLOCKS partials (the order of
+// k_seg_finish), for the fits whose flag is set
+__global__ void k_finish_flagged(const double* part, int nq, const int* flag, double* out) {
+  const int j = blockIdx.x, Fa = gridDim.x;
+  if (flag && !flag[j]) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int q = wid; q < nq; q += nw) {
+    double x = lane < SEG_BLOCKS ? part[((int64_t)q * Fa + j) * SEG_BLOCKS + lane] : 0.0;
+    x = warp_sum(x);
+    if (lane == 0) out[(int64_t)j * nq + q] = x;
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ L-BFGS control
+struct LbState {
+  double *L, *Q, *Qn, *n, *res, *slope, *mh, *SY, *YY;
+  int *active, *it, *stop, *reset, *nh, *ok, *stamp, *step;
+};
+
+// the compact L-BFGS direction of fit f (one warp): q = gam g + S p - gam Y t over the fit's pairs in the order they
+// entered (R = triu(S^T Y), R t = S^T g, R^T p = (D + gam Y^T Y) t - gam Y^T g); the scaled gradient when there are
+// no pairs or the direction is not an ascent one (which also clears the memory). Block 0 advances the step counter.
+__global__ void k_lb_dir(int m, const int* fid, const int* live, const double* vals, LbState s, double* cq_all) {
+  const int j = blockIdx.x, lane = threadIdx.x, f = fid[j];
+  if (j == 0 && lane == 0) (*s.step)++;
+  const int nc = 1 + 2 * m;
+  double* cq = cq_all + (int64_t)j * nc;
+  for (int i = lane; i < nc; i += 32) cq[i] = 0.0;
+  if (!live[f]) return;
+  __syncwarp();
+  const double* v = vals + (int64_t)j * (2 * m + 2);
+  const double gg = v[2 * m], ee = v[2 * m + 1];
+  const double first = 1e-3 * sqrt(fmax(ee, 0.0) / fmax(gg, 1e-300));
+  int* stamp = s.stamp + (int64_t)f * m;
+  __shared__ int ord[LB_MMAX];
+  __shared__ int kk;
+  __shared__ double R[LB_MMAX][LB_MMAX + 1], Yy[LB_MMAX][LB_MMAX + 1], ts[LB_MMAX];
+  if (lane == 0) {
+    int k = 0;
+    for (int q = 0; q < m; q++)
+      if (stamp[q] >= 0) ord[k++] = q;
+    for (int i = 1; i < k; i++) {                     // chronological order of the stored pairs
+      const int x = ord[i];
+      int jj = i - 1;
+      while (jj >= 0 && stamp[ord[jj]] > stamp[x]) { ord[jj + 1] = ord[jj]; jj--; }
+      ord[jj + 1] = x;
+    }
+    kk = k;
+  }
+  __syncwarp();
+  const int k = kk;
+  bool first_only = true;
+  double slope = 0.0, gam = 0.0, t_l = 0.0, p_l = 0.0;
+  if (k > 0) {
+    const double* SY = s.SY + (int64_t)f * m * m;
+    const double* YY = s.YY + (int64_t)f * m * m;
+    for (int idx = lane; idx < k * k; idx += 32) {
+      const int i = idx / k, c = idx - (idx / k) * k;
+      R[i][c] = c >= i ? SY[ord[i] * m + ord[c]] : 0.0;
+      Yy[i][c] = YY[ord[i] * m + ord[c]];
+    }
+    __syncwarp();
+    const int last = ord[k - 1];
+    gam = SY[last * m + last] / YY[last * m + last];
+    const double ao = lane < k ? v[ord[lane]] : 0.0, bo = lane < k ? v[m + ord[lane]] : 0.0;
+    double r = ao;                                    // back substitution, R t = ao
+    for (int i = k - 1; i >= 0; i--) {
+      const double ti = __shfl_sync(0xffffffffu, r, i) / R[i][i];
+      if (lane == i) t_l = ti;
+      if (lane < i) r -= R[lane][i] * ti;
+    }
+    if (lane < k) ts[lane] = t_l;
+    __syncwarp();
+    r = 0.0;
+    if (lane < k) {
+      double acc = 0.0;
+      for (int c = 0; c < k; c++) acc += ((c == lane ? R[lane][lane] : 0.0) + gam * Yy[lane][c]) * ts[c];
+      r = acc - gam * bo;
+    }
+    for (int i = 0; i < k; i++) {                     // forward substitution, R^T p = rhs
+      const double pi = __shfl_sync(0xffffffffu, r, i) / R[i][i];
+      if (lane == i) p_l = pi;
+      if (lane > i && lane < k) r -= R[i][lane] * pi;
+    }
+    const double s1 = warp_allsum(lane < k ? ao * p_l : 0.0), s2 = warp_allsum(lane < k ? bo * t_l : 0.0);
+    slope = gam * gg + s1 - gam * s2;
+    first_only = !(slope > 0);
+  }
+  __syncwarp();
+  if (first_only) {
+    if (lane == 0) { cq[0] = first; s.slope[f] = first * gg; }
+    if (k > 0)
+      for (int q = lane; q < m; q += 32) stamp[q] = -1;
+  } else {
+    if (lane == 0) { cq[0] = gam; s.slope[f] = slope; }
+    if (lane < k) { cq[1 + ord[lane]] = p_l; cq[1 + m + ord[lane]] = -gam * t_l; }
+  }
+}
+
+// the Armijo choice of every fit from the one-pass trials: the first t = 2^-j with L(t) >= L + 1e-4 t slope; a
+// failed search clears the memory once and stops the fit ('stall') when it fails again or had no pairs
+__global__ void k_lb_select(int Fa, int m, const int* fid, const int* live, const double* tr_all, LbState s,
+                            double* tA, double* cS, double* cY, double* cG) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  double t = 0.0;
+  int ok = 0;
+  if (live[f]) {
+    const double* tr = tr_all + (int64_t)j * (LB_NT + 3);
+    const double A = tr[LB_NT] + tr[LB_NT + 1], Cc = tr[LB_NT + 2], Qa = s.Q[f], La = s.L[f], na = s.n[f];
+    double ts = 1.0;
+    for (int jj = 0; jj < LB_NT; jj++) {
+      const double Qt = Qa + ts * A + ts * ts * Cc;
+      const double Lt = Qt > 0 ? tr[jj] - na * log(Qt) : -INFINITY;
+      if (Lt >= La + 1e-4 * ts * s.slope[f]) { ok = 1; t = ts; break; }
+      ts *= 0.5;
+    }
+    int* stamp = s.stamp + (int64_t)f * m;
+    if (!ok) {
+      bool nopairs = true;
+      for (int q = 0; q < m; q++) nopairs &= stamp[q] < 0;
+      if (s.reset[f] || nopairs) { s.stop[f] = STOP_STALL; s.active[f] = 0; }
+      else { for (int q = 0; q < m; q++) stamp[q] = -1; s.reset[f] = 1; }
+    } else {
+      s.reset[f] = 0;
+    }
+  }
+  s.ok[f] = ok;
+  const double o = ok ? 1.0 : 0.0;
+  tA[j] = t;
+  cS[2 * j] = t; cS[2 * j + 1] = 1.0 - o;
+  cY[3 * j] = o; cY[3 * j + 1] = -o; cY[3 * j + 2] = 1.0 - o;
+  cG[2 * j] = o; cG[2 * j + 1] = 1.0 - o;
+}
+
+// Q at the new point, and the scales of the gradient finish (n / Q) and of the residual (n / sqrt Q)
+__global__ void k_lb_qeff(int Fa, const int* fid, const int* live, const double* outC, LbState s, double* nqA,
+                          double* scrA) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  if (!live[f]) { nqA[j] = 0.0; scrA[j] = 1.0; return; }
+  const double Qn = outC[j];
+  s.Qn[f] = Qn;
+  const double Qe = s.ok[f] ? Qn : s.Q[f];
+  nqA[j] = s.n[f] / Qe;
+  scrA[j] = Qe > 0 ? s.n[f] / sqrt(fmax(Qe, 1e-300)) : 1.0;
+}
+
+// the end of an iteration: the new pair (s, y) into slot p when its curvature is positive, the accepted state, the
+// likelihood window, then the stop rules the next iteration starts with (tol, ll_tol, the iteration cap)
+__global__ void k_lb_post(int Fa, int m, int p, double tol, double ftol, long long cap, const int* fid, int* live,
+                          const blml_seg* segs_c, blml_seg* segs_eff, const double* outA, const double* outD,
+                          const double* outE, LbState s) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  if (!live[f]) { set_live(j, f, 0, live, segs_c, segs_eff); return; }
+  const int ok = s.ok[f];
+  const double nf = s.n[f], Qn = s.Qn[f];
+  const double Ln = Qn > 0 ? outD[j] - nf * log(Qn) : -INFINITY;
+  const double r = outE[2 * j + 1] > 0 ? NAN : outE[2 * j];
+  const double* v = outA + (int64_t)j * (3 + 2 * m);
+  const double sy = v[0], ss = v[1], yy = v[2];
+  const bool enter = ok && (sy > 1e-12 * sqrt(fmax(ss * yy, 0.0)));
+  int* stamp = s.stamp + (int64_t)f * m;
+  if (ok) stamp[p] = -1;
+  if (enter) {
+    stamp[p] = *s.step;
+    double* SY = s.SY + (int64_t)f * m * m;
+    double* YY = s.YY + (int64_t)f * m * m;
+    for (int q = 0; q < m; q++) SY[q * m + p] = v[3 + q];
+    SY[p * m + p] = sy;
+    for (int q = 0; q < m; q++) { YY[q * m + p] = v[3 + m + q]; YY[p * m + q] = v[3 + m + q]; }
+    YY[p * m + p] = yy;
+  }
+  double* h = s.mh + (int64_t)f * (LB_FWIN + 1);
+  if (ok) {
+    s.L[f] = Ln; s.Q[f] = Qn; s.res[f] = r;
+    for (int i = 0; i < LB_FWIN; i++) h[i] = h[i + 1];
+    h[LB_FWIN] = Ln / nf;
+    s.nh[f]++;
+    if (r < tol) s.active[f] = 0;
+  }
+  int a = s.active[f];
+  if (a && s.nh[f] > LB_FWIN && h[LB_FWIN] - h[0] < ftol) { s.stop[f] = STOP_LLTOL; a = 0; }
+  if (a && s.it[f] >= cap) a = 0;
+  if (a) s.it[f]++;
+  s.active[f] = a;
+  set_live(j, f, a, live, segs_c, segs_eff);
+}
+
+// set-up: the scale n / sqrt(Q) that normalises E and U, and Q after it
+__global__ void k_lbi_scale(int Fa, const int* fid, const double* outC, LbState s, double* sc, double* nqA,
+                            double* scrA) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  const double Qv = outC[j], nf = s.n[f];
+  const double c = Qv > 0 ? nf / sqrt(fmax(Qv, 1e-300)) : 1.0;
+  sc[j] = c;
+  const double Q = Qv * c * c;
+  s.Q[f] = Q;
+  nqA[j] = nf / Q;
+  scrA[j] = Q > 0 ? nf / sqrt(fmax(Q, 1e-300)) : 1.0;
+}
+
+__global__ void k_lbi_state(int Fa, int m, double tol, long long cap, const int* fid, int* live,
+                            const blml_seg* segs_c, blml_seg* segs_eff, const double* outD, const double* outE,
+                            LbState s) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  const double nf = s.n[f];
+  s.L[f] = outD[j] - nf * log(s.Q[f]);
+  const double r = outE[2 * j + 1] > 0 ? NAN : outE[2 * j];
+  s.res[f] = r;
+  for (int q = 0; q < m; q++) s.stamp[(int64_t)f * m + q] = -1;
+  for (int q = 0; q < m * m; q++) { s.SY[(int64_t)f * m * m + q] = 0.0; s.YY[(int64_t)f * m * m + q] = 0.0; }
+  double* h = s.mh + (int64_t)f * (LB_FWIN + 1);
+  for (int i = 0; i < LB_FWIN; i++) h[i] = NAN;
+  h[LB_FWIN] = s.L[f] / nf;
+  s.nh[f] = 1; s.reset[f] = 0; s.stop[f] = STOP_TOL; s.ok[f] = 0; s.it[f] = 0;
+  int a = r >= tol;
+  if (a && 0 >= cap) a = 0;
+  if (a) s.it[f] = 1;
+  s.active[f] = a;
+  set_live(j, f, a, live, segs_c, segs_eff);
+  if (j == 0) *s.step = -1;
+}
+
+// --------------------------------------------------------------------------------------------------- start control
+struct StState {
+  double *n, *s0, *cur, *res, *best_res, *best_m, *mJ, *G;
+  int *valid, *has_prev, *best_it, *it, *active;
+};
+
+// per fit: the Anderson normal equations on the valid history slots, (G + 1e-12 tr(G) I) gamma = rhs, by LU with
+// partial pivoting (blml_binned.py:1470-1474); false when singular or not finite
+__device__ bool anderson_solve(int mA, const double* G, const int* valid, const double* rhs, double* gam) {
+  double A[AA_MMAX][AA_MMAX + 1];
+  double tr = 0.0;
+  for (int i = 0; i < mA; i++) tr += valid[i] ? G[i * mA + i] : 0.0;
+  for (int i = 0; i < mA; i++) {
+    for (int c = 0; c < mA; c++) A[i][c] = (valid[i] && valid[c]) ? G[i * mA + c] : 0.0;
+    A[i][i] += valid[i] ? 1e-12 * tr : 1.0;
+    A[i][mA] = valid[i] ? rhs[i] : 0.0;
+  }
+  for (int c = 0; c < mA; c++) {
+    int piv = c;
+    for (int i = c + 1; i < mA; i++)
+      if (fabs(A[i][c]) > fabs(A[piv][c])) piv = i;
+    if (A[piv][c] == 0.0) return false;
+    if (piv != c)
+      for (int k = 0; k <= mA; k++) { const double t = A[c][k]; A[c][k] = A[piv][k]; A[piv][k] = t; }
+    for (int i = c + 1; i < mA; i++) {
+      const double l = A[i][c] / A[c][c];
+      for (int k = c; k <= mA; k++) A[i][k] -= l * A[c][k];
+    }
+  }
+  for (int i = mA - 1; i >= 0; i--) {
+    double x = A[i][mA];
+    for (int k = i + 1; k < mA; k++) x -= A[i][k] * gam[k];
+    gam[i] = x / A[i][i];
+  }
+  for (int i = 0; i < mA; i++)
+    if (!isfinite(gam[i])) return false;
+  for (int i = 0; i < mA; i++)
+    if (!valid[i]) gam[i] = 0.0;
+  return true;
+}
+
+// Anderson step of every fit: slot p of the difference history, the mixing weights, the coefficients of
+// E_A = E + f - DX gamma - DF gamma over [E, f, DX_0.., DF_0..]
+__global__ void k_st_anderson(int Fa, int mA, int p, const int* fid, const int* live, const double* outM1,
+                              const double* outA, StState s, double* cA, int* useA) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  const int nc = 2 + 2 * mA;
+  double* row = cA + (int64_t)j * nc;
+  for (int i = 0; i < nc; i++) row[i] = 0.0;
+  row[0] = 1.0;
+  useA[j] = 0;
+  if (!live[f]) return;
+  s.mJ[f] = merit_value(outM1 + 3 * j, s.n[f]);
+  int* valid = s.valid + (int64_t)f * mA;
+  double* G = s.G + (int64_t)f * mA * mA;
+  const double* vals = outA + (int64_t)j * 2 * mA;
+  valid[p] = s.has_prev[f];
+  for (int q = 0; q < mA; q++) { G[p * mA + q] = vals[q]; G[q * mA + p] = vals[q]; }
+  s.has_prev[f] = 1;
+  int nv = 0;
+  for (int q = 0; q < mA; q++) nv += valid[q] ? 1 : 0;
+  if (nv < 2) return;
+  double gam[AA_MMAX];
+  if (!anderson_solve(mA, G, valid, vals + mA, gam)) {
+    for (int q = 0; q < mA; q++) valid[q] = 0;
+    s.has_prev[f] = 0;
+    return;
+  }
+  row[1] = 1.0;
+  for (int q = 0; q < mA; q++) { row[2 + q] = -gam[q]; row[2 + mA + q] = -gam[q]; }
+  useA[j] = 1;
+}
+
+// the better of the Jacobi and Anderson points, and whether the step needs damping (no ascent of the merit)
+__global__ void k_st_take(int Fa, int mA, const int* fid, const int* live, const double* outM1, const double* outM2,
+                          const int* useA, StState s, double* cT, int* damp) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  cT[2 * j] = 0.0; cT[2 * j + 1] = 1.0; damp[j] = 0;
+  if (!live[f]) return;
+  double mJ = mA ? s.mJ[f] : merit_value(outM1 + 3 * j, s.n[f]);
+  if (mA && useA[j]) {
+    const double mAc = merit_value(outM2 + 3 * j, s.n[f]);
+    if (mAc > mJ) { mJ = mAc; cT[2 * j] = 1.0; cT[2 * j + 1] = 0.0; }
+  }
+  s.mJ[f] = mJ;
+  const double cur = s.cur[f];
+  if (mJ < cur - 1e-12 * fabs(cur)) {
+    damp[j] = 1;
+    for (int q = 0; q < mA; q++) s.valid[(int64_t)f * mA + q] = 0;
+    s.has_prev[f] = 0;
+  }
+}
+
+// the damped Jacobi steps of the fits that need them, every trial a = 2^-1 .. 2^-26 in one pass: the merit terms of
+// E + a (E_J - E), U + a (U_J - U), formed as the linear-combination kernel forms them
+__global__ void __launch_bounds__(256) k_st_damp_trials(const blml_seg* segs, const int* damp, const double* E,
+                                                        const double* EJ, const double* U, const double* UJ,
+                                                        const double* c, const double* sg, double* part) {
+  if (!damp[blockIdx.y]) return;
+  const blml_seg S = segs[blockIdx.y];
+  double v[3 * DAMP_NT];
+#pragma unroll
+  for (int q = 0; q < 3 * DAMP_NT; q++) v[q] = 0.0;
+  SEG_LOOP(b, S) {
+    const double e0 = E[S.off + b], e1 = EJ[S.off + b], u0 = U[S.off + b], u1 = UJ[S.off + b];
+    const double cb = c[S.boff + b], sgb = sg[S.boff + b];
+    double a = 0.5;
+#pragma unroll
+    for (int k = 0; k < DAMP_NT; k++) {
+      const double e = fma(a, e1, (1.0 - a) * e0), u = fma(a, u1, (1.0 - a) * u0);
+      v[3 * k] += e * u;
+      if (cb > 0) { v[3 * k + 1] += cb * log(fabs(e)); if (sgb * e <= 0) v[3 * k + 2] += 1.0; }
+      a *= 0.5;
+    }
+  }
+  seg_partials<3 * DAMP_NT>(v, part);
+}
+
+// the first damped trial whose merit does not fall below the current one; the coefficients of the new iterate over
+// [E, E_J, E_T] (no step found: the iterate stays)
+__global__ void k_st_damp_pick(int Fa, const int* fid, const int* live, const int* damp, const double* outDT,
+                               StState s, double* cE) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  double* ce = cE + 3 * (int64_t)j;
+  ce[0] = 0.0; ce[1] = 0.0; ce[2] = 1.0;
+  if (!live[f] || !damp[j]) return;
+  ce[0] = 1.0; ce[2] = 0.0;
+  const double cur = s.cur[f];
+  double a = 0.5;
+  for (int k = 0; k < DAMP_NT; k++) {
+    const double mt = merit_value(outDT + (int64_t)j * 3 * DAMP_NT + 3 * k, s.n[f]);
+    if (mt >= cur) { ce[0] = 1.0 - a; ce[1] = a; s.mJ[f] = mt; return; }
+    a *= 0.5;
+  }
+}
+
+__global__ void k_st_scale(int Fa, const int* fid, const double* outQ, const double* n, double* sc) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const double Qv = outQ[j], nf = n[fid[j]];
+  sc[j] = Qv > 0 ? nf / sqrt(fmax(Qv, 1e-300)) : 1.0;
+}
+
+// NaN-propagating min / max (np.minimum / np.maximum)
+__device__ __forceinline__ double nmin(double a, double b) { return (a != a || b != b) ? NAN : fmin(a, b); }
+__device__ __forceinline__ double nmax(double a, double b) { return (a != a || b != b) ? NAN : fmax(a, b); }
+
+// the end of a start sweep (or the set-up when init): merit and residual of the new iterate, the progress record,
+// then the stop rules the next sweep starts with (tol, stall, the sweep cap)
+__global__ void k_st_post(int Fa, int init, double tol, long long cap, long long stall, const int* fid, int* live,
+                          const blml_seg* segs_c, blml_seg* segs_eff, const double* outM1, const double* outR,
+                          StState s) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
+  if (!init && !live[f]) { set_live(j, f, 0, live, segs_c, segs_eff); return; }
+  const double cur = merit_value(outM1 + 3 * j, s.n[f]);
+  const double r = outR[2 * j + 1] > 0 ? NAN : outR[2 * j];
+  s.cur[f] = cur; s.res[f] = r;
+  int a;
+  if (init) {
+    s.it[f] = 0; s.best_res[f] = r; s.best_it[f] = 0; s.best_m[f] = cur; s.has_prev[f] = 0;
+    a = r >= tol;
+  } else {
+    const double bm = s.best_m[f];
+    if ((r < 0.9 * s.best_res[f]) || (cur > bm + 1e-13 * fabs(bm))) {
+      s.best_res[f] = nmin(r, s.best_res[f]); s.best_it[f] = s.it[f]; s.best_m[f] = nmax(cur, bm);
+    }
+    a = s.active[f] && r >= tol;
+  }
+  if (a && (long long)(s.it[f] - s.best_it[f]) >= stall) a = 0;
+  if (a && s.it[f] >= cap) a = 0;
+  if (a) s.it[f]++;
+  s.active[f] = a;
+  set_live(j, f, a, live, segs_c, segs_eff);
+}
+
+// ------------------------------------------------------------------------------------------------ the runner base
+#define RC(x) do { int _r = (x); if (_r) return _r; } while (0)
+#define KCHECK(where) BLML_CHECK_LAUNCH(where)
+
+struct Runner {
+  static constexpr long long kMaxSteps = 4000000;   // a host-side bound on the iterations of one run
+  int F = 0, Fa = 0;
+  std::vector<blml_seg> segs_all;
+  std::vector<int> ids;                 // current compact set (fit ids)
+  blml_seg *d_segs_c = nullptr, *d_segs_eff = nullptr;
+  int *d_fid = nullptr, *d_live = nullptr, *h_live = nullptr;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long nodes = 0, steps = 0, replays = 0, rebuilds = 0;
+  std::vector<void*> allocs;
+
+  void* dalloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, std::max<size_t>(bytes, 16)) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    return p;
+  }
+  int base_init(int F_, const blml_seg* segs) {
+    F = F_;
+    segs_all.assign(segs, segs + F);
+    d_segs_c = (blml_seg*)dalloc(F * sizeof(blml_seg));
+    d_segs_eff = (blml_seg*)dalloc(F * sizeof(blml_seg));
+    d_fid = (int*)dalloc(F * sizeof(int));
+    d_live = (int*)dalloc(F * sizeof(int));
+    if (!d_segs_c || !d_segs_eff || !d_fid || !d_live) { set_error("batch runner: device allocation"); return BLML_ERR_CUDA; }
+    if (cudaMallocHost(&h_live, F * sizeof(int)) != cudaSuccess) { set_error("batch runner: pinned allocation"); return BLML_ERR_CUDA; }
+    RC(cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "batch runner stream"));
+    RC(cuda_status(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "batch runner event"));
+    return BLML_OK;
+  }
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr; graph = nullptr;
+  }
+  void base_free() {
+    drop_graph();
+    if (st) cudaStreamSynchronize(st);
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+    if (h_live) cudaFreeHost(h_live);
+    if (ev) cudaEventDestroy(ev);
+    if (st) cudaStreamDestroy(st);
+    h_live = nullptr; ev = nullptr; st = nullptr;
+  }
+  // the compact set: fits `sel` (ascending ids), all live
+  int set_compact(const std::vector<int>& sel) {
+    ids = sel; Fa = (int)sel.size();
+    std::vector<blml_seg> sc(Fa);
+    for (int j = 0; j < Fa; j++) sc[j] = segs_all[sel[j]];
+    RC(cuda_status(cudaMemcpyAsync(d_segs_c, sc.data(), Fa * sizeof(blml_seg), cudaMemcpyHostToDevice, st), "compact"));
+    RC(cuda_status(cudaMemcpyAsync(d_segs_eff, sc.data(), Fa * sizeof(blml_seg), cudaMemcpyHostToDevice, st), "compact"));
+    RC(cuda_status(cudaMemcpyAsync(d_fid, sel.data(), Fa * sizeof(int), cudaMemcpyHostToDevice, st), "compact"));
+    return cuda_status(cudaStreamSynchronize(st), "compact");
+  }
+  // the live mask of every fit -> the fits still iterating
+  int read_live(std::vector<int>& on) {
+    RC(cuda_status(cudaMemcpyAsync(h_live, d_live, F * sizeof(int), cudaMemcpyDeviceToHost, st), "live mask"));
+    RC(cuda_status(cudaStreamSynchronize(st), "live mask"));
+    on.clear();
+    for (int f = 0; f < F; f++)
+      if (h_live[f]) on.push_back(f);
+    return BLML_OK;
+  }
+  // capture `ring` iterations enqueued by iter(i) into a graph (launches counted at replay, not at capture)
+  template <typename Iter>
+  int capture(int ring, Iter iter) {
+    drop_graph();
+    const long long l0 = blml_launch_count();
+    RC(cuda_status(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture"));
+    int rc = BLML_OK;
+    for (int i = 0; i < ring && rc == BLML_OK; i++) rc = iter(i);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    nodes = blml_launch_count() - l0;
+    count_launches((int)-nodes);
+    if (rc != BLML_OK) { if (g) cudaGraphDestroy(g); return rc; }
+    RC(cuda_status(ce, "graph capture end"));
+    graph = g;
+    RC(cuda_status(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate"));
+    rebuilds++;
+    return BLML_OK;
+  }
+  int replay() {
+    RC(cuda_status(cudaGraphLaunch(exec, st), "graph launch"));
+    count_launches((int)nodes);
+    replays++;
+    return BLML_OK;
+  }
+  // run until no fit is live: replay the ring, re-capture over the fits still iterating when they fall to 3/4;
+  // before each capture, prep() uploads what the compact set needs
+  template <typename Iter, typename Prep>
+  int run_rings(int ring, Iter iter, Prep prep) {
+    std::vector<int> on;
+    for (;;) {
+      RC(read_live(on));
+      if (on.empty()) return BLML_OK;
+      if (!exec || (int)on.size() * 4 <= Fa * 3) {
+        RC(set_compact(on));
+        RC(prep());
+        RC(capture(ring, iter));
+      }
+      RC(replay());
+      steps += ring;
+      if (steps > kMaxSteps) { set_error("batch runner: more than %lld iterations", kMaxSteps); return BLML_ERR_ARG; }
+    }
+  }
+  int begin(void* caller) {
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(caller);
+    RC(cuda_status(cudaEventRecord(ev, cs), "runner begin"));
+    return cuda_status(cudaStreamWaitEvent(st, ev, 0), "runner begin");
+  }
+  int end(void* caller) {
+    cudaStream_t cs = reinterpret_cast<cudaStream_t>(caller);
+    RC(cuda_status(cudaEventRecord(ev, st), "runner end"));
+    return cuda_status(cudaStreamWaitEvent(cs, ev, 0), "runner end");
+  }
+  int all_live() {
+    std::vector<int> all(F);
+    for (int f = 0; f < F; f++) all[f] = f;
+    RC(set_compact(all));
+    k_fill_int<<<(F + 255) / 256, 256, 0, st>>>(d_live, F, 1);
+    KCHECK("runner live");
+    return BLML_OK;
+  }
+};
+
+static inline unsigned nblk(int n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace blml
+
+using namespace blml;
+
+// ------------------------------------------------------------------------------------------------ L-BFGS runner
+struct blml_lbfgs_batch_s : Runner {
+  int m = 20, dtype = BLML_F64;
+  double tol = 1e-5, ftol = 1e-11;
+  long long cap = LLONG_MAX;
+  blml_group gEU = nullptr, gq = nullptr, gV = nullptr;
+  void *E = nullptr, *U = nullptr;
+  const void *w = nullptr, *c = nullptr;
+  void *g = nullptr, *gn = nullptr, *q = nullptr, *Sq = nullptr, *V = nullptr, *SV = nullptr;
+  void *Sh[LB_MMAX] = {}, *Yh[LB_MMAX] = {};
+  double *part = nullptr, *outA = nullptr, *outB = nullptr, *outC = nullptr, *outD = nullptr, *outE = nullptr;
+  double *cq = nullptr, *tA = nullptr, *cS = nullptr, *cY = nullptr, *cG = nullptr, *nqA = nullptr, *scrA = nullptr,
+         *ones = nullptr, *sc = nullptr;
+  LbState s{};
+
+  int iter(int p) {
+    const int dt = dtype, Fa_ = Fa;
+    const blml_seg* S = d_segs_eff;
+    void* sv = st;
+    const void* a[48]; const void* b[48];
+    // direction
+    for (int i = 0; i < m; i++) { a[i] = Sh[i]; b[i] = g; a[m + i] = Yh[i]; b[m + i] = g; }
+    a[2 * m] = g; b[2 * m] = g; a[2 * m + 1] = E; b[2 * m + 1] = E;
+    RC(blml_seg_dots(dt, Fa_, S, 1, 2 * m + 2, a, b, part, outA, sv));
+    k_lb_dir<<<Fa_, 32, 0, st>>>(m, d_fid, d_live, outA, s, cq);
+    KCHECK("lbfgs direction");
+    const void* terms[48];
+    terms[0] = g;
+    for (int i = 0; i < m; i++) { terms[1 + i] = Sh[i]; terms[1 + m + i] = Yh[i]; }
+    RC(blml_seg_lincomb(dt, Fa_, S, 1, q, 1 + 2 * m, cq, terms, sv));
+    RC(blml_group_matvec_masked(gq, d_fid, Fa_, d_live, sv));
+    // every fit's Armijo search in one pass, then the accepted steps and U = S E exactly
+    RC(blml_seg_trials(dt, Fa_, S, 1, E, q, U, Sq, w, part, outB, sv));
+    k_lb_select<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, m, d_fid, d_live, outB, s, tA, cS, cY, cG);
+    KCHECK("lbfgs select");
+    RC(blml_seg_axpy2(dt, Fa_, S, 1, E, q, U, Sq, tA, sv));
+    RC(blml_group_matvec_masked(gEU, d_fid, Fa_, d_live, sv));
+    a[0] = E; b[0] = U;
+    RC(blml_seg_dots(dt, Fa_, S, 1, 1, a, b, part, outC, sv));
+    k_lb_qeff<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, outC, s, nqA, scrA);
+    KCHECK("lbfgs qeff");
+    // gradient at the new point, the new pair into slot p, the residual and the pair's inner products
+    RC(blml_seg_lgrad_weights(dt, Fa_, S, 1, U, w, ones, V, part, outD, sv));
+    RC(blml_group_matvec_masked(gV, d_fid, Fa_, d_live, sv));
+    RC(blml_seg_lgrad_finish(dt, Fa_, S, 1, SV, U, w, nqA, gn, sv));
+    terms[0] = q; terms[1] = Sh[p];
+    RC(blml_seg_lincomb(dt, Fa_, S, 1, Sh[p], 2, cS, terms, sv));
+    terms[0] = g; terms[1] = gn; terms[2] = Yh[p];
+    RC(blml_seg_lincomb(dt, Fa_, S, 1, Yh[p], 3, cY, terms, sv));
+    RC(blml_seg_resid(dt, Fa_, S, 1, E, U, c, scrA, part, outE, sv));
+    a[0] = Sh[p]; b[0] = Yh[p]; a[1] = Sh[p]; b[1] = Sh[p]; a[2] = Yh[p]; b[2] = Yh[p];
+    for (int i = 0; i < m; i++) { a[3 + i] = Sh[i]; b[3 + i] = Yh[p]; a[3 + m + i] = Yh[i]; b[3 + m + i] = Yh[p]; }
+    RC(blml_seg_dots(dt, Fa_, S, 1, 3 + 2 * m, a, b, part, outA, sv));
+    terms[0] = gn; terms[1] = g;
+    RC(blml_seg_lincomb(dt, Fa_, S, 1, g, 2, cG, terms, sv));
+    k_lb_post<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, m, p, tol, ftol, cap, d_fid, d_live, d_segs_c, d_segs_eff, outA,
+                                              outD, outE, s);
+    KCHECK("lbfgs post");
+    return BLML_OK;
+  }
+
+  int setup() {
+    RC(all_live());
+    const int dt = dtype;
+    const blml_seg* S = d_segs_eff;
+    void* sv = st;
+    RC(blml_group_matvec_masked(gEU, d_fid, F, d_live, sv));
+    const void* a[1] = {E}; const void* b[1] = {U};
+    RC(blml_seg_dots(dt, F, S, 1, 1, a, b, part, outC, sv));
+    k_lbi_scale<<<nblk(F, 128), 128, 0, st>>>(F, d_fid, outC, s, sc, nqA, scrA);
+    KCHECK("lbfgs set-up");
+    const void* t1[1] = {E};
+    RC(blml_seg_lincomb(dt, F, S, 1, E, 1, sc, t1, sv));
+    t1[0] = U;
+    RC(blml_seg_lincomb(dt, F, S, 1, U, 1, sc, t1, sv));
+    RC(blml_seg_lgrad_weights(dt, F, S, 1, U, w, ones, V, part, outD, sv));
+    RC(blml_group_matvec_masked(gV, d_fid, F, d_live, sv));
+    RC(blml_seg_lgrad_finish(dt, F, S, 1, SV, U, w, nqA, gn, sv));
+    t1[0] = gn;
+    RC(blml_seg_lincomb(dt, F, S, 1, g, 1, ones, t1, sv));
+    RC(blml_seg_resid(dt, F, S, 1, E, U, c, scrA, part, outE, sv));
+    k_lbi_state<<<nblk(F, 128), 128, 0, st>>>(F, m, tol, cap, d_fid, d_live, d_segs_c, d_segs_eff, outD, outE, s);
+    KCHECK("lbfgs set-up");
+    return BLML_OK;
+  }
+
+  void release() {
+    if (gEU) blml_group_destroy(gEU);
+    if (gq) blml_group_destroy(gq);
+    if (gV) blml_group_destroy(gV);
+    base_free();
+  }
+};
+
+// ------------------------------------------------------------------------------------------------- start runner
+struct blml_start_batch_s : Runner {
+  int mA = 5;
+  double tol = 1e-5;
+  long long cap = LLONG_MAX, stall = 1000;
+  blml_group gEU = nullptr, gJ = nullptr, gA = nullptr;
+  double* E = nullptr;
+  const double *c = nullptr, *sg = nullptr;
+  double *U, *EJ, *UJ, *EA, *UA, *ET, *UT, *fv, *pX, *pF;
+  double *DX[AA_MMAX] = {}, *DF[AA_MMAX] = {};
+  double *part = nullptr, *outM1, *outM2, *outA, *outQ, *outR, *outDT;
+  double *c1m1, *ones, *cA, *cT, *cE, *scA, *s0c;
+  int *useA, *damp;
+  std::vector<double> s0_host;
+  StState s{};
+
+  int rescale_post(int init) {
+    const blml_seg* S = d_segs_eff;
+    void* sv = st;
+    const int Fa_ = Fa;
+    const void* a[1] = {E}; const void* b[1] = {U};
+    RC(blml_seg_dots(BLML_F64, Fa_, S, 0, 1, a, b, part, outQ, sv));
+    k_st_scale<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, outQ, s.n, scA);
+    KCHECK("start scale");
+    const void* t1[1] = {E};
+    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, E, 1, scA, t1, sv));
+    t1[0] = U;
+    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, U, 1, scA, t1, sv));
+    RC(blml_seg_merit(BLML_F64, Fa_, S, 0, 0, E, U, c, sg, part, outM1, sv));
+    RC(blml_seg_resid(BLML_F64, Fa_, S, 0, E, U, c, ones, part, outR, sv));
+    k_st_post<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, init, tol, cap, stall, d_fid, d_live, d_segs_c, d_segs_eff,
+                                              outM1, outR, s);
+    KCHECK("start post");
+    return BLML_OK;
+  }
+
+  int iter(int p) {
+    const blml_seg* S = d_segs_eff;
+    void* sv = st;
+    const int Fa_ = Fa;
+    RC(blml_seg_update_real1(BLML_F64, Fa_, S, E, U, c, sg, s0c, EJ, sv));
+    RC(blml_group_matvec_masked(gJ, d_fid, Fa_, d_live, sv));
+    RC(blml_seg_merit(BLML_F64, Fa_, S, 0, 0, EJ, UJ, c, sg, part, outM1, sv));
+    const void* t[2 + 2 * AA_MMAX];
+    if (mA) {
+      t[0] = EJ; t[1] = E;
+      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, fv, 2, c1m1, t, sv));
+      t[0] = E; t[1] = pX;
+      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, DX[p], 2, c1m1, t, sv));
+      t[0] = fv; t[1] = pF;
+      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, DF[p], 2, c1m1, t, sv));
+      const void* a[2 * AA_MMAX]; const void* b[2 * AA_MMAX];
+      for (int q = 0; q < mA; q++) { a[q] = DF[p]; b[q] = DF[q]; a[mA + q] = DF[q]; b[mA + q] = fv; }
+      RC(blml_seg_dots(BLML_F64, Fa_, S, 0, 2 * mA, a, b, part, outA, sv));
+      t[0] = E;
+      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, pX, 1, ones, t, sv));
+      t[0] = fv;
+      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, pF, 1, ones, t, sv));
+      k_st_anderson<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, mA, p, d_fid, d_live, outM1, outA, s, cA, useA);
+      KCHECK("start anderson");
+      t[0] = E; t[1] = fv;
+      for (int q = 0; q < mA; q++) { t[2 + q] = DX[q]; t[2 + mA + q] = DF[q]; }
+      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, EA, 2 + 2 * mA, cA, t, sv));
+      RC(blml_group_matvec_masked(gA, d_fid, Fa_, d_live, sv));
+      RC(blml_seg_merit(BLML_F64, Fa_, S, 0, 0, EA, UA, c, sg, part, outM2, sv));
+    }
+    k_st_take<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, mA, d_fid, d_live, outM1, outM2, useA, s, cT, damp);
+    KCHECK("start take");
+    t[0] = EA; t[1] = EJ;
+    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, ET, 2, cT, t, sv));
+    t[0] = UA; t[1] = UJ;
+    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, UT, 2, cT, t, sv));
+    k_st_damp_trials<<<dim3(SEG_BLOCKS, (unsigned)Fa_), 256, 0, st>>>(S, damp, E, EJ, U, UJ, c, sg, part);
+    KCHECK("start damping trials");
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 3 * DAMP_NT, damp, outDT);
+    KCHECK("start damping finish");
+    k_st_damp_pick<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, damp, outDT, s, cE);
+    KCHECK("start damping pick");
+    t[0] = E; t[1] = EJ; t[2] = ET;
+    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, E, 3, cE, t, sv));
+    t[0] = U; t[1] = UJ; t[2] = UT;
+    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, U, 3, cE, t, sv));
+    return rescale_post(0);
+  }
+
+  // the kernel values K(0) of the compact set's fits, in compact order
+  int upload_s0() {
+    std::vector<double> v(Fa);
+    for (int j = 0; j < Fa; j++) v[j] = s0_host[ids[j]];
+    RC(cuda_status(cudaMemcpyAsync(s0c, v.data(), Fa * sizeof(double), cudaMemcpyHostToDevice, st), "start s0"));
+    return cuda_status(cudaStreamSynchronize(st), "start s0");
+  }
+
+  int setup() {
+    RC(all_live());
+    RC(upload_s0());
+    RC(blml_seg_start_root(BLML_F64, F, d_segs_eff, c, sg, s0c, E, st));
+    RC(blml_group_matvec_masked(gEU, d_fid, F, d_live, st));
+    return rescale_post(1);
+  }
+
+  void release() {
+    if (gEU) blml_group_destroy(gEU);
+    if (gJ) blml_group_destroy(gJ);
+    if (gA) blml_group_destroy(gA);
+    base_free();
+  }
+};
+
+static int make_group(int F, const blml_plan* plans, int xc, const void* x, void* y, const std::vector<int64_t>& off,
+                      blml_group* out) {
+  std::vector<int> nb(F, 1);
+  return blml_group_create(F, plans, nb.data(), xc, x, off.data(), y, off.data(), out);
+}
+
+extern "C" {
+
+int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_plan* plans, int m, double tol,
+                            double ll_tol, int64_t max_iters, const double* n, const void* w, const void* c, void* E,
+                            void* U, blml_lbfgs_batch* out) {
+  if ((dtype != BLML_F64 && dtype != BLML_F32) || F < 1 || F > 65535 || !segs || !plans || !n || !w || !c || !E ||
+      !U || !out || m < 1 || m > LB_MMAX) {
+    set_error("blml_lbfgs_batch_create: dtype, 1 <= F <= 65535 fits, 1 <= m <= 20 and every pointer");
+    return BLML_ERR_ARG;
+  }
+  int64_t tot = 0;
+  std::vector<int64_t> off(F);
+  for (int f = 0; f < F; f++) {
+    if (segs[f].K != 1 || segs[f].B < 1) { set_error("blml_lbfgs_batch_create: one mode per fit"); return BLML_ERR_ARG; }
+    if (!plans[f] || plans[f]->dtype != dtype) { set_error("blml_lbfgs_batch_create: plan dtype"); return BLML_ERR_ARG; }
+    off[f] = segs[f].off;
+    tot = std::max<int64_t>(tot, segs[f].off + segs[f].B);
+  }
+  blml_lbfgs_batch_s* r = new blml_lbfgs_batch_s();
+  r->m = m; r->dtype = dtype; r->tol = tol; r->ftol = ll_tol; r->cap = max_iters < 0 ? LLONG_MAX : max_iters;
+  r->E = E; r->U = U; r->w = w; r->c = c;
+  int rc = r->base_init(F, segs);
+  const size_t esz = dtype == BLML_F64 ? 16 : 8;
+  char* vec = rc ? nullptr : (char*)r->dalloc((6 + 2 * (size_t)m) * tot * esz);
+  if (!rc && !vec) { set_error("blml_lbfgs_batch_create: vector allocation"); rc = BLML_ERR_CUDA; }
+  if (!rc) {
+    void** v6[6] = {&r->g, &r->gn, &r->q, &r->Sq, &r->V, &r->SV};
+    for (int i = 0; i < 6; i++) *v6[i] = vec + (size_t)i * tot * esz;
+    for (int i = 0; i < m; i++) {
+      r->Sh[i] = vec + (6 + (size_t)i) * tot * esz;
+      r->Yh[i] = vec + (6 + (size_t)m + i) * tot * esz;
+    }
+    cudaMemsetAsync(vec, 0, (6 + 2 * (size_t)m) * tot * esz, r->st);
+    const int nq = 48;                    // the widest reduction: blml_seg_dots' 48 accumulators
+    double* scr = (double*)r->dalloc(sizeof(double) * ((size_t)F * (nq * SEG_BLOCKS + 48 + 43 + 1 + 1 + 2 +
+                                                                   (1 + 2 * m) + 1 + 2 + 3 + 2 + 1 + 1 + 1 + 1)));
+    double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (7 + (LB_FWIN + 1) + 2 * (size_t)m * m));
+    int* ist = (int*)r->dalloc(sizeof(int) * ((size_t)F * (7 + m) + 1));
+    if (!scr || !stt || !ist) { set_error("blml_lbfgs_batch_create: allocation"); rc = BLML_ERR_CUDA; }
+    else {
+      double* x = scr;
+      auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
+      r->part = take((size_t)nq * SEG_BLOCKS); r->outA = take(48); r->outB = take(43); r->outC = take(1);
+      r->outD = take(1); r->outE = take(2); r->cq = take(1 + 2 * m); r->tA = take(1); r->cS = take(2);
+      r->cY = take(3); r->cG = take(2); r->nqA = take(1); r->scrA = take(1); r->ones = take(1); r->sc = take(1);
+      double* y = stt;
+      auto tk = [&](size_t k) { double* p = y; y += k * F; return p; };
+      r->s.L = tk(1); r->s.Q = tk(1); r->s.Qn = tk(1); r->s.n = tk(1); r->s.res = tk(1); r->s.slope = tk(1);
+      tk(1);
+      r->s.mh = tk(LB_FWIN + 1); r->s.SY = tk((size_t)m * m); r->s.YY = tk((size_t)m * m);
+      int* z = ist;
+      auto ti = [&](size_t k) { int* p = z; z += k * F; return p; };
+      r->s.active = ti(1); r->s.it = ti(1); r->s.stop = ti(1); r->s.reset = ti(1); r->s.nh = ti(1); r->s.ok = ti(1);
+      ti(1);
+      r->s.stamp = ti(m); r->s.step = z;
+      k_fill_double<<<nblk(F, 256), 256, 0, r->st>>>(r->ones, F, 1.0);
+      rc = cuda_status(cudaMemcpyAsync(r->s.n, n, F * sizeof(double), cudaMemcpyHostToDevice, r->st), "lbfgs n");
+      if (!rc) rc = cuda_status(cudaStreamSynchronize(r->st), "lbfgs create");
+    }
+  }
+  if (!rc) rc = make_group(F, plans, 1, E, U, off, &r->gEU);
+  if (!rc) rc = make_group(F, plans, 1, r->q, r->Sq, off, &r->gq);
+  if (!rc) rc = make_group(F, plans, 1, r->V, r->SV, off, &r->gV);
+  if (rc) { r->release(); delete r; return rc; }
+  *out = r;
+  return BLML_OK;
+}
+
+int blml_lbfgs_batch_run(blml_lbfgs_batch r, void* stream) {
+  if (!r) { set_error("blml_lbfgs_batch_run: null runner"); return BLML_ERR_ARG; }
+  RC(r->begin(stream));
+  RC(r->setup());
+  RC(r->run_rings(r->m, [r](int i) { return r->iter(i); }, [] { return (int)BLML_OK; }));
+  return r->end(stream);
+}
+
+int blml_lbfgs_batch_result(blml_lbfgs_batch r, int64_t* iters, int32_t* stop, double* L, double* Q, double* res) {
+  if (!r) { set_error("blml_lbfgs_batch_result: null runner"); return BLML_ERR_ARG; }
+  const int F = r->F;
+  std::vector<int> it(F), sp(F);
+  RC(cuda_status(cudaStreamSynchronize(r->st), "lbfgs result"));
+  RC(cuda_status(cudaMemcpy(it.data(), r->s.it, F * sizeof(int), cudaMemcpyDeviceToHost), "lbfgs result"));
+  RC(cuda_status(cudaMemcpy(sp.data(), r->s.stop, F * sizeof(int), cudaMemcpyDeviceToHost), "lbfgs result"));
+  if (L) RC(cuda_status(cudaMemcpy(L, r->s.L, F * sizeof(double), cudaMemcpyDeviceToHost), "lbfgs result"));
+  if (Q) RC(cuda_status(cudaMemcpy(Q, r->s.Q, F * sizeof(double), cudaMemcpyDeviceToHost), "lbfgs result"));
+  if (res) RC(cuda_status(cudaMemcpy(res, r->s.res, F * sizeof(double), cudaMemcpyDeviceToHost), "lbfgs result"));
+  for (int f = 0; f < F; f++) {
+    if (iters) iters[f] = it[f];
+    if (stop) stop[f] = sp[f];
+  }
+  return BLML_OK;
+}
+
+int blml_lbfgs_batch_stats(blml_lbfgs_batch r, int64_t* out4) {
+  if (!r || !out4) { set_error("blml_lbfgs_batch_stats: bad arguments"); return BLML_ERR_ARG; }
+  out4[0] = r->steps; out4[1] = r->replays; out4[2] = r->rebuilds; out4[3] = r->nodes;
+  return BLML_OK;
+}
+
+int blml_lbfgs_batch_destroy(blml_lbfgs_batch r) {
+  if (!r) return BLML_OK;
+  r->release();
+  delete r;
+  return BLML_OK;
+}
+
+int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans, int mA, double tol,
+                            int64_t max_sweeps, int64_t stall, const double* n, const double* s0, const double* c,
+                            const double* sg, double* E, blml_start_batch* out) {
+  if (F < 1 || F > 65535 || !segs || !plans || !n || !s0 || !c || !sg || !E || !out || mA < 0 || mA > AA_MMAX) {
+    set_error("blml_start_batch_create: 1 <= F <= 65535 fits, 0 <= anderson <= 8 and every pointer");
+    return BLML_ERR_ARG;
+  }
+  int64_t tot = 0;
+  std::vector<int64_t> off(F);
+  for (int f = 0; f < F; f++) {
+    if (segs[f].K != 1 || segs[f].B < 1) { set_error("blml_start_batch_create: one mode per fit"); return BLML_ERR_ARG; }
+    if (!plans[f] || plans[f]->dtype != BLML_F64) { set_error("blml_start_batch_create: float64 plans"); return BLML_ERR_ARG; }
+    off[f] = segs[f].off;
+    tot = std::max<int64_t>(tot, segs[f].off + segs[f].B);
+  }
+  blml_start_batch_s* r = new blml_start_batch_s();
+  r->mA = mA; r->tol = tol; r->cap = max_sweeps < 0 ? LLONG_MAX : max_sweeps; r->stall = stall;
+  r->E = E; r->c = c; r->sg = sg;
+  r->s0_host.assign(s0, s0 + F);
+  int rc = r->base_init(F, segs);
+  double* vec = rc ? nullptr : (double*)r->dalloc((10 + 2 * (size_t)mA) * tot * sizeof(double));
+  if (!rc && !vec) { set_error("blml_start_batch_create: vector allocation"); rc = BLML_ERR_CUDA; }
+  if (!rc) {
+    double** v10[10] = {&r->U, &r->EJ, &r->UJ, &r->EA, &r->UA, &r->ET, &r->UT, &r->fv, &r->pX, &r->pF};
+    for (int i = 0; i < 10; i++) *v10[i] = vec + (size_t)i * tot;
+    for (int i = 0; i < mA; i++) { r->DX[i] = vec + (10 + (size_t)i) * tot; r->DF[i] = vec + (10 + (size_t)mA + i) * tot; }
+    cudaMemsetAsync(vec, 0, (10 + 2 * (size_t)mA) * tot * sizeof(double), r->st);
+    const int nq = 3 * DAMP_NT;           // the widest reduction: the damping trials' 78 quantities
+    double* scr = (double*)r->dalloc(sizeof(double) * (size_t)F *
+                                     (nq * SEG_BLOCKS + 3 + 3 + 2 * AA_MMAX + 1 + 2 + nq + 2 + 1 + (2 + 2 * AA_MMAX) +
+                                      2 + 3 + 1 + 1));
+    double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (8 + (size_t)AA_MMAX * AA_MMAX));
+    int* ist = (int*)r->dalloc(sizeof(int) * (size_t)F * (6 + AA_MMAX + 2));
+    if (!scr || !stt || !ist) { set_error("blml_start_batch_create: allocation"); rc = BLML_ERR_CUDA; }
+    else {
+      double* x = scr;
+      auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
+      r->part = take((size_t)nq * SEG_BLOCKS); r->outM1 = take(3); r->outM2 = take(3); r->outA = take(2 * AA_MMAX);
+      r->outQ = take(1); r->outR = take(2); r->outDT = take(nq); r->c1m1 = take(2); r->ones = take(1);
+      r->cA = take(2 + 2 * AA_MMAX); r->cT = take(2); r->cE = take(3); r->scA = take(1); r->s0c = take(1);
+      double* y = stt;
+      auto tk = [&](size_t k) { double* p = y; y += k * F; return p; };
+      r->s.n = tk(1); r->s.s0 = tk(1); r->s.cur = tk(1); r->s.res = tk(1); r->s.best_res = tk(1); r->s.best_m = tk(1);
+      r->s.mJ = tk(1); tk(1); r->s.G = tk((size_t)AA_MMAX * AA_MMAX);
+      int* z = ist;
+      auto ti = [&](size_t k) { int* p = z; z += k * F; return p; };
+      r->s.valid = ti(AA_MMAX); r->s.has_prev = ti(1); r->s.best_it = ti(1); r->s.it = ti(1); r->s.active = ti(1);
+      r->useA = ti(1); r->damp = ti(1);
+      std::vector<double> cm(2 * (size_t)F);
+      for (int f = 0; f < F; f++) { cm[2 * f] = 1.0; cm[2 * f + 1] = -1.0; }
+      rc = cuda_status(cudaMemcpyAsync(r->c1m1, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, r->st),
+                       "start");
+      k_fill_double<<<nblk(F, 256), 256, 0, r->st>>>(r->ones, F, 1.0);
+      cudaMemsetAsync(r->s.G, 0, sizeof(double) * (size_t)F * AA_MMAX * AA_MMAX, r->st);
+      cudaMemsetAsync(r->s.valid, 0, sizeof(int) * (size_t)F * AA_MMAX, r->st);
+      cudaMemsetAsync(r->outM2, 0, sizeof(double) * 3 * (size_t)F, r->st);
+      cudaMemsetAsync(r->useA, 0, sizeof(int) * (size_t)F, r->st);
+      if (!rc) rc = cuda_status(cudaMemcpyAsync(r->s.n, n, F * sizeof(double), cudaMemcpyHostToDevice, r->st), "start n");
+      if (!rc) rc = cuda_status(cudaStreamSynchronize(r->st), "start create");
+    }
+  }
+  if (!rc) rc = make_group(F, plans, 0, E, r->U, off, &r->gEU);
+  if (!rc) rc = make_group(F, plans, 0, r->EJ, r->UJ, off, &r->gJ);
+  if (!rc) rc = make_group(F, plans, 0, r->EA, r->UA, off, &r->gA);
+  if (rc) { r->release(); delete r; return rc; }
+  *out = r;
+  return BLML_OK;
+}
+
+int blml_start_batch_run(blml_start_batch r, void* stream) {
+  if (!r) { set_error("blml_start_batch_run: null runner"); return BLML_ERR_ARG; }
+  RC(r->begin(stream));
+  RC(r->setup());
+  const int ring = r->mA > 0 ? r->mA : 1;
+  RC(r->run_rings(ring, [r](int i) { return r->iter(i); }, [r] { return r->upload_s0(); }));
+  return r->end(stream);
+}
+
+int blml_start_batch_result(blml_start_batch r, int64_t* sweeps, double* res) {
+  if (!r) { set_error("blml_start_batch_result: null runner"); return BLML_ERR_ARG; }
+  const int F = r->F;
+  std::vector<int> it(F);
+  RC(cuda_status(cudaStreamSynchronize(r->st), "start result"));
+  RC(cuda_status(cudaMemcpy(it.data(), r->s.it, F * sizeof(int), cudaMemcpyDeviceToHost), "start result"));
+  if (res) RC(cuda_status(cudaMemcpy(res, r->s.res, F * sizeof(double), cudaMemcpyDeviceToHost), "start result"));
+  if (sweeps)
+    for (int f = 0; f < F; f++) sweeps[f] = it[f];
+  return BLML_OK;
+}
+
+int blml_start_batch_stats(blml_start_batch r, int64_t* out4) {
+  if (!r || !out4) { set_error("blml_start_batch_stats: bad arguments"); return BLML_ERR_ARG; }
+  out4[0] = r->steps; out4[1] = r->replays; out4[2] = r->rebuilds; out4[3] = r->nodes;
+  return BLML_OK;
+}
+
+int blml_start_batch_destroy(blml_start_batch r) {
+  if (!r) return BLML_OK;
+  r->release();
+  delete r;
+  return BLML_OK;
+}
+
+}

@@ -6,48 +6,9 @@
 // block partials summed in a fixed order by blml_seg_finish.
 #include "common.cuh"
 #include "plan.cuh"
+#include "segmented.cuh"
 
 namespace blml {
-
-struct SegView { const blml_seg* s; };
-
-template <typename T, bool CPLX>
-struct SAcc {
-  static __device__ __forceinline__ void get(const void* p, int64_t i, double& re, double& im) {
-    if (CPLX) { const cpx<T> v = reinterpret_cast<const cpx<T>*>(p)[i]; re = (double)v.re; im = (double)v.im; }
-    else { re = (double)reinterpret_cast<const T*>(p)[i]; im = 0.0; }
-  }
-  static __device__ __forceinline__ void put(void* p, int64_t i, double re, double im) {
-    if (CPLX) reinterpret_cast<cpx<T>*>(p)[i] = cpx<T>{(T)re, (T)im};
-    else reinterpret_cast<T*>(p)[i] = (T)re;
-  }
-};
-
-#define SEG_LOOP(b, sg) for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < (sg).B; \
-                             b += (int64_t)gridDim.x * blockDim.x)
-
-// partials layout, quantity-major so it does not depend on how many accumulators a kernel carries:
-// part[((q * F) + f) * gridDim.x + blockIdx.x], F = gridDim.y fits
-template <int NQ>
-__device__ __forceinline__ void seg_partials(double (&v)[NQ], double* part, unsigned maxmask = 0u) {
-  __shared__ double sh[NQ][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NQ; q++) {
-    double x = ((maxmask >> q) & 1u) ? warp_max(v[q]) : warp_sum(v[q]);
-    if (lane == 0) sh[q][wid] = x;
-  }
-  __syncthreads();
-  if (wid == 0) {
-#pragma unroll
-    for (int q = 0; q < NQ; q++) {
-      const bool mx = (maxmask >> q) & 1u;
-      double x = lane < nw ? sh[q][lane] : (mx ? -INFINITY : 0.0);
-      x = mx ? warp_max(x) : warp_sum(x);
-      if (lane == 0) part[((int64_t)q * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = x;
-    }
-  }
-}
 
 // one block per fit: out[f * nq + q] = fixed-order reduction of its partials (F = gridDim.x fits)
 __global__ void k_seg_finish(const double* part, int nq, int nblk, unsigned maxmask, double* out) {
@@ -92,8 +53,6 @@ __global__ void k_seg_finish_strided(const double* part, int nq, int nblk, doubl
     __syncthreads();
   }
 }
-
-constexpr int SEG_BLOCKS = 16;        // blocks per fit (x); 64 fits x 16 blocks x 256 threads covers a B200 ~2 times
 
 template <typename T>
 __global__ void k_seg_start_root(const blml_seg* segs, const T* c, const T* sg, const double* s0, T* e0) {
@@ -179,7 +138,7 @@ __global__ void k_seg_resid(const blml_seg* segs, const void* E, const void* U, 
   seg_partials<2>(v, part, 1u);
 }
 
-struct SegPairs { const void* a[16]; const void* b[16]; };
+struct SegPairs { const void* a[48]; const void* b[48]; };
 
 // per-fit real inner products over the fit's K B elements (complex: 2 K B reals)
 template <typename T, int NP>
@@ -373,7 +332,9 @@ static void seg_dots_launch(dim3 g, const blml_seg* s, int cplx, int np, const S
   else if (np <= 2) k_seg_dots<T, 2><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
   else if (np <= 4) k_seg_dots<T, 4><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
   else if (np <= 8) k_seg_dots<T, 8><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
-  else k_seg_dots<T, 16><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else if (np <= 16) k_seg_dots<T, 16><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else if (np <= 24) k_seg_dots<T, 24><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
+  else k_seg_dots<T, 48><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
 }
 
 }  // namespace blml
@@ -452,18 +413,14 @@ int blml_seg_dots(int dtype, int F, const blml_seg* segs, int cplx, int npairs, 
                   const void* const* b, double* part, double* out, void* stream) {
   if (seg_args(dtype, F, segs, "blml_seg_dots")) return BLML_ERR_ARG;
   if (npairs < 1 || npairs > 48) { set_error("blml_seg_dots: 1..48 pairs"); return BLML_ERR_ARG; }
-  // 16 accumulators per pass; the passes write fit-major slices out[f * npairs + q0 ...] via a strided finish
-  for (int q0 = 0; q0 < npairs; q0 += 16) {
-    const int np = std::min(16, npairs - q0);
-    SegPairs pp;
-    for (int q = 0; q < 16; q++) { pp.a[q] = q < np ? a[q0 + q] : nullptr; pp.b[q] = q < np ? b[q0 + q] : nullptr; }
-    double* pt = part + (size_t)q0 * F * SEG_BLOCKS;
-    if (dtype == BLML_F64) seg_dots_launch<double>(SGRID(F), segs, cplx, np, pp, pt, SST);
-    else seg_dots_launch<float>(SGRID(F), segs, cplx, np, pp, pt, SST);
-    BLML_CHECK_LAUNCH("blml_seg_dots");
-    k_seg_finish_strided<<<F, 256, 0, SST>>>(pt, np, SEG_BLOCKS, out + q0, npairs);
-    BLML_CHECK_LAUNCH("blml_seg_dots finish");
-  }
+  // one pass (at most 48 accumulators per thread); out[f * npairs + q]
+  SegPairs pp;
+  for (int q = 0; q < 48; q++) { pp.a[q] = q < npairs ? a[q] : nullptr; pp.b[q] = q < npairs ? b[q] : nullptr; }
+  if (dtype == BLML_F64) seg_dots_launch<double>(SGRID(F), segs, cplx, npairs, pp, part, SST);
+  else seg_dots_launch<float>(SGRID(F), segs, cplx, npairs, pp, part, SST);
+  BLML_CHECK_LAUNCH("blml_seg_dots");
+  k_seg_finish_strided<<<F, 256, 0, SST>>>(part, npairs, SEG_BLOCKS, out, npairs);
+  BLML_CHECK_LAUNCH("blml_seg_dots finish");
   return BLML_OK;
 }
 

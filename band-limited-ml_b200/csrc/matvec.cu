@@ -197,10 +197,14 @@ struct StageDesc {
 constexpr int GR = 32, GN = 32, GK = 16;
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_contract_grouped(const StageDesc* __restrict__ descs) {
+__global__ void __launch_bounds__(256) k_contract_grouped(const StageDesc* __restrict__ descs,
+                                                          const int* __restrict__ subset,
+                                                          const int* __restrict__ live) {
   __shared__ cpx<T> Xs[GK][GR + 1];
   __shared__ cpx<T> Ts[GK][GN + 1];
-  const StageDesc D = descs[blockIdx.z];
+  const int gi = subset ? subset[blockIdx.z] : blockIdx.z;
+  if (live && !live[gi]) return;                       // uniform per CTA: a problem that has stopped
+  const StageDesc D = descs[gi];
   const int64_t rows = D.R * D.nb;
   const int64_t r0 = (int64_t)blockIdx.x * GR;
   const int n0 = blockIdx.y * GN;
@@ -252,13 +256,123 @@ __global__ void __launch_bounds__(256) k_contract_grouped(const StageDesc* __res
     }
 }
 
+// The same stage with 64 x 64 output tiles (4 x 4 outputs per thread) and the operand tiles staged by cp.async into
+// a double buffer, the next K slice loading while the current one is multiplied; for launches with enough tiles to
+// fill the GPU. Dynamic shared memory: 2 buffers x (X tile + T tile), BK x (64 + 1) complex each.
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? bytes : 0;                 // 0: nothing read, the destination is zero-filled
+  if (bytes == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+  else if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+constexpr int BR = 64, BN = 64, BK = 16, BLD = 65;
+template <typename T>
+constexpr size_t big_smem() { return 2 * 2 * (size_t)BK * BLD * sizeof(cpx<T>); }
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_contract_grouped_big(const StageDesc* __restrict__ descs,
+                                                                 const int* __restrict__ subset,
+                                                                 const int* __restrict__ live) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<T>* Xs = reinterpret_cast<cpx<T>*>(smem_raw);             // [2][BK][BLD]
+  cpx<T>* Ts = Xs + 2 * BK * BLD;                                // [2][BK][BLD]
+  const int gi = subset ? subset[blockIdx.z] : blockIdx.z;
+  if (live && !live[gi]) return;
+  const StageDesc D = descs[gi];
+  const int64_t rows = D.R * D.nb;
+  const int64_t r0 = (int64_t)blockIdx.x * BR;
+  const int n0 = blockIdx.y * BN;
+  if (r0 >= rows || n0 >= D.N) return;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const bool xreal = D.flags & 1;
+  const int M = D.M, N = D.N;
+  const cpx<T>* Tw = reinterpret_cast<const cpx<T>*>(D.T);
+  if (xreal) {                                   // real input: cp.async fills .re only, .im stays zero
+    for (int i = tid; i < 2 * BK * BLD; i += 256) Xs[i] = cpx<T>{T(0), T(0)};
+    __syncthreads();
+  }
+  auto load = [&](int buf, int m0) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) {              // X tile: BR rows x BK (m); m = tid % 16, row = tid / 16 + 16 i
+      const int mm = tid & 15, rr = (tid >> 4) + 16 * i;
+      const int64_t rho = r0 + rr; const int m = m0 + mm;
+      const bool ok = rho < rows && m < M;
+      cpx<T>* dst = Xs + ((size_t)buf * BK + mm) * BLD + rr;
+      if (xreal) {
+        const T* src = reinterpret_cast<const T*>(D.X) + (ok ? rho * M + m : 0);
+        cp_async(&dst->re, src, (int)sizeof(T), ok);
+      } else {
+        const cpx<T>* src = reinterpret_cast<const cpx<T>*>(D.X) + (ok ? rho * M + m : 0);
+        cp_async(dst, src, (int)sizeof(cpx<T>), ok);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {              // T tile: BK (m) x BN; n = tid % 64, m = tid / 64 + 4 i
+      const int nn = tid & 63, mm = (tid >> 6) + 4 * i;
+      const int n = n0 + nn, m = m0 + mm;
+      const bool ok = n < N && m < M;
+      cp_async(Ts + ((size_t)buf * BK + mm) * BLD + nn, Tw + (ok ? (int64_t)m * N + n : 0), (int)sizeof(cpx<T>), ok);
+    }
+    cp_async_commit();
+  };
+  cpx<T> acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = {T(0), T(0)};
+  const int nk = (M + BK - 1) / BK;
+  load(0, 0);
+  for (int kt = 0; kt < nk; kt++) {
+    const int buf = kt & 1;
+    if (kt + 1 < nk) { load(buf ^ 1, (kt + 1) * BK); cp_async_wait<1>(); }
+    else cp_async_wait<0>();
+    __syncthreads();
+    const cpx<T>* xs = Xs + (size_t)buf * BK * BLD;
+    const cpx<T>* ts = Ts + (size_t)buf * BK * BLD;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk++) {
+      cpx<T> a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = xs[kk * BLD + tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = ts[kk * BLD + ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = cfma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();                             // the buffer is refilled by the next iteration's load
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int n = n0 + ty + 16 * j;
+    if (n >= N) continue;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int64_t rho = r0 + tx + 16 * i;
+      if (rho >= rows) continue;
+      const int64_t b = rho / D.R, r = rho - b * D.R;
+      const int64_t o = b * (int64_t)N * D.R + (int64_t)n * D.R + r;
+      cpx<T> v = acc[i][j];
+      if (D.flags & 2) { const T wv = reinterpret_cast<const T*>(D.W)[(int64_t)n * D.R + r]; v.re *= wv; v.im *= wv; }
+      if (D.flags & 4) reinterpret_cast<T*>(D.Y)[o] = v.re;
+      else reinterpret_cast<cpx<T>*>(D.Y)[o] = v;
+    }
+  }
+}
+
 }  // namespace blml
 
 // a set of mat-vecs applied together: per stage a device array of descriptors and the grid that covers them
 struct blml_group_s {
   int G, d_max, dtype, nstages;
   std::vector<blml::StageDesc*> dev;    // one descriptor array per stage index
-  std::vector<dim3> grids;
+  std::vector<dim3> grids, grids_big;   // 32 x 32 and 64 x 64 tile grids per stage
+  std::vector<double> tiles_big;        // 64 x 64 tiles of a stage over all problems
   void* ws;                             // the group's own intermediate buffers
 };
 
@@ -363,6 +477,13 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
     if (!plans[g] || plans[g]->d != d || plans[g]->dtype != dtype || nbatch[g] < 1) {
       set_error("blml_group_create: every plan of a group has one dimension count and dtype"); return BLML_ERR_ARG;
     }
+  // the 64 x 64 stage kernel's dynamic shared memory (set here, outside any stream capture)
+  int e0 = cuda_status(cudaFuncSetAttribute(k_contract_grouped_big<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)big_smem<double>()), "blml_group_create");
+  if (!e0) e0 = cuda_status(cudaFuncSetAttribute(k_contract_grouped_big<float>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem<float>()),
+                            "blml_group_create");
+  if (e0) return e0;
   const size_t esz = dtype == BLML_F64 ? 16 : 8, rsz = dtype == BLML_F64 ? 8 : 4;
   const size_t xsz = x_complex ? esz : rsz, ysz = x_complex ? esz : rsz;
   std::vector<size_t> wso(G + 1, 0);
@@ -374,6 +495,7 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
   }
   std::vector<std::vector<StageDesc>> host(2 * d, std::vector<StageDesc>(G));
   std::vector<int64_t> maxr(2 * d, 0), maxn(2 * d, 0);
+  grp->tiles_big.assign(2 * d, 0.0);
   for (int g = 0; g < G; g++) {
     const blml_plan_s* p = plans[g];
     std::vector<int64_t> dims(p->shape, p->shape + d);
@@ -392,6 +514,7 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
       D.R = R; D.M = (int)M; D.N = (int)N; D.nb = nbatch[g];
       D.flags = ((s == 0 && !x_complex) ? 1 : 0) | ((s == d - 1) ? 2 : 0) | ((last && !x_complex) ? 4 : 0);
       maxr[s] = std::max(maxr[s], R * nbatch[g]); maxn[s] = std::max<int64_t>(maxn[s], N);
+      grp->tiles_big[s] += (double)((R * nbatch[g] + BR - 1) / BR) * (double)((N + BN - 1) / BN);
       dims.pop_back(); dims.insert(dims.begin(), N);
       cur = outp;
     }
@@ -402,6 +525,7 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
     if (cudaMalloc(&grp->dev[s], G * sizeof(StageDesc)) != cudaSuccess) { set_error("blml_group_create: allocation"); e = BLML_ERR_CUDA; break; }
     e = cuda_status(cudaMemcpy(grp->dev[s], host[s].data(), G * sizeof(StageDesc), cudaMemcpyHostToDevice), "blml_group_create");
     grp->grids.push_back(dim3((unsigned)((maxr[s] + GR - 1) / GR), (unsigned)((maxn[s] + GN - 1) / GN), (unsigned)G));
+    grp->grids_big.push_back(dim3((unsigned)((maxr[s] + BR - 1) / BR), (unsigned)((maxn[s] + BN - 1) / BN), (unsigned)G));
   }
   if (e) { blml_group_destroy(grp); return e; }
   *out = grp;
@@ -409,11 +533,27 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
 }
 
 int blml_group_matvec(blml_group grp, void* stream) {
+  return blml_group_matvec_masked(grp, nullptr, grp ? grp->G : 0, nullptr, stream);
+}
+
+int blml_group_matvec_masked(blml_group grp, const int* subset, int n, const int* live, void* stream) {
   if (!grp) { set_error("blml_group_matvec: null group"); return BLML_ERR_ARG; }
+  if (n < 0 || n > grp->G) { set_error("blml_group_matvec_masked: 0 <= n <= G"); return BLML_ERR_ARG; }
+  if (n == 0) return BLML_OK;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   for (int s = 0; s < grp->nstages; s++) {
-    if (grp->dtype == BLML_F64) k_contract_grouped<double><<<grp->grids[s], 256, 0, st>>>(grp->dev[s]);
-    else k_contract_grouped<float><<<grp->grids[s], 256, 0, st>>>(grp->dev[s]);
+    // 64 x 64 tiles when the launch has enough of them to fill the GPU twice over (the problems of a subset are
+    // taken as average ones), else 32 x 32
+    const bool big = grp->tiles_big[s] * n / grp->G >= 2.0 * 148;
+    dim3 g = big ? grp->grids_big[s] : grp->grids[s]; g.z = (unsigned)n;
+    if (big) {
+      if (grp->dtype == BLML_F64)
+        k_contract_grouped_big<double><<<g, 256, big_smem<double>(), st>>>(grp->dev[s], subset, live);
+      else k_contract_grouped_big<float><<<g, 256, big_smem<float>(), st>>>(grp->dev[s], subset, live);
+    } else {
+      if (grp->dtype == BLML_F64) k_contract_grouped<double><<<g, 256, 0, st>>>(grp->dev[s], subset, live);
+      else k_contract_grouped<float><<<g, 256, 0, st>>>(grp->dev[s], subset, live);
+    }
     BLML_CHECK_LAUNCH("blml_group_matvec");
   }
   return BLML_OK;

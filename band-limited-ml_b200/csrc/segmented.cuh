@@ -1,0 +1,49 @@
+// Segmented-kernel helpers shared by the batched solver kernels (batched.cu) and the device-side control of the
+// batched engine (batch_runner.cu): fit f owns the slice [off_f, off_f + K_f B_f) of every flat mode array and
+// [boff_f, boff_f + B_f) of every flat bin array; blockIdx.y is the fit, blockIdx.x strides over its bins.
+#pragma once
+#include "common.cuh"
+
+namespace blml {
+
+constexpr int SEG_BLOCKS = 16;        // blocks per fit (x); 64 fits x 16 blocks x 256 threads covers a B200 ~2 times
+
+template <typename T, bool CPLX>
+struct SAcc {
+  static __device__ __forceinline__ void get(const void* p, int64_t i, double& re, double& im) {
+    if (CPLX) { const cpx<T> v = reinterpret_cast<const cpx<T>*>(p)[i]; re = (double)v.re; im = (double)v.im; }
+    else { re = (double)reinterpret_cast<const T*>(p)[i]; im = 0.0; }
+  }
+  static __device__ __forceinline__ void put(void* p, int64_t i, double re, double im) {
+    if (CPLX) reinterpret_cast<cpx<T>*>(p)[i] = cpx<T>{(T)re, (T)im};
+    else reinterpret_cast<T*>(p)[i] = (T)re;
+  }
+};
+
+#define SEG_LOOP(b, sg) for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < (sg).B; \
+                             b += (int64_t)gridDim.x * blockDim.x)
+
+// partials layout, quantity-major so it does not depend on how many accumulators a kernel carries:
+// part[((q * F) + f) * gridDim.x + blockIdx.x], F = gridDim.y fits
+template <int NQ>
+__device__ __forceinline__ void seg_partials(double (&v)[NQ], double* part, unsigned maxmask = 0u) {
+  __shared__ double sh[NQ][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    double x = ((maxmask >> q) & 1u) ? warp_max(v[q]) : warp_sum(v[q]);
+    if (lane == 0) sh[q][wid] = x;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      const bool mx = (maxmask >> q) & 1u;
+      double x = lane < nw ? sh[q][lane] : (mx ? -INFINITY : 0.0);
+      x = mx ? warp_max(x) : warp_sum(x);
+      if (lane == 0) part[((int64_t)q * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = x;
+    }
+  }
+}
+
+}  // namespace blml

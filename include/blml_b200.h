@@ -59,6 +59,10 @@ typedef struct blml_group_s* blml_group;
 int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_complex, const void* x_base,
                       const int64_t* x_off, void* y_base, const int64_t* y_off, blml_group* group);
 int blml_group_matvec(blml_group group, void* stream);
+/* the same for the n problems g = subset[i] (device int array; null: problems 0 .. n-1), skipping those with
+   live[g] == 0 (device int array over all G problems, or null), both read when the kernels run, so a captured CUDA
+   graph follows problems that stop between its replays */
+int blml_group_matvec_masked(blml_group group, const int* subset, int n, const int* live, void* stream);
 int blml_group_destroy(blml_group group);
 
 /* ---- coordinate (Jacobi) update of every bin (BLMLBinned._update / _secular / _cd_root,
@@ -132,7 +136,8 @@ int blml_cert_weights(int dtype, int K, int64_t B, int cplx, const void* E, cons
 /* ---- segmented (batched) solver kernels: F independent fits in lockstep, one launch per phase ----
  * Fit f owns elements [off, off + K B) of every flat mode array (its (K, B) block) and [boff, boff + B) of every flat
  * bin array (counts, signs); `segs` is a device array of F entries. Per-fit scalars are device arrays of F doubles
- * (coefficient tables: F x nterms). Reductions give out[f * nq + q] (part: F * nq * blml_seg_blocks() doubles).
+ * (coefficient tables: F x nterms). Reductions give out[f * nq + q] (part: F * nq * blml_seg_blocks() doubles;
+ * blml_seg_dots: F * 48 * blml_seg_blocks()).
  * These are the reference's single-fit operations (blml_binned.py:171-220, 278-355, 415-445, 630-645) applied to a
  * sweep of fits at once, as selector._search / the cut-off sweeps run them one after another. */
 typedef struct { int64_t off; int64_t boff; int64_t B; int32_t K; int32_t pad; } blml_seg;
@@ -166,6 +171,40 @@ int blml_seg_log_score(int dtype, int F, const blml_seg* segs, int cplx, const v
 int blml_seg_phases(int dtype, int F, const blml_seg* segs, double pn, const double* z, void* E, void* stream);
 int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const blml_seg* cplx_segs, const void* er,
                              void* E, void* stream);
+
+/* ---- batched solver phases with device-side control (one-mode fits, K = 1): the per-fit decisions of every
+ *      iteration run as kernels, a ring of iterations is one CUDA graph replayed until every fit has stopped, the
+ *      host reading one active mask per replay; the graph is captured again over the fits still iterating when
+ *      they fall to three quarters of those it covers. Stop codes: 0 tol, 1 ll_tol, 2 stall. ----
+ * L-BFGS ascent of L = sum w log F - n log Q from E (complex of dtype, the segs layout; U: S E is written there),
+ * memory m <= 20, Armijo over t = 2^-j, j < 40, U = S E recomputed at accepted steps, stop at max|rho| < tol, at a
+ * likelihood gain below ll_tol over 10 iterations, or after max_iters (< 0: none) -- blml_trivial.py:2590-2645
+ * (lbfgs_psd) as BLMLBinned.fit runs it (blml_binned.py:278-355, 429-445) for each fit of a cut-off sweep
+ * (selector.py:488-553). w, c: float of dtype per bin (counts / n and counts); n: F host doubles. */
+typedef struct blml_lbfgs_batch_s* blml_lbfgs_batch;
+int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_plan* plans, int m, double tol,
+                            double ll_tol, int64_t max_iters, const double* n, const void* w, const void* c, void* E,
+                            void* U, blml_lbfgs_batch* runner);
+int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);
+/* per fit (host arrays of F, any may be null): iterations, stop code, L, Q, max|rho| */
+int blml_lbfgs_batch_result(blml_lbfgs_batch runner, int64_t* iters, int32_t* stop, double* L, double* Q,
+                            double* res);
+/* [iterations enqueued, graph replays, graph captures, kernels per replay] */
+int blml_lbfgs_batch_stats(blml_lbfgs_batch runner, int64_t* out4);
+int blml_lbfgs_batch_destroy(blml_lbfgs_batch runner);
+/* the real rank-1 start of every fit in float64 (BLMLBinned._start with psd False, blml_binned.py:223-276): the
+ * seeded root, Jacobi updates with Anderson mixing (history anderson <= 8) and the merit safeguard, the damped
+ * step a = 2^-1 .. 2^-26 when no ascent, stop at max|rho| < tol, after `stall` sweeps without progress or after
+ * max_sweeps (< 0: none). c = w n, sg: float64 per bin; n, s0 (K(0) of each fit's kernel): F host doubles; E:
+ * float64 output in the segs layout. */
+typedef struct blml_start_batch_s* blml_start_batch;
+int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans, int anderson, double tol,
+                            int64_t max_sweeps, int64_t stall, const double* n, const double* s0, const double* c,
+                            const double* sg, double* E, blml_start_batch* runner);
+int blml_start_batch_run(blml_start_batch runner, void* stream);
+int blml_start_batch_result(blml_start_batch runner, int64_t* sweeps, double* res);
+int blml_start_batch_stats(blml_start_batch runner, int64_t* out4);
+int blml_start_batch_destroy(blml_start_batch runner);
 
 /* ---- pair accumulation over lattice bins from the row-kernel value tables (blml_local_gpu.rows / cols,
  *      blml_local_gpu.py:42-105, 320-361, 408-455; numba twins blml_local.py:117-191) ----
