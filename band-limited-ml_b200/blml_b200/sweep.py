@@ -2,18 +2,23 @@
 sweeps of dslit_job.py:158-171 and results/p3_window_pball.py:27-30) and rolling windows run their fits one after
 another through the reference's single-fit solver (blml_binned.py:223-355); here F fits of uneven lattice size and
 cut-off advance together, every phase one launch over all fits (csrc/batched.cu, grouped mat-vecs in
-csrc/matvec.cu), and the per-fit scalar control (Anderson weights, the L-BFGS direction, Armijo choices, stop rules)
-runs vectorised on the host with a fixed number of host syncs per iteration, whatever F is.
+csrc/matvec.cu). With control='device' (the default) the per-fit decisions (Anderson weights, the L-BFGS direction,
+Armijo choices, stop rules) run as kernels too and each phase is a CUDA graph of a ring of iterations, replayed until
+every fit has stopped (csrc/batch_runner.cu); control='host' makes the same decisions in vectorised NumPy with a few
+host syncs per iteration.
 
-    fits = BLMLBinnedBatch(tol=1e-6, dtype=np.float32).fit(counts_list, modes_list)   # complex_g, L-BFGS
+    batch = BLMLBinnedBatch(tol=1e-6, dtype=np.float64)
+    fits = batch.fit(counts_list, modes_list)              # complex_g, L-BFGS
     fits[i].loglik_, fits[i].density_, fits[i].n_sweeps_, fits[i].stop_reason_
-    scores = batch.log_density(val_counts_list)                                       # held-out scores
+    scores = batch.log_density(val_counts_list)            # held-out scores, one launch for all fits
 
 Each fit is the reference's algorithm: the real rank-1 start under the fit's kernel by Jacobi coordinate updates
 with Anderson mixing and the merit safeguard (in float64, see BLMLBinned._start), the seeded phases, L-BFGS ascent
 of L = sum w log F - n log Q with Armijo backtracking (the first of t = 1, 1/2, ..., 2^-39 that passes; all forty
-trials in one pass), memory 20, the canonical form at the end. One mode per fit (shared kernel), complex_g."""
+trials in one pass), memory 20, U = S E recomputed at every accepted step, the canonical form at the end. One mode
+per fit (shared kernel), complex_g."""
 import ctypes as C
+from collections import OrderedDict
 
 import numpy as np
 import torch
@@ -24,6 +29,9 @@ from .spec import parse_modes, spec_key
 from .operator import pad_rule, mode_transform, kernel_at_zero, Plan
 
 NT = 40
+_PLANS = OrderedDict()          # (kernel spec, lattice, dtype, device) -> (Plan, K(0))
+_PLAN_CACHE_SIZE = 512
+STOP_CODES = ('tol', 'll_tol', 'stall')
 
 
 class _Seg(C.Structure):
@@ -63,16 +71,34 @@ class _Group:
 class BLMLBinnedBatch:
     """F independent complex one-mode BLMLBinned fits (L-BFGS) in lockstep; see the module docstring."""
 
-    def __init__(self, tol=1e-5, max_sweeps=None, anderson=5, dtype=np.float32, phase_noise=0.1, seed=0, stall=1000,
-                 ll_tol=None, ll_window=100, lbfgs_m=20, device=None, verbose=False):
+    def __init__(self, tol=1e-5, max_sweeps=None, anderson=5, dtype=np.float64, phase_noise=0.1, seed=0, stall=1000,
+                 ll_tol=None, ll_window=100, lbfgs_m=20, device=None, verbose=False, control='device'):
         self.tol, self.max_sweeps, self.anderson = tol, max_sweeps, anderson
         self.dtype = np.dtype(dtype); self.phase_noise, self.seed, self.stall = phase_noise, seed, stall
         self.ll_tol, self.ll_window, self.lbfgs_m = ll_tol, ll_window, int(lbfgs_m)
         self.device = torch.device(device or 'cuda'); self.verbose = verbose
         if self.lbfgs_m > 20:
             raise ValueError("lbfgs_m: at most 20")
+        if control not in ('device', 'host'):
+            raise ValueError("control: 'device' (per-fit decisions in kernels, CUDA graphs) or 'host'")
+        if control == 'device' and not 0 <= anderson <= 8:
+            raise ValueError("anderson: 0..8 with control='device'")
+        self.control = control
 
     # ---------------------------------------------------------------- set-up
+    def _plan(self, sp, shape, code):
+        key = (spec_key(sp), tuple(shape), code, str(self.device))
+        hit = _PLANS.pop(key, None)
+        if hit is None:
+            h = np.ones(2)
+            freqs, W = mode_transform(sp, shape, h, pad_rule(shape, h, [sp]))
+            with torch.cuda.device(self.device):
+                hit = (Plan(freqs, W, shape, code, _lib.ENGINE_SIMT), kernel_at_zero(sp, 2))
+        _PLANS[key] = hit                                   # most recent last
+        while len(_PLANS) > _PLAN_CACHE_SIZE:
+            _PLANS.popitem(last=False)
+        return hit
+
     def _prepare(self, counts_list, modes_list):
         if not torch.cuda.is_available():
             raise _lib.BLMLError('BLMLBinnedBatch needs a CUDA device (no CPU path)')
@@ -85,47 +111,48 @@ class BLMLBinnedBatch:
         self.code = _lib.F32 if f32 else _lib.F64
         self.rt = torch.float32 if f32 else torch.float64
         self.ct = torch.complex64 if f32 else torch.complex128
-        shapes, specs, ws, ns, Bs = [], [], [], [], []
+        shapes, specs, parts = [], [], []
         for counts, modes in zip(counts_list, modes_list):
-            counts = np.asarray(counts, float)
-            if counts.ndim != 2 or np.any(counts < 0) or not np.all(np.isfinite(counts)):
+            if isinstance(counts, torch.Tensor):            # counts already on the device stay there
+                ct = counts.to(dev, torch.float64)
+            else:
+                ct = torch.as_tensor(np.asarray(counts, float)).to(dev)
+            if ct.ndim != 2:
                 raise ValueError("counts: non-negative finite 2-D arrays")
             sp, dep = parse_modes(modes, 2)
             if dep is not None or len(sp) != 1:
                 raise ValueError("BLMLBinnedBatch fits one mode per lattice (shared kernel)")
-            n = float(counts.sum())
-            if not n > 0:
-                raise ValueError("counts: no observations")
-            shapes.append(counts.shape); specs.append(sp[0]); ws.append(counts.ravel()); ns.append(n)
-            Bs.append(counts.size)
-        self.shapes, self.specs, self.n = shapes, specs, np.array(ns)
-        self.B = np.array(Bs, np.int64)
+            shapes.append(tuple(ct.shape)); specs.append(sp[0]); parts.append(ct.reshape(-1))
+        w64 = torch.cat(parts)
+        if bool(((w64 < 0) | ~torch.isfinite(w64)).any()):
+            raise ValueError("counts: non-negative finite 2-D arrays")
+        self.n = torch.stack([p.sum() for p in parts]).cpu().numpy()
+        if not np.all(self.n > 0):
+            raise ValueError("counts: no observations")
+        self.shapes, self.specs = shapes, specs
+        self.B = np.array([a * b for a, b in shapes], np.int64)
         boff = np.concatenate([[0], np.cumsum(self.B)])
         self.boff = boff
-        segs = (_Seg * F)(*[_Seg(int(boff[f]), int(boff[f]), int(self.B[f]), 1, 0) for f in range(F)])
+        self.segs_all = [_Seg(int(boff[f]), int(boff[f]), int(self.B[f]), 1, 0) for f in range(F)]
+        segs = (_Seg * F)(*self.segs_all)
         self.segs_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
-        Btot = int(boff[-1])
-        self.Btot = Btot
-        w = np.concatenate(ws)
-        self.w64 = torch.as_tensor(w, dtype=torch.float64).to(dev)
-        self.w = self.w64.to(self.rt)
-        self.c64 = (self.w64 * torch.as_tensor(np.repeat(self.n, self.B), dtype=torch.float64).to(dev))
+        self.Btot = int(boff[-1])
+        self.w64 = w64
+        self.w = w64.to(self.rt)
+        self.c64 = w64 * torch.as_tensor(np.repeat(self.n, self.B)).to(dev)
         self.c = self.c64.to(self.rt)
-        self.sg64 = torch.ones(Btot, dtype=torch.float64, device=dev); self.sg = self.sg64.to(self.rt)
+        self.sg64 = torch.ones(self.Btot, dtype=torch.float64, device=dev); self.sg = self.sg64.to(self.rt)
         nb = _lib.lib().blml_seg_blocks()
         self.part = torch.empty(48 * F * nb + 64, dtype=torch.float64, device=dev)
         self.out = torch.empty(48 * F + 64, dtype=torch.float64, device=dev)
         self.host = torch.empty(48 * F + 64, dtype=torch.float64, pin_memory=True)
-        # plans: float64 for the start, the fit dtype for the L-BFGS
-        self.p64, self.pfit, self.s = [], [], []
+        # plans (cached across batches): float64 for the start, the fit dtype for the L-BFGS
+        self.p64, self.pfit, s0 = [], [], []
         for shape, sp in zip(shapes, specs):
-            h = np.ones(2)
-            pad = pad_rule(shape, h, [sp])
-            freqs, W = mode_transform(sp, shape, h, pad)
-            self.p64.append(Plan(freqs, W, shape, _lib.F64, _lib.ENGINE_SIMT))
-            self.pfit.append(self.p64[-1] if not f32 else Plan(freqs, W, shape, _lib.F32, _lib.ENGINE_SIMT))
-            self.s.append(kernel_at_zero(sp, 2))
-        self.s = np.array(self.s)
+            p64, k0 = self._plan(sp, shape, _lib.F64)
+            self.p64.append(p64); s0.append(k0)
+            self.pfit.append(p64 if not f32 else self._plan(sp, shape, _lib.F32)[0])
+        self.s = np.array(s0)
         self.s_t = torch.as_tensor(self.s, dtype=torch.float64).to(dev)
         self.st = torch.cuda.current_stream(dev).cuda_stream
 
@@ -284,12 +311,62 @@ class BLMLBinnedBatch:
         self.start_sweeps_ = it
         return E
 
+    def _start_device(self):
+        """The same start with its per-fit decisions on the device (blml_start_batch_*: CUDA graphs of `anderson`
+        sweeps replayed until every fit has stopped)."""
+        F = self.F
+        E = torch.empty(self.Btot, dtype=torch.float64, device=self.device)
+        segs = (_Seg * F)(*self.segs_all)
+        plans = (C.c_void_p * F)(*[p._h.value for p in self.p64])
+        h = C.c_void_p()
+        n = np.ascontiguousarray(self.n, np.float64); s0 = np.ascontiguousarray(self.s, np.float64)
+        call('blml_start_batch_create', F, C.cast(segs, C.c_void_p), C.cast(plans, C.c_void_p), int(self.anderson),
+             float(self.tol), -1 if self.max_sweeps is None else int(self.max_sweeps), int(self.stall),
+             n.ctypes.data_as(C.c_void_p), s0.ctypes.data_as(C.c_void_p), self.c64.data_ptr(), self.sg64.data_ptr(),
+             E.data_ptr(), C.byref(h))
+        try:
+            call('blml_start_batch_run', h, self.st)
+            sweeps = np.zeros(F, np.int64)
+            call('blml_start_batch_result', h, sweeps.ctypes.data_as(C.c_void_p), None)
+            stats = np.zeros(4, np.int64)
+            call('blml_start_batch_stats', h, stats.ctypes.data_as(C.c_void_p))
+        finally:
+            _lib.lib().blml_start_batch_destroy(h)
+        self.start_sweeps_ = sweeps
+        self.start_stats_ = dict(zip(('sweeps', 'replays', 'captures', 'kernels_per_replay'), stats.tolist()))
+        return E
+
+    def _lbfgs_device(self, E):
+        """L-BFGS of every fit with its per-fit decisions on the device (blml_lbfgs_batch_*); returns U and the
+        per-fit iterations, stop reasons, L and residuals."""
+        F = self.F
+        U = torch.zeros_like(E)
+        segs = (_Seg * F)(*self.segs_all)
+        plans = (C.c_void_p * F)(*[p._h.value for p in self.pfit])
+        h = C.c_void_p()
+        n = np.ascontiguousarray(self.n, np.float64)
+        ftol = self.ll_tol if self.ll_tol is not None else 1e-11
+        call('blml_lbfgs_batch_create', self.code, F, C.cast(segs, C.c_void_p), C.cast(plans, C.c_void_p),
+             self.lbfgs_m, float(self.tol), float(ftol), -1 if self.max_sweeps is None else int(self.max_sweeps),
+             n.ctypes.data_as(C.c_void_p), self.w.data_ptr(), self.c.data_ptr(), E.data_ptr(), U.data_ptr(),
+             C.byref(h))
+        try:
+            call('blml_lbfgs_batch_run', h, self.st)
+            it = np.zeros(F, np.int64); stop = np.zeros(F, np.int32); L = np.zeros(F); res = np.zeros(F)
+            call('blml_lbfgs_batch_result', h, it.ctypes.data_as(C.c_void_p), stop.ctypes.data_as(C.c_void_p),
+                 L.ctypes.data_as(C.c_void_p), None, res.ctypes.data_as(C.c_void_p))
+            stats = np.zeros(4, np.int64)
+            call('blml_lbfgs_batch_stats', h, stats.ctypes.data_as(C.c_void_p))
+        finally:
+            _lib.lib().blml_lbfgs_batch_destroy(h)
+        self.lbfgs_stats_ = dict(zip(('iterations', 'replays', 'captures', 'kernels_per_replay'), stats.tolist()))
+        return U, it, np.array(STOP_CODES, dtype=object)[stop], L, res
+
     # ---------------------------------------------------------------- fit
     def fit(self, counts_list, modes_list):
         self._prepare(counts_list, modes_list)
         F, code, dev = self.F, self.code, self.device
-        n = self.n
-        er = self._start()
+        er = self._start_device() if self.control == 'device' else self._start()
         # complex start: the real root with the seeded phases exp(i pn N(0,1)) (blml_binned.py:429-436)
         E = torch.zeros(self.Btot, dtype=self.ct, device=dev)
         er_fit = er.to(self.rt)
@@ -299,12 +376,17 @@ class BLMLBinnedBatch:
         zt = torch.as_tensor(z, dtype=torch.float64).to(dev)
         call('blml_seg_phases', code, F, self.segs_t.data_ptr(), float(self.phase_noise), zt.data_ptr(), E.data_ptr(),
              self.st)
-        self._lbfgs(E)
-        return self.results_
+        if self.control == 'device':
+            U, it, stop, L, res = self._lbfgs_device(E)
+        else:
+            U, it, stop, L, res = self._lbfgs(E)
+        return self._finish(E, U, it, stop, L, res)
 
     def _lbfgs(self, E):
+        """L-BFGS of every fit with the per-fit decisions on the host (vectorised NumPy, a few syncs per iteration);
+        returns U and the per-fit iterations, stop reasons, L and residuals."""
         F, code, dev, n, m_ = self.F, self.code, self.device, self.n, self.lbfgs_m
-        U, g, gn, q, Sq, V, SV, tmp = (torch.zeros_like(E) for _ in range(8))
+        U, g, gn, q, Sq, V, SV = (torch.zeros_like(E) for _ in range(7))
         Sh = [torch.zeros_like(E) for _ in range(m_)]; Yh = [torch.zeros_like(E) for _ in range(m_)]
         off = self.boff[:-1]
         g_EU = _Group(self.pfit, E, off, U, off, True)
@@ -438,8 +520,21 @@ class BLMLBinnedBatch:
             step += 1
             if self.verbose and step % 100 == 0:
                 print(f'  batch lbfgs {step}: active {int(active.sum())}/{F} max rho {np.nanmax(res):.2e}', flush=True)
+        return U, it, stop, L, res
+
+    def _finish(self, E, U, it, stop, L, res):
+        """The canonical form per fit (kept unless it loses likelihood), the normalisation, the densities and the
+        per-fit results (blml_trivial.py:2646-2650)."""
+        F, code, dev, n = self.F, self.code, self.device, self.n
+        segs = self.segs_t.data_ptr()
+        stop = np.array(stop, dtype=object)
         stop[(stop == 'tol') & (res >= self.tol)] = 'max_sweeps'
-        # canonical form per fit (kept unless it loses likelihood), then the outputs
+        V, SV, tmp = (torch.zeros_like(E) for _ in range(3))
+        g_V = _Group(self.pfit, V, self.boff[:-1], SV, self.boff[:-1], True)
+
+        def Qdot(E_, U_):
+            return self._dots(code, True, [(E_, U_)])[:, 0]
+
         Qc = Qdot(E, U)
         call('blml_seg_lgrad_weights', code, F, segs, 1, U.data_ptr(), self.w.data_ptr(), self._dev(Qc / n).data_ptr(),
              V.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
@@ -456,7 +551,10 @@ class BLMLBinnedBatch:
         Q = Qdot(E, U)
         sc = np.where(Q > 0, n / np.sqrt(np.maximum(Q, 1e-300)), 1.0)
         self._lin(code, True, E, sc[:, None], [E]); self._lin(code, True, U, sc[:, None], [U])
-        res = resid(np.full(F, 1.0) * n * n)
+        call('blml_seg_resid', code, F, segs, 1, E.data_ptr(), U.data_ptr(), self.c.data_ptr(),
+             self._dev(np.ones(F)).data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
+        r = self._read(2)
+        res = np.where(r[:, 1] > 0, np.nan, r[:, 0])
         dens = torch.empty(self.Btot, dtype=self.rt, device=dev)
         call('blml_seg_finish', code, F, segs, 1, U.data_ptr(), self.w.data_ptr(), self._dev(1.0 / n ** 2).data_ptr(),
              dens.data_ptr(), self.part.data_ptr(), self.out.data_ptr(), self.st)
@@ -475,8 +573,9 @@ class BLMLBinnedBatch:
 
     def log_density(self, counts_list, eps=0.0):
         """Per fit: mean over the counts of log(f_b + eps), f = F / Q (blml_binned.py:630-645), one launch for all."""
-        m = torch.as_tensor(np.concatenate([np.asarray(c, float).ravel() for c in counts_list]),
-                            dtype=self.rt).to(self.device)
+        m = torch.cat([c.reshape(-1).to(self.device, self.rt) if isinstance(c, torch.Tensor) else
+                       torch.as_tensor(np.asarray(c, float).ravel(), dtype=self.rt).to(self.device)
+                       for c in counts_list])
         Q = self._dots(self.code, True, [(self.E_t, self.U_t)])[:, 0]
         call('blml_seg_log_score', self.code, self.F, self.segs_t.data_ptr(), 1, self.U_t.data_ptr(), m.data_ptr(),
              self._dev(1.0 / Q).data_ptr(), float(eps), self.part.data_ptr(), self.out.data_ptr(), self.st)

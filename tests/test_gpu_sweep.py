@@ -43,6 +43,50 @@ def test_grouped_matvec_equals_single(cuda_device):
 
 
 @pytest.mark.parametrize('dt', [np.float64, np.float32])
+def test_grouped_matvec_big_tiles(cuda_device, dt):
+    """A group large enough for the 64 x 64 cp.async tiles (every stage has >= 296 of them), real and complex input,
+    against each plan's own mat-vec: the same products summed in the same order; then the masked launch over a
+    subset with one problem switched off leaves that problem's output untouched."""
+    from blml_b200.sweep import _Group
+    from blml_b200 import operator as op_mod, _lib, workloads
+    from blml_b200.spec import parse_modes
+    from blml_b200._lib import call
+    code = _lib.F64 if dt == np.float64 else _lib.F32
+    ct, rt = (torch.complex128, torch.float64) if dt == np.float64 else (torch.complex64, torch.float32)
+    shapes = [(256, 256), (192, 256), (256, 200), (224, 224)] * 10
+    fcs = [0.4, 0.3, 0.45, 0.35, 0.25, 0.42]
+    plans, offs, tot = [], [0], 0
+    for i, shape in enumerate(shapes):
+        sp, _ = parse_modes(workloads.pball_modes(shape, fcs[i % len(fcs)]), 2)
+        plans.append(op_mod.Plan(*op_mod.mode_transform(sp[0], shape, np.ones(2), shape), shape, code, _lib.ENGINE_SIMT))
+        tot += shape[0] * shape[1]; offs.append(tot)
+    st = torch.cuda.current_stream().cuda_stream
+    tol = 1e-12 if dt == np.float64 else 1e-5
+    for xc in (True, False):
+        x = torch.randn(tot, dtype=ct if xc else rt, device='cuda')
+        y = torch.empty_like(x)
+        grp = _Group(plans, x, offs[:-1], y, offs[:-1], xc)
+        grp(st)
+        for g in range(len(plans)):
+            ref = torch.empty(offs[g + 1] - offs[g], dtype=x.dtype, device='cuda')
+            plans[g].apply(x[offs[g]:offs[g + 1]].contiguous(), ref, 1, xc, st)
+            err = (y[offs[g]:offs[g + 1]] - ref).abs().max().item()
+            assert err <= tol * ref.abs().max().item(), (g, xc, err)
+    # masked: problems 3..39 with problem 5 switched off
+    y.fill_(0)
+    subset = torch.arange(3, len(plans), dtype=torch.int32, device='cuda')
+    live = torch.ones(len(plans), dtype=torch.int32, device='cuda'); live[5] = 0
+    call('blml_group_matvec_masked', grp._h, subset.data_ptr(), len(plans) - 3, live.data_ptr(), st)
+    torch.cuda.synchronize()
+    for g in (0, 2, 5):
+        assert y[offs[g]:offs[g + 1]].abs().max().item() == 0.0
+    for g in (3, 4, 6, 39):
+        ref = torch.empty(offs[g + 1] - offs[g], dtype=x.dtype, device='cuda')
+        plans[g].apply(x[offs[g]:offs[g + 1]].contiguous(), ref, 1, False, st)
+        assert (y[offs[g]:offs[g + 1]] - ref).abs().max().item() <= tol * ref.abs().max().item()
+
+
+@pytest.mark.parametrize('dt', [np.float64, np.float32])
 def test_batch_matches_single_fits(cuda_device, dt):
     from blml_b200.sweep import BLMLBinnedBatch
     from blml_b200.binned import BLMLBinned
@@ -69,3 +113,59 @@ def test_batch_held_out_scores(cuda_device):
         dens = r.density_
         ref = float(np.sum(val[f][val[f] > 0] * np.log(dens[val[f] > 0] / dens.sum())) / val[f].sum())
         assert abs(scores[f] - ref) <= 1e-6 * abs(ref)
+
+
+@pytest.mark.parametrize('dt', [np.float64, np.float32])
+def test_device_control_matches_host_control(cuda_device, dt):
+    """The per-fit decisions made by kernels inside CUDA graphs (control='device') against the same decisions made
+    by vectorised NumPy on the host (control='host'): the start sweeps agree up to rounding-level trajectory
+    differences, the likelihood within the certification bar."""
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _sweep(6, seed=3)
+    counts = [c for c, _ in fits]; modes = [m for _, m in fits]
+    dev = BLMLBinnedBatch(tol=1e-6, dtype=dt, control='device')
+    rd = dev.fit(counts, modes)
+    host = BLMLBinnedBatch(tol=1e-6, dtype=dt, control='host')
+    rh = host.fit(counts, modes)
+    bar = 1e-6 if dt == np.float64 else 5e-5
+    for a, b in zip(rd, rh):
+        assert abs(a.loglik_ - b.loglik_) <= bar * abs(b.loglik_), (a.loglik_, b.loglik_, a.stop_reason_, b.stop_reason_)
+        assert abs(a.start_sweeps_ - b.start_sweeps_) <= max(2, 0.1 * b.start_sweeps_), (a.start_sweeps_, b.start_sweeps_)
+        assert np.all(np.isfinite(a.density_))
+    st = dev.lbfgs_stats_
+    assert st['captures'] >= 1 and st['replays'] >= 1 and st['kernels_per_replay'] > 0
+
+
+def test_device_control_limits(cuda_device):
+    """max_sweeps caps both phases on the device; a fit stopped by the cap reports max_sweeps (or an earlier
+    likelihood / stall stop)."""
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _sweep(3, seed=5)
+    res = BLMLBinnedBatch(tol=1e-12, max_sweeps=7, dtype=np.float64).fit([c for c, _ in fits], [m for _, m in fits])
+    for r in res:
+        assert r.start_sweeps_ <= 7 and r.n_sweeps_ <= 7
+        assert r.stop_reason_ in ('max_sweeps', 'll_tol', 'stall')
+        assert np.isfinite(r.loglik_)
+
+
+def test_full_sweep_against_the_port(cuda_device):
+    """All 64 fits of the cut-off sweep (sides 64..384, 2.5e6 bins) in one batch, float64, against the CPU port's
+    full fits of the same counts (oracle/make_sweep_counts.py): the fits are non-convex in the complex amplitudes, so
+    a rounding-level difference in the trajectory may end at a nearby optimum; the bars are that every fit is within
+    1e-4 or higher, most reach the port's likelihood within 1e-6 or higher, and the iteration counts agree in
+    distribution."""
+    import json, os
+    from conftest import ROOT
+    from blml_b200 import workloads
+    from blml_b200.sweep import BLMLBinnedBatch
+    port = json.load(open(os.path.join(ROOT, 'oracle', 'sweep64_counts.json')))
+    sweep = workloads.cutoff_sweep(seed=0, n_fits=64)
+    res = BLMLBinnedBatch(tol=1e-6, dtype=np.float64).fit([f['train'] for f in sweep],
+                                                          [workloads.pball_modes(f['shape'], f['fc']) for f in sweep])
+    ll = np.array([r.loglik_ for r in res]); ref = np.array([p['loglik'] for p in port])
+    rel = (ll - ref) / np.abs(ref)
+    print('rel dloglik min / median / max', rel.min(), np.median(rel), rel.max(), 'one-sided 1e-6:', np.mean(rel >= -1e-6))
+    assert np.all(rel >= -1e-4), rel.min()
+    assert np.mean(rel >= -1e-6) >= 0.75, np.mean(rel >= -1e-6)
+    its = np.array([r.n_sweeps_ for r in res]); rits = np.array([p['lbfgs_its'] for p in port])
+    assert 0.5 <= np.median(its) / np.median(rits) <= 2.0
