@@ -59,6 +59,22 @@ _SIGS = {
     'blml_seg_phases': (_I, [_I, _I, _P, _D, _P, _P, _P]),
     'blml_seg_real_to_complex': (_I, [_I, _I, _P, _P, _P, _P, _P]),
     'blml_group_matvec_masked': (_I, [_P, _P, _I, _P, _P]),
+    'blml_nn_gemm_bf16': (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _P]),
+    'blml_nn_im2col': (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _I, _P]),
+    'blml_nn_col2im': (_I, [_P, _I, _I, _I, _I, _P, _I, _I, _P]),
+    'blml_nn_bias_act': (_I, [_P, _I, _L, _I, _P, _I, _P, _I, _I, _P]),
+    'blml_nn_relu_bwd': (_I, [_P, _I, _I, _P, _I, _I, _L, _I, _P, _P, _P]),
+    'blml_nn_bias_grad': (_I, [_P, _I, _I, _P, _I, _I, _L, _I, _I, _I, _P, _P, _P]),
+    'blml_nn_sum_splits': (_I, [_P, _I, _L, _P, _P]),
+    'blml_nn_pool_fwd': (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _I, _I, _P]),
+    'blml_nn_pool_bwd_add': (_I, [_P, _I, _I, _I, _I, _P, _I, _I, _P]),
+    'blml_nn_up_fwd': (_I, [_P, _I, _I, _I, _I, _P, _I, _I, _P]),
+    'blml_nn_up_bwd': (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _P]),
+    'blml_nn_head_fwd': (_I, [_P, _L, _I, _P, _P, _I, _P, _P]),
+    'blml_nn_head_bwd': (_I, [_P, _P, _L, _I, _I, _P, _P, _I, _P, _P, _P]),
+    'blml_nn_phase_loss': (_I, [_P, _P, _L, _I, _P, _P, _P, _P]),
+    'blml_nn_adam': (_I, [_P, _P, _P, _P, _L, C.c_float, C.c_float, C.c_float, C.c_float, _I, _P, _P, _I, _I, _P]),
+    'blml_nn_to_bf16': (_I, [_P, _L, _P, _P, _I, _I, _P]),
     'blml_lbfgs_batch_create': (_I, [_I, _I, _P, _P, _I, _D, _D, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     'blml_lbfgs_batch_run': (_I, [_P, _P]),
     'blml_lbfgs_batch_result': (_I, [_P, _P, _P, _P, _P, _P]),

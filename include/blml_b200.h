@@ -206,6 +206,54 @@ int blml_start_batch_result(blml_start_batch runner, int64_t* sweeps, double* re
 int blml_start_batch_stats(blml_start_batch runner, int64_t* out4);
 int blml_start_batch_destroy(blml_start_batch runner);
 
+/* ---- the learned warm start: a small convolutional U-Net mapping (log counts, cut-off, kernel kind) on a lattice to
+ *      the fit's field u = S e / n (no counterpart in the reference: it replaces the real rank-1 start of
+ *      blml_binned.py:415-436 for the fits it covers). Activations NHWC BF16 in channel slices (Cs channels per
+ *      pixel, the slice starting at c0); gradients FP32 in the same layout. ----
+ * C[z] = A B^T over split z of K (A: M x K, B: N x K, K-major BF16, K a multiple of 8, 16-byte aligned; C: FP32,
+ * splits x M x N): tcgen05 kind::f16, TMA-staged 128-byte-swizzled tiles, TMEM accumulators. *err (device int) is
+ * set when a bounded wait gave up (the results are then invalid). */
+int blml_nn_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int K, int splits, int* err,
+                      void* stream);
+/* 3 x 3 (pad 1) im2col of a BF16 slice: col[p][(ky 3 + kx) C + c], or its transpose [9 C][p] */
+int blml_nn_im2col(const void* X, int Nb, int H, int W, int Cs, int c0, int C, void* col, int transposed,
+                   void* stream);
+/* the gradient of im2col: dX slice = sum of the 9 taps of dcol ([P][9 C] FP32), overwritten */
+int blml_nn_col2im(const float* dcol, int Nb, int H, int W, int C, float* dX, int Cs, int c0, void* stream);
+/* Y slice = act(sum of the split partials + bias) in BF16 (relu: max(., 0)) */
+int blml_nn_bias_act(const float* Cm, int splits, int64_t P, int N, const float* bias, int relu, void* Y, int Cs,
+                     int c0, void* stream);
+/* dPre = dY (Y > 0) in BF16, [P x C] and [C x P] */
+int blml_nn_relu_bwd(const float* dY, int Csd, int c0d, const void* Y, int Csy, int c0y, int64_t P, int C,
+                     void* dpre, void* dpreT, void* stream);
+/* db[c] = sum_p dY[p, c] (restricted to Y > 0 when relu), fixed-order chunk partials (part: chunks x C floats) */
+int blml_nn_bias_grad(const float* dY, int Csd, int c0d, const void* Y, int Csy, int c0y, int64_t P, int C, int relu,
+                      int chunks, float* part, float* db, void* stream);
+/* out = sum over splits of in (fixed order) */
+int blml_nn_sum_splits(const float* in, int splits, int64_t n, float* out, void* stream);
+/* 2 x 2 average pooling (forward into a slice; gradient added into a slice) */
+int blml_nn_pool_fwd(const void* X, int Nb, int H, int W, int Csx, int c0x, int C, void* Y, int Csy, int c0y,
+                     void* stream);
+int blml_nn_pool_bwd_add(const float* dY, int Nb, int H, int W, int C, float* dX, int Csx, int c0x, void* stream);
+/* nearest x2 upsampling of an (h, w) tensor into a slice, and its gradient */
+int blml_nn_up_fwd(const void* X, int Nb, int h, int w, int C, void* Y, int Csy, int c0y, void* stream);
+int blml_nn_up_bwd(const float* dY, int Nb, int h, int w, int Csy, int c0y, int C, float* dX, void* stream);
+/* the 1 x 1 output head (Cout <= 4, FP32 weights [Cout x Cin] and bias): forward, data gradient (dX may be null) and
+   weight / bias gradient gw [Cout x (Cin + 1)] from chunk partials (part: chunks x Cout (Cin + 1) floats) */
+int blml_nn_head_fwd(const void* X, int64_t P, int Cin, const float* W, const float* b, int Cout, float* Y,
+                     void* stream);
+int blml_nn_head_bwd(const float* dY, const void* X, int64_t P, int Cin, int Cout, const float* W, float* dX,
+                     int chunks, float* part, float* gw, void* stream);
+/* per sample s (HW complex values, interleaved FP32): loss[s] = min over a global phase and conjugation of
+   |u - e^{i th} t|^2 / |t|^2, and du = d(mean loss)/du; stats: 6 S doubles */
+int blml_nn_phase_loss(const float* u, const float* t, int64_t HW, int S, double* stats, float* du, double* loss,
+                       void* stream);
+/* Adam (bias-corrected, step >= 1) on FP32 weights; optional BF16 copy wb and BF16 transpose wbt of a rows x cols
+   matrix */
+int blml_nn_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                 int step, void* wb, void* wbt, int rows, int cols, void* stream);
+int blml_nn_to_bf16(const float* x, int64_t n, void* y, void* yt, int rows, int cols, void* stream);
+
 /* ---- pair accumulation over lattice bins from the row-kernel value tables (blml_local_gpu.rows / cols,
  *      blml_local_gpu.py:42-105, 320-361, 408-455; numba twins blml_local.py:117-191) ----
  * ZA (R, d), ZB (M, d): int64 lattice coordinates as the tables read them (rank columns: ranks). Table arrays are
