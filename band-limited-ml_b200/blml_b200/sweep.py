@@ -363,19 +363,34 @@ class BLMLBinnedBatch:
         return U, it, np.array(STOP_CODES, dtype=object)[stop], L, res
 
     # ---------------------------------------------------------------- fit
-    def fit(self, counts_list, modes_list):
+    def fit(self, counts_list, modes_list, init=None):
+        """init: None (the seeded start), or one complex start E0 per fit (arrays of the counts' shapes, host or
+        device), e.g. from blml_b200.warmstart; the start phase is then skipped (blml_binned.py:403-408)."""
         self._prepare(counts_list, modes_list)
         F, code, dev = self.F, self.code, self.device
-        er = self._start_device() if self.control == 'device' else self._start()
-        # complex start: the real root with the seeded phases exp(i pn N(0,1)) (blml_binned.py:429-436)
-        E = torch.zeros(self.Btot, dtype=self.ct, device=dev)
-        er_fit = er.to(self.rt)
-        call('blml_seg_real_to_complex', code, F, self.segs_t.data_ptr(), self.segs_t.data_ptr(), er_fit.data_ptr(),
-             E.data_ptr(), self.st)
-        z = np.concatenate([np.random.default_rng(self.seed).standard_normal(shape).ravel() for shape in self.shapes])
-        zt = torch.as_tensor(z, dtype=torch.float64).to(dev)
-        call('blml_seg_phases', code, F, self.segs_t.data_ptr(), float(self.phase_noise), zt.data_ptr(), E.data_ptr(),
-             self.st)
+        if init is not None:
+            if len(init) != F:
+                raise ValueError("init: one start per fit")
+            parts = []
+            for e0, shape in zip(init, self.shapes):
+                t = e0 if isinstance(e0, torch.Tensor) else torch.as_tensor(np.asarray(e0, complex))
+                if tuple(t.shape) != tuple(shape):
+                    raise ValueError("init: each start has its counts' shape")
+                parts.append(t.to(dev, self.ct).reshape(-1))
+            E = torch.cat(parts)
+            self.start_sweeps_ = np.zeros(F, np.int64)
+        else:
+            er = self._start_device() if self.control == 'device' else self._start()
+            # complex start: the real root with the seeded phases exp(i pn N(0,1)) (blml_binned.py:429-436)
+            E = torch.zeros(self.Btot, dtype=self.ct, device=dev)
+            er_fit = er.to(self.rt)
+            call('blml_seg_real_to_complex', code, F, self.segs_t.data_ptr(), self.segs_t.data_ptr(),
+                 er_fit.data_ptr(), E.data_ptr(), self.st)
+            z = np.concatenate([np.random.default_rng(self.seed).standard_normal(shape).ravel()
+                                for shape in self.shapes])
+            zt = torch.as_tensor(z, dtype=torch.float64).to(dev)
+            call('blml_seg_phases', code, F, self.segs_t.data_ptr(), float(self.phase_noise), zt.data_ptr(),
+                 E.data_ptr(), self.st)
         if self.control == 'device':
             U, it, stop, L, res = self._lbfgs_device(E)
         else:
@@ -566,6 +581,11 @@ class BLMLBinnedBatch:
                                    shape_=self.shapes[f], start_sweeps_=int(self.start_sweeps_[f]), _batch=self, _f=f)
                          for f in range(F)]
         return self.results_
+
+    def field(self, f):
+        """u = S e / n of fit f on the device (complex, the counts' shape): |u|^2 is the density."""
+        a, b = self.boff[f], self.boff[f + 1]
+        return (self.U_t[a:b] / float(self.n[f])).reshape(self.shapes[f])
 
     def density(self, f):
         a, b = self.boff[f], self.boff[f + 1]

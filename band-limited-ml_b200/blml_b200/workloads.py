@@ -6,6 +6,8 @@ any CPU checker see identical arrays). There is no public dataset on this path; 
   two_disk_field       counts ~ Poisson(N p) on an (M1, M2) torus, p = 0.95 |h|^2 / sum |h|^2 + 0.05 / (M1 M2), h the
                        inverse DFT of two displaced disks in the band with a random relative phase: the pball fits.
   cutoff_sweep         64 such fits of uneven size and cut-off with an 80/20 binomial held-out split.
+  warm_start_set       128 x 128 fits of two-disk (pball kernel) or two-slit (slits x sinc kernel) fields for the
+                       learned warm start.
   points_5d_mixture    n = 2e5 points of an 8-component 5-D Gaussian mixture in the unit cube for the pair path.
 """
 import numpy as np
@@ -36,6 +38,44 @@ def two_disk_field(shape=(256, 256), fc=0.33, N=1e6, seed=0, diameter=None, shif
     h = np.fft.ifft2(A)
     p = (1 - bg) * np.abs(h) ** 2 / np.sum(np.abs(h) ** 2) + bg / (M1 * M2)
     return rng.poisson(N * p).astype(np.float64)
+
+
+def two_slit_field(shape=(128, 128), fc=0.25, N=1e5, seed=0, bg=0.05):
+    """Counts on an (M1, M2) lattice from a field whose spectrum is two slits at +-3 fc / 8 along axis 0 (width
+    fc / 8) of height fc / 2 along axis 1, with a uniformly random relative phase: inside the band of
+    slits_modes(shape, fc)."""
+    rng = np.random.default_rng(seed)
+    M1, M2 = shape
+    k1 = np.fft.fftfreq(M1)[:, None]; k2 = np.fft.fftfreq(M2)[None, :]
+    d, a, b = 3 * fc / 8, fc / 16, fc / 4
+    A = ((np.abs(k1 - d) <= a) & (np.abs(k2) <= b)).astype(complex)
+    A = A + np.exp(2j * np.pi * rng.uniform()) * ((np.abs(k1 + d) <= a) & (np.abs(k2) <= b))
+    h = np.fft.ifft2(A)
+    p = (1 - bg) * np.abs(h) ** 2 / np.sum(np.abs(h) ** 2) + bg / (M1 * M2)
+    return rng.poisson(N * p).astype(np.float64)
+
+
+def slits_modes(shape, fc, fill=0.5):
+    """A product mode: two slits (band fc (1 - fill) / 2 <= |nu| <= fc / 2) on axis 0, sinc of cut-off fc on axis 1."""
+    return [{0: dict(kind='slits', fc=float(fc), fill=float(fill)), 1: dict(kind='sinc', fc=float(fc))}]
+
+
+def warm_start_set(n, seed=0, shape=(128, 128)):
+    """Fits of the warm-start workload: fit i draws, with default_rng(seed + i), a pupil (two disks under a pball
+    kernel or two slits under a slits x sinc kernel), fc ~ U(0.1, 0.4) and N = 10^U(4, 6)."""
+    out = []
+    for i in range(n):
+        rng = np.random.default_rng(seed + i)
+        kind = 'pball' if rng.uniform() < 0.5 else 'slits'
+        fc = float(rng.uniform(0.1, 0.4)); N = float(10 ** rng.uniform(4, 6))
+        if kind == 'pball':
+            counts = two_disk_field(shape, fc=fc, N=N, seed=seed + 7919 * (i + 1))
+            modes = pball_modes(shape, fc)
+        else:
+            counts = two_slit_field(shape, fc=fc, N=N, seed=seed + 7919 * (i + 1))
+            modes = slits_modes(shape, fc)
+        out.append(dict(kind=kind, fc=fc, N=N, counts=counts, modes=modes))
+    return out
 
 
 def pball_modes(shape, fc, bg_fc=None):
