@@ -59,6 +59,7 @@ _SIGS = {
     'blml_seg_phases': (_I, [_I, _I, _P, _D, _P, _P, _P]),
     'blml_seg_real_to_complex': (_I, [_I, _I, _P, _P, _P, _P, _P]),
     'blml_group_matvec_masked': (_I, [_P, _P, _I, _P, _P]),
+    'blml_seg_dots2': (_I, [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_nn_gemm_bf16': (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _P]),
     'blml_nn_im2col': (_I, [_P, _I, _I, _I, _I, _I, _I, _P, _I, _P]),
     'blml_nn_col2im': (_I, [_P, _I, _I, _I, _I, _P, _I, _I, _P]),

@@ -48,14 +48,15 @@ __global__ void k_fill_double(double* a, int64_t n, double v) {
   if (i < n) a[i] = v;
 }
 
-// one warp per quantity: out[j * nq + q] = the fixed-order sum of the fit's SEG_BLOCKS partials (the order of
-// k_seg_finish), for the fits whose flag is set
-__global__ void k_finish_flagged(const double* part, int nq, const int* flag, double* out) {
+// one warp per quantity: out[j * nq + q] = the fixed-order sum of the fit's nblk partials, for the fits whose flag
+// is set
+__global__ void k_finish_flagged(const double* part, int nq, int nblk, const int* flag, double* out) {
   const int j = blockIdx.x, Fa = gridDim.x;
   if (flag && !flag[j]) return;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int q = wid; q < nq; q += nw) {
-    double x = lane < SEG_BLOCKS ? part[((int64_t)q * Fa + j) * SEG_BLOCKS + lane] : 0.0;
+    double x = 0.0;
+    for (int i = lane; i < nblk; i += 32) x += part[((int64_t)q * Fa + j) * nblk + i];
     x = warp_sum(x);
     if (lane == 0) out[(int64_t)j * nq + q] = x;
   }
@@ -63,14 +64,15 @@ __global__ void k_finish_flagged(const double* part, int nq, const int* flag, do
 
 // ------------------------------------------------------------------------------------------------ L-BFGS control
 struct LbState {
-  double *L, *Q, *Qn, *n, *res, *slope, *mh, *SY, *YY;
+  double *L, *Q, *Qn, *n, *res, *slope, *qq, *mh, *SY, *YY;
   int *active, *it, *stop, *reset, *nh, *ok, *stamp, *step;
 };
 
 // the compact L-BFGS direction of fit f (one warp): q = gam g + S p - gam Y t over the fit's pairs in the order they
 // entered (R = triu(S^T Y), R t = S^T g, R^T p = (D + gam Y^T Y) t - gam Y^T g); the scaled gradient when there are
 // no pairs or the direction is not an ascent one (which also clears the memory). Block 0 advances the step counter.
-__global__ void k_lb_dir(int m, const int* fid, const int* live, const double* vals, LbState s, double* cq_all) {
+__global__ void k_lb_dir(int m, const int* fid, const int* live, const double* H1, const double* H2, LbState s,
+                         double* cq_all) {
   const int j = blockIdx.x, lane = threadIdx.x, f = fid[j];
   if (j == 0 && lane == 0) (*s.step)++;
   const int nc = 1 + 2 * m;
@@ -78,8 +80,11 @@ __global__ void k_lb_dir(int m, const int* fid, const int* live, const double* v
   for (int i = lane; i < nc; i += 32) cq[i] = 0.0;
   if (!live[f]) return;
   __syncwarp();
-  const double* v = vals + (int64_t)j * (2 * m + 2);
-  const double gg = v[2 * m], ee = v[2 * m + 1];
+  // the history scan of the previous iteration: H1 = [S_q . y_p, S_q . g, y_p . y_p, g . g, E . E],
+  // H2 = [Y_q . y_p, Y_q . g, ...] (stride 2 m + 3)
+  const double* h1 = H1 + (int64_t)j * (2 * m + 3);
+  const double* h2 = H2 + (int64_t)j * (2 * m + 3);
+  const double gg = h1[2 * m + 1], ee = h1[2 * m + 2];
   const double first = 1e-3 * sqrt(fmax(ee, 0.0) / fmax(gg, 1e-300));
   int* stamp = s.stamp + (int64_t)f * m;
   __shared__ int ord[LB_MMAX];
@@ -112,7 +117,7 @@ __global__ void k_lb_dir(int m, const int* fid, const int* live, const double* v
     __syncwarp();
     const int last = ord[k - 1];
     gam = SY[last * m + last] / YY[last * m + last];
-    const double ao = lane < k ? v[ord[lane]] : 0.0, bo = lane < k ? v[m + ord[lane]] : 0.0;
+    const double ao = lane < k ? h1[m + ord[lane]] : 0.0, bo = lane < k ? h2[m + ord[lane]] : 0.0;
     double r = ao;                                    // back substitution, R t = ao
     for (int i = k - 1; i >= 0; i--) {
       const double ti = __shfl_sync(0xffffffffu, r, i) / R[i][i];
@@ -147,24 +152,89 @@ __global__ void k_lb_dir(int m, const int* fid, const int* live, const double* v
   }
 }
 
-// the Armijo choice of every fit from the one-pass trials: the first t = 2^-j with L(t) >= L + 1e-4 t slope; a
-// failed search clears the memory once and stops the fit ('stall') when it fails again or had no pairs
-__global__ void k_lb_select(int Fa, int m, const int* fid, const int* live, const double* tr_all, LbState s,
-                            double* tA, double* cS, double* cY, double* cG) {
+// the Armijo trials t_j = 2^-j, j0 <= j < j0 + NTG, of the fits whose flag is set (all when null): sum_occ w log F(U +
+// t_j S q); the first group also <q, U>, <E, S q>, <q, S q> (Q(t) = Q + t (<q, U> + <E, S q>) + t^2 <q, S q>) and <q, q>
+template <typename T, int NTG, bool FIRST>
+__global__ void __launch_bounds__(256) k_lb_trials(const blml_seg* segs, const int* flag, int j0, const void* E,
+                                                   const void* q, const void* U, const void* Sq, const T* w,
+                                                   double* part) {
+  if (flag && !flag[blockIdx.y]) return;
+  const blml_seg S = segs[blockIdx.y];
+  constexpr int NQ = NTG + (FIRST ? 4 : 0);
+  double v[NQ];
+#pragma unroll
+  for (int j = 0; j < NQ; j++) v[j] = 0.0;
+  const double t0 = ldexp(1.0, -j0);
+  SEG_LOOP(b, S) {
+    const double wb = (double)w[S.boff + b];
+    double a = 0.0, bb = 0.0, cc = 0.0;        // F(t) = a + 2 t b + t^2 c
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double er, ei, qr, qi, ur, ui, sr, si;
+      SAcc<T, true>::get(E, i, er, ei); SAcc<T, true>::get(q, i, qr, qi);
+      SAcc<T, true>::get(U, i, ur, ui); SAcc<T, true>::get(Sq, i, sr, si);
+      a += ur * ur + ui * ui; bb += ur * sr + ui * si; cc += sr * sr + si * si;
+      if (FIRST) {
+        v[NTG] += qr * ur + qi * ui; v[NTG + 1] += er * sr + ei * si; v[NTG + 2] += qr * sr + qi * si;
+        v[NTG + 3] += qr * qr + qi * qi;
+      }
+    }
+    if (wb > 0) {
+      double t = t0;
+#pragma unroll
+      for (int j = 0; j < NTG; j++) { v[j] += wb * log(a + t * (2.0 * bb + t * cc)); t *= 0.5; }
+    }
+  }
+  seg_partials<NQ>(v, part);
+}
+
+constexpr int LB_T1 = 8, LB_T2 = LB_NT - LB_T1;
+
+__device__ __forceinline__ bool armijo_scan(const double* tr, int nt, double t, double Qa, double A, double Cc,
+                                            double La, double na, double slope, double& tok) {
+  for (int jj = 0; jj < nt; jj++) {
+    const double Qt = Qa + t * A + t * t * Cc;
+    const double Lt = Qt > 0 ? tr[jj] - na * log(Qt) : -INFINITY;
+    if (Lt >= La + 1e-4 * t * slope) { tok = t; return true; }
+    t *= 0.5;
+  }
+  return false;
+}
+
+// the Armijo choice over the first 8 trials; need2[j] marks the fits that try the other 32
+__global__ void k_lb_select1(int Fa, const int* fid, const int* live, const double* T1, LbState s, double* tA,
+                             int* need2) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Fa) return;
   const int f = fid[j];
+  need2[j] = 0; tA[j] = 0.0;
+  if (!live[f]) { s.ok[f] = 0; return; }
+  const double* tr = T1 + (int64_t)j * (LB_T1 + 4);
+  const double A = tr[LB_T1] + tr[LB_T1 + 1], Cc = tr[LB_T1 + 2];
+  s.qq[f] = tr[LB_T1 + 3];
   double t = 0.0;
+  const bool ok = armijo_scan(tr, LB_T1, 1.0, s.Q[f], A, Cc, s.L[f], s.n[f], s.slope[f], t);
+  s.ok[f] = ok; tA[j] = ok ? t : 0.0;
+  need2[j] = !ok;
+}
+
+// the remaining trials of the fits that need them, then every fit's outcome: a failed search clears the memory once
+// and stops the fit ('stall') when it fails again or had no pairs; the coefficient rows of the pair and g updates
+__global__ void k_lb_select2(int Fa, int m, const int* fid, const int* live, const double* T1, const double* T2,
+                             const int* need2, LbState s, double* tA, double* cS, double* cY, double* cG) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa) return;
+  const int f = fid[j];
   int ok = 0;
+  double t = 0.0;
   if (live[f]) {
-    const double* tr = tr_all + (int64_t)j * (LB_NT + 3);
-    const double A = tr[LB_NT] + tr[LB_NT + 1], Cc = tr[LB_NT + 2], Qa = s.Q[f], La = s.L[f], na = s.n[f];
-    double ts = 1.0;
-    for (int jj = 0; jj < LB_NT; jj++) {
-      const double Qt = Qa + ts * A + ts * ts * Cc;
-      const double Lt = Qt > 0 ? tr[jj] - na * log(Qt) : -INFINITY;
-      if (Lt >= La + 1e-4 * ts * s.slope[f]) { ok = 1; t = ts; break; }
-      ts *= 0.5;
+    ok = s.ok[f]; t = tA[j];
+    if (need2[j]) {
+      const double* tr1 = T1 + (int64_t)j * (LB_T1 + 4);
+      const double A = tr1[LB_T1] + tr1[LB_T1 + 1], Cc = tr1[LB_T1 + 2];
+      ok = armijo_scan(T2 + (int64_t)j * LB_T2, LB_T2, ldexp(1.0, -LB_T1), s.Q[f], A, Cc, s.L[f], s.n[f],
+                       s.slope[f], t);
+      if (!ok) t = 0.0;
     }
     int* stamp = s.stamp + (int64_t)f * m;
     if (!ok) {
@@ -184,14 +254,42 @@ __global__ void k_lb_select(int Fa, int m, const int* fid, const int* live, cons
   cG[2 * j] = o; cG[2 * j + 1] = 1.0 - o;
 }
 
+// the gradient weights at the new point fused with Q: F = sum_k |U_k|^2, V = (w / F) U on occupied bins,
+// [sum_occ w log F, Re <E, U>] per fit
+template <typename T>
+__global__ void __launch_bounds__(256) k_lb_weights(const blml_seg* segs, const void* E, const void* U, const T* w,
+                                                    void* V, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  double v[2] = {0.0, 0.0};
+  SEG_LOOP(b, S) {
+    double F = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double er, ei, ur, ui;
+      SAcc<T, true>::get(E, i, er, ei); SAcc<T, true>::get(U, i, ur, ui);
+      F += ur * ur + ui * ui; v[1] += er * ur + ei * ui;
+    }
+    const double wb = (double)w[S.boff + b];
+    const bool occ = wb > 0;
+    if (occ) v[0] += wb * log(F);
+    const double fw = occ ? wb / F : 0.0;
+    for (int k = 0; k < S.K; k++) {
+      const int64_t i = S.off + (int64_t)k * S.B + b;
+      double ur, ui; SAcc<T, true>::get(U, i, ur, ui);
+      SAcc<T, true>::put(V, i, occ ? ur * fw : 0.0, occ ? ui * fw : 0.0);
+    }
+  }
+  seg_partials<2>(v, part);
+}
+
 // Q at the new point, and the scales of the gradient finish (n / Q) and of the residual (n / sqrt Q)
-__global__ void k_lb_qeff(int Fa, const int* fid, const int* live, const double* outC, LbState s, double* nqA,
+__global__ void k_lb_qeff(int Fa, const int* fid, const int* live, const double* outD, LbState s, double* nqA,
                           double* scrA) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Fa) return;
   const int f = fid[j];
   if (!live[f]) { nqA[j] = 0.0; scrA[j] = 1.0; return; }
-  const double Qn = outC[j];
+  const double Qn = outD[2 * j + 1];
   s.Qn[f] = Qn;
   const double Qe = s.ok[f] ? Qn : s.Q[f];
   nqA[j] = s.n[f] / Qe;
@@ -201,18 +299,19 @@ __global__ void k_lb_qeff(int Fa, const int* fid, const int* live, const double*
 // the end of an iteration: the new pair (s, y) into slot p when its curvature is positive, the accepted state, the
 // likelihood window, then the stop rules the next iteration starts with (tol, ll_tol, the iteration cap)
 __global__ void k_lb_post(int Fa, int m, int p, double tol, double ftol, long long cap, const int* fid, int* live,
-                          const blml_seg* segs_c, blml_seg* segs_eff, const double* outA, const double* outD,
-                          const double* outE, LbState s) {
+                          const blml_seg* segs_c, blml_seg* segs_eff, const double* H1, const double* H2,
+                          const double* outD, const double* outE, const double* tA, LbState s) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Fa) return;
   const int f = fid[j];
   if (!live[f]) { set_live(j, f, 0, live, segs_c, segs_eff); return; }
   const int ok = s.ok[f];
   const double nf = s.n[f], Qn = s.Qn[f];
-  const double Ln = Qn > 0 ? outD[j] - nf * log(Qn) : -INFINITY;
+  const double Ln = Qn > 0 ? outD[2 * j] - nf * log(Qn) : -INFINITY;
   const double r = outE[2 * j + 1] > 0 ? NAN : outE[2 * j];
-  const double* v = outA + (int64_t)j * (3 + 2 * m);
-  const double sy = v[0], ss = v[1], yy = v[2];
+  const double* h1 = H1 + (int64_t)j * (2 * m + 3);
+  const double* h2 = H2 + (int64_t)j * (2 * m + 3);
+  const double sy = h1[p], yy = h1[2 * m], ss = tA[j] * tA[j] * s.qq[f];     // s_p = t q
   const bool enter = ok && (sy > 1e-12 * sqrt(fmax(ss * yy, 0.0)));
   int* stamp = s.stamp + (int64_t)f * m;
   if (ok) stamp[p] = -1;
@@ -220,9 +319,9 @@ __global__ void k_lb_post(int Fa, int m, int p, double tol, double ftol, long lo
     stamp[p] = *s.step;
     double* SY = s.SY + (int64_t)f * m * m;
     double* YY = s.YY + (int64_t)f * m * m;
-    for (int q = 0; q < m; q++) SY[q * m + p] = v[3 + q];
+    for (int q = 0; q < m; q++) SY[q * m + p] = h1[q];
     SY[p * m + p] = sy;
-    for (int q = 0; q < m; q++) { YY[q * m + p] = v[3 + m + q]; YY[p * m + q] = v[3 + m + q]; }
+    for (int q = 0; q < m; q++) { YY[q * m + p] = h2[q]; YY[p * m + q] = h2[q]; }
     YY[p * m + p] = yy;
   }
   double* h = s.mh + (int64_t)f * (LB_FWIN + 1);
@@ -263,7 +362,7 @@ __global__ void k_lbi_state(int Fa, int m, double tol, long long cap, const int*
   if (j >= Fa) return;
   const int f = fid[j];
   const double nf = s.n[f];
-  s.L[f] = outD[j] - nf * log(s.Q[f]);
+  s.L[f] = outD[2 * j] - nf * log(s.Q[f]);
   const double r = outE[2 * j + 1] > 0 ? NAN : outE[2 * j];
   s.res[f] = r;
   for (int q = 0; q < m; q++) s.stamp[(int64_t)f * m + q] = -1;
@@ -613,53 +712,85 @@ struct blml_lbfgs_batch_s : Runner {
   const void *w = nullptr, *c = nullptr;
   void *g = nullptr, *gn = nullptr, *q = nullptr, *Sq = nullptr, *V = nullptr, *SV = nullptr;
   void *Sh[LB_MMAX] = {}, *Yh[LB_MMAX] = {};
-  double *part = nullptr, *outA = nullptr, *outB = nullptr, *outC = nullptr, *outD = nullptr, *outE = nullptr;
+  double *part = nullptr, *H1 = nullptr, *H2 = nullptr, *T1 = nullptr, *T2 = nullptr, *outC = nullptr,
+         *outD = nullptr, *outE = nullptr;
   double *cq = nullptr, *tA = nullptr, *cS = nullptr, *cY = nullptr, *cG = nullptr, *nqA = nullptr, *scrA = nullptr,
          *ones = nullptr, *sc = nullptr;
+  int* need2 = nullptr;
   LbState s{};
+
+  // the history scan: H1 = [S_q . y_p, S_q . g, y_p . y_p, g . g, E . E], H2 = [Y_q . y_p, Y_q . g, ...]
+  int hist(int Fa_, const blml_seg* S, int p) {
+    const void* a[LB_MMAX];
+    for (int i = 0; i < m; i++) a[i] = Sh[i];
+    RC(blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, E, part, H1, st));
+    for (int i = 0; i < m; i++) a[i] = Yh[i];
+    return blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, nullptr, part, H2, st);
+  }
+
+  template <typename T>
+  int trials(int Fa_, const blml_seg* S) {
+    const dim3 grid((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_);
+    const int nb = seg_blocks_for(Fa_);
+    k_lb_trials<T, LB_T1, true><<<grid, 256, 0, st>>>(S, nullptr, 0, E, q, U, Sq, (const T*)w, part);
+    KCHECK("lbfgs trials");
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, LB_T1 + 4, nb, nullptr, T1);
+    KCHECK("lbfgs trials finish");
+    k_lb_select1<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, T1, s, tA, need2);
+    KCHECK("lbfgs select");
+    k_lb_trials<T, LB_T2, false><<<grid, 256, 0, st>>>(S, need2, LB_T1, E, q, U, Sq, (const T*)w, part);
+    KCHECK("lbfgs trials");
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, LB_T2, nb, need2, T2);
+    KCHECK("lbfgs trials finish");
+    k_lb_select2<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, m, d_fid, d_live, T1, T2, need2, s, tA, cS, cY, cG);
+    KCHECK("lbfgs select");
+    return BLML_OK;
+  }
+
+  template <typename T>
+  int weights(int Fa_, const blml_seg* S) {
+    k_lb_weights<T><<<dim3((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_), 256, 0, st>>>(S, E, U, (const T*)w, V,
+                                                                                        part);
+    KCHECK("lbfgs weights");
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 2, seg_blocks_for(Fa_), nullptr, outD);
+    KCHECK("lbfgs weights finish");
+    return BLML_OK;
+  }
 
   int iter(int p) {
     const int dt = dtype, Fa_ = Fa;
     const blml_seg* S = d_segs_eff;
     void* sv = st;
-    const void* a[48]; const void* b[48];
-    // direction
-    for (int i = 0; i < m; i++) { a[i] = Sh[i]; b[i] = g; a[m + i] = Yh[i]; b[m + i] = g; }
-    a[2 * m] = g; b[2 * m] = g; a[2 * m + 1] = E; b[2 * m + 1] = E;
-    RC(blml_seg_dots(dt, Fa_, S, 1, 2 * m + 2, a, b, part, outA, sv));
-    k_lb_dir<<<Fa_, 32, 0, st>>>(m, d_fid, d_live, outA, s, cq);
+    // direction from the previous iteration's history scan
+    k_lb_dir<<<Fa_, 32, 0, st>>>(m, d_fid, d_live, H1, H2, s, cq);
     KCHECK("lbfgs direction");
     const void* terms[48];
     terms[0] = g;
     for (int i = 0; i < m; i++) { terms[1 + i] = Sh[i]; terms[1 + m + i] = Yh[i]; }
     RC(blml_seg_lincomb(dt, Fa_, S, 1, q, 1 + 2 * m, cq, terms, sv));
     RC(blml_group_matvec_masked(gq, d_fid, Fa_, d_live, sv));
-    // every fit's Armijo search in one pass, then the accepted steps and U = S E exactly
-    RC(blml_seg_trials(dt, Fa_, S, 1, E, q, U, Sq, w, part, outB, sv));
-    k_lb_select<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, m, d_fid, d_live, outB, s, tA, cS, cY, cG);
-    KCHECK("lbfgs select");
+    // every fit's Armijo search (8 trials, then 32 more for the fits that need them), the accepted steps, U = S E
+    RC(dt == BLML_F64 ? trials<double>(Fa_, S) : trials<float>(Fa_, S));
     RC(blml_seg_axpy2(dt, Fa_, S, 1, E, q, U, Sq, tA, sv));
-    RC(blml_group_matvec_masked(gEU, d_fid, Fa_, d_live, sv));
-    a[0] = E; b[0] = U;
-    RC(blml_seg_dots(dt, Fa_, S, 1, 1, a, b, part, outC, sv));
-    k_lb_qeff<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, outC, s, nqA, scrA);
+    // U + t S q is S(E + t q) up to rounding: float32 state recomputes U = S E exactly at every step (its rounding
+    // would otherwise accumulate into the null space of S); float64 once per ring of m steps
+    if (dt == BLML_F32 || p == m - 1) RC(blml_group_matvec_masked(gEU, d_fid, Fa_, d_live, sv));
+    // gradient at the new point (with Q), the new pair into slot p, g, the residual, the history scan
+    RC(dt == BLML_F64 ? weights<double>(Fa_, S) : weights<float>(Fa_, S));
+    k_lb_qeff<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, outD, s, nqA, scrA);
     KCHECK("lbfgs qeff");
-    // gradient at the new point, the new pair into slot p, the residual and the pair's inner products
-    RC(blml_seg_lgrad_weights(dt, Fa_, S, 1, U, w, ones, V, part, outD, sv));
     RC(blml_group_matvec_masked(gV, d_fid, Fa_, d_live, sv));
     RC(blml_seg_lgrad_finish(dt, Fa_, S, 1, SV, U, w, nqA, gn, sv));
     terms[0] = q; terms[1] = Sh[p];
     RC(blml_seg_lincomb(dt, Fa_, S, 1, Sh[p], 2, cS, terms, sv));
     terms[0] = g; terms[1] = gn; terms[2] = Yh[p];
     RC(blml_seg_lincomb(dt, Fa_, S, 1, Yh[p], 3, cY, terms, sv));
-    RC(blml_seg_resid(dt, Fa_, S, 1, E, U, c, scrA, part, outE, sv));
-    a[0] = Sh[p]; b[0] = Yh[p]; a[1] = Sh[p]; b[1] = Sh[p]; a[2] = Yh[p]; b[2] = Yh[p];
-    for (int i = 0; i < m; i++) { a[3 + i] = Sh[i]; b[3 + i] = Yh[p]; a[3 + m + i] = Yh[i]; b[3 + m + i] = Yh[p]; }
-    RC(blml_seg_dots(dt, Fa_, S, 1, 3 + 2 * m, a, b, part, outA, sv));
     terms[0] = gn; terms[1] = g;
     RC(blml_seg_lincomb(dt, Fa_, S, 1, g, 2, cG, terms, sv));
-    k_lb_post<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, m, p, tol, ftol, cap, d_fid, d_live, d_segs_c, d_segs_eff, outA,
-                                              outD, outE, s);
+    RC(blml_seg_resid(dt, Fa_, S, 1, E, U, c, scrA, part, outE, sv));
+    RC(hist(Fa_, S, p));
+    k_lb_post<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, m, p, tol, ftol, cap, d_fid, d_live, d_segs_c, d_segs_eff, H1,
+                                              H2, outD, outE, tA, s);
     KCHECK("lbfgs post");
     return BLML_OK;
   }
@@ -678,12 +809,13 @@ struct blml_lbfgs_batch_s : Runner {
     RC(blml_seg_lincomb(dt, F, S, 1, E, 1, sc, t1, sv));
     t1[0] = U;
     RC(blml_seg_lincomb(dt, F, S, 1, U, 1, sc, t1, sv));
-    RC(blml_seg_lgrad_weights(dt, F, S, 1, U, w, ones, V, part, outD, sv));
+    RC(dt == BLML_F64 ? weights<double>(F, S) : weights<float>(F, S));
     RC(blml_group_matvec_masked(gV, d_fid, F, d_live, sv));
     RC(blml_seg_lgrad_finish(dt, F, S, 1, SV, U, w, nqA, gn, sv));
     t1[0] = gn;
     RC(blml_seg_lincomb(dt, F, S, 1, g, 1, ones, t1, sv));
     RC(blml_seg_resid(dt, F, S, 1, E, U, c, scrA, part, outE, sv));
+    RC(hist(F, S, 0));                                  // empty history: g . g and E . E for the first direction
     k_lbi_state<<<nblk(F, 128), 128, 0, st>>>(F, m, tol, cap, d_fid, d_live, d_segs_c, d_segs_eff, outD, outE, s);
     KCHECK("lbfgs set-up");
     return BLML_OK;
@@ -769,9 +901,10 @@ struct blml_start_batch_s : Runner {
     RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, ET, 2, cT, t, sv));
     t[0] = UA; t[1] = UJ;
     RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, UT, 2, cT, t, sv));
-    k_st_damp_trials<<<dim3(SEG_BLOCKS, (unsigned)Fa_), 256, 0, st>>>(S, damp, E, EJ, U, UJ, c, sg, part);
+    k_st_damp_trials<<<dim3((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_), 256, 0, st>>>(S, damp, E, EJ, U, UJ, c, sg,
+                                                                                         part);
     KCHECK("start damping trials");
-    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 3 * DAMP_NT, damp, outDT);
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 3 * DAMP_NT, seg_blocks_for(Fa_), damp, outDT);
     KCHECK("start damping finish");
     k_st_damp_pick<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, damp, outDT, s, cE);
     KCHECK("start damping pick");
@@ -845,27 +978,31 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
       r->Yh[i] = vec + (6 + (size_t)m + i) * tot * esz;
     }
     cudaMemsetAsync(vec, 0, (6 + 2 * (size_t)m) * tot * esz, r->st);
+    const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     const int nq = 48;                    // the widest reduction: blml_seg_dots' 48 accumulators
-    double* scr = (double*)r->dalloc(sizeof(double) * ((size_t)F * (nq * SEG_BLOCKS + 48 + 43 + 1 + 1 + 2 +
-                                                                   (1 + 2 * m) + 1 + 2 + 3 + 2 + 1 + 1 + 1 + 1)));
+    const int hs = 2 * m + 3;
+    double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F * (2 * hs + (LB_T1 + 4) + LB_T2 + 1 + 2 + 2 +
+                                                                             (1 + 2 * m) + 1 + 2 + 3 + 2 + 1 + 1 + 1 +
+                                                                             1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (7 + (LB_FWIN + 1) + 2 * (size_t)m * m));
-    int* ist = (int*)r->dalloc(sizeof(int) * ((size_t)F * (7 + m) + 1));
+    int* ist = (int*)r->dalloc(sizeof(int) * ((size_t)F * (8 + m) + 1));
     if (!scr || !stt || !ist) { set_error("blml_lbfgs_batch_create: allocation"); rc = BLML_ERR_CUDA; }
     else {
-      double* x = scr;
+      r->part = scr;
+      double* x = scr + nq * pw;
       auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
-      r->part = take((size_t)nq * SEG_BLOCKS); r->outA = take(48); r->outB = take(43); r->outC = take(1);
-      r->outD = take(1); r->outE = take(2); r->cq = take(1 + 2 * m); r->tA = take(1); r->cS = take(2);
+      r->H1 = take(hs); r->H2 = take(hs); r->T1 = take(LB_T1 + 4); r->T2 = take(LB_T2); r->outC = take(1);
+      r->outD = take(2); r->outE = take(2); r->cq = take(1 + 2 * m); r->tA = take(1); r->cS = take(2);
       r->cY = take(3); r->cG = take(2); r->nqA = take(1); r->scrA = take(1); r->ones = take(1); r->sc = take(1);
       double* y = stt;
       auto tk = [&](size_t k) { double* p = y; y += k * F; return p; };
       r->s.L = tk(1); r->s.Q = tk(1); r->s.Qn = tk(1); r->s.n = tk(1); r->s.res = tk(1); r->s.slope = tk(1);
-      tk(1);
+      r->s.qq = tk(1);
       r->s.mh = tk(LB_FWIN + 1); r->s.SY = tk((size_t)m * m); r->s.YY = tk((size_t)m * m);
       int* z = ist;
       auto ti = [&](size_t k) { int* p = z; z += k * F; return p; };
       r->s.active = ti(1); r->s.it = ti(1); r->s.stop = ti(1); r->s.reset = ti(1); r->s.nh = ti(1); r->s.ok = ti(1);
-      ti(1);
+      r->need2 = ti(1); ti(1);
       r->s.stamp = ti(m); r->s.step = z;
       k_fill_double<<<nblk(F, 256), 256, 0, r->st>>>(r->ones, F, 1.0);
       rc = cuda_status(cudaMemcpyAsync(r->s.n, n, F * sizeof(double), cudaMemcpyHostToDevice, r->st), "lbfgs n");
@@ -946,16 +1083,17 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
     for (int i = 0; i < mA; i++) { r->DX[i] = vec + (10 + (size_t)i) * tot; r->DF[i] = vec + (10 + (size_t)mA + i) * tot; }
     cudaMemsetAsync(vec, 0, (10 + 2 * (size_t)mA) * tot * sizeof(double), r->st);
     const int nq = 3 * DAMP_NT;           // the widest reduction: the damping trials' 78 quantities
-    double* scr = (double*)r->dalloc(sizeof(double) * (size_t)F *
-                                     (nq * SEG_BLOCKS + 3 + 3 + 2 * AA_MMAX + 1 + 2 + nq + 2 + 1 + (2 + 2 * AA_MMAX) +
-                                      2 + 3 + 1 + 1));
+    const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
+    double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F *
+                                     (3 + 3 + 2 * AA_MMAX + 1 + 2 + nq + 2 + 1 + (2 + 2 * AA_MMAX) + 2 + 3 + 1 + 1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (8 + (size_t)AA_MMAX * AA_MMAX));
     int* ist = (int*)r->dalloc(sizeof(int) * (size_t)F * (6 + AA_MMAX + 2));
     if (!scr || !stt || !ist) { set_error("blml_start_batch_create: allocation"); rc = BLML_ERR_CUDA; }
     else {
-      double* x = scr;
+      r->part = scr;
+      double* x = scr + nq * pw;
       auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
-      r->part = take((size_t)nq * SEG_BLOCKS); r->outM1 = take(3); r->outM2 = take(3); r->outA = take(2 * AA_MMAX);
+      r->outM1 = take(3); r->outM2 = take(3); r->outA = take(2 * AA_MMAX);
       r->outQ = take(1); r->outR = take(2); r->outDT = take(nq); r->c1m1 = take(2); r->ones = take(1);
       r->cA = take(2 + 2 * AA_MMAX); r->cT = take(2); r->cE = take(3); r->scA = take(1); r->s0c = take(1);
       double* y = stt;

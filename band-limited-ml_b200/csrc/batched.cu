@@ -158,6 +158,49 @@ __global__ void k_seg_dots(const blml_seg* segs, int cplx, int np, SegPairs pp, 
   seg_partials<NP>(v, part);
 }
 
+struct SegList { const void* a[20]; };
+
+// the history scan of the batched L-BFGS: per fit, for the np <= 20 vectors a_q, out = [a_q . b0 (np), a_q . b1 (np),
+// b0 . b0, b1 . b1, x . x] (x may be null: 0); b0, b1, x read once per element whatever np is
+template <typename T>
+__global__ void __launch_bounds__(256) k_seg_dots2(const blml_seg* segs, int cplx, int np, SegList al, const void* b0,
+                                                   const void* b1, const void* x, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const int64_t w = cplx ? 2 : 1;
+  const int64_t o = S.off * w, n = (int64_t)S.K * S.B * w;
+  double v[43];
+#pragma unroll
+  for (int q = 0; q < 43; q++) v[q] = 0.0;
+  const T* B0 = reinterpret_cast<const T*>(b0) + o;
+  const T* B1 = reinterpret_cast<const T*>(b1) + o;
+  const T* X = x ? reinterpret_cast<const T*>(x) + o : nullptr;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double y0 = (double)B0[i], y1 = (double)B1[i];
+#pragma unroll
+    for (int q = 0; q < 20; q++)
+      if (q < np) {
+        const double a = (double)reinterpret_cast<const T*>(al.a[q])[o + i];
+        v[q] += a * y0; v[20 + q] += a * y1;
+      }
+    v[40] += y0 * y0; v[41] += y1 * y1;
+    if (X) { const double z = (double)X[i]; v[42] += z * z; }
+  }
+  seg_partials<43>(v, part);
+}
+
+// out[f * (2 np + 3) + q] from the 43-quantity partials (quantities 20.. shifted down when np < 20)
+__global__ void k_seg_finish_dots2(const double* part, int np, int nblk, double* out) {
+  const int f = blockIdx.x, F = gridDim.x, nq = 2 * np + 3;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int q = wid; q < nq; q += nw) {
+    const int src = q < np ? q : (q < 2 * np ? 20 + (q - np) : 40 + (q - 2 * np));
+    double acc = 0.0;
+    for (int i = lane; i < nblk; i += 32) acc += part[((int64_t)src * F + f) * nblk + i];
+    acc = warp_sum(acc);
+    if (lane == 0) out[(int64_t)f * nq + q] = acc;
+  }
+}
+
 struct SegTerms { const void* v[48]; };
 
 // out = sum_i coef[f * nt + i] v_i over each fit's slice
@@ -320,7 +363,7 @@ __global__ void k_seg_real_to_complex(const blml_seg* real_segs, const blml_seg*
 }
 
 static int seg_finish(const double* part, int F, int nq, unsigned maxmask, double* out, cudaStream_t st) {
-  k_seg_finish<<<F, 256, 0, st>>>(part, nq, SEG_BLOCKS, maxmask, out);
+  k_seg_finish<<<F, 256, 0, st>>>(part, nq, seg_blocks_for(F), maxmask, out);
   BLML_CHECK_LAUNCH("seg finish");
   return BLML_OK;
 }
@@ -341,7 +384,7 @@ static void seg_dots_launch(dim3 g, const blml_seg* s, int cplx, int np, const S
 
 using namespace blml;
 #define SST reinterpret_cast<cudaStream_t>(stream)
-#define SGRID(F) dim3(SEG_BLOCKS, (unsigned)(F))
+#define SGRID(F) dim3((unsigned)seg_blocks_for(F), (unsigned)(F))
 #define TYPED(dtype, cplx, K, ...)                                          \
   do {                                                                      \
     if (dtype == BLML_F64) { if (cplx) K<double, true>__VA_ARGS__; else K<double, false>__VA_ARGS__; } \
@@ -357,7 +400,7 @@ static int seg_args(int dtype, int F, const blml_seg* segs, const char* who) {
 
 extern "C" {
 
-int blml_seg_blocks(void) { return SEG_BLOCKS; }
+int blml_seg_blocks(void) { return SEG_BLOCKS_MAX; }
 
 int blml_seg_start_root(int dtype, int F, const blml_seg* segs, const void* c, const void* sg, const double* s0,
                         void* e0, void* stream) {
@@ -419,8 +462,22 @@ int blml_seg_dots(int dtype, int F, const blml_seg* segs, int cplx, int npairs, 
   if (dtype == BLML_F64) seg_dots_launch<double>(SGRID(F), segs, cplx, npairs, pp, part, SST);
   else seg_dots_launch<float>(SGRID(F), segs, cplx, npairs, pp, part, SST);
   BLML_CHECK_LAUNCH("blml_seg_dots");
-  k_seg_finish_strided<<<F, 256, 0, SST>>>(part, npairs, SEG_BLOCKS, out, npairs);
+  k_seg_finish_strided<<<F, 256, 0, SST>>>(part, npairs, seg_blocks_for(F), out, npairs);
   BLML_CHECK_LAUNCH("blml_seg_dots finish");
+  return BLML_OK;
+}
+
+int blml_seg_dots2(int dtype, int F, const blml_seg* segs, int cplx, int np, const void* const* a, const void* b0,
+                   const void* b1, const void* x, double* part, double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_dots2")) return BLML_ERR_ARG;
+  if (np < 1 || np > 20 || !a || !b0 || !b1) { set_error("blml_seg_dots2: 1..20 vectors, b0 and b1"); return BLML_ERR_ARG; }
+  SegList al;
+  for (int q = 0; q < 20; q++) al.a[q] = q < np ? a[q] : nullptr;
+  if (dtype == BLML_F64) k_seg_dots2<double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
+  else k_seg_dots2<float><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
+  BLML_CHECK_LAUNCH("blml_seg_dots2");
+  k_seg_finish_dots2<<<F, 256, 0, SST>>>(part, np, seg_blocks_for(F), out);
+  BLML_CHECK_LAUNCH("blml_seg_dots2 finish");
   return BLML_OK;
 }
 

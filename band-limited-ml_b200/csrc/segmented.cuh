@@ -6,7 +6,14 @@
 
 namespace blml {
 
-constexpr int SEG_BLOCKS = 16;        // blocks per fit (x); 64 fits x 16 blocks x 256 threads covers a B200 ~2 times
+// blocks per fit (gridDim.x) of a segmented launch over F fits: ~4096 blocks in all, 16 to 256 per fit, so a few large
+// fits (or the last fits still iterating) still spread over every SM; the partials of a reduction over F fits take
+// nq * F * seg_blocks_for(F) <= nq * max(4096, 16 F) doubles
+constexpr int SEG_BLOCKS_MIN = 16, SEG_BLOCKS_MAX = 256;
+__host__ __device__ inline int seg_blocks_for(int F) {
+  int x = 4096 / (F > 0 ? F : 1);
+  return x < SEG_BLOCKS_MIN ? SEG_BLOCKS_MIN : (x > SEG_BLOCKS_MAX ? SEG_BLOCKS_MAX : x);
+}
 
 template <typename T, bool CPLX>
 struct SAcc {

@@ -136,8 +136,9 @@ int blml_cert_weights(int dtype, int K, int64_t B, int cplx, const void* E, cons
 /* ---- segmented (batched) solver kernels: F independent fits in lockstep, one launch per phase ----
  * Fit f owns elements [off, off + K B) of every flat mode array (its (K, B) block) and [boff, boff + B) of every flat
  * bin array (counts, signs); `segs` is a device array of F entries. Per-fit scalars are device arrays of F doubles
- * (coefficient tables: F x nterms). Reductions give out[f * nq + q] (part: F * nq * blml_seg_blocks() doubles;
- * blml_seg_dots: F * 48 * blml_seg_blocks()).
+ * (coefficient tables: F x nterms). Reductions give out[f * nq + q] (part: F * nq * blml_seg_blocks() doubles, an
+ * upper bound: a launch over F fits uses min(256, max(16, 4096 / F)) blocks per fit; blml_seg_dots takes nq = 48,
+ * blml_seg_dots2 nq = 43).
  * These are the reference's single-fit operations (blml_binned.py:171-220, 278-355, 415-445, 630-645) applied to a
  * sweep of fits at once, as selector._search / the cut-off sweeps run them one after another. */
 typedef struct { int64_t off; int64_t boff; int64_t B; int32_t K; int32_t pad; } blml_seg;
@@ -152,6 +153,10 @@ int blml_seg_resid(int dtype, int F, const blml_seg* segs, int cplx, const void*
                    const double* scale, double* part, double* out, void* stream);                   /* nq = 2 */
 int blml_seg_dots(int dtype, int F, const blml_seg* segs, int cplx, int npairs, const void* const* a,
                   const void* const* b, double* part, double* out, void* stream);                   /* npairs <= 48 */
+/* the L-BFGS history scan (blml_binned.py:297-313 reads the same products pair by pair): for np <= 20 vectors a_q,
+   out[f * (2 np + 3) + .] = [a_q . b0 (np), a_q . b1 (np), b0 . b0, b1 . b1, x . x] (x may be null: 0) */
+int blml_seg_dots2(int dtype, int F, const blml_seg* segs, int cplx, int np, const void* const* a, const void* b0,
+                   const void* b1, const void* x, double* part, double* out, void* stream);
 int blml_seg_lincomb(int dtype, int F, const blml_seg* segs, int cplx, void* out, int nterms, const double* coef,
                      const void* const* v, void* stream);                                           /* nterms <= 48 */
 int blml_seg_lgrad_weights(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* w,
