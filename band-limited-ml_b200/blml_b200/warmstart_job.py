@@ -78,9 +78,25 @@ def train(args):
                       'loss_first': hist[0], 'loss_last': hist[-1], 'loss_history': hist}))
 
 
+def to_bf16_bits(a):
+    """float32 -> BF16 bit patterns (round to nearest even), uint16."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def from_bf16_bits(b):
+    return (np.asarray(b, np.uint32) << 16).view(np.float32)
+
+
+def save_bf16(params, path):
+    """The weights as BF16 bit patterns (what the network computes with), half the size of float32."""
+    np.savez_compressed(path, **{k: to_bf16_bits(v) for k, v in params.items()})
+
+
 def load(path, device='cuda'):
     z = np.load(path)
-    return WarmStartNet(device=device, params={k: z[k] for k in z.files})
+    p = {k: (from_bf16_bits(z[k]) if z[k].dtype == np.uint16 else z[k]) for k in z.files}
+    return WarmStartNet(device=device, params=p)
 
 
 def evaluate(net, fits, tol=1e-6, batch=64):

@@ -614,8 +614,11 @@ struct Runner {
     if (st) cudaStreamDestroy(st);
     h_live = nullptr; ev = nullptr; st = nullptr;
   }
-  // the compact set: fits `sel` (ascending ids), all live
-  int set_compact(const std::vector<int>& sel) {
+  // the compact set: fits `sel`, all live, largest first (launches over fits dispatch their blocks in compact order,
+  // so the longest-running fits start first and the small ones fill in behind them)
+  int set_compact(const std::vector<int>& sel_in) {
+    std::vector<int> sel = sel_in;
+    std::stable_sort(sel.begin(), sel.end(), [this](int a, int b) { return segs_all[a].B > segs_all[b].B; });
     ids = sel; Fa = (int)sel.size();
     std::vector<blml_seg> sc(Fa);
     for (int j = 0; j < Fa; j++) sc[j] = segs_all[sel[j]];
