@@ -1,12 +1,12 @@
 """Training and evaluation of the learned warm start on one GPU (the engine makes its own training data).
 
     python -m blml_b200.warmstart_job train --fits 2048 --sweeps 8 --epochs 20 --out weights.npz
-    python -m blml_b200.warmstart_job eval --weights weights.npz --fits 512
+    python -m blml_b200.warmstart_job eval --weights weights.npz --fits 512 [--set sweep]
 
 train: fits of workloads.warm_start_set (128 x 128, two-disk pupils under a pball kernel or two-slit pupils under a
 slits x sinc kernel, fc ~ U(0.1, 0.4), N = 10^U(4, 6)) plus cut-off sweeps of other seeds than the benchmark's
 (workloads.cutoff_sweep: 2-D pball, sides 64..384) are fitted cold by the batched engine (float64, tol 1e-6); the
-network learns their fields u = S e / n; weights are saved as float32 .npz.
+network learns their fields u = S e / n; weights are saved as BF16 bit patterns (.npz).
 eval: fresh seeds, fitted cold (the seeded real start + L-BFGS) and warm (the network's start + L-BFGS) by the batched
 engine: iterations, seconds, certified fraction (warm loglik >= cold loglik - 1e-6 relative). One JSON line."""
 import argparse
@@ -72,7 +72,7 @@ def train(args):
         hist.append(sum(l * n for l, n in losses) / sum(n for _, n in losses))
         print(f'epoch {ep}: loss {hist[-1]:.4f}', flush=True)
     torch.cuda.synchronize()
-    np.savez(args.out, **{k: v.astype(np.float32) for k, v in net.params_numpy().items()})
+    save_bf16(net.params_numpy(), args.out)
     print(json.dumps({'fits': len(fits), 'shapes': len(by_shape), 'fit_seconds': fit_secs,
                       'train_seconds': time.perf_counter() - t1, 'total_seconds': time.perf_counter() - t0,
                       'loss_first': hist[0], 'loss_last': hist[-1], 'loss_history': hist}))
@@ -136,13 +136,19 @@ def main():
     ap.add_argument('--seed', type=int, default=0)
     ap.add_argument('--out', default='warmstart_weights.npz')
     ap.add_argument('--weights', default='warmstart_weights.npz')
+    ap.add_argument('--set', default='ws', choices=['ws', 'sweep'], help='eval on the warm-start set or the sweep')
     args = ap.parse_args()
     if args.mode == 'train':
         return train(args)
     net = load(args.weights)
-    fits = workloads.warm_start_set(args.fits, seed=EVAL_SEED, shape=(128, 128))
-    out = evaluate(net, fits)
-    out['workload'] = '128x128 warm-start set, fresh seeds'
+    if args.set == 'sweep':                         # the benchmark's 64-fit cut-off sweep (seed 0)
+        fits = sweep_fits(1, seed=0)
+        out = evaluate(net, fits)
+        out['workload'] = '64-fit cut-off sweep of the benchmark (sides 64..384, pball)'
+    else:
+        fits = workloads.warm_start_set(args.fits, seed=EVAL_SEED, shape=(128, 128))
+        out = evaluate(net, fits)
+        out['workload'] = '128x128 warm-start set, fresh seeds'
     print(json.dumps(out), flush=True)
 
 
