@@ -42,14 +42,15 @@ def two_disk_field(shape=(256, 256), fc=0.33, N=1e6, seed=0, diameter=None, shif
 
 def two_slit_field(shape=(128, 128), fc=0.25, N=1e5, seed=0, bg=0.05):
     """Counts on an (M1, M2) lattice from a field whose spectrum is two slits at +-3 fc / 8 along axis 0 (width
-    fc / 8) of height fc / 2 along axis 1, with a uniformly random relative phase: inside the band of
-    slits_modes(shape, fc)."""
+    fc / 8) of height fc / 2 along axis 1 (rounded to DFT bins, at least one bin), with a uniformly random relative
+    phase: inside the band of slits_modes(shape, fc)."""
     rng = np.random.default_rng(seed)
     M1, M2 = shape
-    k1 = np.fft.fftfreq(M1)[:, None]; k2 = np.fft.fftfreq(M2)[None, :]
-    d, a, b = 3 * fc / 8, fc / 16, fc / 4
-    A = ((np.abs(k1 - d) <= a) & (np.abs(k2) <= b)).astype(complex)
-    A = A + np.exp(2j * np.pi * rng.uniform()) * ((np.abs(k1 + d) <= a) & (np.abs(k2) <= b))
+    # in DFT bins, at least one bin wide (a slit narrower than the grid would be empty on small lattices)
+    i1 = np.fft.fftfreq(M1, 1.0 / M1)[:, None]; i2 = np.fft.fftfreq(M2, 1.0 / M2)[None, :]
+    d = max(1, int(round(3 * fc / 8 * M1))); a = int(round(fc / 16 * M1)); b = int(round(fc / 4 * M2))
+    A = ((np.abs(i1 - d) <= a) & (np.abs(i2) <= b)).astype(complex)
+    A = A + np.exp(2j * np.pi * rng.uniform()) * ((np.abs(i1 + d) <= a) & (np.abs(i2) <= b))
     h = np.fft.ifft2(A)
     p = (1 - bg) * np.abs(h) ** 2 / np.sum(np.abs(h) ** 2) + bg / (M1 * M2)
     return rng.poisson(N * p).astype(np.float64)

@@ -63,15 +63,23 @@ def up(x):
     return x.repeat(2, axis=1).repeat(2, axis=2)
 
 
-def forward(p, x):
-    """x (N, H, W, 8) -> (u (N, H, W, 2), cache)."""
-    c = {'x': x}
-    r = lambda v: np.maximum(v, 0.0)
+def bf16(a):
+    """Round to the nearest BF16 value (ties to even), returned as float64: the storage rounding of the GPU path."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32)
+    return (((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16).astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward(p, x, store=None):
+    """x (N, H, W, 8) -> (u (N, H, W, 2), cache). store: a rounding applied to every stored activation (bf16 to
+    follow the GPU's BF16 activations exactly), identity by default."""
+    st = store or (lambda v: v)
+    c = {'x': x, 'store': store}
+    r = lambda v: st(np.maximum(v, 0.0))
     h = x
     for lvl in (1, 2, 3):
         a = r(conv(h, p[f'enc{lvl}a.w'], p[f'enc{lvl}a.b'])); c[f'enc{lvl}a'] = a
         e = r(conv(a, p[f'enc{lvl}b.w'], p[f'enc{lvl}b.b'])); c[f'enc{lvl}b'] = e
-        h = pool(e); c[f'pool{lvl}'] = h
+        h = st(pool(e)); c[f'pool{lvl}'] = h
     b1 = r(conv(h, p['bot1.w'], p['bot1.b'])); c['bot1'] = b1
     h = r(conv(b1, p['bot2.w'], p['bot2.b'])); c['bot2'] = h
     for lvl in (3, 2, 1):
@@ -110,10 +118,13 @@ def backward(p, c, du):
     g['head.b'] = du.reshape(-1, 2).sum(0)
     dh = du @ p['head.w']
 
+    st = c.get('store') or (lambda v: v)
+
     def conv_bwd(name, x, y, dy, need_dx=True):
         dpre = dy * (y > 0)
-        g[name + '.w'] = dpre.reshape(-1, dpre.shape[3]).T @ im2col(x)
         g[name + '.b'] = dpre.reshape(-1, dpre.shape[3]).sum(0)
+        dpre = st(dpre)                                 # the GPU multiplies a BF16 copy
+        g[name + '.w'] = dpre.reshape(-1, dpre.shape[3]).T @ im2col(x)
         if not need_dx:
             return None
         return col2im(dpre.reshape(-1, dpre.shape[3]) @ p[name + '.w'], x.shape)

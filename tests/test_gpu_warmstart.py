@@ -50,16 +50,19 @@ def test_forward_and_gradients_match_oracle(cuda_device):
     # the oracle on the same BF16-rounded weights and input (convolution weights are BF16 on the GPU)
     po = {k: (_bf16(v) if k.endswith('.w') and not k.startswith('head') else np.asarray(v, np.float32).astype(float))
           for k, v in p.items()}
-    uo_, c = uo.forward(po, _bf16(x))
+    # the oracle rounds every stored activation and the ReLU-masked gradient the GEMMs take to BF16, as the GPU does,
+    # so what remains is FP32 (GPU) against FP64 (oracle) accumulation
+    uo_, c = uo.forward(po, uo.bf16(x), store=uo.bf16)
     lo, duo = uo.loss(uo_, t)
     go = uo.backward(po, c, duo)
     ug = u.double().cpu().numpy()
-    assert np.linalg.norm(ug - uo_) <= 5e-2 * np.linalg.norm(uo_), np.linalg.norm(ug - uo_) / np.linalg.norm(uo_)
-    assert np.allclose(ls.cpu().numpy(), lo, rtol=5e-2)
+    assert np.linalg.norm(ug - uo_) <= 1e-2 * np.linalg.norm(uo_), np.linalg.norm(ug - uo_) / np.linalg.norm(uo_)
+    assert np.allclose(ls.cpu().numpy(), lo, rtol=1e-2)
+    worst = {}
     for k in go:
         gg = net.g[k].double().cpu().numpy().reshape(go[k].shape)
-        rel = np.linalg.norm(gg - go[k]) / max(np.linalg.norm(go[k]), 1e-30)
-        assert rel <= 0.1, (k, rel)
+        worst[k] = np.linalg.norm(gg - go[k]) / max(np.linalg.norm(go[k]), 1e-30)
+    assert max(worst.values()) <= 2e-2, worst
 
 
 def test_short_training_lowers_loss_and_starts_converge(cuda_device):
