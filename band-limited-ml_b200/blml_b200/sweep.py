@@ -368,6 +368,8 @@ class BLMLBinnedBatch:
         device), e.g. from blml_b200.warmstart; the start phase is then skipped (blml_binned.py:403-408)."""
         self._prepare(counts_list, modes_list)
         F, code, dev = self.F, self.code, self.device
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
         if init is not None:
             if len(init) != F:
                 raise ValueError("init: one start per fit")
@@ -391,11 +393,17 @@ class BLMLBinnedBatch:
             zt = torch.as_tensor(z, dtype=torch.float64).to(dev)
             call('blml_seg_phases', code, F, self.segs_t.data_ptr(), float(self.phase_noise), zt.data_ptr(),
                  E.data_ptr(), self.st)
+        ev[1].record()
         if self.control == 'device':
             U, it, stop, L, res = self._lbfgs_device(E)
         else:
             U, it, stop, L, res = self._lbfgs(E)
-        return self._finish(E, U, it, stop, L, res)
+        ev[2].record()
+        out = self._finish(E, U, it, stop, L, res)
+        ev[3].record(); ev[3].synchronize()
+        self.timing_ = dict(start_s=ev[0].elapsed_time(ev[1]) / 1e3, lbfgs_s=ev[1].elapsed_time(ev[2]) / 1e3,
+                            finish_s=ev[2].elapsed_time(ev[3]) / 1e3)
+        return out
 
     def _lbfgs(self, E):
         """L-BFGS of every fit with the per-fit decisions on the host (vectorised NumPy, a few syncs per iteration);

@@ -260,7 +260,8 @@ def main():
         print(json.dumps({'launches': int(_lib.lib().blml_launch_count() - l0), 'bins': int(b.Btot),
                           'iterations_max': max(r.n_sweeps_ for r in res),
                           'loglik_mean': float(np.mean([r.loglik_ for r in res])),
-                          'start': getattr(b, 'start_stats_', None), 'lbfgs': getattr(b, 'lbfgs_stats_', None)}))
+                          'start': getattr(b, 'start_stats_', None), 'lbfgs': getattr(b, 'lbfgs_stats_', None),
+                          'phase_seconds': getattr(b, 'timing_', None)}))
         return
     train_dev = [torch.as_tensor(c).to(dev) for c in train]
     val_dev = [torch.as_tensor(c).to(dev) for c in val]
@@ -298,7 +299,8 @@ def main():
             certified += c1; two_sided += c2
             iters = np.array([r.n_sweeps_ for r in res]); starts = np.array([r.start_sweeps_ for r in res])
     launches = _lib.lib().blml_launch_count() - l0
-    graphs = {'start': getattr(b, 'start_stats_', None), 'lbfgs': getattr(b, 'lbfgs_stats_', None)}
+    graphs = {'start': getattr(b, 'start_stats_', None), 'lbfgs': getattr(b, 'lbfgs_stats_', None),
+              'phase_seconds': getattr(b, 'timing_', None)}
     barrier_sync(ws)
     tmax = max_over_ranks(tot, ws)
     value = sum_over_ranks(certified, ws) / tmax if tmax > 0 else 0.0
