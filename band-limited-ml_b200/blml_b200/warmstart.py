@@ -128,7 +128,7 @@ class WarmStartNet:
         dpre = self._ws('dpre', P * co, torch.bfloat16); dpreT = self._ws('dpreT', P * co, torch.bfloat16)
         call('blml_nn_relu_bwd', dY[0].data_ptr(), dY[1], dY[2], yt.data_ptr(), ycs, yc0, P, co, dpre.data_ptr(),
              dpreT.data_ptr(), self.st)
-        chunks = 128
+        chunks = int(min(2048, max(1, P // 256)))     # ~256 rows per block
         part = self._ws('bpart', chunks * co, torch.float32)
         call('blml_nn_bias_grad', dY[0].data_ptr(), dY[1], dY[2], yt.data_ptr(), ycs, yc0, P, co, 1, chunks,
              part.data_ptr(), self.g[name + '.b'].data_ptr(), self.st)
@@ -198,7 +198,7 @@ class WarmStartNet:
                                                            cat3=P3 * 384, b2=P4 * 256, b1=P4 * 256, p3=P4 * 128,
                                                            a3=P3 * 128, p2=P3 * 64, a2=P2 * 64, p1=P2 * 32,
                                                            a1=P1 * 32).items()}
-        chunks = 128
+        chunks = int(min(2048, max(1, P1 // 256)))
         part = self._ws('hpart', chunks * HEAD[1] * (HEAD[0] + 1), f)
         call('blml_nn_head_bwd', du.data_ptr(), A['d1'].data_ptr(), P1, 32, 2, self.p['head.w'].data_ptr(),
              D['d1'].data_ptr(), chunks, part.data_ptr(), self.gw_head.data_ptr(), st)

@@ -30,7 +30,7 @@ __device__ __forceinline__ void nn_mbar_expect_tx(uint64_t* bar, uint32_t bytes)
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(nn_smem_u32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool nn_mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (long it = 0; it < (1L << 22); it++) {
+  for (long it = 0; it < (1L << 20); it++) {
     uint32_t done;
     asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
                  : "=r"(done) : "r"(nn_smem_u32(bar)), "r"(parity) : "memory");

@@ -65,12 +65,13 @@ def test_forward_and_gradients_match_oracle(cuda_device):
     assert max(worst.values()) <= 2e-2, worst
 
 
+@pytest.mark.timeout(600)
 def test_short_training_lowers_loss_and_starts_converge(cuda_device):
     from blml_b200 import workloads
     from blml_b200.sweep import BLMLBinnedBatch
     from blml_b200.warmstart import WarmStartNet, make_training_set
     fits = workloads.warm_start_set(48, seed=100, shape=(32, 32))
-    b = BLMLBinnedBatch(tol=1e-5, dtype=np.float64)
+    b = BLMLBinnedBatch(tol=1e-5, dtype=np.float64, max_sweeps=5000)
     b.fit([f['counts'] for f in fits], [f['modes'] for f in fits])
     data = make_training_set(fits, [b.field(i) for i in range(len(fits))])
     net = WarmStartNet(seed=1)
@@ -78,6 +79,7 @@ def test_short_training_lowers_loss_and_starts_converge(cuda_device):
     assert hist[-1] < hist[0], hist
     test = workloads.warm_start_set(8, seed=900, shape=(32, 32))
     E0 = net.start([f['counts'] for f in test], [f['fc'] for f in test], [f['kind'] for f in test])
-    res = BLMLBinnedBatch(tol=1e-5, dtype=np.float64).fit([f['counts'] for f in test], [f['modes'] for f in test],
-                                                         init=E0)
+    res = BLMLBinnedBatch(tol=1e-5, dtype=np.float64, max_sweeps=5000).fit(
+        [f['counts'] for f in test], [f['modes'] for f in test], init=E0)
+    net.check()
     assert all(np.isfinite(r.loglik_) and r.start_sweeps_ == 0 for r in res)
