@@ -58,11 +58,14 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(NN_BM >> 4) << 24);
 }
 
-// C[z][m][n] = sum_{k in split z} A[m][k] B[n][k]; grid (ceil(M / 128), ceil(N / NT), splits); kb per split
+// C[z][m][n] = sum_{k in split z} A[m][k] B[n][k]. Persistent: at most 2 CTAs per SM (their TMEM accumulators fit
+// the SM's 512 columns together), each allocating its accumulator once and walking the tiles (m tile, n tile, split)
+// t = blockIdx.x, blockIdx.x + gridDim.x, ...; between tiles the epilogue's reads finish before the next tile's
+// first MMA overwrites the accumulator.
 __global__ void __launch_bounds__(NN_THREADS) k_gemm_bf16(const __grid_constant__ CUtensorMap mA,
                                                           const __grid_constant__ CUtensorMap mB, int M, int N,
-                                                          int NT, int tcols, int nkb, int kb_per_split, float* C,
-                                                          int* err) {
+                                                          int NT, int tcols, int nkb, int kb_per_split, int splits,
+                                                          float* C, int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(base);
@@ -70,8 +73,8 @@ __global__ void __launch_bounds__(NN_THREADS) k_gemm_bf16(const __grid_constant_
   uint64_t* bars = reinterpret_cast<uint64_t*>(sB + (size_t)NT * NN_BK);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int m0 = blockIdx.x * NN_BM, n0 = blockIdx.y * NT;
-  const int kb0 = blockIdx.z * kb_per_split, kb1 = min(nkb, kb0 + kb_per_split);
+  const int Mt = (M + NN_BM - 1) / NN_BM, Nt = (N + NT - 1) / NT;
+  const long long tiles = (long long)Mt * Nt * splits;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(nn_smem_u32(tslot)), "r"(tcols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -88,39 +91,42 @@ __global__ void __launch_bounds__(NN_THREADS) k_gemm_bf16(const __grid_constant_
   const uint32_t idesc = idesc_bf16(NT);
   bool ok = true;
   uint32_t par_last = 0;
-  int done = 0;
-  for (int kb = kb0; kb < kb1 && ok; kb++, done++) {
-    const uint32_t par = done & 1;
-    par_last = par;
-    if (tid == 0) {
-      nn_mbar_expect_tx(&bars[0], tx);
-      nn_tma_2d(sA, &mA, kb * NN_BK, m0, &bars[0]);
-      nn_tma_2d(sB, &mB, kb * NN_BK, n0, &bars[0]);
-    }
-    ok = nn_mbar_wait(&bars[0], par);
-    if (!ok) break;
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int j = 0; j < NN_BK / 16; j++) {
-        const uint64_t ad = nn_desc(sA + j * 16), bd = nn_desc(sB + j * 16);
-        const uint32_t acc = (done > 0 || j > 0) ? 1u : 0u;
-        asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                     " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                     :: "r"(taddr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+  long long phase = 0;                         // mbarrier phases used so far (both barriers advance together)
+  for (long long t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+    const int z = (int)(t / ((long long)Mt * Nt));
+    const long long rem = t - (long long)z * Mt * Nt;
+    const int nt_i = (int)(rem / Mt), mt_i = (int)(rem - (long long)nt_i * Mt);
+    const int m0 = mt_i * NN_BM, n0 = nt_i * NT;
+    const int kb0 = z * kb_per_split, kb1 = min(nkb, kb0 + kb_per_split);
+    int done = 0;
+    for (int kb = kb0; kb < kb1 && ok; kb++, done++, phase++) {
+      const uint32_t par = (uint32_t)(phase & 1);
+      par_last = par;
+      if (tid == 0) {
+        nn_mbar_expect_tx(&bars[0], tx);
+        nn_tma_2d(sA, &mA, kb * NN_BK, m0, &bars[0]);
+        nn_tma_2d(sB, &mB, kb * NN_BK, n0, &bars[0]);
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                   :: "r"(nn_smem_u32(&bars[1])) : "memory");
+      ok = nn_mbar_wait(&bars[0], par);
+      if (!ok) break;
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < NN_BK / 16; j++) {
+          const uint64_t ad = nn_desc(sA + j * 16), bd = nn_desc(sB + j * 16);
+          const uint32_t acc = (done > 0 || j > 0) ? 1u : 0u;
+          asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                       :: "r"(taddr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(nn_smem_u32(&bars[1])) : "memory");
+      }
+      ok = nn_mbar_wait(&bars[1], par);
     }
-    ok = nn_mbar_wait(&bars[1], par);
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  float* Cz = C + (size_t)blockIdx.z * M * N;
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    nn_mbar_wait(&bars[0], par_last);
-    nn_mbar_wait(&bars[1], par_last);
-  } else {
+    if (!ok) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    float* Cz = C + (size_t)z * M * N;
     const int row = m0 + 32 * warp + lane;
     for (int c0 = 0; c0 < NT; c0 += 16) {
       uint32_t v[16];
@@ -144,6 +150,17 @@ __global__ void __launch_bounds__(NN_THREADS) k_gemm_bf16(const __grid_constant_
         }
       }
     }
+    // every warp's accumulator reads are done before thread 0 issues the next tile's first MMA
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (!ok) {
+    // a bounded wait gave up: record it, then give the copy and the MMAs in flight one more bounded wait before the
+    // tensor memory is released
+    if (tid == 0) atomicExch(err, 1);
+    nn_mbar_wait(&bars[0], par_last);
+    nn_mbar_wait(&bars[1], par_last);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -457,16 +474,20 @@ int blml_nn_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int 
   if (e) return e;
   const int nkb = (K + NN_BK - 1) / NN_BK;
   const int per = (nkb + splits - 1) / splits;
-  const size_t smem = 1024 + (size_t)(NN_BM + NT) * NN_BK * 2 + 64;
+  // shared memory sized so at most 2 CTAs share an SM (their TMEM accumulators then always fit its 512 columns)
+  const size_t smem = std::max<size_t>(1024 + (size_t)(NN_BM + NT) * NN_BK * 2 + 64, 80 * 1024);
   static bool attr = false;
   if (!attr) {
-    e = cuda_status(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         1024 + (NN_BM + 256) * NN_BK * 2 + 64), "blml_nn_gemm_bf16");
+    e = cuda_status(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024),
+                    "blml_nn_gemm_bf16");
     if (e) return e;
     attr = true;
   }
-  dim3 grid((unsigned)((M + NN_BM - 1) / NN_BM), (unsigned)((N + NT - 1) / NT), (unsigned)splits);
-  k_gemm_bf16<<<grid, NN_THREADS, smem, NST>>>(mA, mB, M, N, NT, tcols, nkb, per, C, err);
+  const long long tiles = (long long)((M + NN_BM - 1) / NN_BM) * ((N + NT - 1) / NT) * splits;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  const unsigned grid = (unsigned)std::min<long long>(tiles, 2LL * sms);    // 2 CTAs per SM: TMEM 2 x 256 columns
+  k_gemm_bf16<<<grid, NN_THREADS, smem, NST>>>(mA, mB, M, N, NT, tcols, nkb, per, splits, C, err);
   BLML_CHECK_LAUNCH("blml_nn_gemm_bf16");
   return BLML_OK;
 }
