@@ -28,19 +28,20 @@ TRAIN_SEED, SWEEP_SEED, EVAL_SEED = 10_000, 20_000, 50_000
 CAP = 5000
 
 
-def engine_fields(fits, batch=64, tol=1e-6):
+def engine_fields(fits, batch=64, tol=1e-6, cap=CAP):
     """Cold fits of `fits` (dicts with counts, modes) by the batched engine, grouped in batches; returns the fields
     (device complex tensors), the BLMLBinnedBatch results and the seconds spent."""
     fields, results, secs = [], [], 0.0
     for b0 in range(0, len(fits), batch):
         part = fits[b0:b0 + batch]
         t0 = time.perf_counter()
-        b = BLMLBinnedBatch(tol=tol, dtype=np.float64, max_sweeps=CAP)
+        b = BLMLBinnedBatch(tol=tol, dtype=np.float64, max_sweeps=cap)
         res = b.fit([f['counts'] for f in part], [f['modes'] for f in part])
         torch.cuda.synchronize()
         secs += time.perf_counter() - t0
         fields += [b.field(i).clone() for i in range(len(part))]
         results += res
+        print(f'  engine fits {b0 + len(part)}/{len(fits)}: {time.perf_counter() - t0:.1f} s', flush=True)
     return fields, results, secs
 
 
@@ -56,7 +57,7 @@ def sweep_fits(n_sweeps, seed=SWEEP_SEED):
 def train(args):
     fits = workloads.warm_start_set(args.fits, seed=TRAIN_SEED, shape=(128, 128)) + sweep_fits(args.sweeps)
     t0 = time.perf_counter()
-    fields, _, fit_secs = engine_fields(fits)
+    fields, _, fit_secs = engine_fields(fits, cap=args.data_cap)
     by_shape = {}
     for f, u in zip(fits, fields):
         by_shape.setdefault(tuple(np.shape(f['counts'])), []).append((f, u))
@@ -75,7 +76,7 @@ def train(args):
                           seed=args.seed + ep)
             losses.append((h[0], data['x'].shape[0]))
         hist.append(sum(l * n for l, n in losses) / sum(n for _, n in losses))
-        print(f'epoch {ep}: loss {hist[-1]:.4f}', flush=True)
+        print(f'epoch {ep}: loss {hist[-1]:.4f} ({time.perf_counter() - t1:.1f} s)', flush=True)
     torch.cuda.synchronize()
     save_bf16(net.params_numpy(), args.out)
     print(json.dumps({'fits': len(fits), 'shapes': len(by_shape), 'fit_seconds': fit_secs,
@@ -142,6 +143,7 @@ def main():
     ap.add_argument('--out', default='warmstart_weights.npz')
     ap.add_argument('--weights', default='warmstart_weights.npz')
     ap.add_argument('--set', default='ws', choices=['ws', 'sweep'], help='eval on the warm-start set or the sweep')
+    ap.add_argument('--data-cap', type=int, default=CAP, help='iteration cap of the training fits')
     args = ap.parse_args()
     if args.mode == 'train':
         return train(args)
