@@ -521,6 +521,97 @@ __global__ void k_st_damp_pick(int Fa, const int* fid, const int* live, const in
   }
 }
 
+// the Anderson history update fused with its inner products (the real start, one mode): f = E_J - E,
+// DX_p = E - pX, DF_p = f - pF, pX = E, pF = f (each formed as the linear-combination kernel forms it), and per fit
+// [DF_p . DF_q, DF_q . f] for q < mA (quantities q and AA_MMAX + q)
+struct StHist { double* DX[AA_MMAX]; double* DF[AA_MMAX]; };
+__global__ void __launch_bounds__(256) k_st_hist(const blml_seg* segs, int mA, int p, const double* EJ, const double* E,
+                                                 double* fv, double* pX, double* pF, StHist h, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  double v[2 * AA_MMAX];
+#pragma unroll
+  for (int q = 0; q < 2 * AA_MMAX; q++) v[q] = 0.0;
+  SEG_LOOP(b, S) {
+    const int64_t i = S.off + b;
+    const double ej = EJ[i], e = E[i], px = pX[i], pf = pF[i];
+    const double f = fma(-1.0, e, ej), dx = fma(-1.0, px, e), df = fma(-1.0, pf, f);
+    fv[i] = f; h.DX[p][i] = dx; h.DF[p][i] = df; pX[i] = e; pF[i] = f;
+#pragma unroll
+    for (int q = 0; q < AA_MMAX; q++)
+      if (q < mA) {
+        const double dq = q == p ? df : h.DF[q][i];
+        v[q] += df * dq; v[AA_MMAX + q] += dq * f;
+      }
+  }
+  seg_partials<2 * AA_MMAX>(v, part);
+}
+
+// out[j * 2 mA + k]: quantity k (k < mA) or AA_MMAX + k - mA of the fit's partials, summed in order (one warp each)
+__global__ void k_st_hist_finish(const double* part, int mA, int nblk, double* out) {
+  const int j = blockIdx.x, Fa = gridDim.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = wid; k < 2 * mA; k += nw) {
+    const int q = k < mA ? k : AA_MMAX + (k - mA);
+    double x = 0.0;
+    for (int i = lane; i < nblk; i += 32) x += part[((int64_t)q * Fa + j) * nblk + i];
+    x = warp_sum(x);
+    if (lane == 0) out[(int64_t)j * 2 * mA + k] = x;
+  }
+}
+
+// two real linear combinations with the same per-fit coefficients (nt <= 3 terms; zero coefficients skipped, as in
+// the linear-combination kernel): oa = sum_i c_i a_i, ob = sum_i c_i b_i (out may alias an input)
+struct Terms3 { const double* v[3]; };
+__global__ void k_st_lin2(const blml_seg* segs, int nt, const double* coef, Terms3 a, double* oa, Terms3 b,
+                          double* ob) {
+  const blml_seg S = segs[blockIdx.y];
+  const double* cf = coef + (int64_t)blockIdx.y * nt;
+  SEG_LOOP(i, S) {
+    const int64_t o = S.off + i;
+    double xa = 0.0, xb = 0.0;
+    for (int q = 0; q < nt; q++) {
+      const double c = cf[q];
+      if (c != 0.0) { xa += c * a.v[q][o]; xb += c * b.v[q][o]; }
+    }
+    oa[o] = xa; ob[o] = xb;
+  }
+}
+
+// merit terms and residual of the real iterate (E, U) in one pass: [sum e u, sum_occ c log|e|, #(sg e <= 0),
+// max rho, #NaN rho] (the merit and residual kernels' formulas at scale 1)
+__global__ void __launch_bounds__(256) k_st_merit_resid(const blml_seg* segs, const double* E, const double* U,
+                                                        const double* c, const double* sg, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  SEG_LOOP(b, S) {
+    const double e = E[S.off + b], u = U[S.off + b], cb = c[S.boff + b];
+    v[0] += e * u;
+    if (cb > 0) {
+      v[1] += cb * log(fabs(e));
+      if (sg[S.boff + b] * e <= 0) v[2] += 1.0;
+      const double nrm2 = e * e, f = nrm2 / cb, dr = u * f - e;
+      const double r = sqrt(dr * dr) / sqrt(fmax(nrm2, 1e-300));
+      if (r != r) v[4] += 1.0; else v[3] = fmax(v[3], r);
+    }
+  }
+  seg_partials<5>(v, part, 1u << 3);
+}
+
+// out[j * 5 + q] from the fused merit / residual partials (q = 3 a maximum), one warp per quantity
+__global__ void k_finish_mr(const double* part, int nblk, double* out) {
+  const int j = blockIdx.x, Fa = gridDim.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (wid >= 5) return;
+  const bool mx = wid == 3;
+  double x = mx ? -INFINITY : 0.0;
+  for (int i = lane; i < nblk; i += 32) {
+    const double y = part[((int64_t)wid * Fa + j) * nblk + i];
+    x = mx ? fmax(x, y) : x + y;
+  }
+  x = mx ? warp_max(x) : warp_sum(x);
+  if (lane == 0) out[(int64_t)j * 5 + wid] = x;
+}
+
 __global__ void k_st_scale(int Fa, const int* fid, const double* outQ, const double* n, double* sc) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Fa) return;
@@ -535,14 +626,14 @@ __device__ __forceinline__ double nmax(double a, double b) { return (a != a || b
 // the end of a start sweep (or the set-up when init): merit and residual of the new iterate, the progress record,
 // then the stop rules the next sweep starts with (tol, stall, the sweep cap)
 __global__ void k_st_post(int Fa, int init, double tol, long long cap, long long stall, const int* fid, int* live,
-                          const blml_seg* segs_c, blml_seg* segs_eff, const double* outM1, const double* outR,
-                          StState s) {
+                          const blml_seg* segs_c, blml_seg* segs_eff, const double* outMR, StState s) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Fa) return;
   const int f = fid[j];
   if (!init && !live[f]) { set_live(j, f, 0, live, segs_c, segs_eff); return; }
-  const double cur = merit_value(outM1 + 3 * j, s.n[f]);
-  const double r = outR[2 * j + 1] > 0 ? NAN : outR[2 * j];
+  const double* mr = outMR + 5 * (int64_t)j;                 // [merit terms (3), max rho, #NaN]
+  const double cur = merit_value(mr, s.n[f]);
+  const double r = mr[4] > 0 ? NAN : mr[3];
   s.cur[f] = cur; s.res[f] = r;
   int a;
   if (init) {
@@ -856,15 +947,22 @@ struct blml_start_batch_s : Runner {
     RC(blml_seg_dots(BLML_F64, Fa_, S, 0, 1, a, b, part, outQ, sv));
     k_st_scale<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, outQ, s.n, scA);
     KCHECK("start scale");
-    const void* t1[1] = {E};
-    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, E, 1, scA, t1, sv));
-    t1[0] = U;
-    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, U, 1, scA, t1, sv));
-    RC(blml_seg_merit(BLML_F64, Fa_, S, 0, 0, E, U, c, sg, part, outM1, sv));
-    RC(blml_seg_resid(BLML_F64, Fa_, S, 0, E, U, c, ones, part, outR, sv));
-    k_st_post<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, init, tol, cap, stall, d_fid, d_live, d_segs_c, d_segs_eff,
-                                              outM1, outR, s);
+    const dim3 grid((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_);
+    k_st_lin2<<<grid, 256, 0, st>>>(S, 1, scA, Terms3{{E, nullptr, nullptr}}, E, Terms3{{U, nullptr, nullptr}}, U);
+    KCHECK("start rescale");
+    k_st_merit_resid<<<grid, 256, 0, st>>>(S, E, U, c, sg, part);
+    KCHECK("start merit / residual");
+    RC(seg_finish_mr(Fa_));
+    k_st_post<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, init, tol, cap, stall, d_fid, d_live, d_segs_c, d_segs_eff, outR,
+                                              s);
     KCHECK("start post");
+    return BLML_OK;
+  }
+
+  // the fused merit / residual partials -> outR [Fa x 5] (sums, the residual as a maximum)
+  int seg_finish_mr(int Fa_) {
+    k_finish_mr<<<Fa_, 256, 0, st>>>(part, seg_blocks_for(Fa_), outR);
+    KCHECK("start merit / residual finish");
     return BLML_OK;
   }
 
@@ -876,20 +974,14 @@ struct blml_start_batch_s : Runner {
     RC(blml_group_matvec_masked(gJ, d_fid, Fa_, d_live, sv));
     RC(blml_seg_merit(BLML_F64, Fa_, S, 0, 0, EJ, UJ, c, sg, part, outM1, sv));
     const void* t[2 + 2 * AA_MMAX];
+    const dim3 grid((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_);
     if (mA) {
-      t[0] = EJ; t[1] = E;
-      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, fv, 2, c1m1, t, sv));
-      t[0] = E; t[1] = pX;
-      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, DX[p], 2, c1m1, t, sv));
-      t[0] = fv; t[1] = pF;
-      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, DF[p], 2, c1m1, t, sv));
-      const void* a[2 * AA_MMAX]; const void* b[2 * AA_MMAX];
-      for (int q = 0; q < mA; q++) { a[q] = DF[p]; b[q] = DF[q]; a[mA + q] = DF[q]; b[mA + q] = fv; }
-      RC(blml_seg_dots(BLML_F64, Fa_, S, 0, 2 * mA, a, b, part, outA, sv));
-      t[0] = E;
-      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, pX, 1, ones, t, sv));
-      t[0] = fv;
-      RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, pF, 1, ones, t, sv));
+      StHist h{};
+      for (int q = 0; q < mA; q++) { h.DX[q] = DX[q]; h.DF[q] = DF[q]; }
+      k_st_hist<<<grid, 256, 0, st>>>(S, mA, p, EJ, E, fv, pX, pF, h, part);
+      KCHECK("start history");
+      k_st_hist_finish<<<Fa_, 256, 0, st>>>(part, mA, seg_blocks_for(Fa_), outA);
+      KCHECK("start history finish");
       k_st_anderson<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, mA, p, d_fid, d_live, outM1, outA, s, cA, useA);
       KCHECK("start anderson");
       t[0] = E; t[1] = fv;
@@ -900,10 +992,8 @@ struct blml_start_batch_s : Runner {
     }
     k_st_take<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, mA, d_fid, d_live, outM1, outM2, useA, s, cT, damp);
     KCHECK("start take");
-    t[0] = EA; t[1] = EJ;
-    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, ET, 2, cT, t, sv));
-    t[0] = UA; t[1] = UJ;
-    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, UT, 2, cT, t, sv));
+    k_st_lin2<<<grid, 256, 0, st>>>(S, 2, cT, Terms3{{EA, EJ, nullptr}}, ET, Terms3{{UA, UJ, nullptr}}, UT);
+    KCHECK("start candidate");
     k_st_damp_trials<<<dim3((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_), 256, 0, st>>>(S, damp, E, EJ, U, UJ, c, sg,
                                                                                          part);
     KCHECK("start damping trials");
@@ -911,10 +1001,8 @@ struct blml_start_batch_s : Runner {
     KCHECK("start damping finish");
     k_st_damp_pick<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, damp, outDT, s, cE);
     KCHECK("start damping pick");
-    t[0] = E; t[1] = EJ; t[2] = ET;
-    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, E, 3, cE, t, sv));
-    t[0] = U; t[1] = UJ; t[2] = UT;
-    RC(blml_seg_lincomb(BLML_F64, Fa_, S, 0, U, 3, cE, t, sv));
+    k_st_lin2<<<grid, 256, 0, st>>>(S, 3, cE, Terms3{{E, EJ, ET}}, E, Terms3{{U, UJ, UT}}, U);
+    KCHECK("start step");
     return rescale_post(0);
   }
 
@@ -1088,7 +1176,7 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
     const int nq = 3 * DAMP_NT;           // the widest reduction: the damping trials' 78 quantities
     const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F *
-                                     (3 + 3 + 2 * AA_MMAX + 1 + 2 + nq + 2 + 1 + (2 + 2 * AA_MMAX) + 2 + 3 + 1 + 1)));
+                                     (3 + 3 + 2 * AA_MMAX + 1 + 5 + nq + 2 + 1 + (2 + 2 * AA_MMAX) + 2 + 3 + 1 + 1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (8 + (size_t)AA_MMAX * AA_MMAX));
     int* ist = (int*)r->dalloc(sizeof(int) * (size_t)F * (6 + AA_MMAX + 2));
     if (!scr || !stt || !ist) { set_error("blml_start_batch_create: allocation"); rc = BLML_ERR_CUDA; }
@@ -1097,7 +1185,7 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
       double* x = scr + nq * pw;
       auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
       r->outM1 = take(3); r->outM2 = take(3); r->outA = take(2 * AA_MMAX);
-      r->outQ = take(1); r->outR = take(2); r->outDT = take(nq); r->c1m1 = take(2); r->ones = take(1);
+      r->outQ = take(1); r->outR = take(5); r->outDT = take(nq); r->c1m1 = take(2); r->ones = take(1);
       r->cA = take(2 + 2 * AA_MMAX); r->cT = take(2); r->cE = take(3); r->scA = take(1); r->s0c = take(1);
       double* y = stt;
       auto tk = [&](size_t k) { double* p = y; y += k * F; return p; };
