@@ -296,15 +296,17 @@ class WarmStartNet:
         """One complex start per fit: e0 = w / conj(u) on the occupied bins (w = counts), 0 elsewhere. Fits are
         grouped by lattice shape for the network."""
         out = [None] * len(counts_list)
+        host = [c.detach().cpu().numpy() if isinstance(c, torch.Tensor) else np.asarray(c, float) for c in counts_list]
         by_shape = {}
-        for i, c in enumerate(counts_list):
+        for i, c in enumerate(host):
             by_shape.setdefault(tuple(np.shape(c)), []).append(i)
         for shape, ids in by_shape.items():
-            x = torch.as_tensor(features([counts_list[i] for i in ids], [fcs[i] for i in ids],
+            x = torch.as_tensor(features([host[i] for i in ids], [fcs[i] for i in ids],
                                          [kinds[i] for i in ids])).to(self.device, torch.bfloat16)
             u = self.predict(x, batch)
             for j, i in enumerate(ids):
-                w = torch.as_tensor(np.asarray(counts_list[i], float)).to(self.device)
+                c = counts_list[i]
+                w = (c if isinstance(c, torch.Tensor) else torch.as_tensor(host[i])).to(self.device, torch.float64)
                 uc = u[j].to(torch.complex128)
                 ok = (w > 0) & (uc.abs() > 0)
                 e0 = torch.where(ok, w / torch.conj(torch.where(ok, uc, torch.ones_like(uc))), torch.zeros_like(uc))
