@@ -108,12 +108,19 @@ def dist_init():
     return 0, 1, 0
 
 
+def _red_device():
+    """Where the process group reduces: the GPU under NCCL, the host under gloo (the CPU tests of the N > 1 path)."""
+    import torch.distributed as dist
+    return 'cuda' if dist.get_backend() == 'nccl' else 'cpu'
+
+
 def barrier_sync(ws):
     import torch
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def max_over_ranks(x, ws):
@@ -121,7 +128,7 @@ def max_over_ranks(x, ws):
     if ws == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    t = torch.tensor([float(x)], dtype=torch.float64, device=_red_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -131,9 +138,15 @@ def sum_over_ranks(x, ws):
     if ws == 1:
         return x
     import torch.distributed as dist
-    t = torch.tensor([float(x)], dtype=torch.float64, device='cuda')
+    t = torch.tensor([float(x)], dtype=torch.float64, device=_red_device())
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def replica_value(certified, seconds, ws):
+    """Whole-job certified fits/s of N replicas: every rank's certified fits over the slowest rank's time."""
+    tmax = max_over_ranks(seconds, ws)
+    return (sum_over_ranks(certified, ws) / tmax if tmax > 0 else 0.0), tmax
 
 
 def grouped_matvec_roofline(batch, reps=20):
@@ -340,8 +353,7 @@ def main():
     graphs = {'start': getattr(b, 'start_stats_', None), 'lbfgs': getattr(b, 'lbfgs_stats_', None),
               'phase_seconds': getattr(b, 'timing_', None)}
     barrier_sync(ws)
-    tmax = max_over_ranks(tot, ws)
-    value = sum_over_ranks(certified, ws) / tmax if tmax > 0 else 0.0
+    value, tmax = replica_value(certified, tot, ws)
     # end to end through the public API: host counts in, densities and held-out scores out, every step
     e2e_t = 0.0; e2e_cert = 0; d2h = 0
     for _ in range(args.steps):
