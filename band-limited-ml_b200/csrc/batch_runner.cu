@@ -476,46 +476,65 @@ __global__ void k_st_take(int Fa, int mA, const int* fid, const int* live, const
   }
 }
 
-// the damped Jacobi steps of the fits that need them, every trial a = 2^-1 .. 2^-26 in one pass: the merit terms of
-// E + a (E_J - E), U + a (U_J - U), formed as the linear-combination kernel forms them
-__global__ void __launch_bounds__(256) k_st_damp_trials(const blml_seg* segs, const int* damp, const double* E,
+// the damped Jacobi steps of the fits whose flag is set, the trials a = 2^-(j0 + 1) .. 2^-(j0 + NTG) in one pass: the
+// merit terms of E + a (E_J - E), U + a (U_J - U), formed as the linear-combination kernel forms them
+constexpr int DAMP_T1 = 4, DAMP_T2 = DAMP_NT - DAMP_T1;
+template <int NTG>
+__global__ void __launch_bounds__(256) k_st_damp_trials(const blml_seg* segs, const int* flag, int j0, const double* E,
                                                         const double* EJ, const double* U, const double* UJ,
                                                         const double* c, const double* sg, double* part) {
-  if (!damp[blockIdx.y]) return;
+  if (!flag[blockIdx.y]) return;
   const blml_seg S = segs[blockIdx.y];
-  double v[3 * DAMP_NT];
+  double v[3 * NTG];
 #pragma unroll
-  for (int q = 0; q < 3 * DAMP_NT; q++) v[q] = 0.0;
+  for (int q = 0; q < 3 * NTG; q++) v[q] = 0.0;
+  const double a0 = ldexp(1.0, -(j0 + 1));
   SEG_LOOP(b, S) {
     const double e0 = E[S.off + b], e1 = EJ[S.off + b], u0 = U[S.off + b], u1 = UJ[S.off + b];
     const double cb = c[S.boff + b], sgb = sg[S.boff + b];
-    double a = 0.5;
+    double a = a0;
 #pragma unroll
-    for (int k = 0; k < DAMP_NT; k++) {
+    for (int k = 0; k < NTG; k++) {
       const double e = fma(a, e1, (1.0 - a) * e0), u = fma(a, u1, (1.0 - a) * u0);
       v[3 * k] += e * u;
       if (cb > 0) { v[3 * k + 1] += cb * log(fabs(e)); if (sgb * e <= 0) v[3 * k + 2] += 1.0; }
       a *= 0.5;
     }
   }
-  seg_partials<3 * DAMP_NT>(v, part);
+  seg_partials<3 * NTG>(v, part);
 }
 
-// the first damped trial whose merit does not fall below the current one; the coefficients of the new iterate over
-// [E, E_J, E_T] (no step found: the iterate stays)
-__global__ void k_st_damp_pick(int Fa, const int* fid, const int* live, const int* damp, const double* outDT,
-                               StState s, double* cE) {
+// the first damped trial (of the first 4) whose merit does not fall below the current one; the coefficients of the
+// new iterate over [E, E_J, E_T]; need2 marks the damping fits that try the other 22
+__global__ void k_st_damp_pick1(int Fa, const int* fid, const int* live, const int* damp, const double* T1, StState s,
+                                double* cE, int* need2) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= Fa) return;
   const int f = fid[j];
   double* ce = cE + 3 * (int64_t)j;
   ce[0] = 0.0; ce[1] = 0.0; ce[2] = 1.0;
+  need2[j] = 0;
   if (!live[f] || !damp[j]) return;
-  ce[0] = 1.0; ce[2] = 0.0;
+  ce[0] = 1.0; ce[2] = 0.0;                       // no step found: the iterate stays
   const double cur = s.cur[f];
   double a = 0.5;
-  for (int k = 0; k < DAMP_NT; k++) {
-    const double mt = merit_value(outDT + (int64_t)j * 3 * DAMP_NT + 3 * k, s.n[f]);
+  for (int k = 0; k < DAMP_T1; k++) {
+    const double mt = merit_value(T1 + (int64_t)j * 3 * DAMP_T1 + 3 * k, s.n[f]);
+    if (mt >= cur) { ce[0] = 1.0 - a; ce[1] = a; s.mJ[f] = mt; return; }
+    a *= 0.5;
+  }
+  need2[j] = 1;
+}
+
+__global__ void k_st_damp_pick2(int Fa, const int* fid, const int* need2, const double* T2, StState s, double* cE) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= Fa || !need2[j]) return;
+  const int f = fid[j];
+  double* ce = cE + 3 * (int64_t)j;
+  const double cur = s.cur[f];
+  double a = ldexp(1.0, -(DAMP_T1 + 1));
+  for (int k = 0; k < DAMP_T2; k++) {
+    const double mt = merit_value(T2 + (int64_t)j * 3 * DAMP_T2 + 3 * k, s.n[f]);
     if (mt >= cur) { ce[0] = 1.0 - a; ce[1] = a; s.mJ[f] = mt; return; }
     a *= 0.5;
   }
@@ -933,9 +952,9 @@ struct blml_start_batch_s : Runner {
   const double *c = nullptr, *sg = nullptr;
   double *U, *EJ, *UJ, *EA, *UA, *ET, *UT, *fv, *pX, *pF;
   double *DX[AA_MMAX] = {}, *DF[AA_MMAX] = {};
-  double *part = nullptr, *outM1, *outM2, *outA, *outQ, *outR, *outDT;
+  double *part = nullptr, *outM1, *outM2, *outA, *outQ, *outR, *outDT, *outDT2;
   double *c1m1, *ones, *cA, *cT, *cE, *scA, *s0c;
-  int *useA, *damp;
+  int *useA, *damp, *need2d;
   std::vector<double> s0_host;
   StState s{};
 
@@ -994,12 +1013,18 @@ struct blml_start_batch_s : Runner {
     KCHECK("start take");
     k_st_lin2<<<grid, 256, 0, st>>>(S, 2, cT, Terms3{{EA, EJ, nullptr}}, ET, Terms3{{UA, UJ, nullptr}}, UT);
     KCHECK("start candidate");
-    k_st_damp_trials<<<dim3((unsigned)seg_blocks_for(Fa_), (unsigned)Fa_), 256, 0, st>>>(S, damp, E, EJ, U, UJ, c, sg,
-                                                                                         part);
+    // damped steps: 4 trials, then 22 more for the fits none of the 4 served
+    k_st_damp_trials<DAMP_T1><<<grid, 256, 0, st>>>(S, damp, 0, E, EJ, U, UJ, c, sg, part);
     KCHECK("start damping trials");
-    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 3 * DAMP_NT, seg_blocks_for(Fa_), damp, outDT);
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 3 * DAMP_T1, seg_blocks_for(Fa_), damp, outDT);
     KCHECK("start damping finish");
-    k_st_damp_pick<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, damp, outDT, s, cE);
+    k_st_damp_pick1<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, d_live, damp, outDT, s, cE, need2d);
+    KCHECK("start damping pick");
+    k_st_damp_trials<DAMP_T2><<<grid, 256, 0, st>>>(S, need2d, DAMP_T1, E, EJ, U, UJ, c, sg, part);
+    KCHECK("start damping trials");
+    k_finish_flagged<<<Fa_, 256, 0, st>>>(part, 3 * DAMP_T2, seg_blocks_for(Fa_), need2d, outDT2);
+    KCHECK("start damping finish");
+    k_st_damp_pick2<<<nblk(Fa_, 128), 128, 0, st>>>(Fa_, d_fid, need2d, outDT2, s, cE);
     KCHECK("start damping pick");
     k_st_lin2<<<grid, 256, 0, st>>>(S, 3, cE, Terms3{{E, EJ, ET}}, E, Terms3{{U, UJ, UT}}, U);
     KCHECK("start step");
@@ -1176,16 +1201,17 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
     const int nq = 3 * DAMP_NT;           // the widest reduction: the damping trials' 78 quantities
     const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F *
-                                     (3 + 3 + 2 * AA_MMAX + 1 + 5 + nq + 2 + 1 + (2 + 2 * AA_MMAX) + 2 + 3 + 1 + 1)));
+                                     (3 + 3 + 2 * AA_MMAX + 1 + 5 + nq + nq + 2 + 1 + (2 + 2 * AA_MMAX) + 2 + 3 +
+                                      1 + 1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (8 + (size_t)AA_MMAX * AA_MMAX));
-    int* ist = (int*)r->dalloc(sizeof(int) * (size_t)F * (6 + AA_MMAX + 2));
+    int* ist = (int*)r->dalloc(sizeof(int) * (size_t)F * (6 + AA_MMAX + 3));
     if (!scr || !stt || !ist) { set_error("blml_start_batch_create: allocation"); rc = BLML_ERR_CUDA; }
     else {
       r->part = scr;
       double* x = scr + nq * pw;
       auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
       r->outM1 = take(3); r->outM2 = take(3); r->outA = take(2 * AA_MMAX);
-      r->outQ = take(1); r->outR = take(5); r->outDT = take(nq); r->c1m1 = take(2); r->ones = take(1);
+      r->outQ = take(1); r->outR = take(5); r->outDT = take(nq); r->outDT2 = take(nq); r->c1m1 = take(2); r->ones = take(1);
       r->cA = take(2 + 2 * AA_MMAX); r->cT = take(2); r->cE = take(3); r->scA = take(1); r->s0c = take(1);
       double* y = stt;
       auto tk = [&](size_t k) { double* p = y; y += k * F; return p; };
@@ -1194,7 +1220,7 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
       int* z = ist;
       auto ti = [&](size_t k) { int* p = z; z += k * F; return p; };
       r->s.valid = ti(AA_MMAX); r->s.has_prev = ti(1); r->s.best_it = ti(1); r->s.it = ti(1); r->s.active = ti(1);
-      r->useA = ti(1); r->damp = ti(1);
+      r->useA = ti(1); r->damp = ti(1); r->need2d = ti(1);
       std::vector<double> cm(2 * (size_t)F);
       for (int f = 0; f < F; f++) { cm[2 * f] = 1.0; cm[2 * f + 1] = -1.0; }
       rc = cuda_status(cudaMemcpyAsync(r->c1m1, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, r->st),
