@@ -2,6 +2,7 @@
 
     python -m blml_b200.warmstart_job train --fits 2048 --sweeps 8 --epochs 20 --out weights.npz
     python -m blml_b200.warmstart_job eval --weights weights.npz --fits 512 [--set sweep]
+    python -m blml_b200.warmstart_job gemm [--mnk 262144,288,864]      # the BF16 tcgen05 product alone
 
 train: fits of workloads.warm_start_set (128 x 128, two-disk pupils under a pball kernel or two-slit pupils under a
 slits x sinc kernel, fc ~ U(0.1, 0.4), N = 10^U(4, 6)) plus cut-off sweeps of other seeds than the benchmark's
@@ -131,9 +132,28 @@ def evaluate(net, fits, tol=1e-6, batch=64):
                 warm_iterations_mean=float(itw.mean()), iteration_ratio=float(itc.mean() / max(itw.mean(), 1e-9)))
 
 
+def gemm_bench(M, N, K, reps=10):
+    """The network's BF16 tcgen05 product C = A B^T at one shape (random operands): TFLOP/s by CUDA events."""
+    from ._lib import call
+    g = torch.Generator(device='cuda').manual_seed(0)
+    A = torch.randn(M, K, device='cuda', generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device='cuda', generator=g).to(torch.bfloat16)
+    C = torch.empty(M, N, device='cuda'); err = torch.zeros(1, dtype=torch.int32, device='cuda')
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        call('blml_nn_gemm_bf16', A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K, 1, err.data_ptr(), st)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call('blml_nn_gemm_bf16', A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K, 1, err.data_ptr(), st)
+    e1.record(); torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    return dict(M=M, N=N, K=K, us=t * 1e6, tflops=2.0 * M * N * K / t / 1e12, err=int(err.item()))
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('mode', choices=['train', 'eval'])
+    ap.add_argument('mode', choices=['train', 'eval', 'gemm'])
     ap.add_argument('--fits', type=int, default=2048)
     ap.add_argument('--sweeps', type=int, default=8)
     ap.add_argument('--epochs', type=int, default=20)
@@ -144,9 +164,13 @@ def main():
     ap.add_argument('--weights', default='warmstart_weights.npz')
     ap.add_argument('--set', default='ws', choices=['ws', 'sweep'], help='eval on the warm-start set or the sweep')
     ap.add_argument('--data-cap', type=int, default=CAP, help='iteration cap of the training fits')
+    ap.add_argument('--mnk', default='262144,288,864', help='gemm: M,N,K (the decoder product at 16 x 128^2)')
     args = ap.parse_args()
     if args.mode == 'train':
         return train(args)
+    if args.mode == 'gemm':
+        print(json.dumps(gemm_bench(*[int(v) for v in args.mnk.split(',')])), flush=True)
+        return
     net = load(args.weights)
     if args.set == 'sweep':                         # the benchmark's 64-fit cut-off sweep (seed 0)
         fits = sweep_fits(1, seed=0)
