@@ -188,6 +188,31 @@ __global__ void __launch_bounds__(256) k_seg_dots2(const blml_seg* segs, int cpl
   seg_partials<43>(v, part);
 }
 
+// the same scan for float64 complex vectors, one 16-byte (re, im) load per element and vector
+__global__ void __launch_bounds__(256) k_seg_dots2_c128(const blml_seg* segs, int np, SegList al, const void* b0,
+                                                        const void* b1, const void* x, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  const int64_t o = S.off, n = (int64_t)S.K * S.B;
+  double v[43];
+#pragma unroll
+  for (int q = 0; q < 43; q++) v[q] = 0.0;
+  const double2* B0 = reinterpret_cast<const double2*>(b0) + o;
+  const double2* B1 = reinterpret_cast<const double2*>(b1) + o;
+  const double2* X = x ? reinterpret_cast<const double2*>(x) + o : nullptr;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double2 y0 = B0[i], y1 = B1[i];
+#pragma unroll
+    for (int q = 0; q < 20; q++)
+      if (q < np) {
+        const double2 a = reinterpret_cast<const double2*>(al.a[q])[o + i];
+        v[q] += a.x * y0.x + a.y * y0.y; v[20 + q] += a.x * y1.x + a.y * y1.y;
+      }
+    v[40] += y0.x * y0.x + y0.y * y0.y; v[41] += y1.x * y1.x + y1.y * y1.y;
+    if (X) { const double2 z = X[i]; v[42] += z.x * z.x + z.y * z.y; }
+  }
+  seg_partials<43>(v, part);
+}
+
 // out[f * (2 np + 3) + q] from the 43-quantity partials (quantities 20.. shifted down when np < 20)
 __global__ void k_seg_finish_dots2(const double* part, int np, int nblk, double* out) {
   const int f = blockIdx.x, F = gridDim.x, nq = 2 * np + 3;
@@ -473,7 +498,8 @@ int blml_seg_dots2(int dtype, int F, const blml_seg* segs, int cplx, int np, con
   if (np < 1 || np > 20 || !a || !b0 || !b1) { set_error("blml_seg_dots2: 1..20 vectors, b0 and b1"); return BLML_ERR_ARG; }
   SegList al;
   for (int q = 0; q < 20; q++) al.a[q] = q < np ? a[q] : nullptr;
-  if (dtype == BLML_F64) k_seg_dots2<double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
+  if (dtype == BLML_F64 && cplx) k_seg_dots2_c128<<<SGRID(F), 256, 0, SST>>>(segs, np, al, b0, b1, x, part);
+  else if (dtype == BLML_F64) k_seg_dots2<double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
   else k_seg_dots2<float><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
   BLML_CHECK_LAUNCH("blml_seg_dots2");
   k_seg_finish_dots2<<<F, 256, 0, SST>>>(part, np, seg_blocks_for(F), out);
