@@ -15,7 +15,7 @@ it).
 Multi-GPU: the fits are independent (no exchange step): N ranks run N replicas of the sweep; value is all ranks'
 certified fits over the slowest rank's time.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--one-fit] [--matvec]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--one-fit] [--matvec] [--pairs]
 """
 import argparse
 import json
@@ -270,6 +270,43 @@ def learned_arm(dev, sweep, modes, train_dev, val_dev, ll_ref, flush, ws, steps=
                     'batched L-BFGS; certified against the single-fit engine like the main value'}
 
 
+def pairs_bench(dev, reps=3):
+    """The pair path at the 5-D workload (n = 2e5 points of an 8-component mixture binned at 1/64, B ~ 1.84e5
+    occupied bins, sinc fc = 0.1 cycles per bin per column): one full rows pass s = S w over all B^2 bin pairs, float64
+    and float32 tables (float64 sums), CUDA events; beside it the CPU oracle (NumPy, float64) on a bounded sample of
+    rows against all B bins, scaled to pairs/s."""
+    import torch
+    from blml_b200 import workloads
+    from blml_b200.quick import bin_points
+    from blml_b200.local_gpu import ProductKernel, rows_dev
+    X = workloads.points_5d_mixture(seed=0)
+    u, cnt = bin_points(X, 1 / 64, device=dev)
+    B = int(u.shape[0])
+    tab = ProductKernel(['sinc'] * 5).tables(np.full(5, 0.1 * 64), [None] * 5, np.full(5, 1 / 64), u.cpu().numpy())
+    w = cnt.to(dev)
+    out = {'workload': '5-D pair rows: n = 2e5 points, 8-component mixture, bins at 1/64, sinc fc 0.1 / bin',
+           'bins': B, 'pairs_per_pass': B * B}
+    for name, f32 in (('f64_tables', False), ('f32_tables', True)):
+        rows_dev(u, u, w, tab, f32=f32)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            rows_dev(u, u, w, tab, f32=f32)
+        e1.record(); torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        out[name] = {'seconds_per_pass': t, 'Gpair_per_s': B * B / t / 1e9}
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import pairs_oracle as po
+    Z = u.cpu().numpy()
+    otab = po.build_tables(['sinc'] * 5, np.full(5, 0.1 * 64), [None] * 5, np.full(5, 1 / 64), Z)
+    R = 256
+    t0 = time.perf_counter(); po.rows(otab, Z[:R], Z, cnt.cpu().numpy()); t = time.perf_counter() - t0
+    out['cpu_oracle'] = {'Gpair_per_s': R * B / t / 1e9, 'sample': f'{R} rows x {B} bins in {t:.1f} s',
+                         'cores': os.cpu_count(), 'kind': 'port'}
+    return out
+
+
 def flush_l2(buf):
     buf.add_(1.0)
 
@@ -281,6 +318,8 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     ap.add_argument('--one-fit', action='store_true', help='one batched sweep and exit (profiling runs)')
+    ap.add_argument('--pairs', action='store_true',
+                    help='the 5-D pair path: one full rows pass over all bin pairs, GPU and a CPU-oracle sample')
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
@@ -296,6 +335,9 @@ def main():
     torch.cuda.set_device(dev)
     sweep, modes = workload(seed=0)                    # every rank runs a replica of the same sweep
     train = [f['train'] for f in sweep]; val = [f['val'] for f in sweep]
+    if args.pairs:
+        print(json.dumps(pairs_bench(dev)), flush=True)
+        return
     if args.matvec:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
         b._prepare(train, modes)
