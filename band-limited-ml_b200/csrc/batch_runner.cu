@@ -953,7 +953,7 @@ struct blml_start_batch_s : Runner {
   double *U, *EJ, *UJ, *EA, *UA, *ET, *UT, *fv, *pX, *pF;
   double *DX[AA_MMAX] = {}, *DF[AA_MMAX] = {};
   double *part = nullptr, *outM1, *outM2, *outA, *outQ, *outR, *outDT, *outDT2;
-  double *c1m1, *ones, *cA, *cT, *cE, *scA, *s0c;
+  double *cA, *cT, *cE, *scA, *s0c;
   int *useA, *damp, *need2d;
   std::vector<double> s0_host;
   StState s{};
@@ -1201,8 +1201,7 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
     const int nq = 3 * DAMP_NT;           // the widest reduction: the damping trials' 78 quantities
     const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F *
-                                     (3 + 3 + 2 * AA_MMAX + 1 + 5 + nq + nq + 2 + 1 + (2 + 2 * AA_MMAX) + 2 + 3 +
-                                      1 + 1)));
+                                     (3 + 3 + 2 * AA_MMAX + 1 + 5 + nq + nq + (2 + 2 * AA_MMAX) + 2 + 3 + 1 + 1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (8 + (size_t)AA_MMAX * AA_MMAX));
     int* ist = (int*)r->dalloc(sizeof(int) * (size_t)F * (6 + AA_MMAX + 3));
     if (!scr || !stt || !ist) { set_error("blml_start_batch_create: allocation"); rc = BLML_ERR_CUDA; }
@@ -1211,7 +1210,7 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
       double* x = scr + nq * pw;
       auto take = [&](size_t k) { double* p = x; x += k * F; return p; };
       r->outM1 = take(3); r->outM2 = take(3); r->outA = take(2 * AA_MMAX);
-      r->outQ = take(1); r->outR = take(5); r->outDT = take(nq); r->outDT2 = take(nq); r->c1m1 = take(2); r->ones = take(1);
+      r->outQ = take(1); r->outR = take(5); r->outDT = take(nq); r->outDT2 = take(nq);
       r->cA = take(2 + 2 * AA_MMAX); r->cT = take(2); r->cE = take(3); r->scA = take(1); r->s0c = take(1);
       double* y = stt;
       auto tk = [&](size_t k) { double* p = y; y += k * F; return p; };
@@ -1221,16 +1220,11 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
       auto ti = [&](size_t k) { int* p = z; z += k * F; return p; };
       r->s.valid = ti(AA_MMAX); r->s.has_prev = ti(1); r->s.best_it = ti(1); r->s.it = ti(1); r->s.active = ti(1);
       r->useA = ti(1); r->damp = ti(1); r->need2d = ti(1);
-      std::vector<double> cm(2 * (size_t)F);
-      for (int f = 0; f < F; f++) { cm[2 * f] = 1.0; cm[2 * f + 1] = -1.0; }
-      rc = cuda_status(cudaMemcpyAsync(r->c1m1, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice, r->st),
-                       "start");
-      k_fill_double<<<nblk(F, 256), 256, 0, r->st>>>(r->ones, F, 1.0);
       cudaMemsetAsync(r->s.G, 0, sizeof(double) * (size_t)F * AA_MMAX * AA_MMAX, r->st);
       cudaMemsetAsync(r->s.valid, 0, sizeof(int) * (size_t)F * AA_MMAX, r->st);
       cudaMemsetAsync(r->outM2, 0, sizeof(double) * 3 * (size_t)F, r->st);
       cudaMemsetAsync(r->useA, 0, sizeof(int) * (size_t)F, r->st);
-      if (!rc) rc = cuda_status(cudaMemcpyAsync(r->s.n, n, F * sizeof(double), cudaMemcpyHostToDevice, r->st), "start n");
+      rc = cuda_status(cudaMemcpyAsync(r->s.n, n, F * sizeof(double), cudaMemcpyHostToDevice, r->st), "start n");
       if (!rc) rc = cuda_status(cudaStreamSynchronize(r->st), "start create");
     }
   }
