@@ -56,6 +56,7 @@ _SIGS = {
     'blml_seg_axpy2': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P]),
     'blml_seg_finish': (_I, [_I, _I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_seg_log_score': (_I, [_I, _I, _P, _I, _P, _P, _P, _D, _P, _P, _P]),
+    'blml_seg_val_score': (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     'blml_seg_phases': (_I, [_I, _I, _P, _D, _P, _P, _P]),
     'blml_seg_real_to_complex': (_I, [_I, _I, _P, _P, _P, _P, _P]),
     'blml_group_matvec_masked': (_I, [_P, _P, _I, _P, _P]),

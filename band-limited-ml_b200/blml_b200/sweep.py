@@ -599,6 +599,21 @@ class BLMLBinnedBatch:
         a, b = self.boff[f], self.boff[f + 1]
         return self.dens_t[a:b].cpu().numpy().reshape(self.shapes[f])
 
+    def val_score(self, counts_list):
+        """Per fit: the mean log-probability of the counts (validation counts on the fit's lattice) with bin
+        probabilities p = f / sum f over every bin, f floored at 1e-300 (the cut-off search's objective,
+        selector.py:712-716); one launch for all fits."""
+        m = torch.cat([c.reshape(-1).to(self.device, self.rt) if isinstance(c, torch.Tensor) else
+                       torch.as_tensor(np.asarray(c, float).ravel(), dtype=self.rt).to(self.device)
+                       for c in counts_list])
+        if m.numel() != self.Btot:
+            raise ValueError("val_score: one lattice per fit, of the fit's shape")
+        call('blml_seg_val_score', self.code, self.F, self.segs_t.data_ptr(), self.dens_t.data_ptr(), m.data_ptr(),
+             self.part.data_ptr(), self.out.data_ptr(), self.st)
+        r = self._read(3)
+        with np.errstate(divide='ignore', invalid='ignore'):
+            return (r[:, 1] - r[:, 2] * np.log(r[:, 0])) / r[:, 2]
+
     def log_density(self, counts_list, eps=0.0):
         """Per fit: mean over the counts of log(f_b + eps), f = F / Q (blml_binned.py:630-645), one launch for all."""
         m = torch.cat([c.reshape(-1).to(self.device, self.rt) if isinstance(c, torch.Tensor) else

@@ -370,6 +370,22 @@ __global__ void k_seg_log_score(const blml_seg* segs, const void* U, const T* m,
   seg_partials<2>(v, part);
 }
 
+// the cut-off search's validation score per fit (selector.py:712-716): with f the fitted density on every bin of the
+// lattice and p = max(f, 1e-300), the three sums sum_b p, sum_b va log p and sum_b va; the score is
+// (sum va log p - sum va log sum p) / sum va, the mean log-probability of the validation counts
+template <typename T>
+__global__ void k_seg_val_score(const blml_seg* segs, const T* dens, const T* va, double* part) {
+  const blml_seg S = segs[blockIdx.y];
+  double v[3] = {0.0, 0.0, 0.0};
+  SEG_LOOP(b, S) {
+    const double p = fmax((double)dens[S.boff + b], 1e-300);
+    const double a = (double)va[S.boff + b];
+    v[0] += p;
+    if (a > 0) { v[1] += a * log(p); v[2] += a; }
+  }
+  seg_partials<3>(v, part);
+}
+
 // start noise of every fit (the phases of mode 0; complex fits of one mode): E[0] *= exp(i pn z), z per fit at boff
 template <typename T>
 __global__ void k_seg_phases(const blml_seg* segs, double pn, const double* z, void* E) {
@@ -595,6 +611,16 @@ int blml_seg_log_score(int dtype, int F, const blml_seg* segs, int cplx, const v
   }
   BLML_CHECK_LAUNCH("blml_seg_log_score");
   return seg_finish(part, F, 2, 0u, out, SST);
+}
+
+int blml_seg_val_score(int dtype, int F, const blml_seg* segs, const void* dens, const void* va, double* part,
+                       double* out, void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_val_score") || !dens || !va || !part || !out) return BLML_ERR_ARG;
+  if (dtype == BLML_F64)
+    k_seg_val_score<double><<<SGRID(F), 256, 0, SST>>>(segs, (const double*)dens, (const double*)va, part);
+  else k_seg_val_score<float><<<SGRID(F), 256, 0, SST>>>(segs, (const float*)dens, (const float*)va, part);
+  BLML_CHECK_LAUNCH("blml_seg_val_score");
+  return seg_finish(part, F, 3, 0u, out, SST);
 }
 
 int blml_seg_phases(int dtype, int F, const blml_seg* segs, double pn, const double* z, void* E, void* stream) {

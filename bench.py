@@ -16,6 +16,7 @@ Multi-GPU: the fits are independent (no exchange step): N ranks run N replicas o
 certified fits over the slowest rank's time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--one-fit] [--matvec] [--pairs]
+                    [--select]
 """
 import argparse
 import json
@@ -307,6 +308,58 @@ def pairs_bench(dev, reps=3):
     return out
 
 
+def select_bench(dev, n_search=16, seq_sample=2, batch=256):
+    """The cut-off search over many lattices (selector.py:488-553 `_search`, run on binned counts as
+    dslit_job.py:158-171 does): 16 lattices of 64 x 64 from two-disk fields (band fc geomspace(0.08, 0.4, 16),
+    N = 5e4, 80/20 binomial split), sinc x sinc cut-offs searched from fc0 = 0.02 with factors sqrt 2, 2^1/4, 2^1/8
+    inside [2/64, 0.5]; each candidate a complex L-BFGS fit to tol 1e-6 (at most 3000 iterations, float64) scored on
+    its validation counts. Batched: every search at once, speculative rounds of about `batch` fits. Sequential: the
+    reference's order, one candidate after another through the single-fit GPU engine, on a sample of the searches."""
+    import torch
+    from blml_b200 import workloads, selector as ps, make_modes
+    from blml_b200.binned import BLMLBinned
+    tr, va = [], []
+    for i, fc in enumerate(np.geomspace(0.08, 0.4, n_search)):
+        c = workloads.two_disk_field((64, 64), fc=float(fc), N=5e4, seed=100 + i)
+        t = np.random.default_rng(i).binomial(c.astype(np.int64), 0.8).astype(float)
+        tr.append(t); va.append(c - t)
+    kw = dict(fc0=0.02, fc_min=2 / 64, fc_max=0.5, factors=ps.SEARCH_FACTORS, tol=1e-6, max_fit_sweeps=3000)
+    ps.select_counts_batched(tr[:2], va[:2], batch=32, **{**kw, 'factors': (ps.SQRT2,)})     # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out, stats = ps.select_counts_batched(tr, va, batch=batch, return_stats=True, **kw)
+    torch.cuda.synchronize()
+    t_b = time.perf_counter() - t0
+    picks = [np.array([m[0][0]['fc'], m[0][1]['fc']]) for m, _ in out]
+    seq_fits, same = 0, 0
+    t0 = time.perf_counter()
+    for s in range(seq_sample):
+        trd = torch.as_tensor(tr[s]).to(dev)
+
+        def obj(fc, s=s, trd=trd):
+            nonlocal seq_fits
+            if np.any(fc > 0.5 * (1 + 1e-9)) or np.any(fc < 2 / 64):
+                return -np.inf
+            seq_fits += 1
+            m = BLMLBinned(tol=1e-6, max_sweeps=3000, solver='lbfgs', dtype=np.float64, device=dev).fit(
+                trd, make_modes(list(fc), ['sinc', 'sinc']), complex_g=True)
+            p = np.maximum(m.density_, 1e-300)
+            return float(np.sum(va[s] * np.log(p / p.sum())) / va[s].sum())
+        fc, _ = ps.search(obj, 2, ['sinc', 'sinc'], [None, None], fc0=kw['fc0'], factors=kw['factors'])
+        same += int(np.array_equal(fc, picks[s]))
+    torch.cuda.synchronize()
+    t_s = (time.perf_counter() - t0) / seq_sample
+    return {'workload': '16 cut-off searches (sinc x sinc, 3 refinement factors) on 64 x 64 two-disk lattices, '
+                        'candidates = complex L-BFGS fits to tol 1e-6 (<= 3000 its), validation-scored',
+            'batched': {'selections_per_s': n_search / t_b, 'seconds': t_b, 'rounds': stats['rounds'],
+                        'fits': stats['fits'], 'fits_used': stats['used'], 'batch': batch},
+            'sequential_single_fit_gpu': {'selections_per_s': 1.0 / t_s, 'seconds_per_selection': t_s,
+                                          'sample': f'{seq_sample} searches, {seq_fits} fits',
+                                          'same_pick_as_batched': f'{same}/{seq_sample}'},
+            'speedup': t_s * n_search / t_b,
+            'picks': [[round(float(x), 5) for x in p] for p in picks]}
+
+
 def flush_l2(buf):
     buf.add_(1.0)
 
@@ -320,6 +373,8 @@ def main():
     ap.add_argument('--one-fit', action='store_true', help='one batched sweep and exit (profiling runs)')
     ap.add_argument('--pairs', action='store_true',
                     help='the 5-D pair path: one full rows pass over all bin pairs, GPU and a CPU-oracle sample')
+    ap.add_argument('--select', action='store_true',
+                    help='the batched cut-off search over 16 lattices beside the sequential single-fit search')
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
@@ -337,6 +392,9 @@ def main():
     train = [f['train'] for f in sweep]; val = [f['val'] for f in sweep]
     if args.pairs:
         print(json.dumps(pairs_bench(dev)), flush=True)
+        return
+    if args.select:
+        print(json.dumps(select_bench(dev)), flush=True)
         return
     if args.matvec:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)

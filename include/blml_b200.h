@@ -173,6 +173,12 @@ int blml_seg_finish(int dtype, int F, const blml_seg* segs, int cplx, const void
                     const double* inv_n2, void* density, double* part, double* out, void* stream);  /* nq = 1 */
 int blml_seg_log_score(int dtype, int F, const blml_seg* segs, int cplx, const void* U, const void* m,
                        const double* inv_z, double eps, double* part, double* out, void* stream);   /* nq = 2 */
+/* the cut-off search's validation score (replaces the objective of select_counts, selector.py:712-716, and of
+   dslit_job.py:165-168, one fit at a time): per fit, with p = max(density, 1e-300) over every bin of its lattice,
+   out[3 f + 0..2] = sum_b p, sum_b va log p, sum_b va; score = (sum va log p - sum va log sum p) / sum va.
+   density and va are real arrays of the fit dtype laid out like the bins (boff) */
+int blml_seg_val_score(int dtype, int F, const blml_seg* segs, const void* density, const void* va, double* part,
+                       double* out, void* stream);                                                  /* nq = 3 */
 int blml_seg_phases(int dtype, int F, const blml_seg* segs, double pn, const double* z, void* E, void* stream);
 int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const blml_seg* cplx_segs, const void* er,
                              void* E, void* stream);
