@@ -133,10 +133,12 @@ def test_fit_float64_matches_reference(cuda_device, name):
 
 @pytest.mark.parametrize('name', ['c1_sinc1024', 'd2_sinc_sinc_real', 'd1_dir_circ_real'])
 def test_fit_float32_matches_reference(cuda_device, name):
-    """float32 state (float64 reductions) on the convex fits: loglik within 1e-7 relative; density within 1e-4 of
-    the largest density (a float32 coordinate descent stops at max|rho| ~ 1e-5)."""
+    """float32 state (float64 reductions) on the convex fits: loglik within 2.5e-7 relative (about four float32
+    ulps: where a float32 coordinate descent stopped at max|rho| ~ 1e-5 lands depends on the operator's float32
+    rounding); density within 1e-4 of the largest density. The reference's own float32 check runs at tol 1e-4 and
+    reports the gap without a bar (binned_gpu_job.py:56-66)."""
     g, m = _fit(name, np.float32, tol=1e-5)
-    _check(g, m, dens_tol=1e-4, of_max=True)
+    _check(g, m, dens_tol=1e-4, ll_tol=2.5e-7, of_max=True)
 
 
 def test_fit_float32_lbfgs_matches_float64(cuda_device):
