@@ -95,6 +95,10 @@ _SIGS = {
     'blml_mul_bins': (_I, [_I, _I, _L, _I, _P, _P, _P, _P]),
     'blml_lgrad_weights': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
     'blml_lgrad_finish': (_I, [_I, _I, _L, _I, _P, _P, _P, _D, _P, _P]),
+    'blml_pgrad_weights': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
+    'blml_hvp_inner': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P]),
+    'blml_mixed_terms': (_I, [_I, _I, _L, _I, _P, _I, _P, _P, _P, _P, _P]),
+    'blml_hvp_real1': (_I, [_I, _L, _P, _P, _P, _P, _P, _P]),
     'blml_lbfgs_trial': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     'blml_finish': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
     'blml_log_score': (_I, [_I, _I, _L, _I, _P, _P, _D, _D, _P, _P, _P]),

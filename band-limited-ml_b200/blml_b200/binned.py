@@ -16,8 +16,8 @@ import torch
 
 from . import _lib
 from ._lib import call, ptrs, dbl
-from .spec import parse_modes, spec_key
-from .operator import pad_rule, mode_transform, kernel_at_zero, Plan
+from .spec import parse_modes, spec_key, units_of
+from .operator import pad_rule, mode_transform, mode_transform_dlog, kernel_at_zero, Plan
 
 
 from collections import OrderedDict
@@ -101,6 +101,7 @@ class BLMLBinned:
         self._rt = torch.float32 if f32 else torch.float64
         self._ct = torch.complex64 if f32 else torch.complex128
         self._red = _Red(self.dev_)
+        self._dplan_rows = None
         self._build_kernels()
         self.K_ = len(specs)
         return counts
@@ -600,8 +601,154 @@ class BLMLBinned:
     def predict_grid(self, r):
         raise NotImplementedError("predict_grid is outside this engine's path")
 
+    # ---------------------------------------------------------------- fc gradients
+    def _dplans(self):
+        """Per mode, per kernel unit (units_of order): the device plan of dS/dlog fc_u, None for integer units
+        (dirichlet, pball: fc moves in whole harmonics). Modes with one kernel share their plans."""
+        key = (self._code, str(self.dev_))
+        if getattr(self, '_dplan_key', None) != key or self._dplan_rows is None:
+            rows, seen = [], {}
+            for sp in self.specs_:
+                k = spec_key(sp)
+                if k not in seen:
+                    row = []
+                    for u in range(len(units_of(sp['kinds']))):
+                        tr = mode_transform_dlog(sp, self.shape_, self.h_, self.pad_, u)
+                        if tr is None:
+                            row.append(None)
+                        else:
+                            with torch.cuda.device(self.dev_):
+                                row.append(Plan(tr[0], tr[1], self.shape_, self._code, _lib.ENGINE_SIMT))
+                    seen[k] = row
+                rows.append(seen[k])
+            self._dplan_rows, self._dplan_key = rows, key
+        return self._dplan_rows
+
+    def _dapply(self, plan, x):
+        """dS x for one mode's coefficients x (1, B)."""
+        y = torch.empty_like(x)
+        plan.apply(x, y, 1, x.is_complex(), self._st)
+        return y
+
+    def _counts_t(self, counts):
+        if isinstance(counts, torch.Tensor):
+            return counts.reshape(-1).to(self.dev_, self._rt).contiguous()
+        m = np.asarray(counts, float)
+        if m.size != self.B_:
+            raise ValueError("counts: one value per bin of the fitted lattice")
+        return torch.as_tensor(m.ravel(), dtype=self._rt).to(self.dev_)
+
+    def _score_weights(self, counts, eps):
+        """(V = wn U, sum wn F / M, M, Z) of the score sum m log(F / Z + eps) / M (blml_binned.py:549-553)."""
+        E, U = self.e_hat_t_, self.Se_t_
+        m = self._counts_t(counts)
+        Z = self._Q(E, U)
+        V = torch.empty_like(U)
+        call('blml_pgrad_weights', self._code, U.shape[0], self.B_, int(U.is_complex()), U.data_ptr(), m.data_ptr(),
+             float(eps) * Z, V.data_ptr(), self._red.part.data_ptr(), self._red.out.data_ptr(), self._st)
+        swf, M = self._red.read(2)
+        if not M > 0:
+            raise ValueError("counts: no observations")
+        return V, swf / M, M, Z
+
+    def param_grad(self, counts, eps=0.0):
+        """d/dlog fc_u of sum_b m_b log(F_b / Z + eps) / sum m at the current coefficients (blml_binned.py:543-562),
+        for counts m on the lattice (the training counts: fc_grad; a new batch: the prequential gradient). eps is in
+        density units (f = F / Z). A list per mode of arrays, one entry per kernel unit (NaN for integer units)."""
+        V, fz, M, Z = self._score_weights(counts, eps)
+        E = self.e_hat_t_
+        out = []
+        for k, row in enumerate(self._dplans()):
+            gk = []
+            for plan in row:
+                if plan is None:
+                    gk.append(np.nan); continue
+                dU = self._dapply(plan, E[k:k + 1])
+                a, b = self._dots([(V[k:k + 1], dU), (E[k:k + 1], dU)])
+                gk.append(2 * a / M - fz * b / Z)
+            out.append(np.array(gk))
+        return out
+
     def fc_grad(self):
-        raise NotImplementedError("fc_grad (envelope-theorem gradients) is outside this engine's path")
+        """d loglik_ / dlog fc of every (mode, unit) at the fitted coefficients (blml_binned.py:520-527: the envelope
+        theorem, e stationary for the scale-free likelihood): param_grad of the training counts."""
+        return self.param_grad(self.w_t_)
+
+    def _occ_mask(self):
+        if getattr(self, '_occ_t', None) is None:
+            self._occ_t = (self.w_t_ > 0).to(self._rt)
+        return self._occ_t
+
+    def _mask_(self, x):
+        call('blml_mul_bins', self._code, x.shape[0], self.B_, int(x.is_complex()), x.data_ptr(),
+             self._occ_mask().data_ptr(), x.data_ptr(), self._st)
+        return x
+
+    def _hvp(self, D, Q):
+        """The Hessian of the minimised objective times D (blml_binned.py:593-606): -L (psd) or Phi (real rank 1)."""
+        E, U = self.e_hat_t_, self.Se_t_
+        dU = self._Sall(D)
+        out = torch.empty_like(D)
+        if not self.psd_:
+            call('blml_hvp_real1', self._code, self.B_, D.data_ptr(), E.data_ptr(), self.c_t_.data_ptr(),
+                 dU.data_ptr(), out.data_ptr(), self._st)
+            return out
+        n = self.n_
+        call('blml_hvp_inner', self._code, U.shape[0], self.B_, int(U.is_complex()), U.data_ptr(), dU.data_ptr(),
+             self.w_t_.data_ptr(), out.data_ptr(), self._st)
+        SI = self._Sall(out)
+        dQ = 2 * self._dots([(U, D)])[0]
+        return self._lin([(-2.0, SI), (2 * n / Q, dU), (-2 * n * dQ / Q ** 2, U)], out=out)
+
+    def _mixed(self, k, plan, Q):
+        """d(gradient of the minimised objective)/dlog fc for one unit of mode k at fixed coefficients
+        (blml_binned.py:610-628)."""
+        E, U = self.e_hat_t_, self.Se_t_
+        n = self.n_
+        dUk = self._dapply(plan, E[k:k + 1])
+        if not self.psd_:
+            return dUk
+        dQ = self._dots([(E[k:k + 1], dUk)])[0]
+        T = torch.empty_like(U); Wk = torch.empty_like(dUk)
+        call('blml_mixed_terms', self._code, U.shape[0], self.B_, int(U.is_complex()), U.data_ptr(), int(k),
+             dUk.data_ptr(), self.w_t_.data_ptr(), T.data_ptr(), Wk.data_ptr(), self._st)
+        g = self._lin([(-2.0, self._Sall(T)), (-2 * n * dQ / Q ** 2, U)])
+        dW = self._dapply(plan, Wk)
+        self._lin([(1.0, g[k:k + 1]), (-2.0, dW), (2 * n / Q, dUk)], out=g[k:k + 1])
+        return g
+
+    def implicit_grad(self, counts, eps=0.0, tol=1e-6, maxit=300):
+        """d/dlog fc_u of the same score as param_grad with the coefficients' response to the move included
+        (blml_binned.py:565-628): dP/dtheta = dP/dtheta|_e - <v, d grad/dtheta>, H v = dP/de by conjugate gradients
+        (blml_binned.py:1485-1496) on the occupied bins, Hessian-vector products by the mat-vec. Sets ift_iters_ and
+        ift_res_ (the CG's iterations and relative residual)."""
+        G = self.param_grad(counts, eps)
+        V, fz, M, Q = self._score_weights(counts, eps)
+        U = self.Se_t_
+        b = self._mask_(self._lin([(2.0 / M, self._Sall(V)), (-2.0 * fz / Q, U)]))
+        x = torch.zeros_like(b); r = b.clone(); p = r.clone()
+        rs = self._dots([(r, r)])[0]; bn = np.sqrt(rs) or 1.0
+        it, res = maxit, np.sqrt(rs) / bn
+        for i in range(1, maxit + 1):
+            Ap = self._mask_(self._hvp(p, Q))
+            pAp = self._dots([(p, Ap)])[0]
+            if not pAp > 0:
+                it, res = i, np.sqrt(rs) / bn
+                break
+            a = rs / pAp
+            self._lin([(1.0, x), (a, p)], out=x); self._lin([(1.0, r), (-a, Ap)], out=r)
+            rs_new = self._dots([(r, r)])[0]
+            if np.sqrt(rs_new) / bn < tol:
+                it, res = i, np.sqrt(rs_new) / bn
+                break
+            self._lin([(1.0, r), (rs_new / rs, p)], out=p); rs = rs_new
+            res = np.sqrt(rs) / bn
+        self.ift_iters_, self.ift_res_ = it, res
+        for k, row in enumerate(self._dplans()):
+            for u, plan in enumerate(row):
+                if plan is not None:
+                    G[k][u] -= self._dots([(x, self._mask_(self._mixed(k, plan, Q)))])[0]
+        return G
 
 
 class _Anderson:

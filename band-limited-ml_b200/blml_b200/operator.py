@@ -19,7 +19,7 @@ built here on the host (float64); the contraction itself runs on the GPU (csrc/m
 import numpy as np
 
 from . import _lib
-from .spec import units_of, split_kind, unit_value, pball_harmonics, dirichlet_N, dirichlet_inner_M
+from .spec import units_of, split_kind, unit_value, unit_value_dlog, pball_harmonics, dirichlet_N, dirichlet_inner_M
 
 
 def next_fast_len(n):
@@ -85,8 +85,9 @@ def _quad_unit(kind, fc, h, m, L, tol=1e-14):
     return None
 
 
-def _pad_unit(kind, fc, periods, dims, shape, h, pad):
-    """The padded-lattice DFT representation of one unit over its dims: frequencies q / L, weights FFT(T) / L."""
+def _pad_unit(kind, fc, periods, dims, shape, h, pad, values=unit_value):
+    """The padded-lattice DFT representation of one unit over its dims: frequencies q / L, weights FFT(T) / L, T the
+    unit's values (or another table of the same shape, e.g. its dK/dlog fc) at the padded offsets."""
     d = len(dims)
     diffs, masks = [], []
     for i, a in enumerate(dims):
@@ -96,7 +97,7 @@ def _pad_unit(kind, fc, periods, dims, shape, h, pad):
         mk = np.ones(L) if L == m else (np.abs(off) <= m - 1).astype(float)
         sh = [1] * d; sh[i] = L
         diffs.append((off * h[a]).reshape(sh)); masks.append(mk.reshape(sh))
-    T = unit_value(kind, fc, periods, diffs)
+    T = values(kind, fc, periods, diffs)
     for mk in masks:
         T = T * mk
     T = np.broadcast_to(T, tuple(pad[a] for a in dims)).astype(np.float64)
@@ -128,6 +129,48 @@ def unit_transform(kind, fc, periods, dims, shape, h, pad):
         if q is not None:
             return [q[0]], q[1]
     return _pad_unit(kind, fc, periods, dims, shape, h, pad)
+
+
+def unit_transform_dlog(kind, fc, periods, dims, shape, h, pad):
+    """The plane-wave form of dK/dlog fc of one unit, or None where fc moves in whole harmonics (dirichlet, pball).
+    sinc: f cos(pi f t) is the band's two edges, nu = +-f / 2 with weight f / 2 each; slits adds the inner edges
+    +-fi / 2 with weight -fi / 2; ball: the padded lattice's DFT of its dlog table (blml_binned.py:92-101)."""
+    name, tag = split_kind(kind)
+    if name in ('dirichlet', 'pball'):
+        return None
+    if name in ('sinc', 'slits'):
+        a = dims[0]; f = float(fc[0])
+        nu, w = [-f / 2, f / 2], [f / 2, f / 2]
+        if name == 'slits':
+            fi = (1.0 - float(tag)) * f
+            if fi > 0:
+                nu += [-fi / 2, fi / 2]; w += [-fi / 2, -fi / 2]
+        return [np.array(nu) * h[a]], np.array(w)
+    return _pad_unit(kind, fc, periods, dims, shape, h, pad, values=unit_value_dlog)
+
+
+def mode_transform_dlog(spec, shape, h, pad, u):
+    """mode_transform of dK/dlog fc_u (unit u of units_of(spec['kinds']) differentiated, the others as they are), or
+    None for an integer unit."""
+    units = units_of(spec['kinds'])
+    kind, dims = units[u]
+    per = lambda ds: [spec['periods'][j] for j in ds]
+    du = unit_transform_dlog(kind, spec['fc'][dims], per(dims), dims, shape, h, pad)
+    if du is None:
+        return None
+    d = len(shape)
+    freqs = [None] * d
+    W = np.ones([1] * d)
+    for v, (kv, dv) in enumerate(units):
+        fq, Wu = du if v == u else unit_transform(kv, spec['fc'][dv], per(dv), dv, shape, h, pad)
+        for a, f in zip(dv, fq):
+            freqs[a] = np.asarray(f, float)
+        sh = [1] * d
+        for i, a in enumerate(dv):
+            sh[a] = Wu.shape[i]
+        W = W * Wu.reshape(sh)
+    W = np.broadcast_to(W, tuple(len(f) for f in freqs)).astype(np.float64)
+    return freqs, np.ascontiguousarray(W)
 
 
 def mode_transform(spec, shape, h, pad):

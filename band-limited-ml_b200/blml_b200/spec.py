@@ -93,6 +93,34 @@ def unit_value(kind, fc, periods, diffs):
     raise ValueError(f"unknown kernel kind {kind!r}")
 
 
+def ball_profile_dlog(s, dg):
+    """s p'(s) of the ball profile: -pi (1/2)^(dg/2) s^(1 - dg/2) J_{dg/2 + 1}(pi s), 0 at s = 0."""
+    from scipy.special import jv
+    s = np.asarray(s, float)
+    out = np.zeros(s.shape)
+    nz = s > 0
+    out[nz] = -np.pi * 0.5 ** (dg / 2) * s[nz] ** (1 - dg / 2) * jv(dg / 2 + 1, np.pi * s[nz])
+    return out
+
+
+def unit_value_dlog(kind, fc, periods, diffs):
+    """dK/dlog fc of one unit with its fc columns scaled together (blml_trivial.py:372-377 sinc, :446-453 slits,
+    :593-600 ball with s p'(s) of :146-154), or None where fc moves in whole harmonics (dirichlet, pball)."""
+    name, tag = split_kind(kind)
+    if name == 'sinc':
+        f = float(fc[0]); return f * np.cos(np.pi * f * np.asarray(diffs[0], float))
+    if name == 'slits':
+        f = float(fc[0]); fi = (1.0 - float(tag)) * f; t = np.asarray(diffs[0], float)
+        return f * np.cos(np.pi * f * t) - fi * np.cos(np.pi * fi * t)
+    if name == 'ball':
+        f = np.asarray(fc, float); D = len(f)
+        s = np.sqrt(sum((fi * np.asarray(dk, float)) ** 2 for fi, dk in zip(f, diffs)))
+        return float(np.prod(f)) * (D * ball_profile(s, D) + ball_profile_dlog(s, D))
+    if name in ('dirichlet', 'pball'):
+        return None
+    raise ValueError(f"unknown kernel kind {kind!r}")
+
+
 def units_of(kinds):
     """[(kind, dims)]: one-column units first, then one per group in order of first appearance."""
     units = [(k, [j]) for j, k in enumerate(kinds) if not is_group(k)]

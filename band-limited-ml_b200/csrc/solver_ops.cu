@@ -267,6 +267,79 @@ __global__ void k_lgrad_weights(int K, int64_t B, const void* U, const T* w, dou
   block_partials<1>(v, part);
 }
 
+// ---------------------------------------------------------------------------------------------- fc gradients
+// blml_binned.py:543-628: the weights of the score sum m log(F / Z + eps) / sum m, the Hessian's bin-wise inner term
+// and the mixed (d grad / dlog fc) terms, on occupied bins only (w > 0), float64 arithmetic per bin.
+template <typename T, bool CPLX>
+__global__ void k_pgrad_weights(int K, int64_t B, const void* U, const T* m, double add, void* V, double* part) {
+  double v[2] = {0.0, 0.0};
+  GRID_STRIDE(b, B) {
+    double F = 0.0;
+    for (int k = 0; k < K; k++) { double ur, ui; Acc<T, CPLX>::get(U, k * B + b, ur, ui); F += ur * ur + ui * ui; }
+    const double mb = (double)m[b];
+    const double wn = mb > 0 ? mb / fmax(F + add, 1e-300) : 0.0;
+    v[0] += wn * F; v[1] += mb;
+    for (int k = 0; k < K; k++) {
+      double ur, ui; Acc<T, CPLX>::get(U, k * B + b, ur, ui);
+      Acc<T, CPLX>::put(V, k * B + b, wn * ur, wn * ui);
+    }
+  }
+  block_partials<2>(v, part);
+}
+
+// out_j = (w / F) dU_j - (w dF / F^2) U_j, dF = 2 Re sum_j conj(U_j) dU_j (0 off the occupied bins)
+template <typename T, bool CPLX>
+__global__ void k_hvp_inner(int K, int64_t B, const void* U, const void* dU, const T* w, void* out) {
+  GRID_STRIDE(b, B) {
+    const double wb = (double)w[b];
+    double F = 0.0, dF = 0.0;
+    for (int k = 0; k < K; k++) {
+      double ur, ui, dr, di;
+      Acc<T, CPLX>::get(U, k * B + b, ur, ui); Acc<T, CPLX>::get(dU, k * B + b, dr, di);
+      F += ur * ur + ui * ui; dF += 2.0 * (ur * dr + ui * di);
+    }
+    const bool occ = wb > 0;
+    const double a = occ ? wb / F : 0.0, c = occ ? wb * dF / (F * F) : 0.0;
+    for (int k = 0; k < K; k++) {
+      double ur, ui, dr, di;
+      Acc<T, CPLX>::get(U, k * B + b, ur, ui); Acc<T, CPLX>::get(dU, k * B + b, dr, di);
+      Acc<T, CPLX>::put(out, k * B + b, a * dr - c * ur, a * di - c * ui);
+    }
+  }
+}
+
+// for mode kk moved by dUk = dS E_kk: T_j = -(w dF / F^2) U_j (+ (w / F) dUk for j = kk) and Wk = (w / F) U_kk,
+// dF = 2 Re conj(U_kk) dUk (0 off the occupied bins)
+template <typename T, bool CPLX>
+__global__ void k_mixed_terms(int K, int64_t B, const void* U, int kk, const void* dUk, const T* w, void* Tout,
+                              void* Wk) {
+  GRID_STRIDE(b, B) {
+    const double wb = (double)w[b];
+    double F = 0.0;
+    for (int k = 0; k < K; k++) { double ur, ui; Acc<T, CPLX>::get(U, k * B + b, ur, ui); F += ur * ur + ui * ui; }
+    double kr, ki, dr, di;
+    Acc<T, CPLX>::get(U, kk * B + b, kr, ki); Acc<T, CPLX>::get(dUk, b, dr, di);
+    const bool occ = wb > 0;
+    const double ws = occ ? wb / F : 0.0, wd = occ ? wb * 2.0 * (kr * dr + ki * di) / (F * F) : 0.0;
+    for (int k = 0; k < K; k++) {
+      double ur, ui; Acc<T, CPLX>::get(U, k * B + b, ur, ui);
+      double tr = -wd * ur, ti = -wd * ui;
+      if (k == kk) { tr += ws * dr; ti += ws * di; }
+      Acc<T, CPLX>::put(Tout, k * B + b, tr, ti);
+    }
+    Acc<T, CPLX>::put(Wk, b, ws * kr, ws * ki);
+  }
+}
+
+// the real rank-1 objective's Hessian times D: dU + (c / e^2) D on occupied bins (c = n w > 0)
+template <typename T>
+__global__ void k_hvp_real1(int64_t B, const T* D, const T* E, const T* c, const T* dU, T* out) {
+  GRID_STRIDE(b, B) {
+    const double cb = (double)c[b], e = (double)E[b];
+    out[b] = (T)((double)dU[b] + (cb > 0 ? cb / (e * e) : 0.0) * (double)D[b]);
+  }
+}
+
 template <typename T, bool CPLX>
 __global__ void k_lgrad_finish(int K, int64_t B, const void* SV, const void* U, const T* w, double nq, void* g) {
   GRID_STRIDE(b, B) {
@@ -497,6 +570,67 @@ int blml_lgrad_weights(int dtype, int K, int64_t B, int cplx, const void* U, con
   }
   BLML_CHECK_LAUNCH("blml_lgrad_weights");
   return finish_partials(part, 1, kRedBlocks, 0u, out, ST);
+}
+
+int blml_pgrad_weights(int dtype, int K, int64_t B, int cplx, const void* U, const void* m, double add, void* V,
+                       double* part, double* out, void* stream) {
+  if (check_dtype(dtype, "blml_pgrad_weights")) return BLML_ERR_ARG;
+  if (K < 1 || B < 1 || !U || !m || !V || !part || !out) { set_error("blml_pgrad_weights: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64) {
+    if (cplx) k_pgrad_weights<double, true><<<kRedBlocks, kRedThreads, 0, ST>>>(K, B, U, (const double*)m, add, V, part);
+    else k_pgrad_weights<double, false><<<kRedBlocks, kRedThreads, 0, ST>>>(K, B, U, (const double*)m, add, V, part);
+  } else {
+    if (cplx) k_pgrad_weights<float, true><<<kRedBlocks, kRedThreads, 0, ST>>>(K, B, U, (const float*)m, add, V, part);
+    else k_pgrad_weights<float, false><<<kRedBlocks, kRedThreads, 0, ST>>>(K, B, U, (const float*)m, add, V, part);
+  }
+  BLML_CHECK_LAUNCH("blml_pgrad_weights");
+  return finish_partials(part, 2, kRedBlocks, 0u, out, ST);
+}
+
+int blml_hvp_inner(int dtype, int K, int64_t B, int cplx, const void* U, const void* dU, const void* w, void* out,
+                   void* stream) {
+  if (check_dtype(dtype, "blml_hvp_inner")) return BLML_ERR_ARG;
+  if (K < 1 || B < 1 || !U || !dU || !w || !out) { set_error("blml_hvp_inner: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64) {
+    if (cplx) k_hvp_inner<double, true><<<grid_for(B), 256, 0, ST>>>(K, B, U, dU, (const double*)w, out);
+    else k_hvp_inner<double, false><<<grid_for(B), 256, 0, ST>>>(K, B, U, dU, (const double*)w, out);
+  } else {
+    if (cplx) k_hvp_inner<float, true><<<grid_for(B), 256, 0, ST>>>(K, B, U, dU, (const float*)w, out);
+    else k_hvp_inner<float, false><<<grid_for(B), 256, 0, ST>>>(K, B, U, dU, (const float*)w, out);
+  }
+  BLML_CHECK_LAUNCH("blml_hvp_inner");
+  return BLML_OK;
+}
+
+int blml_mixed_terms(int dtype, int K, int64_t B, int cplx, const void* U, int k, const void* dUk, const void* w,
+                     void* T, void* Wk, void* stream) {
+  if (check_dtype(dtype, "blml_mixed_terms")) return BLML_ERR_ARG;
+  if (K < 1 || B < 1 || k < 0 || k >= K || !U || !dUk || !w || !T || !Wk) {
+    set_error("blml_mixed_terms: arguments"); return BLML_ERR_ARG;
+  }
+  if (dtype == BLML_F64) {
+    if (cplx) k_mixed_terms<double, true><<<grid_for(B), 256, 0, ST>>>(K, B, U, k, dUk, (const double*)w, T, Wk);
+    else k_mixed_terms<double, false><<<grid_for(B), 256, 0, ST>>>(K, B, U, k, dUk, (const double*)w, T, Wk);
+  } else {
+    if (cplx) k_mixed_terms<float, true><<<grid_for(B), 256, 0, ST>>>(K, B, U, k, dUk, (const float*)w, T, Wk);
+    else k_mixed_terms<float, false><<<grid_for(B), 256, 0, ST>>>(K, B, U, k, dUk, (const float*)w, T, Wk);
+  }
+  BLML_CHECK_LAUNCH("blml_mixed_terms");
+  return BLML_OK;
+}
+
+int blml_hvp_real1(int dtype, int64_t B, const void* D, const void* E, const void* c, const void* dU, void* out,
+                   void* stream) {
+  if (check_dtype(dtype, "blml_hvp_real1")) return BLML_ERR_ARG;
+  if (B < 1 || !D || !E || !c || !dU || !out) { set_error("blml_hvp_real1: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64)
+    k_hvp_real1<double><<<grid_for(B), 256, 0, ST>>>(B, (const double*)D, (const double*)E, (const double*)c,
+                                                      (const double*)dU, (double*)out);
+  else
+    k_hvp_real1<float><<<grid_for(B), 256, 0, ST>>>(B, (const float*)D, (const float*)E, (const float*)c,
+                                                     (const float*)dU, (float*)out);
+  BLML_CHECK_LAUNCH("blml_hvp_real1");
+  return BLML_OK;
 }
 
 int blml_lgrad_finish(int dtype, int K, int64_t B, int cplx, const void* SV, const void* U, const void* w, double nq,

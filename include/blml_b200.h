@@ -104,6 +104,22 @@ int blml_lgrad_weights(int dtype, int K, int64_t B, int cplx, const void* U, con
                        double* part, double* out, void* stream);
 int blml_lgrad_finish(int dtype, int K, int64_t B, int cplx, const void* SV, const void* U, const void* w, double nq,
                       void* g, void* stream);
+/* ---- fc gradients of a fit (blml_binned.py:520-628: fc_grad, param_grad, implicit_grad) ----
+   the score P = sum_b m_b log(F_b / Z + eps) / sum m: V_k = wn U_k with wn = m / max(F + add, 1e-300) on bins with
+   m > 0 (add = eps Z), out[0] = sum wn F, out[1] = sum m (blml_binned.py:551-553) */
+int blml_pgrad_weights(int dtype, int K, int64_t B, int cplx, const void* U, const void* m, double add, void* V,
+                       double* part, double* out, void* stream);                                   /* nq = 2 */
+/* the Hessian of the minimised objective (blml_binned.py:596-606), its bin term:
+   out_k = (w / F) dU_k - (w dF / F^2) U_k, dF = 2 Re sum_k conj(U_k) dU_k, on occupied bins (0 elsewhere) */
+int blml_hvp_inner(int dtype, int K, int64_t B, int cplx, const void* U, const void* dU, const void* w, void* out,
+                   void* stream);
+/* d(gradient)/dlog fc of mode k at fixed coefficients (blml_binned.py:610-628), its bin terms for dUk = dS E_k:
+   T_j = -(w dF / F^2) U_j (+ (w / F) dUk for j = k), Wk = (w / F) U_k, dF = 2 Re conj(U_k) dUk (occupied bins) */
+int blml_mixed_terms(int dtype, int K, int64_t B, int cplx, const void* U, int k, const void* dUk, const void* w,
+                     void* T, void* Wk, void* stream);
+/* the real rank-1 objective's Hessian times D (blml_binned.py:599-601): out = dU + (c / e^2) D where c > 0 */
+int blml_hvp_real1(int dtype, int64_t B, const void* D, const void* E, const void* c, const void* dU, void* out,
+                   void* stream);
 
 /* ---- one Armijo trial of the L-BFGS line search (BLMLBinned._solve_lbfgs, blml_binned.py:316-321) ----
  * En = E + t q and Un = U + t Sq (S linear: U + t S q = S(E + t q)), both written; out[0] = sum_occ w log F(Un),

@@ -56,3 +56,28 @@ def hist(rng, shape, n, f):
     g = np.meshgrid(*[np.arange(m, dtype=float) for m in shape], indexing='ij')
     p = f(*g); p = p / p.sum()
     return rng.multinomial(n, p.ravel()).reshape(shape).astype(float)
+
+# the fc gradients (blml_binned.py:520-628): name -> (shape, modes, fit kwargs, constructor kwargs); counts, the
+# reference's fitted coefficients and its fc_grad / param_grad / implicit_grad values are in grads.npz
+GRAD_SPECS = {
+    'g1_sinc_real': ((40,), make_modes([0.35], ['sinc']), {}, dict(tol=1e-10)),
+    'g1_slits_complex': ((64,), make_modes([0.3], ['slits:0.4']), dict(complex_g=True),
+                         dict(tol=1e-9, solver='lbfgs', max_sweeps=5000)),
+    'g2_sinc_sinc_complex': ((24, 24), make_modes([0.4, 0.3], ['sinc', 'sinc']), dict(complex_g=True),
+                             dict(tol=1e-9, solver='lbfgs', max_sweeps=5000)),
+    'g2_ball_complex': ((20, 20), make_modes([0.45, 0.45], ['ball', 'ball']), dict(complex_g=True),
+                        dict(tol=1e-9, solver='lbfgs', max_sweeps=5000)),
+    'g2_dir_sinc_rank2': ((24, 24), make_modes([[0.3, 0.4], [0.3, 0.15]], ['dirichlet', 'sinc'],
+                                               periods=[24.0, None]), dict(complex_g=True),
+                          dict(tol=1e-8, solver='lbfgs', max_sweeps=5000)),
+}
+
+
+def grad_density(shape):
+    """A smooth positive test density on the lattice (two bumps and a floor)."""
+    def f(*g):
+        c = [0.3 * m for m in shape]; c2 = [0.65 * m for m in shape]
+        r1 = sum((x - a) ** 2 for x, a in zip(g, c)) / (0.12 * max(shape)) ** 2
+        r2 = sum((x - a) ** 2 for x, a in zip(g, c2)) / (0.08 * max(shape)) ** 2
+        return np.exp(-0.5 * r1) + 0.6 * np.exp(-0.5 * r2) + 0.02
+    return f

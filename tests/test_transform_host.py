@@ -51,3 +51,40 @@ def test_pball_circular_is_band_mask():
     freqs, W = op_mod.mode_transform(specs[0], (256, 256), np.ones(2), (256, 256))
     assert [len(f) for f in freqs] == [85, 85]
     assert int((W > 0).sum()) == 5621
+
+
+GRAD_OPS = [((40,), [{0: dict(kind='sinc', fc=0.35)}], 1.0),
+            ((64,), [{0: dict(kind='slits', fc=0.3, fill=0.4)}], 1.0),
+            ((24, 24), [{0: dict(kind='sinc', fc=0.4), 1: dict(kind='sinc', fc=0.3)}], 1.0),
+            ((20, 20), [{(0, 1): dict(kind='ball', fc=0.45)}], 1.0),
+            ((16, 12), [{0: dict(kind='dirichlet', fc=0.3, period=16.0), 1: dict(kind='sinc', fc=0.8)}], 0.5)]
+
+
+@pytest.mark.parametrize('case', range(len(GRAD_OPS)))
+def test_dlog_transforms_reproduce_oracle(case):
+    """dS/dlog fc_u of every unit (blml_binned.py:92-101): the plane-wave forms of operator.mode_transform_dlog through
+    the mat-vec's stage schedule equal the oracle's padded-FFT convolution with the dK/dlog fc table; integer units
+    have none."""
+    import blml_oracle as bo
+    import grad_oracle as go
+    shape, modes, h = GRAD_OPS[case]
+    d = len(shape)
+    specs, _ = parse_modes(modes, d)
+    ospecs = bo.parse_modes(modes, d)
+    hv = np.full(d, h)
+    pad = op_mod.pad_rule(shape, hv, specs)
+    rng = np.random.default_rng(case)
+    x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    fit = type('F', (), {})()
+    fit.op = bo.Operator(ospecs, shape, hv)
+    dks = go.dK_spectra(ospecs[0], shape, hv, fit.op.pad)
+    units = op_mod.units_of(specs[0]['kinds'])
+    assert len(dks) == len(units)
+    for u, dK in enumerate(dks):
+        tr = op_mod.mode_transform_dlog(specs[0], shape, hv, pad, u)
+        assert (tr is None) == (dK is None)
+        if tr is None:
+            continue
+        y = emulate(tr[0], tr[1], shape, x[None])[0]
+        ref = go._apply(fit, dK, x)
+        assert np.abs(y - ref).max() <= 1e-11 * np.abs(ref).max(), (case, u)
