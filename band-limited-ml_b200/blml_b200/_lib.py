@@ -99,6 +99,10 @@ _SIGS = {
     'blml_hvp_inner': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P]),
     'blml_mixed_terms': (_I, [_I, _I, _L, _I, _P, _I, _P, _P, _P, _P, _P]),
     'blml_hvp_real1': (_I, [_I, _L, _P, _P, _P, _P, _P, _P]),
+    'blml_counts_axpy': (_I, [_I, _L, _D, _P, _D, _P, _I, _P, _P]),
+    'blml_bin_ratio': (_I, [_I, _L, _P, _P, _P, _P]),
+    'blml_new_bins': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P]),
+    'blml_gain_sums': (_I, [_I, _L, _P, _D, _P, _D, _P, _D, _P, _P, _P]),
     'blml_lbfgs_trial': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     'blml_finish': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
     'blml_log_score': (_I, [_I, _I, _L, _I, _P, _P, _D, _D, _P, _P, _P]),

@@ -101,7 +101,6 @@ class BLMLBinned:
         self._rt = torch.float32 if f32 else torch.float64
         self._ct = torch.complex64 if f32 else torch.complex128
         self._red = _Red(self.dev_)
-        self._dplan_rows = None
         self._build_kernels()
         self.K_ = len(specs)
         return counts
@@ -128,6 +127,7 @@ class BLMLBinned:
             _PLANS.popitem(last=False)
         self.shared_ = len(mine) == 1
         self.s_ = np.array([kk[1] for kk in self.kern_])
+        self._dplan_rows = None                          # derivative plans follow the kernels
 
     # ---------------------------------------------------------------- device helpers
     @property

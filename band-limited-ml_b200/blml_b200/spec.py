@@ -207,14 +207,16 @@ def modes_lattice(modes, d):
     return hs[0]
 
 
-def parse_modes(modes, d):
-    """(specs, dep): per mode dict(fc (d,), kinds (d,), periods (d,)) with group kinds tagged by their columns
-    ('pball:0-1') and fills carried in the kind ('slits:0.4'); dep, the dependent columns or None."""
+def parse_modes(modes, d, need_fc=True):
+    """(specs, dep): per mode dict(fc (d,), kinds (d,), periods (d,), fc_trainable (d,)) with group kinds tagged by
+    their columns ('pball:0-1') and fills carried in the kind ('slits:0.4'); dep, the dependent columns or None.
+    fc is a bare value or {'value': v, 'trainable': bool} (trainable by default); need_fc=False lets a trainable fc be
+    left out (NaN: a selector template, blml_trivial.py:1247-1323)."""
     if isinstance(modes, dict) or not isinstance(modes, (list, tuple)) or not modes:
         raise TypeError("modes: a non-empty list of mode dicts {column: {...}}; wrap one mode as [mode]")
     specs, deps = [], []
     for k, m in enumerate(modes):
-        fc = [None] * d; kinds = [None] * d; periods = [None] * d; dep = [False] * d
+        fc = [None] * d; kinds = [None] * d; periods = [None] * d; dep = [False] * d; tr = [True] * d
         for key, c in m.items():
             kind = c.get('kind', 'sinc')
             if kind not in KINDS:
@@ -222,10 +224,15 @@ def parse_modes(modes, d):
             bad = set(c) - _STRUCT - set(_PARAMS[kind])
             if bad:
                 raise ValueError(f"mode {k} columns {key}: unknown keys {sorted(bad)}")
-            fcv = param_value(c.get('fc'))[0]
+            fcv, fct = param_value(c.get('fc'))
+            fct = True if fct is None else bool(fct)
             if fcv is None:
-                raise ValueError(f"mode {k} columns {key}: fc missing")
-            if not float(fcv) > 0:
+                if not fct:
+                    raise ValueError(f"mode {k} columns {key}: a fixed (trainable=False) fc needs a value")
+                if need_fc:
+                    raise ValueError(f"mode {k} columns {key}: fc missing")
+                fcv = np.nan
+            elif not float(fcv) > 0:
                 raise ValueError(f"mode {k} columns {key}: fc must be positive, got {fcv}")
             per = param_value(c.get('period'))[0]
             fill = param_value(c.get('fill'))[0]
@@ -243,7 +250,7 @@ def parse_modes(modes, d):
                 for i, j in enumerate(key):
                     if not 0 <= j < d:
                         raise ValueError(f"mode {k}: column {j} outside 0..{d - 1}")
-                    kinds[j] = f'{kind}:{tag}'; fc[j] = float(fcv)
+                    kinds[j] = f'{kind}:{tag}'; fc[j] = float(fcv); tr[j] = fct
                     periods[j] = None if pv is None else float(pv[i]); dep[j] = bool(c.get('dep', False))
             else:
                 if kind in GROUP_KINDS:
@@ -251,16 +258,57 @@ def parse_modes(modes, d):
                 if not 0 <= key < d:
                     raise ValueError(f"mode {k}: column {key} outside 0..{d - 1}")
                 kinds[key] = f'{kind}:{float(fill)!r}' if kind in ('slits', 'dirichlet') and fill is not None else kind
-                fc[key] = float(fcv); periods[key] = None if per is None else float(per)
+                fc[key] = float(fcv); tr[key] = fct; periods[key] = None if per is None else float(per)
                 dep[key] = bool(c.get('dep', False))
         if any(x is None for x in kinds):
             raise ValueError(f"mode {k}: columns {[j for j in range(d) if kinds[j] is None]} missing; "
                              f"expected every column 0..{d - 1}")
-        specs.append(dict(fc=np.array(fc, float), kinds=kinds, periods=periods)); deps.append(dep)
+        specs.append(dict(fc=np.array(fc, float), kinds=kinds, periods=periods, fc_trainable=np.array(tr, bool)))
+        deps.append(dep)
     if any(dp != deps[0] for dp in deps):
         raise ValueError("dep must mark the same columns in every mode")
     dep = [j for j in range(d) if deps[0][j]]
     return specs, (dep or None)
+
+
+def _columns(m):
+    """{column: its entry} of one mode, tuple keys spread over their columns."""
+    out = {}
+    for key, c in m.items():
+        for j in (key if isinstance(key, tuple) else (key,)):
+            out[j] = c
+    return out
+
+
+def modes_fc(modes):
+    """(K, d) cut-offs of a modes list, NaN where fc is left out (blml_trivial.py:1525-1530)."""
+    rows = [_columns(m) for m in modes]
+    d = max(max(r) for r in rows) + 1
+    val = lambda c: param_value(c.get('fc'))[0]
+    return np.array([[np.nan if val(r[j]) is None else float(val(r[j])) for j in range(d)] for r in rows], float)
+
+
+def modes_trainable(modes):
+    """(K, d) whether each column's fc is trainable (default True; blml_trivial.py:1533-1540)."""
+    rows = [_columns(m) for m in modes]
+    d = max(max(r) for r in rows) + 1
+    tr = lambda c: True if param_value(c.get('fc'))[1] is None else bool(param_value(c.get('fc'))[1])
+    return np.array([[tr(r[j]) for j in range(d)] for r in rows], bool)
+
+
+def with_fc(modes, fc):
+    """modes with fc replaced (scalar, (d,) for every mode, or (K, d)); a unit takes its first column's value;
+    trainability kept (blml_trivial.py:1576-1582)."""
+    F = np.broadcast_to(np.asarray(fc, float), modes_fc(modes).shape)
+    out = []
+    for k, m in enumerate(modes):
+        mm = {}
+        for key, c in m.items():
+            j = key[0] if isinstance(key, tuple) else key
+            t = param_value(c.get('fc'))[1]
+            mm[key] = dict(c, fc=float(F[k, j]) if t is None else dict(value=float(F[k, j]), trainable=t))
+        out.append(mm)
+    return out
 
 
 def spec_key(sp):

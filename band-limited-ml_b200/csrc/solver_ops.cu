@@ -340,6 +340,54 @@ __global__ void k_hvp_real1(int64_t B, const T* D, const T* E, const T* c, const
   }
 }
 
+// ---------------------------------------------------------------------------------------------- streaming
+// blml_binned.py:1040-1112 (BLMLBinnedStreaming): count updates, leave-batch-out shares, the start of newly occupied
+// bins and the paired log-density gains of a hill-climb candidate (blml_binned.py:752-770).
+template <typename T>
+__global__ void k_counts_axpy(int64_t B, double a, const T* w, double b, const T* m, int clamp, T* out) {
+  GRID_STRIDE(i, B) {
+    double v = a * (double)w[i] + b * (double)m[i];
+    out[i] = (T)(clamp && !(v > 0) ? 0.0 : v);
+  }
+}
+
+template <typename T>
+__global__ void k_bin_ratio(int64_t B, const T* num, const T* den, T* out) {
+  GRID_STRIDE(i, B) {
+    const double d = (double)den[i];
+    out[i] = (T)(d > 0 ? (double)num[i] / d : 0.0);
+  }
+}
+
+// out_k = Eu_k on occupied bins whose coefficients are all zero (newly occupied), E_k elsewhere
+template <typename T, bool CPLX>
+__global__ void k_new_bins(int K, int64_t B, const void* E, const void* Eu, const T* w, void* out) {
+  GRID_STRIDE(b, B) {
+    double a = 0.0;
+    for (int k = 0; k < K; k++) { double er, ei; Acc<T, CPLX>::get(E, k * B + b, er, ei); a += fabs(er) + fabs(ei); }
+    const bool fresh = (double)w[b] > 0 && a == 0.0;
+    for (int k = 0; k < K; k++) {
+      double er, ei; Acc<T, CPLX>::get(fresh ? Eu : E, k * B + b, er, ei);
+      Acc<T, CPLX>::put(out, k * B + b, er, ei);
+    }
+  }
+}
+
+// on bins with m > 0: dl = log(da sa + eps) - log(db sb + eps); sums m dl, m dl^2, m
+template <typename T>
+__global__ void k_gain_sums(int64_t B, const T* da, double sa, const T* db, double sb, const T* m, double eps,
+                            double* part) {
+  double v[3] = {0.0, 0.0, 0.0};
+  GRID_STRIDE(i, B) {
+    const double mi = (double)m[i];
+    if (mi > 0) {
+      const double dl = log((double)da[i] * sa + eps) - log((double)db[i] * sb + eps);
+      v[0] += mi * dl; v[1] += mi * dl * dl; v[2] += mi;
+    }
+  }
+  block_partials<3>(v, part);
+}
+
 template <typename T, bool CPLX>
 __global__ void k_lgrad_finish(int K, int64_t B, const void* SV, const void* U, const T* w, double nq, void* g) {
   GRID_STRIDE(b, B) {
@@ -631,6 +679,57 @@ int blml_hvp_real1(int dtype, int64_t B, const void* D, const void* E, const voi
                                                      (const float*)dU, (float*)out);
   BLML_CHECK_LAUNCH("blml_hvp_real1");
   return BLML_OK;
+}
+
+int blml_counts_axpy(int dtype, int64_t B, double a, const void* w, double b, const void* m, int clamp, void* out,
+                     void* stream) {
+  if (check_dtype(dtype, "blml_counts_axpy")) return BLML_ERR_ARG;
+  if (B < 1 || !w || !m || !out) { set_error("blml_counts_axpy: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64)
+    k_counts_axpy<double><<<grid_for(B), 256, 0, ST>>>(B, a, (const double*)w, b, (const double*)m, clamp, (double*)out);
+  else
+    k_counts_axpy<float><<<grid_for(B), 256, 0, ST>>>(B, a, (const float*)w, b, (const float*)m, clamp, (float*)out);
+  BLML_CHECK_LAUNCH("blml_counts_axpy");
+  return BLML_OK;
+}
+
+int blml_bin_ratio(int dtype, int64_t B, const void* num, const void* den, void* out, void* stream) {
+  if (check_dtype(dtype, "blml_bin_ratio")) return BLML_ERR_ARG;
+  if (B < 1 || !num || !den || !out) { set_error("blml_bin_ratio: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64)
+    k_bin_ratio<double><<<grid_for(B), 256, 0, ST>>>(B, (const double*)num, (const double*)den, (double*)out);
+  else k_bin_ratio<float><<<grid_for(B), 256, 0, ST>>>(B, (const float*)num, (const float*)den, (float*)out);
+  BLML_CHECK_LAUNCH("blml_bin_ratio");
+  return BLML_OK;
+}
+
+int blml_new_bins(int dtype, int K, int64_t B, int cplx, const void* E, const void* Eu, const void* w, void* out,
+                  void* stream) {
+  if (check_dtype(dtype, "blml_new_bins")) return BLML_ERR_ARG;
+  if (K < 1 || B < 1 || !E || !Eu || !w || !out) { set_error("blml_new_bins: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64) {
+    if (cplx) k_new_bins<double, true><<<grid_for(B), 256, 0, ST>>>(K, B, E, Eu, (const double*)w, out);
+    else k_new_bins<double, false><<<grid_for(B), 256, 0, ST>>>(K, B, E, Eu, (const double*)w, out);
+  } else {
+    if (cplx) k_new_bins<float, true><<<grid_for(B), 256, 0, ST>>>(K, B, E, Eu, (const float*)w, out);
+    else k_new_bins<float, false><<<grid_for(B), 256, 0, ST>>>(K, B, E, Eu, (const float*)w, out);
+  }
+  BLML_CHECK_LAUNCH("blml_new_bins");
+  return BLML_OK;
+}
+
+int blml_gain_sums(int dtype, int64_t B, const void* da, double sa, const void* db, double sb, const void* m, double eps,
+                   double* part, double* out, void* stream) {
+  if (check_dtype(dtype, "blml_gain_sums")) return BLML_ERR_ARG;
+  if (B < 1 || !da || !db || !m || !part || !out) { set_error("blml_gain_sums: arguments"); return BLML_ERR_ARG; }
+  if (dtype == BLML_F64)
+    k_gain_sums<double><<<kRedBlocks, kRedThreads, 0, ST>>>(B, (const double*)da, sa, (const double*)db, sb,
+                                                            (const double*)m, eps, part);
+  else
+    k_gain_sums<float><<<kRedBlocks, kRedThreads, 0, ST>>>(B, (const float*)da, sa, (const float*)db, sb,
+                                                           (const float*)m, eps, part);
+  BLML_CHECK_LAUNCH("blml_gain_sums");
+  return finish_partials(part, 3, kRedBlocks, 0u, out, ST);
 }
 
 int blml_lgrad_finish(int dtype, int K, int64_t B, int cplx, const void* SV, const void* U, const void* w, double nq,

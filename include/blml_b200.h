@@ -121,6 +121,21 @@ int blml_mixed_terms(int dtype, int K, int64_t B, int cplx, const void* U, int k
 int blml_hvp_real1(int dtype, int64_t B, const void* D, const void* E, const void* c, const void* dU, void* out,
                    void* stream);
 
+/* ---- streaming fits (BLMLBinnedStreaming, blml_binned.py:1040-1112) ----
+   counts: out = a w + b m, clamped at 0 when clamp (decay w + batch; the held counts less a batch, :1070-1074) */
+int blml_counts_axpy(int dtype, int64_t B, double a, const void* w, double b, const void* m, int clamp, void* out,
+                     void* stream);
+/* out = num / den where den > 0, else 0 (each bin's remaining share after leaving a batch out, :1075) */
+int blml_bin_ratio(int dtype, int64_t B, const void* num, const void* den, void* out, void* stream);
+/* out_k = Eu_k on occupied bins whose coefficients are all 0 (newly occupied: their own root from S e, :1098-1100),
+   E_k elsewhere */
+int blml_new_bins(int dtype, int K, int64_t B, int cplx, const void* E, const void* Eu, const void* w, void* out,
+                  void* stream);
+/* a hill-climb candidate's paired gain on a batch m (blml_binned.py:765-770): over bins with m > 0,
+   dl = log(da sa + eps) - log(db sb + eps); out = [sum m dl, sum m dl^2, sum m] */
+int blml_gain_sums(int dtype, int64_t B, const void* da, double sa, const void* db, double sb, const void* m, double eps,
+                   double* part, double* out, void* stream);                                       /* nq = 3 */
+
 /* ---- one Armijo trial of the L-BFGS line search (BLMLBinned._solve_lbfgs, blml_binned.py:316-321) ----
  * En = E + t q and Un = U + t Sq (S linear: U + t S q = S(E + t q)), both written; out[0] = sum_occ w log F(Un),
  * out[1] = Re <En, Un>, from which L(En) = out[0] - n log out[1]. nq = 2. */

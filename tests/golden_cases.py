@@ -81,3 +81,21 @@ def grad_density(shape):
         r2 = sum((x - a) ** 2 for x, a in zip(g, c2)) / (0.08 * max(shape)) ** 2
         return np.exp(-0.5 * r1) + 0.6 * np.exp(-0.5 * r2) + 0.02
     return f
+
+# streaming fits (blml_binned.py:648-1112): name -> (shape, modes, constructor kwargs, how: 'partial' (partial_fit per
+# batch) or ('fit', epochs), fit kwargs, number of batches, counts per batch); the batches, the reference's preq_, fc
+# trajectory and final loglik are in stream.npz
+STREAM_SPECS = {
+    'adam_real': ((64,), make_modes([0.12], ['sinc']), dict(tol=1e-9, lr=0.1, param_every=2), 'partial', {}, 8, 500),
+    'adam_decay_capped': ((64,), make_modes([0.3], ['sinc']),
+                          dict(tol=1e-9, lr=0.1, param_every=1, implicit_grad=False, decay=0.95, batch_sweeps=50),
+                          'partial', {}, 8, 500),
+    'hill_dirichlet': ((40,), make_modes([0.3], ['dirichlet'], periods=[40.0]),
+                       dict(tol=1e-9, param_every=2, z_se=0.5), 'partial', {}, 8, 500),
+    'epochs_loo': ((48,), make_modes([0.15], ['sinc']), dict(tol=1e-9, lr=0.1, param_every=2), ('fit', 2), {}, 6, 500),
+    'burnin_select': ((64,), [{0: dict(kind='sinc')}], dict(tol=1e-9, burn_in=1500, fc_update=None), 'partial', {},
+                      6, 500),
+    'complex_adam': ((48,), make_modes([0.2], ['sinc']),
+                     dict(tol=1e-8, solver='lbfgs', max_sweeps=3000, lr=0.1, param_every=2), 'partial',
+                     dict(complex_g=True), 6, 500),
+}
