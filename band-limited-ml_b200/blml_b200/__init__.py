@@ -3,7 +3,7 @@
 Host code mirrors the reference's Python surface (rahuljhu/band-limited-ml: blml_binned.BLMLBinned,
 blml_trivial.make_modes / with_lattice, blml_local_gpu.rows / cols); every array operation runs in libblml_b200.so
 (hand-written sm_100a CUDA behind a C ABI, include/blml_b200.h). There is no CPU fallback."""
-from .spec import make_modes, parse_modes, with_lattice          # noqa: F401
+from .spec import make_modes, parse_modes, with_lattice, with_fc, modes_fc, modes_trainable   # noqa: F401
 from . import workloads                                           # noqa: F401
 
 
@@ -12,6 +12,9 @@ def __getattr__(name):
     if name == 'BLMLBinned':
         from .binned import BLMLBinned
         return BLMLBinned
+    if name == 'BLMLBinnedStreaming':
+        from .streaming import BLMLBinnedStreaming
+        return BLMLBinnedStreaming
     if name in ('rows', 'cols', 'ProductKernel', 'rank_coords', 'BLMLQuickLattice'):
         from . import local_gpu
         return getattr(local_gpu, name)
