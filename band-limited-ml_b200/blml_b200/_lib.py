@@ -29,6 +29,14 @@ class Tables(C.Structure):
                 ('T32', C.c_void_p), ('RT32', C.c_void_p), ('dT32', C.c_void_p), ('dR32', C.c_void_p)]
 
 
+class PointCol(C.Structure):
+    """blml_point_col: one column's exact kernel for blml_point_rows."""
+    _fields_ = [('kind', C.c_int), ('M', C.c_int), ('Mi', C.c_int), ('f', C.c_double), ('fi', C.c_double),
+                ('P', C.c_double)]
+
+
+PT_SINC, PT_SLITS, PT_DIRICHLET = 0, 1, 2
+
 _P, _I, _L, _D = C.c_void_p, C.c_int, C.c_int64, C.c_double
 _SIGS = {
     'blml_last_error': (C.c_char_p, []),
@@ -103,6 +111,7 @@ _SIGS = {
     'blml_bin_ratio': (_I, [_I, _L, _P, _P, _P, _P]),
     'blml_new_bins': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P]),
     'blml_gain_sums': (_I, [_I, _L, _P, _D, _P, _D, _P, _D, _P, _P, _P]),
+    'blml_point_rows': (_I, [_L, _I, _P, _L, _P, _P, _P, _P, _P]),
     'blml_lbfgs_trial': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     'blml_finish': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
     'blml_log_score': (_I, [_I, _I, _L, _I, _P, _P, _D, _D, _P, _P, _P]),

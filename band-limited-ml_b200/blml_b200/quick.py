@@ -17,7 +17,7 @@ import torch
 from . import _lib
 from ._lib import call
 from .binned import BLMLBinned, _Red, _device
-from .spec import parse_modes, modes_lattice
+from .spec import parse_modes, modes_lattice, with_lattice, split_kind, dirichlet_N, dirichlet_inner_M
 from .local_gpu import ProductKernel, rows_dev
 
 
@@ -25,7 +25,7 @@ def lattice_coords(Z, h, device=None):
     """Integer lattice coordinates round(Z / h) of bin centres (float64, round half to even) on the GPU."""
     device = torch.device(device or 'cuda')
     Zt = torch.as_tensor(np.ascontiguousarray(Z, np.float64)).to(device)
-    ht = torch.as_tensor(np.ascontiguousarray(np.broadcast_to(np.asarray(h, float), (Zt.shape[1],)), np.float64)).to(device)
+    ht = torch.as_tensor(np.array(np.broadcast_to(np.asarray(h, float), (Zt.shape[1],)), np.float64)).to(device)
     out = torch.empty(Zt.shape, dtype=torch.int64, device=device)
     call('blml_lattice_coords', Zt.data_ptr(), Zt.shape[0], Zt.shape[1], ht.data_ptr(), out.data_ptr(),
          torch.cuda.current_stream(device).cuda_stream)
@@ -109,3 +109,137 @@ class BLMLQuickLattice(BLMLBinned):
 
     def _plan64(self):
         raise NotImplementedError("certificate on occupied bins: use a full-lattice fit")
+
+
+# ---------------------------------------------------------------------------------------------------- points path
+def lattice_steps(kinds, periods, h_target):
+    """The lattice steps for target widths (blml_kernels.py:57-68, the kernel classes' step rules,
+    blml_trivial.py:399-400, 556-561): a dirichlet column (and a pball group's columns) tiles its period with whole
+    bins, at least 8; every other column keeps its target width. Radial groups take their columns' finest target
+    (lattice_target, blml_trivial.py:1333-1341)."""
+    h_t = np.array(h_target, float)
+    groups = {}
+    for j, k in enumerate(kinds):
+        if split_kind(k)[0] in ('ball', 'pball'):
+            groups.setdefault(split_kind(k)[1], []).append(j)
+    for dims in groups.values():
+        h_t[dims] = h_t[dims].min()
+    h = np.empty(len(kinds))
+    for j, k in enumerate(kinds):
+        if split_kind(k)[0] in ('dirichlet', 'pball'):
+            P = float(periods[j])
+            h[j] = P / max(8, int(np.ceil(P / h_t[j] - 1e-9)))
+        else:
+            h[j] = float(h_t[j])
+    return h
+
+
+def quantize_points(X, kinds, periods, h):
+    """Bin centres of the points (blml_kernels.py:74-82; blml_trivial.py:402-403, 563-567): round(x / h) h, a periodic
+    column wrapped into [0, P) first; -0.0 becomes +0.0 (bins are unique by their bytes)."""
+    X = np.atleast_2d(np.asarray(X, float))
+    Xq = np.empty_like(X)
+    for j, k in enumerate(kinds):
+        if split_kind(k)[0] in ('dirichlet', 'pball'):
+            P = float(periods[j])
+            Xq[:, j] = np.mod(np.round(np.mod(X[:, j], P) / h[j]) * h[j], P)
+        else:
+            Xq[:, j] = np.round(X[:, j] / h[j]) * h[j]
+    return Xq + 0.0
+
+
+def unique_bins(Xq, sample_weight=None):
+    """The occupied bins in the reference's order (np.unique over each row's raw bytes, blml_trivial.py:2760-2765),
+    their weights (counts, or the points' total weight) and each point's bin."""
+    Xc = np.ascontiguousarray(Xq)
+    vdt = np.dtype((np.void, Xc.dtype.itemsize * Xc.shape[1]))
+    _, idx, inv, counts = np.unique(Xc.view(vdt), return_index=True, return_inverse=True, return_counts=True)
+    inv = np.ravel(inv)
+    w = counts.astype(float) if sample_weight is None else np.bincount(inv, weights=sample_weight, minlength=len(idx))
+    return Xq[idx], w, inv
+
+
+_PT_KIND = {'sinc': _lib.PT_SINC, 'slits': _lib.PT_SLITS, 'dirichlet': _lib.PT_DIRICHLET}
+
+
+class BLMLQuick(BLMLQuickLattice):
+    """The reference's BLMLQuick (engine='gpu', blml_trivial.py:2684-2800), real rank 1: points are snapped to a
+    lattice of steps bin_scale n^-1/4 / fc (a periodic column tiled by whole bins), binned in the reference's order,
+    and fitted as counts on the occupied bins by the pair solver of BLMLQuickLattice; modes with h (with_lattice)
+    are counts on that fixed lattice. predict / sqrt_density evaluate the exact kernel at any points on the GPU
+    (blml_point_rows: sinc, slits and dirichlet columns)."""
+
+    def __init__(self, tol=1e-4, batch_size=2000, seed=0, verbose=False, dtype=np.float32, bin_scale=0.1,
+                 max_sweeps=None, engine='gpu', solver='cd', lbfgs_m=20, device=None):
+        if solver not in ('cd', 'lbfgs'):
+            raise ValueError("solver: 'cd' (block coordinate descent with Anderson mixing) or 'lbfgs'")
+        if engine not in ('cpu', 'gpu'):
+            raise ValueError(f"engine {engine!r}: 'cpu' or 'gpu'")
+        super().__init__(tol=tol, max_sweeps=max_sweeps, dtype=dtype, seed=seed, verbose=verbose, device=device)
+        self.batch_size, self.bin_scale, self.engine = batch_size, bin_scale, engine
+        self.solver, self.lbfgs_m = solver, int(lbfgs_m)
+
+    def fit(self, X, modes, init=None, rebin_tol=1.0, signs=None, complex_g=False, sample_weight=None):
+        X = np.atleast_2d(np.asarray(X.detach().cpu().numpy() if isinstance(X, torch.Tensor) else X, np.float64))
+        n_rows, d = X.shape
+        if complex_g or signs is not None or init is not None:
+            raise NotImplementedError("BLMLQuick on the GPU: real rank-1 fits without signs or warm starts")
+        if modes_lattice(modes, d) is not None:
+            return BLMLQuickLattice.fit(self, X, modes, sample_weight=sample_weight)
+        sw = None if sample_weight is None else np.asarray(sample_weight, np.float64)
+        if sw is not None and (sw.shape != (n_rows,) or not np.all(sw > 0)):
+            raise ValueError("sample_weight: (n,) positive weights")
+        n = float(n_rows) if sw is None else float(sw.sum())
+        specs, dep = parse_modes(modes, d)
+        if dep is not None or len(specs) != 1:
+            raise NotImplementedError("BLMLQuick on the GPU: one real mode (rank 1) without dep columns")
+        sp = specs[0]
+        h = lattice_steps(sp['kinds'], sp['periods'], self.bin_scale * n ** -0.25 / np.asarray(sp['fc'], float))
+        Z, w, inv = unique_bins(quantize_points(X, sp['kinds'], sp['periods'], h), sw)
+        BLMLQuickLattice.fit(self, Z, with_lattice(modes, h), sample_weight=w)
+        self.Z_, self.w_pts_, self._h_vec, self.n_samples_ = Z, w, h, n
+        self.n_bins_, self.dim_ = len(Z), d
+        self._pt_cols = None
+        return self
+
+    # ---------------------------------------------------------------- at arbitrary points
+    def _point_cols(self):
+        if self._pt_cols is None:
+            sp = self.specs_[0]
+            cols = (_lib.PointCol * self.d_)()
+            for j, kind in enumerate(sp['kinds']):
+                name, tag = split_kind(kind)
+                if name not in _PT_KIND:
+                    raise NotImplementedError(f"predict at points: column kind {name!r} (sinc, slits, dirichlet)")
+                c = cols[j]
+                c.kind = _PT_KIND[name]; c.f = float(sp['fc'][j])
+                if name == 'slits':
+                    c.fi = (1.0 - float(tag)) * c.f
+                if name == 'dirichlet':
+                    P = float(sp['periods'][j])
+                    c.P = P; c.M = 2 * dirichlet_N(c.f, P) + 1
+                    c.Mi = dirichlet_inner_M(c.f, P, float(tag) if tag else None)
+            self._pt_cols = cols
+        return self._pt_cols
+
+    def sqrt_density(self, Xq):
+        """g(x) = (1/n) sum_b e_b K(x - z_b) at the points Xq, the exact kernel (blml_trivial.py:3307-3320)."""
+        if getattr(self, 'Z_', None) is None:
+            raise RuntimeError("Call fit() before sqrt_density().")
+        Xq = np.asarray(Xq, float)
+        Xq = Xq[:, None] if Xq.ndim == 1 else Xq
+        if Xq.shape[1] != self.d_:
+            raise ValueError(f"points: {self.d_} columns")
+        dev = self.dev_
+        Xt = torch.as_tensor(np.ascontiguousarray(Xq)).to(dev)
+        Zt = torch.as_tensor(np.ascontiguousarray(self.Z_, np.float64)).to(dev)
+        e = self.e_hat_t_[0].to(torch.float64).contiguous()
+        g = torch.empty(len(Xq), dtype=torch.float64, device=dev)
+        import ctypes as C
+        call('blml_point_rows', len(Xq), self.d_, Xt.data_ptr(), len(self.Z_), Zt.data_ptr(), e.data_ptr(),
+             C.cast(self._point_cols(), C.c_void_p), g.data_ptr(), self._st)
+        return g.cpu().numpy() / self.n_samples_
+
+    def predict(self, Xq):
+        """f(x) = g(x)^2 at the points Xq (blml_trivial.py:3288-3305)."""
+        return self.sqrt_density(Xq) ** 2

@@ -136,6 +136,16 @@ int blml_new_bins(int dtype, int K, int64_t B, int cplx, const void* E, const vo
 int blml_gain_sums(int dtype, int64_t B, const void* da, double sa, const void* db, double sb, const void* m, double eps,
                    double* part, double* out, void* stream);                                       /* nq = 3 */
 
+/* ---- the fitted amplitude at arbitrary points (BLMLQuick.sqrt_density / predict, blml_trivial.py:3288-3320) ----
+   g[i] = sum_b e[b] prod_c K_c(X[i, c] - Z[b, c]) with the exact one-column kernels (X: m x d, Z: B x d row-major
+   float64, d <= 8): sinc f sinc(f t); slits f sinc(f t) - fi sinc(fi t); dirichlet
+   (sin(pi M u / P) - sin(pi Mi u / P)) / (P sin(pi u / P)), u = |t| folded into [0, P / 2], (M - Mi) / P at u = 0 */
+enum { BLML_PT_SINC = 0, BLML_PT_SLITS = 1, BLML_PT_DIRICHLET = 2 };
+typedef struct { int kind; int M, Mi; double f, fi, P; } blml_point_col;
+typedef struct { blml_point_col c[8]; } blml_point_cols;
+int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* e,
+                    const blml_point_col* cols, double* g, void* stream);
+
 /* ---- one Armijo trial of the L-BFGS line search (BLMLBinned._solve_lbfgs, blml_binned.py:316-321) ----
  * En = E + t q and Un = U + t Sq (S linear: U + t S q = S(E + t q)), both written; out[0] = sum_occ w log F(Un),
  * out[1] = Re <En, Un>, from which L(En) = out[0] - n log out[1]. nq = 2. */

@@ -99,3 +99,20 @@ STREAM_SPECS = {
                      dict(tol=1e-8, solver='lbfgs', max_sweeps=3000, lr=0.1, param_every=2), 'partial',
                      dict(complex_g=True), 6, 500),
 }
+
+# the points path of BLMLQuick (blml_trivial.py:2705-2800): name -> (modes, n points, sample weights?, seed); the points,
+# the reference's bins (Z_ in its order), counts, steps, coefficients and predictions are in points.npz
+POINT_SPECS = {
+    'sinc2': (make_modes([3.0, 2.0], ['sinc', 'sinc']), 3000, False, 1),
+    'sinc_dirichlet': (make_modes([3.0, 4.0], ['sinc', 'dirichlet'], periods=[None, 1.0]), 3000, False, 2),
+    'sinc2_weighted': (make_modes([2.5, 2.5], ['sinc', 'sinc']), 2000, True, 3),
+}
+
+
+def point_cloud(n, seed):
+    """Two Gaussian blobs in the unit square (the second column wraps into [0, 1))."""
+    rng = np.random.default_rng(seed)
+    comp = rng.uniform(size=n) < 0.6
+    X = np.where(comp[:, None], rng.normal([0.35, 0.4], 0.08, (n, 2)), rng.normal([0.7, 0.75], 0.05, (n, 2)))
+    X[:, 1] = np.mod(X[:, 1], 1.0)
+    return X
