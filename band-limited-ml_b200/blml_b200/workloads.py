@@ -110,3 +110,13 @@ def points_5d_mixture(seed=0, n=200_000, d=5, comps=8):
     c = rng.choice(comps, n, p=wts)
     X = means[c] + sds[c] * rng.standard_normal((n, d))
     return np.clip(X, 0.0, np.nextafter(1.0, 0.0))
+
+
+def two_blob_points(n=200_000, seed=0):
+    """n points in the unit square from two Gaussian blobs (60% at (0.35, 0.4), sd 0.08; 40% at (0.7, 0.75), sd 0.05);
+    the second column wrapped into [0, 1) (a periodic column of period 1)."""
+    rng = np.random.default_rng(seed)
+    comp = rng.uniform(size=n) < 0.6
+    X = np.where(comp[:, None], rng.normal([0.35, 0.4], 0.08, (n, 2)), rng.normal([0.7, 0.75], 0.05, (n, 2)))
+    X[:, 1] = np.mod(X[:, 1], 1.0)
+    return X

@@ -16,7 +16,7 @@ Multi-GPU: the fits are independent (no exchange step): N ranks run N replicas o
 certified fits over the slowest rank's time.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--one-fit] [--matvec] [--pairs]
-                    [--select]
+                    [--select] [--extras]
 """
 import argparse
 import json
@@ -360,6 +360,96 @@ def select_bench(dev, n_search=16, seq_sample=2, batch=256):
             'picks': [[round(float(x), 5) for x in p] for p in picks]}
 
 
+def _timed(f, reps=1):
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out = f()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / reps, out
+
+
+def extras_bench(dev):
+    """The rows built around the fit, timed on the GPU (synchronised wall time of the public call) beside a bounded
+    CPU-oracle sample where the oracle restates the row:
+      gradients  fc_grad and implicit_grad (CG, at most 300 iterations) of a complex sinc x sinc fit on 128 x 128,
+                 float64, against the oracle's NumPy / SciPy FFT restatement at the same coefficients;
+      points     predict at 2e5 off-lattice points of a 2-D sinc x dirichlet point fit (n = 2e5 points, float32 state,
+                 tol 1e-4 as the reference's defaults; float64 kernel), pairs/s, against the oracle's unit formulas in
+                 NumPy on 1,000 of the points;
+      streaming  partial_fit of a 96 x 96 complex stream in 12 batches (L-BFGS refits to tol 1e-6, implicit
+                 gradients, an Adam step every 3 batches), batches/s; its parity anchor is the reference's own
+                 streams, so no CPU restatement is timed."""
+    import types
+    import torch
+    from blml_b200 import workloads, make_modes
+    from blml_b200.binned import BLMLBinned
+    from blml_b200.quick import BLMLQuick
+    from blml_b200.streaming import BLMLBinnedStreaming
+    sys.path.insert(0, os.path.join(ROOT, 'oracle'))
+    import blml_oracle as bo
+    import grad_oracle as go
+    out = {}
+    # ---- gradients
+    c = workloads.two_disk_field((128, 128), fc=0.3, N=2e5, seed=7)
+    rng = np.random.default_rng(7)
+    tr = rng.binomial(c.astype(np.int64), 0.8).astype(float); va = c - tr
+    modes = make_modes([0.3, 0.3], ['sinc', 'sinc'])
+    m = BLMLBinned(tol=1e-6, solver='lbfgs', max_sweeps=3000, device=dev).fit(tr, modes, complex_g=True)
+    m.fc_grad()
+    t_fc, G0 = _timed(m.fc_grad, 3)
+    t_ig, G1 = _timed(lambda: m.implicit_grad(va, 1e-3))
+    f = bo.BinnedFit(max_sweeps=0, tol=1e-6, solver='lbfgs').fit(
+        tr, modes, init=types.SimpleNamespace(e_hat=m.e_hat_, shape=tr.shape), complex_g=True)
+    f.e_hat = np.asarray(m.e_hat_); f.Se = f.Sall(f.e_hat)
+    t0 = time.perf_counter(); H0 = go.fc_grad(f); c_fc = time.perf_counter() - t0
+    t0 = time.perf_counter(); H1, it_c, _ = go.implicit_grad(f, va, 1e-3); c_ig = time.perf_counter() - t0
+    out['gradients'] = {'workload': 'complex sinc x sinc fit, 128 x 128, float64',
+                        'fc_grad_ms': 1e3 * t_fc, 'implicit_grad_ms': 1e3 * t_ig, 'cg_iterations': int(m.ift_iters_),
+                        'cpu_oracle': {'fc_grad_ms': 1e3 * c_fc, 'implicit_grad_ms': 1e3 * c_ig,
+                                       'cg_iterations': int(it_c), 'cores': os.cpu_count(), 'kind': 'port'},
+                        'fc_grad_rel_diff': float(np.max(np.abs(np.array(G0) - np.array(H0)) / np.abs(np.array(H0))))}
+    # ---- points
+    X = workloads.two_blob_points(200_000, seed=1)
+    pm = make_modes([3.0, 4.0], ['sinc', 'dirichlet'], periods=[None, 1.0])
+    t_fit, q = _timed(lambda: BLMLQuick(tol=1e-4, dtype=np.float32, device=dev).fit(X, pm))   # the reference's defaults
+    Xq = np.random.default_rng(2).uniform(0.0, 1.0, (200_000, 2))
+    q.predict(Xq[:1000])
+    t_pr, P = _timed(lambda: q.predict(Xq))
+    B = q.n_bins_
+    R = 1000
+    t0 = time.perf_counter()
+    g = np.zeros(R)
+    for s0 in range(0, B, 4096):
+        Z = q.Z_[s0:s0 + 4096]
+        K = bo.unit_value('sinc', [3.0], [None], [Xq[:R, 0, None] - Z[None, :, 0]]) * \
+            bo.unit_value('dirichlet', [4.0], [1.0], [Xq[:R, 1, None] - Z[None, :, 1]])
+        g += K @ np.ravel(q.e_hat_)[s0:s0 + 4096]
+    c_pr = time.perf_counter() - t0
+    ref = (g / q.n_samples_) ** 2
+    out['points'] = {'workload': '2-D sinc x dirichlet point fit, n = 2e5 points, predict at 2e5 points',
+                     'bins': int(B), 'fit_s': t_fit, 'fit_sweeps': int(q.n_sweeps_), 'fit_stop': q.stop_reason_,
+                     'predict_s': t_pr, 'Gpair_per_s': 2e5 * B / t_pr / 1e9,
+                     'cpu_oracle': {'Gpair_per_s': R * B / c_pr / 1e9, 'sample': f'{R} points x {B} bins',
+                                    'cores': os.cpu_count(), 'kind': 'port'},
+                     'predict_rel_diff': float(np.max(np.abs(P[:R] - ref)) / np.max(ref))}
+    # ---- streaming
+    full = workloads.two_disk_field((96, 96), fc=0.3, N=3e5, seed=9)
+    parts = np.random.default_rng(9).multinomial(1, [1 / 12] * 12, size=int(full.sum()))
+    idx = np.repeat(np.arange(full.size), full.astype(np.int64).ravel())
+    batches = [np.bincount(idx[parts[:, j] > 0], minlength=full.size).reshape(full.shape).astype(float)
+               for j in range(12)]
+    sm = make_modes([0.25, 0.25], ['sinc', 'sinc'])
+    st = BLMLBinnedStreaming(tol=1e-6, solver='lbfgs', max_sweeps=2000, param_every=3, device=dev)
+    st.partial_fit(batches[0], sm, complex_g=True)
+    t_st, _ = _timed(lambda: [st.partial_fit(b) for b in batches[1:]])
+    out['streaming'] = {'workload': '96 x 96 complex stream, 12 batches, L-BFGS refits tol 1e-6, Adam every 3',
+                        'batches_per_s': 11 / t_st, 'seconds': t_st,
+                        'fc_final': [float(v) for v in st.specs_[0]['fc']]}
+    return out
+
+
 def flush_l2(buf):
     buf.add_(1.0)
 
@@ -375,6 +465,8 @@ def main():
                     help='the 5-D pair path: one full rows pass over all bin pairs, GPU and a CPU-oracle sample')
     ap.add_argument('--select', action='store_true',
                     help='the batched cut-off search over 16 lattices beside the sequential single-fit search')
+    ap.add_argument('--extras', action='store_true',
+                    help='the gradients, point predictions and streaming refits, each beside a CPU-oracle sample')
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
@@ -395,6 +487,9 @@ def main():
         return
     if args.select:
         print(json.dumps(select_bench(dev)), flush=True)
+        return
+    if args.extras:
+        print(json.dumps(extras_bench(dev)), flush=True)
         return
     if args.matvec:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
