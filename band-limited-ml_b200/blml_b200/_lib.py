@@ -112,6 +112,10 @@ _SIGS = {
     'blml_new_bins': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P]),
     'blml_gain_sums': (_I, [_I, _L, _P, _D, _P, _D, _P, _D, _P, _P, _P]),
     'blml_point_rows': (_I, [_L, _I, _P, _L, _P, _P, _P, _P, _P]),
+    'blml_block_root': (_I, [_I, _P, _L, _P, _P, _P, _D, _P, _P]),
+    'blml_block_search': (_I, [_I, _P, _L, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_block_apply': (_I, [_I, _P, _L, _P, _D, _P, _P]),
+    'blml_gather_rows_i64': (_I, [_I, _I, _P, _P, _L, _P, _P]),
     'blml_lbfgs_trial': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
     'blml_finish': (_I, [_I, _I, _L, _I, _P, _P, _D, _P, _P, _P, _P]),
     'blml_log_score': (_I, [_I, _I, _L, _I, _P, _P, _D, _D, _P, _P, _P]),

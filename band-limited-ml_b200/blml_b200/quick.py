@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import call
+from ._lib import call, ptrs, dbl
 from .binned import BLMLBinned, _Red, _device
 from .spec import parse_modes, modes_lattice, with_lattice, split_kind, dirichlet_N, dirichlet_inner_M
 from .local_gpu import ProductKernel, rows_dev
@@ -44,9 +44,12 @@ class BLMLQuickLattice(BLMLBinned):
     """Real rank-1 BLML on counts at occupied lattice bins (see the module docstring)."""
 
     def __init__(self, tol=1e-4, max_sweeps=None, anderson=5, dtype=np.float32, seed=0, verbose=False, stall=1000,
-                 device=None):
+                 device=None, solver='jacobi'):
         super().__init__(tol=tol, max_sweeps=max_sweeps, anderson=anderson, dtype=dtype, seed=seed, verbose=verbose,
                          stall=stall, device=device)
+        if solver not in ('block', 'jacobi'):
+            raise ValueError("solver: 'block' (block coordinate descent) or 'jacobi' (Jacobi updates with Anderson)")
+        self.cd_solver = solver
 
     def fit(self, X, modes, sample_weight=None, init=None):
         Xn = X.detach().cpu().numpy() if isinstance(X, torch.Tensor) else np.asarray(X, np.float64)
@@ -94,10 +97,124 @@ class BLMLQuickLattice(BLMLBinned):
             E = torch.empty((1, B), dtype=self._rt, device=self.dev_)
             call('blml_start_root', self._code, B, self.c_t_.data_ptr(), self.sg_t_.data_ptr(), float(self.s_[0]),
                  E.data_ptr(), self._st)
-        E, U = self._solve_cd(E, self.max_sweeps)
-        # the solution's S e exactly (the solver's U is exact already: every U comes from a full pass)
+        if self.cd_solver == 'block':
+            E, U = self._solve_block_cd(E, self.max_sweeps)
+        else:
+            E, U = self._solve_cd(E, self.max_sweeps)
         self._finish(E, U)
         return self
+
+    def _solve_block_cd(self, E, max_sweeps):
+        """Block coordinate descent (blml_trivial.py:2860-3035) from E: each sweep visits the bins in a seeded random
+        order, in blocks of min(1024, max(32, B / 64)) bins; a block takes its coordinates' exact roots together and
+        S e follows by one rows pass of every bin against the block (B x block pairs), so a sweep costs one full pass
+        in total. Plain sweeps until one raises Phi = e'Se / 2 - sum c log e; that sweep is redone with the block
+        safeguard (the largest t in 2^-k that does not raise Phi along the block's step), which stays on. Stops at
+        max|rho| < tol (S e then recomputed exactly and the test repeated), or when the residual improved by less
+        than 1% over 50 sweeps. State e and S e in float64, pair products in the tables' precision."""
+        B, dev, n, st = self.B_, self.dev_, self.n_, self._st
+        f32 = self._code == _lib.F32
+        Bs = min(1024, max(32, B // 64), B)
+        c64 = self.c_t_.to(torch.float64).contiguous()
+        sg64 = torch.ones(B, dtype=torch.float64, device=dev)
+        sbb = float(self.s_[0])
+        red = self._red
+        D = self._Z.shape[1]
+        d = torch.empty(Bs, dtype=torch.float64, device=dev)
+        Zb = torch.empty((Bs, D), dtype=torch.int64, device=dev)
+        q = torch.empty(65, dtype=torch.float64, device=dev)
+        steps = 0.5 ** np.arange(31)
+        rng = np.random.default_rng(self.seed)
+
+        def exact_Se(e):
+            return rows_dev(self._Z, self._Z, e, self.tab_, grad=False, f32=f32)[0]
+
+        def phi(e, Se):
+            call('blml_merit_terms', _lib.F64, 1, B, 0, 0, e.data_ptr(), Se.data_ptr(), c64.data_ptr(),
+                 sg64.data_ptr(), red.part.data_ptr(), red.out.data_ptr(), st)
+            a, b, _ = red.read(3)
+            return (0.5 * a - b) / n
+
+        def resid(e, Se):
+            call('blml_resid', _lib.F64, 1, B, 0, e.data_ptr(), Se.data_ptr(), c64.data_ptr(), 1.0,
+                 red.part.data_ptr(), red.out.data_ptr(), st)
+            mx, nnan = red.read(2)
+            return float('nan') if nnan > 0 else mx
+
+        def sweep(e, Se, safeguard):
+            perm = torch.as_tensor(rng.permutation(B)).to(dev)
+            for s0 in range(0, B, Bs):
+                I = perm[s0:s0 + Bs]
+                m = int(I.numel())
+                call('blml_block_root', m, I.data_ptr(), B, e.data_ptr(), Se.data_ptr(), c64.data_ptr(), sbb,
+                     d.data_ptr(), st)
+                call('blml_gather_rows_i64', m, D, self._Z.data_ptr(), I.data_ptr(), B, Zb.data_ptr(), st)
+                v = rows_dev(self._Z, Zb[:m], d[:m], self.tab_, grad=False, f32=f32)[0]
+                t = 1.0
+                if safeguard:
+                    call('blml_block_search', m, I.data_ptr(), B, e.data_ptr(), d.data_ptr(), Se.data_ptr(),
+                         v.data_ptr(), c64.data_ptr(), q.data_ptr(), st)
+                    r = q.cpu().numpy()
+                    lin, quad, npos, logs, bad = r[0], r[1], r[2], r[3:34], r[34:65]
+                    if npos > 0:
+                        ok = (steps * lin + 0.5 * steps ** 2 * quad - logs <= 0) & (bad == 0)
+                        t = float(steps[np.argmax(ok)]) if ok.any() else 0.0
+                if t != 0.0:
+                    call('blml_block_apply', m, I.data_ptr(), B, d.data_ptr(), float(t), e.data_ptr(), st)
+                    call('blml_lincomb', _lib.F64, B, Se.data_ptr(), 2, dbl([1.0, t]), ptrs([Se, v]), st)
+
+        e = E[0].to(torch.float64).contiguous().clone()
+        Se = exact_Se(e)
+        safeguard = False
+        obj_prev = phi(e, Se)
+        hist, it, conv = [], 0, False
+        res = resid(e, Se)
+        self.stop_reason_ = 'stall'
+        while True:
+            if max_sweeps is not None and it >= max_sweeps:
+                self.stop_reason_ = 'max_sweeps'
+                break
+            it += 1
+            e_save, Se_save = e.clone(), Se.clone()
+            sweep(e, Se, safeguard)
+            obj_now = phi(e, Se)
+            if not safeguard and obj_now > obj_prev + 1e-10 * abs(obj_prev):
+                e, Se = e_save, Se_save
+                safeguard = True
+                sweep(e, Se, True)
+                obj_now = phi(e, Se)
+            obj_prev = obj_now
+            res = resid(e, Se)
+            if not np.isfinite(res):
+                hist.append(np.inf)
+                self.stop_reason_ = 'nan'
+                break
+            if res < self.tol:
+                Se = exact_Se(e)
+                res = resid(e, Se)
+            hist.append(res)
+            if self.verbose:
+                print(f'  block sweep {it}: max|rho| {res:.2e} Phi/n {obj_now:.8f}', flush=True)
+            if res < self.tol:
+                conv = True
+                self.stop_reason_ = 'tol'
+                break
+            if len(hist) > 50 and hist[-1] > 0.99 * min(hist[:-50]):
+                break
+        if not conv and max_sweeps is not None and np.isfinite(res):       # capped: normalise exactly
+            Se = exact_Se(e)
+            call('blml_dots', _lib.F64, B, 1, ptrs([e]), ptrs([Se]), red.part.data_ptr(), red.out.data_ptr(), st)
+            ee = red.read(1)[0]
+            sc = n / np.sqrt(max(ee, 1e-300))
+            call('blml_lincomb', _lib.F64, B, e.data_ptr(), 1, dbl([sc]), ptrs([e]), st)
+            call('blml_lincomb', _lib.F64, B, Se.data_ptr(), 1, dbl([sc]), ptrs([Se]), st)
+            res = resid(e, Se)
+            conv = res < self.tol
+            hist.append(res)
+        self.n_sweeps_, self.residual_, self.converged_ = it, res, conv
+        self.rho_history_ = hist
+        self.safeguard_ = safeguard
+        return e.to(self._rt).reshape(1, B).contiguous(), Se.to(self._rt).reshape(1, B).contiguous()
 
     def _Sall(self, E, out=None):
         """S E over the occupied bins: one pass of the pair kernel (float64 sums)."""
@@ -165,8 +282,8 @@ _PT_KIND = {'sinc': _lib.PT_SINC, 'slits': _lib.PT_SLITS, 'dirichlet': _lib.PT_D
 class BLMLQuick(BLMLQuickLattice):
     """The reference's BLMLQuick (engine='gpu', blml_trivial.py:2684-2800), real rank 1: points are snapped to a
     lattice of steps bin_scale n^-1/4 / fc (a periodic column tiled by whole bins), binned in the reference's order,
-    and fitted as counts on the occupied bins by the pair solver of BLMLQuickLattice; modes with h (with_lattice)
-    are counts on that fixed lattice. predict / sqrt_density evaluate the exact kernel at any points on the GPU
+    and fitted as counts on the occupied bins by the pair operator of BLMLQuickLattice with the reference's block
+    coordinate descent (_solve_block_cd); modes with h (with_lattice) are counts on that fixed lattice. predict / sqrt_density evaluate the exact kernel at any points on the GPU
     (blml_point_rows: sinc, slits and dirichlet columns)."""
 
     def __init__(self, tol=1e-4, batch_size=2000, seed=0, verbose=False, dtype=np.float32, bin_scale=0.1,
@@ -175,7 +292,8 @@ class BLMLQuick(BLMLQuickLattice):
             raise ValueError("solver: 'cd' (block coordinate descent with Anderson mixing) or 'lbfgs'")
         if engine not in ('cpu', 'gpu'):
             raise ValueError(f"engine {engine!r}: 'cpu' or 'gpu'")
-        super().__init__(tol=tol, max_sweeps=max_sweeps, dtype=dtype, seed=seed, verbose=verbose, device=device)
+        super().__init__(tol=tol, max_sweeps=max_sweeps, dtype=dtype, seed=seed, verbose=verbose, device=device,
+                         solver='block')
         self.batch_size, self.bin_scale, self.engine = batch_size, bin_scale, engine
         self.solver, self.lbfgs_m = solver, int(lbfgs_m)
 

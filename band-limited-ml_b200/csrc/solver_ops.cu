@@ -388,6 +388,80 @@ __global__ void k_gain_sums(int64_t B, const T* da, double sa, const T* db, doub
   block_partials<3>(v, part);
 }
 
+// ---------------------------------------------------------------------------------------------- block CD
+// The block coordinate descent of the point / lattice fits (blml_trivial.py:2860-3035): a block I of bins takes its
+// coordinates' exact roots together, S e follows by one rows pass of every bin against the block, and a safeguarded
+// step searches t in 2^-k (cd_line_search, blml_trivial.py:92-104). State e, S e and c = n w in float64; the block's
+// bin indices are checked against B (an index outside is skipped).
+constexpr int kLsSteps = 31;
+
+__global__ void k_block_root(int m, const int64_t* I, int64_t B, const double* e, const double* Se, const double* c,
+                             double sbb, double* d) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const int64_t b = I[j];
+    if (b < 0 || b >= B) { d[j] = 0.0; continue; }
+    const double eb = e[b];
+    d[j] = cd_root_d(Se[b] - sbb * eb, c[b], sbb) - eb;
+  }
+}
+
+// one block: out[0] = d . Se[I], out[1] = d . v[I], out[2] = bins with e > 0, out[3 + k] = sum_{e > 0} c log1p(t_k r),
+// out[3 + 31 + k] = bins with 1 + t_k r <= 0, r = d / e, t_k = 2^-k
+__global__ void __launch_bounds__(256) k_block_search(int m, const int64_t* I, int64_t B, const double* e,
+                                                     const double* d, const double* Se, const double* v,
+                                                     const double* c, double* out) {
+  constexpr int NQ = 3 + 2 * kLsSteps;
+  double q[NQ];
+#pragma unroll
+  for (int k = 0; k < NQ; k++) q[k] = 0.0;
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const int64_t b = I[j];
+    if (b < 0 || b >= B) continue;
+    const double dj = d[j], eb = e[b];
+    q[0] += dj * Se[b]; q[1] += dj * v[b];
+    if (eb > 0) {
+      q[2] += 1.0;
+      const double r = dj / eb, cc = c[b];
+      double t = 1.0;
+#pragma unroll
+      for (int k = 0; k < kLsSteps; k++) {
+        if (1.0 + t * r > 0) q[3 + k] += cc * log1p(t * r);
+        else q[3 + kLsSteps + k] += 1.0;
+        t *= 0.5;
+      }
+    }
+  }
+  __shared__ double sh[8][NQ];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NQ; k++) {
+    const double x = warp_sum(q[k]);
+    if (lane == 0) sh[wid][k] = x;
+  }
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  for (int k = threadIdx.x; k < NQ; k += blockDim.x) {
+    double s = 0.0;
+    for (int w = 0; w < nw; w++) s += sh[w][k];
+    out[k] = s;
+  }
+}
+
+__global__ void k_block_apply(int m, const int64_t* I, int64_t B, const double* d, double t, double* e) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const int64_t b = I[j];
+    if (b >= 0 && b < B) e[b] += t * d[j];
+  }
+}
+
+__global__ void k_gather_rows_i64(int m, int d, const int64_t* src, const int64_t* I, int64_t B, int64_t* out) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < (int64_t)m * d;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = x / d, k = x % d, b = I[j];
+    out[x] = (b >= 0 && b < B) ? src[b * d + k] : 0;
+  }
+}
+
 template <typename T, bool CPLX>
 __global__ void k_lgrad_finish(int K, int64_t B, const void* SV, const void* U, const T* w, double nq, void* g) {
   GRID_STRIDE(b, B) {
@@ -730,6 +804,41 @@ int blml_gain_sums(int dtype, int64_t B, const void* da, double sa, const void* 
                                                            (const float*)m, eps, part);
   BLML_CHECK_LAUNCH("blml_gain_sums");
   return finish_partials(part, 3, kRedBlocks, 0u, out, ST);
+}
+
+int blml_block_root(int m, const int64_t* I, int64_t B, const double* e, const double* Se, const double* c, double sbb,
+                    double* d, void* stream) {
+  if (m < 0 || B < 1 || (m > 0 && (!I || !e || !Se || !c || !d))) { set_error("blml_block_root: arguments"); return BLML_ERR_ARG; }
+  if (m == 0) return BLML_OK;
+  k_block_root<<<grid_for(m), 256, 0, ST>>>(m, I, B, e, Se, c, sbb, d);
+  BLML_CHECK_LAUNCH("blml_block_root");
+  return BLML_OK;
+}
+
+int blml_block_search(int m, const int64_t* I, int64_t B, const double* e, const double* d, const double* Se,
+                      const double* v, const double* c, double* out, void* stream) {
+  if (m < 0 || B < 1 || !out || (m > 0 && (!I || !e || !d || !Se || !v || !c))) {
+    set_error("blml_block_search: arguments"); return BLML_ERR_ARG;
+  }
+  k_block_search<<<1, 256, 0, ST>>>(m, I, B, e, d, Se, v, c, out);
+  BLML_CHECK_LAUNCH("blml_block_search");
+  return BLML_OK;
+}
+
+int blml_block_apply(int m, const int64_t* I, int64_t B, const double* d, double t, double* e, void* stream) {
+  if (m < 0 || B < 1 || (m > 0 && (!I || !d || !e))) { set_error("blml_block_apply: arguments"); return BLML_ERR_ARG; }
+  if (m == 0) return BLML_OK;
+  k_block_apply<<<grid_for(m), 256, 0, ST>>>(m, I, B, d, t, e);
+  BLML_CHECK_LAUNCH("blml_block_apply");
+  return BLML_OK;
+}
+
+int blml_gather_rows_i64(int m, int d, const int64_t* src, const int64_t* I, int64_t B, int64_t* out, void* stream) {
+  if (m < 0 || d < 1 || B < 1 || (m > 0 && (!src || !I || !out))) { set_error("blml_gather_rows_i64: arguments"); return BLML_ERR_ARG; }
+  if (m == 0) return BLML_OK;
+  k_gather_rows_i64<<<grid_for((int64_t)m * d), 256, 0, ST>>>(m, d, src, I, B, out);
+  BLML_CHECK_LAUNCH("blml_gather_rows_i64");
+  return BLML_OK;
 }
 
 int blml_lgrad_finish(int dtype, int K, int64_t B, int cplx, const void* SV, const void* U, const void* w, double nq,

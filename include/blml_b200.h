@@ -136,6 +136,19 @@ int blml_new_bins(int dtype, int K, int64_t B, int cplx, const void* E, const vo
 int blml_gain_sums(int dtype, int64_t B, const void* da, double sa, const void* db, double sb, const void* m, double eps,
                    double* part, double* out, void* stream);                                       /* nq = 3 */
 
+/* ---- block coordinate descent of the point / lattice fits (blml_trivial.py:2860-3035), float64 state ----
+   root:   d[j] = cd_root(Se[b] - sbb e[b], c[b], sbb) - e[b], b = I[j] (the block's exact roots, less e)
+   search: out[0] = d . Se[I], out[1] = d . v[I] (v = S[:, I] d), out[2] = #{e[I] > 0}, out[3 + k] =
+           sum_{e > 0} c log1p(2^-k d / e), out[34 + k] = #{1 + 2^-k d / e <= 0}, k < 31 (cd_line_search, :92-104)
+   apply:  e[I[j]] += t d[j];   gather: out[j, :] = src[I[j], :] (int64 rows, d columns)
+   indices outside [0, B) are skipped */
+int blml_block_root(int m, const int64_t* I, int64_t B, const double* e, const double* Se, const double* c, double sbb,
+                    double* d, void* stream);
+int blml_block_search(int m, const int64_t* I, int64_t B, const double* e, const double* d, const double* Se,
+                      const double* v, const double* c, double* out, void* stream);        /* out: 65 doubles */
+int blml_block_apply(int m, const int64_t* I, int64_t B, const double* d, double t, double* e, void* stream);
+int blml_gather_rows_i64(int m, int d, const int64_t* src, const int64_t* I, int64_t B, int64_t* out, void* stream);
+
 /* ---- the fitted amplitude at arbitrary points (BLMLQuick.sqrt_density / predict, blml_trivial.py:3288-3320) ----
    g[i] = sum_b e[b] prod_c K_c(X[i, c] - Z[b, c]) with the exact one-column kernels (X: m x d, Z: B x d row-major
    float64, d <= 8): sinc f sinc(f t); slits f sinc(f t) - fi sinc(fi t); dirichlet
