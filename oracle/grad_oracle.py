@@ -16,7 +16,7 @@ fitted coefficients).
 """
 import numpy as np
 
-from blml_oracle import ball_profile, split_kind, units_of, mode_table, rdot
+from blml_oracle import ball_profile, split_kind, units_of, unit_value, rdot
 
 
 def ball_profile_dlog(s, dg):
@@ -71,7 +71,6 @@ def dK_spectra(spec, shape, h, pad):
             if v == u:
                 T = T * unit_value_dlog(kv, fcv, per, dd)
             else:
-                from blml_oracle import unit_value
                 T = T * unit_value(kv, fcv, per, dd)
         for mk in masks:
             T = T * mk
