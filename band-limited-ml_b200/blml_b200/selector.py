@@ -84,18 +84,19 @@ def search_walk(d, kinds, periods_scaled, fc0=0.2, patience=2, max_sweeps=6, fac
                 free=None):
     """The search of selector.py:488-553 as a generator.
 
-    Yields (fc, best) for each candidate not scored before, best being the score it is compared with (None for the
-    first); receives the candidate's score; returns (fc, best, n_scored). Stage 1 doubles every growing column (free,
+    Yields (fc, best, stage) for each candidate not scored before, best being the score it is compared with (None
+    for the first) and stage the step that proposes it ('double', 'volume' or 'refine'); receives the candidate's
+    score; returns (fc, best, n_scored). Stage 1 doubles every growing column (free,
     without a start) until `patience` doublings in a row fail to improve, then walks the volume grid
     centre * 2^(j / dg) from the best doubling, up first and down only if no up-step improved. Stage 2 steps each free
     block by each factor (up, then down if up did not move), repeating full sweeps, at most `max_sweeps` per factor,
     until a sweep accepts nothing; a step must improve by more than 1e-6."""
     scored = {}
 
-    def score(fc, best):
+    def score(fc, best, stage):
         k = _key(fc)
         if k not in scored:
-            scored[k] = yield fc, best
+            scored[k] = yield fc, best, stage
         return scored[k]
 
     st = np.full(d, np.nan) if start is None else np.asarray(start, float)
@@ -104,11 +105,11 @@ def search_walk(d, kinds, periods_scaled, fc0=0.2, patience=2, max_sweeps=6, fac
     dg = int(grow.sum())
     fc = np.where(grow, float(fc0), st)
     best_fc = fc.copy()
-    best = yield from score(fc, None)
+    best = yield from score(fc, None, 'double')
     misses = 0
     while dg and misses <= patience:
         fc = np.where(grow, fc * 2.0, fc)
-        v = yield from score(fc, best)
+        v = yield from score(fc, best, 'double')
         if v > best:
             best, best_fc, misses = v, fc.copy(), 0
         else:
@@ -118,7 +119,7 @@ def search_walk(d, kinds, periods_scaled, fc0=0.2, patience=2, max_sweeps=6, fac
         took = False
         for j in range(1, dg):
             cand = np.where(grow, centre * 2.0 ** (sign * j / dg), centre)
-            v = yield from score(cand, best)
+            v = yield from score(cand, best, 'volume')
             if not v > best:
                 break
             best, best_fc, took = v, cand, True
@@ -134,7 +135,7 @@ def search_walk(d, kinds, periods_scaled, fc0=0.2, patience=2, max_sweeps=6, fac
                     stepped = False
                     cand = move(fc, blk, fac, kinds, periods_scaled)
                     while cand is not None:
-                        v = yield from score(cand, best)
+                        v = yield from score(cand, best, 'refine')
                         if not v > best + 1e-6:
                             break
                         best, fc, moved, stepped = v, cand, True, True
@@ -152,9 +153,9 @@ def search(obj, d, kinds, periods_scaled, fc0=0.2, patience=2, max_sweeps=6, tag
     obj(fc) -> validation score (higher is better)."""
     walk = search_walk(d, kinds, periods_scaled, fc0, patience, max_sweeps, factors, start, free)
     try:
-        fc, _ = next(walk)
+        fc = next(walk)[0]
         while True:
-            fc, _ = walk.send(float(obj(fc)))
+            fc = walk.send(float(obj(fc)))[0]
     except StopIteration as done:
         fc, best, n = done.value
     if verbose:
@@ -175,7 +176,7 @@ class _Walk:
         walk = search_walk(*self.args)
         i = 0
         try:
-            fc, best = next(walk)
+            fc, best, stage = next(walk)
             while True:
                 k = _key(fc)
                 v = self.known.get(k)
@@ -185,10 +186,10 @@ class _Walk:
                         v = self.known[k] = float(v)
                 if v is None:
                     if i == len(hyp):
-                        return False, (fc, best)
+                        return False, (fc, best, stage)
                     v = hyp[i]
                     i += 1
-                fc, best = walk.send(v)
+                fc, best, stage = walk.send(v)
         except StopIteration as done:
             return True, done.value
 
@@ -205,7 +206,7 @@ class _Walk:
                 if not hyp:
                     self.result = r
                 continue
-            fc, best = r
+            fc, best, _ = r
             k = _key(fc)
             if k not in keys:
                 keys.add(k)
