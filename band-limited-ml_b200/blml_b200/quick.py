@@ -302,8 +302,14 @@ class BLMLQuick(BLMLQuickLattice):
         n_rows, d = X.shape
         if complex_g or signs is not None or init is not None:
             raise NotImplementedError("BLMLQuick on the GPU: real rank-1 fits without signs or warm starts")
-        if modes_lattice(modes, d) is not None:
-            return BLMLQuickLattice.fit(self, X, modes, sample_weight=sample_weight)
+        h_fixed = modes_lattice(modes, d)
+        if h_fixed is not None:                           # counts on a fixed lattice: the occupied bins as given
+            BLMLQuickLattice.fit(self, X, modes, sample_weight=sample_weight)
+            keep = np.ones(n_rows, bool) if sample_weight is None else np.asarray(sample_weight, float) > 0
+            self.Z_, self._h_vec = X[keep], np.asarray(h_fixed, float)
+            self.n_bins_, self.dim_, self.n_samples_ = int(keep.sum()), d, self.n_
+            self._pt_cols = None
+            return self
         sw = None if sample_weight is None else np.asarray(sample_weight, np.float64)
         if sw is not None and (sw.shape != (n_rows,) or not np.all(sw > 0)):
             raise ValueError("sample_weight: (n,) positive weights")

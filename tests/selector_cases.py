@@ -52,3 +52,79 @@ CASES = {
                        kw=dict(fc0=0.05, patience=3, max_sweeps=4, factors=(R2, 2.0 ** 0.25)),
                        obj=hashed(7, 0.5)),
 }
+
+
+def first_mode_fc(modes, d):
+    """fc per column of the first mode (a tuple key gives its value to each of its columns)."""
+    fc = np.full(d, np.nan)
+    for key, c in modes[0].items():
+        v = c.get('fc')
+        v = v['value'] if isinstance(v, dict) else v
+        for j in (key if isinstance(key, tuple) else (key,)):
+            fc[j] = float(v)
+    return fc
+
+
+class StubQuick:
+    """A deterministic stand-in for BLMLQuick in the selector tests: fit keeps the points, their weights and the first
+    mode's fc per column (recorded in StubQuick.calls); predict is the weighted product-Gaussian kernel density with
+    bandwidth 0.2 / fc per column. Smooth in fc, with an interior optimum of the validation log-likelihood."""
+    calls = []
+
+    def __init__(self, *a, **k):
+        pass
+
+    def fit(self, X, modes, signs=None, complex_g=False, sample_weight=None, init=None):
+        X = np.atleast_2d(np.asarray(X, float))
+        self.X = X
+        self.sw = np.ones(len(X)) if sample_weight is None else np.asarray(sample_weight, float)
+        self.fc = first_mode_fc(modes, X.shape[1])
+        self.bw = 0.2 / self.fc
+        StubQuick.calls.append(self.fc.copy())
+        return self
+
+    def predict(self, Xq):
+        Xq = np.atleast_2d(np.asarray(Xq, float))
+        z = (Xq[:, None, :] - self.X[None, :, :]) / self.bw
+        k = np.exp(-0.5 * (z * z).sum(2)) / np.prod(self.bw * np.sqrt(2 * np.pi))
+        return (k @ self.sw) / self.sw.sum()
+
+
+def select_points(n, seed, d=2):
+    rng = np.random.default_rng(seed)
+    comp = rng.uniform(size=n) < 0.55
+    X = np.where(comp[:, None], rng.normal(0.3, 0.07, (n, d)), rng.normal(0.65, 0.12, (n, d)))
+    X[:, -1] *= 3.0                                         # columns on different scales (the IQR scaling matters)
+    return X
+
+
+SINC2 = [{0: dict(kind='sinc'), 1: dict(kind='sinc')}]
+# name: (points n, seed, modes template, select keywords, with X_val, with weights)
+SELECT_CASES = {
+    'shared': (240, 1, SINC2, dict(search='shared'), False, False),
+    'shared_volume': (240, 2, SINC2, dict(search='shared', shared_step='volume'), False, False),
+    'hillclimb': (240, 3, SINC2, dict(search='hillclimb'), False, False),
+    'shared_hillclimb': (240, 4, SINC2, dict(), False, False),
+    'auto': (240, 5, SINC2, dict(search='auto', factors=(2 ** 0.5, 2 ** 0.25)), False, False),
+    'auto_val_weights': (200, 6, SINC2, dict(search='auto'), True, True),
+    'auto_fixed_column': (240, 7, [{0: dict(kind='sinc', fc=dict(value=4.0, trainable=False)), 1: dict(kind='sinc')}],
+                          dict(search='auto'), False, False),
+    'ball_group': (240, 8, [{(0, 1): dict(kind='ball')}], dict(), False, False),
+}
+# name: (lattice shape, seed, modes template, select_counts keywords)
+COUNTS_CASES = {
+    'counts_default': ((24, 24), 11, SINC2, dict()),
+    'counts_capped': ((20, 28), 12, SINC2, dict(fc0=2.0, fc_max=9.0, factors=(2 ** 0.5, 2 ** 0.25))),
+}
+
+
+def counts_lattice(shape, seed):
+    """Training / validation counts on a full lattice of bin centres (h = 1 / side per column)."""
+    rng = np.random.default_rng(seed)
+    h = np.array([1.0 / m for m in shape])
+    g = np.meshgrid(*[(np.arange(m) + 0.5) * hh for m, hh in zip(shape, h)], indexing='ij')
+    Z = np.stack([x.ravel() for x in g], 1)
+    p = np.exp(-0.5 * (((Z - 0.4) / 0.12) ** 2).sum(1)) + 0.5 * np.exp(-0.5 * (((Z - 0.7) / 0.06) ** 2).sum(1))
+    p = p / p.sum()
+    w_tr = rng.multinomial(3000, p).astype(float); w_va = rng.multinomial(800, p).astype(float)
+    return Z, w_tr, w_va, h
