@@ -433,15 +433,46 @@ def _vll_fn(Est, Xa, Xb, kinds, periods_scaled, rank, complex_g, wa, wb, jac):
     return vll
 
 
+def _cond_vll_fn(Est, Xa, Xb, kinds, periods_scaled, dep, iqr, rank, complex_g, wa, wb):
+    """The conditional validation score (selector.py:318-357, method 'ratio' with separate fits): the mean of
+    log p_joint - log p_marginal over the validation points, the marginal fitted on the other columns with the same
+    fc, less the dep columns' log IQR (original units)."""
+    d = Xa.shape[1]
+    dep_idx = sorted(set(int(i) for i in np.atleast_1d(dep)))
+    if not dep_idx or any(i < 0 or i >= d for i in dep_idx):
+        raise ValueError(f"dep indices {dep_idx} out of range for {d} dims")
+    keep = [k for k in range(d) if k not in dep_idx]
+    if not keep:
+        raise ValueError("dep covers all dims; need at least one conditioning dim for the marginal")
+    kinds_m = [kinds[k] for k in keep] if kinds else None
+    per_m = [periods_scaled[k] for k in keep] if periods_scaled else None
+    jac = np.log(iqr[dep_idx]).sum()
+
+    def cvll(fc):
+        fc = list(fc)
+        mj = _fit(Est, Xa, fc, kinds, periods_scaled, rank, complex_g, sw=wa)
+        mm = _fit(Est, Xa[:, keep], [fc[k] for k in keep], kinds_m, per_m, rank, complex_g, sw=wa)
+        lj = np.log(np.maximum(mj.predict(Xb).ravel(), 1e-300))
+        lm = np.log(np.maximum(mm.predict(Xb[:, keep]).ravel(), 1e-300))
+        return _wmean(lj - lm, wb) - jac
+    return cvll
+
+
+def _objective(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep):
+    if dep is None:
+        return _vll_fn(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, np.log(iqr).sum())
+    return _cond_vll_fn(Est, Xa, Xb, kinds, per, dep, iqr, rank, complex_g, wa, wb)
+
+
 def _select_shared(X, kinds, periods, seed=0, engine='cpu', X_val=None, shared_step='double', complex_g=False,
-                   rank=1, start=None, free=None, sw=None, sw_val=None):
+                   rank=1, start=None, free=None, sw=None, sw_val=None, dep=None):
     """One fc for every growing scaled column, doubled from 0.2 until the validation score first drops; the peak
-    (selector.py:162-195). Returns (fc in data units, best)."""
+    (selector.py:162-195; conditional, dep given: :360-392). Returns (fc in data units, best)."""
     Est = _estimator_class(engine)
     Xs, per, iqr = _scale_data(X, kinds, periods, sw)
     Xa, Xb, wa, wb = _split(Xs, iqr, seed, X_val, sw, sw_val)
     step = _shared_step(shared_step, Xa.shape[1])
-    vll = _vll_fn(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, np.log(iqr).sum())
+    vll = _objective(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep)
     st, fr, grow = _start_free(start, free, iqr, Xa.shape[1])
     vec = lambda c: np.where(grow, c, st)
     fc = 0.2
@@ -462,16 +493,19 @@ def _select_shared(X, kinds, periods, seed=0, engine='cpu', X_val=None, shared_s
 
 
 def _select_hillclimb(X, kinds, periods, seed=0, init_fc=None, engine='cpu', X_val=None, complex_g=False, rank=1,
-                      start=None, free=None, sw=None, sw_val=None):
+                      start=None, free=None, sw=None, sw_val=None, dep=None):
     """Per-block doubling (x2 while it improves, else x0.5 while it improves), full sweeps until none moves
-    (selector.py:197-247). Returns (fc in data units, best)."""
+    (selector.py:197-247; conditional: :394-440, started at 0.2 in every scaled column). Returns (fc in data
+    units, best)."""
     Est = _estimator_class(engine)
     Xs, per, iqr = _scale_data(X, kinds, periods, sw)
     Xa, Xb, wa, wb = _split(Xs, iqr, seed, X_val, sw, sw_val)
     n2, d = Xa.shape
-    vll = _vll_fn(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, np.log(iqr).sum())
+    vll = _objective(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep)
     if init_fc is not None:
         fc = np.array(init_fc, dtype=float)
+    elif dep is not None:
+        fc = np.full(d, 0.2)
     else:
         ranges = np.maximum(Xa.max(axis=0) - Xa.min(axis=0), 1e-10)
         fc = 0.5 * 0.1 * (n2 ** -0.25) / ranges
@@ -500,14 +534,14 @@ def _select_hillclimb(X, kinds, periods, seed=0, init_fc=None, engine='cpu', X_v
 
 
 def _select_auto(X, kinds, periods, seed=0, engine='cpu', X_val=None, fc0=0.2, complex_g=False, rank=1,
-                 factors=(SQRT2,), start=None, free=None, sw=None, sw_val=None):
-    """The volume-grid shared search and the harmonic-aware refinement (search) on the validation score
-    (selector.py:554-613, rank 1 / shared modes). Returns (fc in data units, best)."""
+                 factors=(SQRT2,), start=None, free=None, sw=None, sw_val=None, dep=None):
+    """The volume-grid shared search and the harmonic-aware refinement (search) on the validation score, joint or
+    conditional (selector.py:554-613, rank 1 / shared modes). Returns (fc in data units, best)."""
     X = np.asarray(X, dtype=float)
     Xs, per, iqr = _scale_data(X, kinds, periods, sw)
     Xa, Xb, wa, wb = _split(Xs, iqr, seed, X_val, sw, sw_val)
     d = Xa.shape[1]
-    obj = _vll_fn(_estimator_class(engine), Xa, Xb, kinds, per, rank, complex_g, wa, wb, np.log(iqr).sum())
+    obj = _objective(_estimator_class(engine), Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep)
     st = None if start is None else np.asarray(start, float) * iqr
     fc, best = search(obj, d, kinds, per, fc0=fc0, factors=factors, start=st, free=free)
     return fc / iqr, best
@@ -518,8 +552,9 @@ def select(Xtr_raw, modes, search='shared_hillclimb', seed=0, init_fc=None, engi
            sample_weight=None, val_weight=None):
     """fc for a modes template on points (selector.py:617-666): IQR-scaled columns, a validation split (or X_val), the
     search pattern 'shared_hillclimb' (default), 'shared', 'hillclimb' or 'auto', each candidate a BLMLQuick fit
-    scored by the mean log density of the validation points (in data units). Returns (modes with the selected fc,
-    best). The GPU fits are real rank 1: conditional (dep) objectives, signs, complex_g, rank > 1 and
+    scored by the mean log density of the validation points (in data units); dep columns in the modes give the
+    conditional score, mean log(p_joint / p_marginal), the marginal a second fit on the other columns with the same
+    fc. Returns (modes with the selected fc, best). The GPU fits are real rank 1: signs, complex_g, rank > 1 and
     separate_modes raise NotImplementedError."""
     if search not in ('shared_hillclimb', 'shared', 'hillclimb', 'auto'):
         raise ValueError(f"search must be 'shared_hillclimb', 'shared', 'hillclimb' or 'auto', got {search}")
@@ -529,14 +564,16 @@ def select(Xtr_raw, modes, search='shared_hillclimb', seed=0, init_fc=None, engi
     sw = None if sample_weight is None else np.asarray(sample_weight, float)
     sw_val = None if val_weight is None else np.asarray(val_weight, float)
     kinds, periods, dep, K, F = _template(modes, Xtr_raw.shape[1])
-    if dep is not None or signs is not None or complex_g or K > 1 or separate_modes:
-        raise NotImplementedError("select on the GPU: real rank-1 joint fits (no dep, signs, complex_g, rank > 1)")
+    if signs is not None and dep is not None:
+        raise ValueError("signs with dep=... (the marginal's g has its own signs)")
+    if signs is not None or complex_g or K > 1 or separate_modes:
+        raise NotImplementedError("select on the GPU: real rank-1 fits (no signs, complex_g, rank > 1)")
     from .spec import modes_trainable, with_fc
     T = modes_trainable(modes)
     start, free = F[0], T[0]
     start = None if np.all(np.isnan(start)) else start
     free = None if np.all(free) else free
-    sf = dict(start=start, free=free, sw=sw, sw_val=sw_val)
+    sf = dict(start=start, free=free, sw=sw, sw_val=sw_val, dep=dep)
     if search == 'auto':
         fc, best = _select_auto(Xtr_raw, kinds, periods, seed, engine, X_val, factors=factors, **sf)
     elif search == 'shared':
@@ -547,7 +584,7 @@ def select(Xtr_raw, modes, search='shared_hillclimb', seed=0, init_fc=None, engi
         fc_shared, _ = _select_shared(Xtr_raw, kinds, periods, seed, engine, X_val, shared_step, **sf)
         _, _, iqr = _scale_data(Xtr_raw, kinds, periods, sw)
         fc, best = _select_hillclimb(Xtr_raw, kinds, periods, seed, fc_shared * iqr, engine, X_val, free=free, sw=sw,
-                                     sw_val=sw_val)
+                                     sw_val=sw_val, dep=dep)
     return with_fc(modes, fc), best
 
 

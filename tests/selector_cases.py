@@ -110,6 +110,13 @@ SELECT_CASES = {
     'auto_fixed_column': (240, 7, [{0: dict(kind='sinc', fc=dict(value=4.0, trainable=False)), 1: dict(kind='sinc')}],
                           dict(search='auto'), False, False),
     'ball_group': (240, 8, [{(0, 1): dict(kind='ball')}], dict(), False, False),
+    'cond_shared': (240, 9, [{0: dict(kind='sinc', dep=True), 1: dict(kind='sinc')}], dict(search='shared'), False,
+                    False),
+    'cond_hillclimb': (240, 10, [{0: dict(kind='sinc'), 1: dict(kind='sinc', dep=True)}], dict(search='hillclimb'),
+                       False, False),
+    'cond_shared_hillclimb': (240, 11, [{0: dict(kind='sinc', dep=True), 1: dict(kind='sinc')}], dict(), False, True),
+    'cond_auto_val': (200, 12, [{0: dict(kind='sinc'), 1: dict(kind='sinc', dep=True)}], dict(search='auto'), True,
+                      False),
 }
 # name: (lattice shape, seed, modes template, select_counts keywords)
 COUNTS_CASES = {
