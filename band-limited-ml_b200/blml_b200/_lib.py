@@ -12,6 +12,7 @@ LIB_PATH = os.path.join(_HERE, 'libblml_b200.so')
 
 F64, F32 = 0, 1
 ENGINE_SIMT, ENGINE_TC = 0, 1
+ROUTE_AUTO, ROUTE_CONTRACT, ROUTE_FFT = 0, 1, 2
 
 
 class BLMLError(RuntimeError):
@@ -51,6 +52,10 @@ _SIGS = {
     'blml_group_create': (_I, [_I, _P, _P, _I, _P, _P, _P, _P, C.POINTER(_P)]),
     'blml_group_matvec': (_I, [_P, _P]),
     'blml_group_destroy': (_I, [_P]),
+    'blml_plan_set_route': (_I, [_P, _I]),
+    'blml_plan_route': (_I, [_P]),
+    'blml_group_set_route': (_I, [_P, _I]),
+    'blml_group_route': (_I, [_P]),
     'blml_seg_blocks': (_I, []),
     'blml_seg_start_root': (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     'blml_seg_update_real1': (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),

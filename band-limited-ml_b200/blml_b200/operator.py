@@ -223,6 +223,15 @@ class Plan:
             _lib.lib().blml_plan_destroy(h)
             self._h = None
 
+    @property
+    def route(self):
+        """_lib.ROUTE_FFT when blml_matvec runs the row / column FFTs of a DFT-mask kernel, else ROUTE_CONTRACT."""
+        return int(_lib.lib().blml_plan_route(self._h))
+
+    @route.setter
+    def route(self, r):
+        _lib.call('blml_plan_set_route', self._h, int(r))
+
     def workspace(self, nb, device):
         import torch
         need = int(_lib.lib().blml_matvec_workspace(self._h, nb))

@@ -50,10 +50,12 @@ class FitResult:
 
 
 class _Group:
-    def __init__(self, plans, x, x_off, y, y_off, x_complex):
+    """One grouped mat-vec: problem g applies plans[g] to nbatch[g] lattices from x_off[g] (default one each)."""
+
+    def __init__(self, plans, x, x_off, y, y_off, x_complex, nbatch=None):
         G = len(plans)
         arr = (C.c_void_p * G)(*[p._h.value for p in plans])
-        nb = np.ones(G, np.int32)
+        nb = np.ones(G, np.int32) if nbatch is None else np.ascontiguousarray(nbatch, np.int32)
         xo = np.ascontiguousarray(x_off, np.int64); yo = np.ascontiguousarray(y_off, np.int64)
         h = C.c_void_p()
         call('blml_group_create', G, C.cast(arr, C.c_void_p), nb.ctypes.data_as(C.c_void_p), int(x_complex),
@@ -62,6 +64,14 @@ class _Group:
 
     def __call__(self, stream):
         call('blml_group_matvec', self._h, stream)
+
+    @property
+    def route(self):
+        return int(_lib.lib().blml_group_route(self._h))
+
+    @route.setter
+    def route(self, r):
+        call('blml_group_set_route', self._h, int(r))
 
     def __del__(self):
         if getattr(self, '_h', None) is not None and self._h.value and _lib._lib is not None:

@@ -1,0 +1,475 @@
+// The FFT route of the mat-vec for kernels that are exact DFT masks on a circular 2-D lattice.
+//
+// A pball group, or dirichlet columns, on a lattice whose every axis is one period (the reference's circular pad,
+// blml_binned.py:130-136) has plane waves at integer harmonics: nu = k / M on an M-point axis. Then
+//     S e = sum_q W_q v_q v_q^H e
+// is the unnormalised inverse 2-D DFT of W times the forward DFT of e, restricted to the band's harmonics: the
+// reference's rfftn -> x Kf -> irfftn (blml_binned.py:156-168) with Kf zero outside the band. Three grouped stages
+// run it over every fit of a batch, each a batch of 1-D FFTs in shared memory:
+//   A  rows:    FFT of every lattice row (length M2), keep the H2 harmonics of axis 1 -> Z (nb, H2, M1)
+//   B  columns: FFT of every Z column (length M1), times W over the band (zero elsewhere), inverse FFT -> Z
+//   C  rows:    scatter each row's H2 harmonics into a zero spectrum, inverse FFT (length M2) -> the lattice row
+// The FFTs are mixed-radix (2, 3, 4, 6, 8) Stockham passes: sides 2^a 3^b (the benchmark sweep's {64, ..., 384}).
+// Each CTA holds two buffers of up to kFE complex values (several rows or columns, one padded row per transform;
+// a single transform when the side is longer) and the length's twiddle table; passes run out of place between them.
+// Versus the restricted transforms (matvec.cu) this costs O(M log M) per row instead of O(M H), and in float64 it
+// rounds like an FFT (~1e-16 log M relative), so the route changes no result beyond rounding.
+#include <vector>
+#include <algorithm>
+#include <cmath>
+#include "plan.cuh"
+
+namespace blml {
+
+constexpr int kFT = 256;                 // threads per CTA
+constexpr int kFE = 2048;                // complex values per CTA buffer (transforms x length); one transform when longer
+constexpr int kMaxSide = 4096;           // longest side of the route
+constexpr int kMaxRad = 12;
+
+static int fft_smem_once();
+
+// per-plan data of the route (host struct holding device pointers)
+struct FftPlan {
+  int M1, M2, H1, H2;
+  int nrad1, nrad2;
+  int8_t rad1[kMaxRad], rad2[kMaxRad];
+  void* tw1; void* tw2;                  // exp(-2 pi i t / M) for t < M, complex of the plan's dtype
+  int* k2;                               // the H2 harmonics of axis 1 as DFT indices (k mod M2)
+  int* map1;                             // per DFT index of axis 0: its position in the band's axis-0 list, or -1
+};
+
+struct FftDesc {
+  const void* X; void* Y; void* Z; const void* W;
+  const void* tw1; const void* tw2; const int* k2; const int* map1;
+  int M1, M2, H1, H2, nb, flags;         // flags: 1 real input, 4 real output
+  int rows, cols;                        // transforms per CTA: rows (stages A, C), columns (stage B)
+  int ctasA, ctasB;                      // CTAs of this problem in stages A / C and B
+  int nrad1, nrad2;
+  int8_t rad1[kMaxRad], rad2[kMaxRad];
+};
+
+// ------------------------------------------------------------------------------------------------- butterflies
+// y_s = sum_r a_r exp(sign 2 pi i r s / R), sign = +1 for the inverse transform, -1 forward.
+template <typename T, bool INV> __device__ __forceinline__ cpx<T> mul_i(cpx<T> a) {   // a * (sign i)
+  return INV ? cpx<T>{-a.im, a.re} : cpx<T>{a.im, -a.re};
+}
+template <typename T> __device__ __forceinline__ cpx<T> cadd(cpx<T> a, cpx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T> __device__ __forceinline__ cpx<T> csub(cpx<T> a, cpx<T> b) { return {a.re - b.re, a.im - b.im}; }
+
+template <typename T, bool INV> __device__ __forceinline__ void dft2(cpx<T>& a0, cpx<T>& a1) {
+  const cpx<T> t = a0; a0 = cadd(t, a1); a1 = csub(t, a1);
+}
+template <typename T, bool INV> __device__ __forceinline__ void dft4(cpx<T>& a0, cpx<T>& a1, cpx<T>& a2, cpx<T>& a3) {
+  const cpx<T> t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = mul_i<T, INV>(csub(a1, a3));
+  a0 = cadd(t0, t2); a2 = csub(t0, t2); a1 = cadd(t1, t3); a3 = csub(t1, t3);
+}
+template <typename T, bool INV> __device__ __forceinline__ void dft3(cpx<T>& a0, cpx<T>& a1, cpx<T>& a2) {
+  const T h = T(0.8660254037844386);      // sin(pi / 3)
+  const cpx<T> t = cadd(a1, a2), u = csub(a1, a2);
+  const cpx<T> m = {a0.re - T(0.5) * t.re, a0.im - T(0.5) * t.im};
+  const cpx<T> v = mul_i<T, INV>(cpx<T>{h * u.re, h * u.im});
+  a0 = cadd(a0, t); a1 = cadd(m, v); a2 = csub(m, v);
+}
+template <typename T, int R, bool INV> __device__ __forceinline__ void butterfly(cpx<T> (&a)[R]) {
+  if constexpr (R == 2) {
+    dft2<T, INV>(a[0], a[1]);
+  } else if constexpr (R == 3) {
+    dft3<T, INV>(a[0], a[1], a[2]);
+  } else if constexpr (R == 4) {
+    dft4<T, INV>(a[0], a[1], a[2], a[3]);
+  } else if constexpr (R == 6) {            // evens and odds by DFT3, joined with exp(sign 2 pi i s / 6)
+    cpx<T> e0 = a[0], e1 = a[2], e2 = a[4], o0 = a[1], o1 = a[3], o2 = a[5];
+    dft3<T, INV>(e0, e1, e2); dft3<T, INV>(o0, o1, o2);
+    const T h = T(0.8660254037844386);
+    const cpx<T> w1 = {T(0.5), INV ? h : -h}, w2 = {T(-0.5), INV ? h : -h};
+    const cpx<T> p1 = cmul(o1, w1), p2 = cmul(o2, w2);
+    a[0] = cadd(e0, o0); a[3] = csub(e0, o0);
+    a[1] = cadd(e1, p1); a[4] = csub(e1, p1);
+    a[2] = cadd(e2, p2); a[5] = csub(e2, p2);
+  } else {                                  // R == 8: evens and odds by DFT4, joined with exp(sign 2 pi i s / 8)
+    cpx<T> e0 = a[0], e1 = a[2], e2 = a[4], e3 = a[6], o0 = a[1], o1 = a[3], o2 = a[5], o3 = a[7];
+    dft4<T, INV>(e0, e1, e2, e3); dft4<T, INV>(o0, o1, o2, o3);
+    const T c = T(0.7071067811865476);       // cos(pi / 4)
+    const cpx<T> p1 = INV ? cpx<T>{c * (o1.re - o1.im), c * (o1.im + o1.re)}
+                          : cpx<T>{c * (o1.re + o1.im), c * (o1.im - o1.re)};
+    const cpx<T> p2 = mul_i<T, INV>(o2);
+    const cpx<T> p3 = INV ? cpx<T>{c * (-o3.re - o3.im), c * (o3.re - o3.im)}
+                          : cpx<T>{c * (-o3.re + o3.im), c * (-o3.re - o3.im)};
+    a[0] = cadd(e0, o0); a[4] = csub(e0, o0);
+    a[1] = cadd(e1, p1); a[5] = csub(e1, p1);
+    a[2] = cadd(e2, p2); a[6] = csub(e2, p2);
+    a[3] = cadd(e3, p3); a[7] = csub(e3, p3);
+  }
+}
+
+// One Stockham pass of radix R over ntr transforms of length N, from src to dst in shared memory (transform t at
+// + t * ld in both), after Ns points of each sub-transform are done: butterfly j (of N / R) reads src[j + r N / R]
+// times w^(r (j mod Ns) N / (Ns R)) and writes its R outputs to dst[(j - j mod Ns) R + j mod Ns + s Ns]. A thread
+// holds one butterfly's R values at a time; one barrier per pass.
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void fft_pass(const cpx<T>* src, cpx<T>* dst, const cpx<T>* tw, int N, int ld, int ntr,
+                                         int Ns) {
+  const int nbt = N / R, total = nbt * ntr, stride = N / (Ns * R);
+  for (int b = threadIdx.x; b < total; b += kFT) {
+    const int t = b / nbt, j = b - t * nbt, k = j % Ns;
+    const cpx<T>* s = src + t * ld + j;
+    cpx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = s[r * nbt];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        cpx<T> w = tw[r * k * stride];
+        if (INV) w.im = -w.im;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    butterfly<T, R, INV>(v);
+    cpx<T>* d = dst + t * ld + (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) d[r * Ns] = v[r];
+  }
+  __syncthreads();
+}
+
+// All passes of the transform, alternating between the two buffers; returns the one holding the result.
+template <typename T, bool INV>
+__device__ cpx<T>* smem_fft(cpx<T>* a, cpx<T>* b, const cpx<T>* tw, int N, int ld, int ntr, const int8_t* rad,
+                            int nrad) {
+  int Ns = 1;
+  for (int p = 0; p < nrad; p++) {
+    const int R = rad[p];
+    switch (R) {
+      case 8: fft_pass<T, 8, INV>(a, b, tw, N, ld, ntr, Ns); break;
+      case 6: fft_pass<T, 6, INV>(a, b, tw, N, ld, ntr, Ns); break;
+      case 4: fft_pass<T, 4, INV>(a, b, tw, N, ld, ntr, Ns); break;
+      case 3: fft_pass<T, 3, INV>(a, b, tw, N, ld, ntr, Ns); break;
+      default: fft_pass<T, 2, INV>(a, b, tw, N, ld, ntr, Ns); break;
+    }
+    Ns *= R;
+    cpx<T>* t = a; a = b; b = t;
+  }
+  return a;
+}
+
+// ------------------------------------------------------------------------------------------------- stages
+// Each stage is a device body over one problem's descriptor and one CTA index, behind two entry points: grouped
+// (grid (max CTAs of a problem, 1, n); problem gi = subset[blockIdx.z] or blockIdx.z; problems with live[gi] == 0 and
+// CTAs past the problem's own count return at once, uniformly per CTA) and single-plan (the descriptor by value).
+// Dynamic shared memory: (2 x transforms x (length + 1) + length) complex values.
+template <typename T>
+__device__ __forceinline__ void rows_fwd_body(const FftDesc& D, int cta, unsigned char* smem) {
+  const int tid = threadIdx.x;
+  const int N = D.M2, ld = N + 1, rows_tot = D.nb * D.M1;
+  const int r0 = cta * D.rows, nr = min(D.rows, rows_tot - r0);
+  cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem);
+  cpx<T>* alt = buf + D.rows * ld;
+  cpx<T>* tw = alt + D.rows * ld;
+  for (int i = tid; i < N; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
+  const int64_t base = (int64_t)r0 * N;
+  if (D.flags & 1) {
+    const T* X = reinterpret_cast<const T*>(D.X) + base;
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + (i - t * N)] = cpx<T>{X[i], T(0)}; }
+  } else {
+    const cpx<T>* X = reinterpret_cast<const cpx<T>*>(D.X) + base;
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + (i - t * N)] = X[i]; }
+  }
+  __syncthreads();
+  buf = smem_fft<T, false>(buf, alt, tw, N, ld, nr, D.rad2, D.nrad2);
+  cpx<T>* Z = reinterpret_cast<cpx<T>*>(D.Z);
+  for (int i = tid; i < nr * D.H2; i += kFT) {
+    const int q2 = i / nr, t = i - q2 * nr;
+    const int row = r0 + t, b = row / D.M1, r = row - b * D.M1;
+    Z[((int64_t)b * D.H2 + q2) * D.M1 + r] = buf[t * ld + __ldg(D.k2 + q2)];
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void cols_body(const FftDesc& D, int cta, unsigned char* smem) {
+  const int tid = threadIdx.x;
+  const int N = D.M1, ld = N + 1, cols_tot = D.nb * D.H2;
+  const int c0 = cta * D.cols, nc = min(D.cols, cols_tot - c0);
+  cpx<T>* base = reinterpret_cast<cpx<T>*>(smem);
+  cpx<T>* buf = base;
+  cpx<T>* alt = base + D.cols * ld;
+  cpx<T>* tw = alt + D.cols * ld;
+  for (int i = tid; i < N; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw1)[i];
+  cpx<T>* Z = reinterpret_cast<cpx<T>*>(D.Z) + (int64_t)c0 * N;
+  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; buf[t * ld + (i - t * N)] = Z[i]; }
+  __syncthreads();
+  buf = smem_fft<T, false>(buf, alt, tw, N, ld, nc, D.rad1, D.nrad1);
+  alt = buf == base ? base + D.cols * ld : base;
+  const T* W = reinterpret_cast<const T*>(D.W);
+  for (int i = tid; i < nc * N; i += kFT) {
+    const int t = i / N, k1 = i - t * N;
+    const int q1 = __ldg(D.map1 + k1), q2 = (c0 + t) % D.H2;
+    const T w = q1 >= 0 ? W[(int64_t)q1 * D.H2 + q2] : T(0);
+    cpx<T>& v = buf[t * ld + k1];
+    v.re *= w; v.im *= w;
+  }
+  __syncthreads();
+  buf = smem_fft<T, true>(buf, alt, tw, N, ld, nc, D.rad1, D.nrad1);
+  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; Z[i] = buf[t * ld + (i - t * N)]; }
+}
+
+template <typename T>
+__device__ __forceinline__ void rows_inv_body(const FftDesc& D, int cta, unsigned char* smem) {
+  const int tid = threadIdx.x;
+  const int N = D.M2, ld = N + 1, rows_tot = D.nb * D.M1;
+  const int r0 = cta * D.rows, nr = min(D.rows, rows_tot - r0);
+  cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem);
+  cpx<T>* alt = buf + D.rows * ld;
+  cpx<T>* tw = alt + D.rows * ld;
+  for (int i = tid; i < N; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
+  for (int i = tid; i < nr * ld; i += kFT) buf[i] = cpx<T>{T(0), T(0)};
+  __syncthreads();
+  const cpx<T>* Z = reinterpret_cast<const cpx<T>*>(D.Z);
+  for (int i = tid; i < nr * D.H2; i += kFT) {
+    const int q2 = i / nr, t = i - q2 * nr;
+    const int row = r0 + t, b = row / D.M1, r = row - b * D.M1;
+    buf[t * ld + __ldg(D.k2 + q2)] = Z[((int64_t)b * D.H2 + q2) * D.M1 + r];
+  }
+  __syncthreads();
+  buf = smem_fft<T, true>(buf, alt, tw, N, ld, nr, D.rad2, D.nrad2);
+  const int64_t base = (int64_t)r0 * N;
+  if (D.flags & 4) {
+    T* Y = reinterpret_cast<T*>(D.Y) + base;
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; Y[i] = buf[t * ld + (i - t * N)].re; }
+  } else {
+    cpx<T>* Y = reinterpret_cast<cpx<T>*>(D.Y) + base;
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; Y[i] = buf[t * ld + (i - t * N)]; }
+  }
+}
+
+#define FFT_STAGE(NAME, BODY, NCTAS)                                                                              \
+  template <typename T>                                                                                          \
+  __global__ void __launch_bounds__(kFT) NAME##_grp(const FftDesc* __restrict__ descs,                           \
+                                                    const int* __restrict__ subset, const int* __restrict__ live) { \
+    extern __shared__ __align__(16) unsigned char fft_smem[];                                                    \
+    const int gi = subset ? subset[blockIdx.z] : (int)blockIdx.z;                                                \
+    if (live && !live[gi]) return;                                                                               \
+    const FftDesc D = descs[gi];                                                                                 \
+    if ((int)blockIdx.x >= D.NCTAS) return;                                                                      \
+    BODY<T>(D, blockIdx.x, fft_smem);                                                                            \
+  }                                                                                                              \
+  template <typename T>                                                                                          \
+  __global__ void __launch_bounds__(kFT) NAME##_one(const FftDesc D) {                                           \
+    extern __shared__ __align__(16) unsigned char fft_smem[];                                                    \
+    BODY<T>(D, blockIdx.x, fft_smem);                                                                            \
+  }
+
+FFT_STAGE(k_fft_rows_fwd, rows_fwd_body, ctasA)
+FFT_STAGE(k_fft_cols, cols_body, ctasB)
+FFT_STAGE(k_fft_rows_inv, rows_inv_body, ctasA)
+
+// ------------------------------------------------------------------------------------------------- host side
+// radices of an N = 2^a 3^b point FFT: 8s, then a 4 or 2, then 3s, a 2 and a 3 merged into a 6 (fewest passes); 0
+// when N has another prime factor or needs more than kMaxRad passes
+static int radix_plan(int N, int8_t* rad) {
+  int a = 0, b = 0, m = N;
+  while (m % 2 == 0) { m /= 2; a++; }
+  while (m % 3 == 0) { m /= 3; b++; }
+  if (m != 1 || N < 2) return 0;
+  std::vector<int> r;
+  for (; a >= 3; a -= 3) r.push_back(8);
+  int two = 0;
+  if (a == 2) r.push_back(4);
+  else if (a == 1) two = 1;
+  for (int i = 0; i < b; i++) {
+    if (two) { r.push_back(6); two = 0; }
+    else r.push_back(3);
+  }
+  if (two) r.push_back(2);
+  if ((int)r.size() > kMaxRad) return 0;
+  for (size_t i = 0; i < r.size(); i++) rad[i] = (int8_t)r[i];
+  return (int)r.size();
+}
+
+static int transforms_per_cta(int N) { return std::max(1, kFE / N); }
+
+// two buffers of ntr padded transforms, then the twiddle table
+static size_t stage_smem(int ntr, int N, size_t esz) { return (2 * (size_t)ntr * (N + 1) + N) * esz; }
+
+int fft_plan_init(blml_plan_s* p, const double* freqs) {
+  p->fft = nullptr;
+  if (p->d != 2 || p->engine != BLML_ENGINE_SIMT) return BLML_OK;
+  const int M1 = (int)p->shape[0], M2 = (int)p->shape[1], H1 = p->nfreq[0], H2 = p->nfreq[1];
+  if (M1 > kMaxSide || M2 > kMaxSide || H1 > M1 || H2 > M2) return BLML_OK;
+  FftPlan fp{};
+  fp.M1 = M1; fp.M2 = M2; fp.H1 = H1; fp.H2 = H2;
+  fp.nrad1 = radix_plan(M1, fp.rad1); fp.nrad2 = radix_plan(M2, fp.rad2);
+  if (!fp.nrad1 || !fp.nrad2) return BLML_OK;
+  // integer harmonics, distinct modulo the side: then S is exactly the DFT mask
+  std::vector<int> k2(H2), map1(M1, -1), seen2(M2, 0);
+  for (int q = 0; q < H1 + H2; q++) {
+    const int M = q < H1 ? M1 : M2;
+    const double x = freqs[q] * M, r = std::nearbyint(x);
+    if (std::fabs(x - r) > 1e-9 * std::max(1.0, std::fabs(r))) return BLML_OK;
+    const int k = (int)(((long long)r % M + M) % M);
+    if (q < H1) {
+      if (map1[k] >= 0) return BLML_OK;
+      map1[k] = q;
+    } else {
+      if (seen2[k]) return BLML_OK;
+      seen2[k] = 1; k2[q - H1] = k;
+    }
+  }
+  const bool f64 = p->dtype == BLML_F64;
+  const size_t esz = f64 ? 16 : 8;
+  auto table = [&](int M, void** dst) -> int {
+    std::vector<double> t(2 * (size_t)M);
+    for (int i = 0; i < M; i++) {
+      const double ph = 2.0 * M_PI * (double)i / (double)M;
+      t[2 * i] = std::cos(ph); t[2 * i + 1] = -std::sin(ph);
+    }
+    if (cudaMalloc(dst, M * esz) != cudaSuccess) { set_error("FFT plan: device allocation"); return BLML_ERR_CUDA; }
+    if (f64) return cuda_status(cudaMemcpy(*dst, t.data(), M * esz, cudaMemcpyHostToDevice), "FFT plan twiddles");
+    std::vector<float> t32(t.begin(), t.end());
+    return cuda_status(cudaMemcpy(*dst, t32.data(), M * esz, cudaMemcpyHostToDevice), "FFT plan twiddles");
+  };
+  int rc = table(M1, &fp.tw1);
+  if (!rc) rc = table(M2, &fp.tw2);
+  if (!rc && cudaMalloc(&fp.k2, H2 * sizeof(int)) != cudaSuccess) { set_error("FFT plan: device allocation"); rc = BLML_ERR_CUDA; }
+  if (!rc) rc = cuda_status(cudaMemcpy(fp.k2, k2.data(), H2 * sizeof(int), cudaMemcpyHostToDevice), "FFT plan");
+  if (!rc && cudaMalloc(&fp.map1, M1 * sizeof(int)) != cudaSuccess) { set_error("FFT plan: device allocation"); rc = BLML_ERR_CUDA; }
+  if (!rc) rc = cuda_status(cudaMemcpy(fp.map1, map1.data(), M1 * sizeof(int), cudaMemcpyHostToDevice), "FFT plan");
+  if (rc) {
+    cudaFree(fp.tw1); cudaFree(fp.tw2); cudaFree(fp.k2); cudaFree(fp.map1);
+    return rc;
+  }
+  p->fft = new FftPlan(fp);
+  return fft_smem_once();
+}
+
+void fft_plan_free(blml_plan_s* p) {
+  FftPlan* fp = reinterpret_cast<FftPlan*>(p->fft);
+  if (!fp) return;
+  cudaFree(fp->tw1); cudaFree(fp->tw2); cudaFree(fp->k2); cudaFree(fp->map1);
+  delete fp;
+  p->fft = nullptr;
+}
+
+static FftDesc make_desc(const blml_plan_s* p, const void* x, void* y, void* z, int nb, int xc) {
+  const FftPlan* fp = reinterpret_cast<const FftPlan*>(p->fft);
+  FftDesc D{};
+  D.X = x; D.Y = y; D.Z = z; D.W = p->W;
+  D.tw1 = fp->tw1; D.tw2 = fp->tw2; D.k2 = fp->k2; D.map1 = fp->map1;
+  D.M1 = fp->M1; D.M2 = fp->M2; D.H1 = fp->H1; D.H2 = fp->H2; D.nb = nb;
+  D.flags = xc ? 0 : (1 | 4);
+  D.rows = transforms_per_cta(fp->M2); D.cols = transforms_per_cta(fp->M1);
+  D.ctasA = (nb * fp->M1 + D.rows - 1) / D.rows;
+  D.ctasB = (nb * fp->H2 + D.cols - 1) / D.cols;
+  D.nrad1 = fp->nrad1; D.nrad2 = fp->nrad2;
+  std::copy(fp->rad1, fp->rad1 + kMaxRad, D.rad1); std::copy(fp->rad2, fp->rad2 + kMaxRad, D.rad2);
+  return D;
+}
+
+struct FftGroup {
+  FftDesc* dev;                  // G descriptors
+  int maxA, maxB;                // largest CTA count of a problem in stages A / C and B
+  size_t smemA, smemB;           // largest dynamic shared memory of a problem's stage
+};
+
+// the largest dynamic shared memory any stage asks for: two buffers of one kMaxSide-point transform (the longest
+// transform that has a CTA to itself) and its twiddles, in float64; shorter transforms fill kFE values per buffer
+constexpr size_t kMaxSmem = (size_t)(3 * kMaxSide + 2) * 16;
+
+// the six kernels' dynamic shared-memory limit, set once per device (outside any stream capture: at plan creation)
+template <typename T>
+static int set_fft_smem() {
+  const int v = (int)kMaxSmem;
+  int e = BLML_OK;
+  auto set = [&](const void* f) {
+    if (!e) e = cuda_status(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, v), "FFT route");
+  };
+  set((const void*)k_fft_rows_fwd_grp<T>); set((const void*)k_fft_cols_grp<T>); set((const void*)k_fft_rows_inv_grp<T>);
+  set((const void*)k_fft_rows_fwd_one<T>); set((const void*)k_fft_cols_one<T>); set((const void*)k_fft_rows_inv_one<T>);
+  return e;
+}
+
+static int fft_smem_once() {
+  static bool done[64] = {};
+  int dev = 0;
+  int e = cuda_status(cudaGetDevice(&dev), "FFT route");
+  if (e || (dev < 64 && done[dev])) return e;
+  e = set_fft_smem<double>();
+  if (!e) e = set_fft_smem<float>();
+  if (!e && dev < 64) done[dev] = true;
+  return e;
+}
+
+template <typename T>
+static int launch_fft_grp(const FftDesc* dev, dim3 gA, dim3 gB, size_t smA, size_t smB, const int* subset,
+                          const int* live, cudaStream_t st) {
+  k_fft_rows_fwd_grp<T><<<gA, kFT, smA, st>>>(dev, subset, live);
+  BLML_CHECK_LAUNCH("FFT route: rows");
+  k_fft_cols_grp<T><<<gB, kFT, smB, st>>>(dev, subset, live);
+  BLML_CHECK_LAUNCH("FFT route: columns");
+  k_fft_rows_inv_grp<T><<<gA, kFT, smA, st>>>(dev, subset, live);
+  BLML_CHECK_LAUNCH("FFT route: inverse rows");
+  return BLML_OK;
+}
+
+template <typename T>
+static int launch_fft_one(const FftDesc& D, size_t smA, size_t smB, cudaStream_t st) {
+  k_fft_rows_fwd_one<T><<<D.ctasA, kFT, smA, st>>>(D);
+  BLML_CHECK_LAUNCH("FFT route: rows");
+  k_fft_cols_one<T><<<D.ctasB, kFT, smB, st>>>(D);
+  BLML_CHECK_LAUNCH("FFT route: columns");
+  k_fft_rows_inv_one<T><<<D.ctasA, kFT, smA, st>>>(D);
+  BLML_CHECK_LAUNCH("FFT route: inverse rows");
+  return BLML_OK;
+}
+
+int fft_group_init(void** out, int G, const blml_plan* plans, const int* nbatch, int xc, const void* const* x,
+                   void* const* y, void* const* z) {
+  *out = nullptr;
+  for (int g = 0; g < G; g++)
+    if (!plans[g]->fft) return BLML_OK;
+  const size_t esz = plans[0]->dtype == BLML_F64 ? 16 : 8;
+  std::vector<FftDesc> h(G);
+  FftGroup fg{};
+  for (int g = 0; g < G; g++) {
+    h[g] = make_desc(plans[g], x[g], y[g], z[g], nbatch[g], xc);
+    fg.maxA = std::max(fg.maxA, h[g].ctasA); fg.maxB = std::max(fg.maxB, h[g].ctasB);
+    fg.smemA = std::max(fg.smemA, stage_smem(h[g].rows, h[g].M2, esz));
+    fg.smemB = std::max(fg.smemB, stage_smem(h[g].cols, h[g].M1, esz));
+  }
+  int e = fft_smem_once();
+  if (e) return e;
+  if (cudaMalloc(&fg.dev, G * sizeof(FftDesc)) != cudaSuccess) { set_error("FFT route: allocation"); return BLML_ERR_CUDA; }
+  e = cuda_status(cudaMemcpy(fg.dev, h.data(), G * sizeof(FftDesc), cudaMemcpyHostToDevice), "FFT route");
+  if (e) { cudaFree(fg.dev); return e; }
+  *out = new FftGroup(fg);
+  return BLML_OK;
+}
+
+void fft_group_free(void* fgv) {
+  FftGroup* fg = reinterpret_cast<FftGroup*>(fgv);
+  if (!fg) return;
+  cudaFree(fg->dev);
+  delete fg;
+}
+
+int fft_group_launch(void* fgv, int dtype, const int* subset, int n, const int* live, cudaStream_t st) {
+  const FftGroup* fg = reinterpret_cast<const FftGroup*>(fgv);
+  const dim3 gA((unsigned)fg->maxA, 1, (unsigned)n), gB((unsigned)fg->maxB, 1, (unsigned)n);
+  return dtype == BLML_F64 ? launch_fft_grp<double>(fg->dev, gA, gB, fg->smemA, fg->smemB, subset, live, st)
+                           : launch_fft_grp<float>(fg->dev, gA, gB, fg->smemA, fg->smemB, subset, live, st);
+}
+
+// one plan over nb lattices: Z (nb, H2, M1) in the caller's workspace, the descriptor passed by value
+int64_t fft_workspace(const blml_plan_s* p, int nb) {
+  const FftPlan* fp = reinterpret_cast<const FftPlan*>(p->fft);
+  const size_t esz = p->dtype == BLML_F64 ? 16 : 8;
+  return (int64_t)((size_t)nb * fp->H2 * fp->M1 * esz);
+}
+
+int fft_matvec(blml_plan_s* p, const void* x, void* y, int nb, int xc, void* ws, cudaStream_t st) {
+  const size_t esz = p->dtype == BLML_F64 ? 16 : 8;
+  const FftDesc D = make_desc(p, x, y, ws, nb, xc);
+  const size_t smA = stage_smem(D.rows, D.M2, esz), smB = stage_smem(D.cols, D.M1, esz);
+  return p->dtype == BLML_F64 ? launch_fft_one<double>(D, smA, smB, st) : launch_fft_one<float>(D, smA, smB, st);
+}
+
+}  // namespace blml

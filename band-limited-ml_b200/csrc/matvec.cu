@@ -374,6 +374,8 @@ struct blml_group_s {
   std::vector<dim3> grids, grids_big;   // 32 x 32 and 64 x 64 tile grids per stage
   std::vector<double> tiles_big;        // 64 x 64 tiles of a stage over all problems
   void* ws;                             // the group's own intermediate buffers
+  void* fft;                            // the FFT route's descriptors (every plan a DFT mask), or null
+  int route;                            // BLML_ROUTE_CONTRACT or BLML_ROUTE_FFT
 };
 
 using namespace blml;
@@ -449,6 +451,8 @@ int blml_plan_create(int d, const int64_t* shape, const int32_t* nfreq, const do
     }
   }
   if (rc == BLML_OK && engine == BLML_ENGINE_TC) rc = tc_plan_init(p, fwd_all, inv_all);
+  if (rc == BLML_OK && engine == BLML_ENGINE_SIMT) rc = fft_plan_init(p, freqs);
+  p->route = p->fft ? BLML_ROUTE_FFT : BLML_ROUTE_CONTRACT;
   if (rc != BLML_OK) {
     if (rc == BLML_ERR_CUDA && blml_last_error()[0] == 0) set_error("blml_plan_create: device allocation failed");
     blml_plan_destroy(p);
@@ -463,6 +467,7 @@ int blml_plan_destroy(blml_plan p) {
   for (int a = 0; a < p->d; a++) { cudaFree(p->tf[a]); cudaFree(p->ti[a]); }
   cudaFree(p->W);
   if (p->tc) tc_plan_free(p);
+  if (p->fft) fft_plan_free(p);
   delete p;
   return BLML_OK;
 }
@@ -490,6 +495,7 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
   for (int g = 0; g < G; g++) wso[g + 1] = wso[g] + 2 * (size_t)nbatch[g] * plans[g]->max_elems * esz;
   blml_group_s* grp = new blml_group_s();
   grp->G = G; grp->d_max = d; grp->dtype = dtype; grp->nstages = 2 * d; grp->ws = nullptr;
+  grp->fft = nullptr; grp->route = BLML_ROUTE_CONTRACT;
   if (cudaMalloc(&grp->ws, std::max<size_t>(wso[G], 16)) != cudaSuccess) {
     delete grp; set_error("blml_group_create: workspace allocation"); return BLML_ERR_CUDA;
   }
@@ -527,6 +533,16 @@ int blml_group_create(int G, const blml_plan* plans, const int* nbatch, int x_co
     grp->grids.push_back(dim3((unsigned)((maxr[s] + GR - 1) / GR), (unsigned)((maxn[s] + GN - 1) / GN), (unsigned)G));
     grp->grids_big.push_back(dim3((unsigned)((maxr[s] + BR - 1) / BR), (unsigned)((maxn[s] + BN - 1) / BN), (unsigned)G));
   }
+  if (!e) {      // the FFT route: problem g keeps its spectrum in the first of its two intermediate buffers
+    std::vector<const void*> xs(G); std::vector<void*> ys(G), zs(G);
+    for (int g = 0; g < G; g++) {
+      xs[g] = reinterpret_cast<const char*>(x_base) + x_off[g] * xsz;
+      ys[g] = reinterpret_cast<char*>(y_base) + y_off[g] * ysz;
+      zs[g] = reinterpret_cast<char*>(grp->ws) + wso[g];
+    }
+    e = fft_group_init(&grp->fft, G, plans, nbatch, x_complex, xs.data(), ys.data(), zs.data());
+    if (!e && grp->fft) grp->route = BLML_ROUTE_FFT;
+  }
   if (e) { blml_group_destroy(grp); return e; }
   *out = grp;
   return BLML_OK;
@@ -541,6 +557,7 @@ int blml_group_matvec_masked(blml_group grp, const int* subset, int n, const int
   if (n < 0 || n > grp->G) { set_error("blml_group_matvec_masked: 0 <= n <= G"); return BLML_ERR_ARG; }
   if (n == 0) return BLML_OK;
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (grp->route == BLML_ROUTE_FFT) return fft_group_launch(grp->fft, grp->dtype, subset, n, live, st);
   for (int s = 0; s < grp->nstages; s++) {
     // 64 x 64 tiles when the launch has enough of them to fill the GPU twice over (the problems of a subset are
     // taken as average ones), else 32 x 32
@@ -563,6 +580,7 @@ int blml_group_destroy(blml_group grp) {
   if (!grp) return BLML_OK;
   for (auto p : grp->dev) cudaFree(p);
   cudaFree(grp->ws);
+  fft_group_free(grp->fft);
   delete grp;
   return BLML_OK;
 }
@@ -578,6 +596,7 @@ int blml_plan_status(blml_plan p) {
 int64_t blml_matvec_workspace(blml_plan p, int nb) {
   if (!p || nb < 1) return -1;
   if (p->engine == BLML_ENGINE_TC) return tc_workspace(p, nb);
+  if (p->route == BLML_ROUTE_FFT) return fft_workspace(p, nb);
   return 2 * (int64_t)nb * p->max_elems * (p->dtype == BLML_F64 ? 16 : 8);
 }
 
@@ -590,8 +609,36 @@ int blml_matvec(blml_plan p, const void* x, void* y, int nb, int xc, void* ws, i
   }
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (p->engine == BLML_ENGINE_TC) return tc_matvec(p, x, y, nb, xc, ws, wsb, st);
+  if (p->route == BLML_ROUTE_FFT) return fft_matvec(p, x, y, nb, xc, ws, st);
   return p->dtype == BLML_F64 ? simt_matvec<double>(p, x, y, nb, xc, ws, st)
                               : simt_matvec<float>(p, x, y, nb, xc, ws, st);
 }
+
+int blml_plan_set_route(blml_plan p, int route) {
+  if (!p) { set_error("blml_plan_set_route: null plan"); return BLML_ERR_ARG; }
+  if (route == BLML_ROUTE_AUTO) route = p->fft ? BLML_ROUTE_FFT : BLML_ROUTE_CONTRACT;
+  if (route == BLML_ROUTE_FFT && !p->fft) {
+    set_error("blml_plan_set_route: this kernel has no FFT route (not a 2-D DFT mask on sides 2^a 3^b)");
+    return BLML_ERR_UNSUPPORTED;
+  }
+  if (route != BLML_ROUTE_FFT && route != BLML_ROUTE_CONTRACT) { set_error("blml_plan_set_route: route"); return BLML_ERR_ARG; }
+  p->route = route;
+  return BLML_OK;
+}
+
+int blml_plan_route(blml_plan p) { return p ? p->route : BLML_ERR_ARG; }
+
+int blml_group_set_route(blml_group grp, int route) {
+  if (!grp) { set_error("blml_group_set_route: null group"); return BLML_ERR_ARG; }
+  if (route == BLML_ROUTE_AUTO) route = grp->fft ? BLML_ROUTE_FFT : BLML_ROUTE_CONTRACT;
+  if (route == BLML_ROUTE_FFT && !grp->fft) {
+    set_error("blml_group_set_route: a plan of this group has no FFT route"); return BLML_ERR_UNSUPPORTED;
+  }
+  if (route != BLML_ROUTE_FFT && route != BLML_ROUTE_CONTRACT) { set_error("blml_group_set_route: route"); return BLML_ERR_ARG; }
+  grp->route = route;
+  return BLML_OK;
+}
+
+int blml_group_route(blml_group grp) { return grp ? grp->route : BLML_ERR_ARG; }
 
 }

@@ -150,9 +150,10 @@ def replica_value(certified, seconds, ws):
     return (sum_over_ranks(certified, ws) / tmax if tmax > 0 else 0.0), tmax
 
 
-def grouped_matvec_roofline(batch, reps=20):
-    """The dominant kernel chain of the sweep: one grouped mat-vec (4 grouped stage launches) over all 64 fits,
-    timed with CUDA events on the fits' stream; algorithmic bytes = read E + write U of every lattice (complex128)."""
+def grouped_matvec_roofline(batch, reps=20, route=0):
+    """The dominant kernel chain of the sweep: one grouped mat-vec over all 64 fits (route 0: the group's own choice,
+    the FFT route's 3 launches on these DFT-mask kernels; 1: the 4 restricted-transform stages), timed with CUDA
+    events on the fits' stream; algorithmic bytes = read E + write U of every lattice (complex128)."""
     import torch
     from blml_b200.sweep import _Group
     st = torch.cuda.current_stream(batch.device)
@@ -160,6 +161,8 @@ def grouped_matvec_roofline(batch, reps=20):
     y = torch.empty_like(x)
     off = batch.boff[:-1]
     grp = _Group(batch.p64, x, off, y, off, True)
+    if route:
+        grp.route = route
     for _ in range(3):
         grp(st.cuda_stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -494,9 +497,11 @@ def main():
     if args.matvec:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
         b._prepare(train, modes)
-        t_mv, mv_bytes, mv_flops = grouped_matvec_roofline(b)
-        print(json.dumps({'us_per_chain': t_mv * 1e6, 'bytes': mv_bytes, 'flop': mv_flops,
-                          'GB/s': mv_bytes / t_mv / 1e9, 'TFLOP/s': mv_flops / t_mv / 1e12}))
+        out = {}
+        for name, route in (('auto', 0), ('contract', _lib.ROUTE_CONTRACT), ('fft', _lib.ROUTE_FFT)):
+            t_mv, mv_bytes, mv_flops = grouped_matvec_roofline(b, route=route)
+            out[name] = {'us_per_chain': t_mv * 1e6, 'bytes': mv_bytes, 'GB/s': mv_bytes / t_mv / 1e9}
+        print(json.dumps(out))
         return
     if args.one_fit:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)

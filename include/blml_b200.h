@@ -24,6 +24,9 @@ enum { BLML_F64 = 0, BLML_F32 = 1 };
 /* mat-vec engines: SIMT contraction (float64 or float32), or tcgen05 tensor cores with split-TF32 operands
    (float32 storage, three products per term, FP32 accumulation in TMEM) */
 enum { BLML_ENGINE_SIMT = 0, BLML_ENGINE_TC = 1 };
+/* routes of the SIMT engine: restricted-transform contractions, or FFTs of the lattice rows and columns when the
+   kernel is a DFT mask (2-D, every axis one period, integer harmonics; sides 2^a 3^b up to 4,096) */
+enum { BLML_ROUTE_AUTO = 0, BLML_ROUTE_CONTRACT = 1, BLML_ROUTE_FFT = 2 };
 
 typedef struct blml_plan_s* blml_plan;
 
@@ -49,6 +52,12 @@ int blml_matvec(blml_plan plan, const void* x, void* y, int nbatch, int x_comple
 /* synchronises the device and reports whether a tensor-core mat-vec gave up on a bounded wait since the plan was
    made (BLML_ERR_TIMEOUT; the results of that call are invalid) or BLML_OK */
 int blml_plan_status(blml_plan plan);
+/* choose the route of blml_matvec (BLML_ROUTE_AUTO: the FFT route wherever the plan has one); BLML_ERR_UNSUPPORTED
+   when the FFT route is asked of a kernel without one. Both routes apply the same operator; the FFT route is the
+   reference's own FFT convolution (blml_binned.py:156-168) restricted to the band's harmonics. */
+int blml_plan_set_route(blml_plan plan, int route);
+/* the route blml_matvec takes (BLML_ROUTE_CONTRACT or BLML_ROUTE_FFT) */
+int blml_plan_route(blml_plan plan);
 
 /* ---- grouped mat-vecs: many plans (fits of uneven lattice size and band) applied in one launch per stage ----
  * Problem g: y_base[y_off[g] ...] = S_g x_base[x_off[g] ...] over nbatch[g] lattices of plan g (SIMT engine); every
@@ -64,6 +73,10 @@ int blml_group_matvec(blml_group group, void* stream);
    graph follows problems that stop between its replays */
 int blml_group_matvec_masked(blml_group group, const int* subset, int n, const int* live, void* stream);
 int blml_group_destroy(blml_group group);
+/* the route of every stage launch of a group: the FFT route (three launches: row FFTs, column FFT x weight x inverse
+   FFT, inverse row FFTs) when every plan has one and BLML_ROUTE_AUTO, else the 2 d restricted-transform stages */
+int blml_group_set_route(blml_group group, int route);
+int blml_group_route(blml_group group);
 
 /* ---- coordinate (Jacobi) update of every bin (BLMLBinned._update / _secular / _cd_root,
  *      blml_binned.py:184-206, 1549-1573; cd_root blml_trivial.py:84-89) ----
