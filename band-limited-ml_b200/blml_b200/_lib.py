@@ -72,6 +72,8 @@ _SIGS = {
     'blml_seg_val_score': (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     'blml_seg_phases': (_I, [_I, _I, _P, _D, _P, _P, _P]),
     'blml_seg_real_to_complex': (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    'blml_seg_cert_weights': (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    'blml_seg_append_mode': (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     'blml_group_matvec_masked': (_I, [_P, _P, _I, _P, _P]),
     'blml_seg_dots2': (_I, [_I, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_nn_gemm_bf16': (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _P]),

@@ -68,3 +68,106 @@ def lanczos_max(plan, dh, red, stream, tol=1e-6, seed=0, max_basis=96, max_resta
         nrm = float(np.sqrt(dots([(w, w)])[0]))
         lin([(1.0 / nrm, w)], V[0])
     return theta
+
+
+def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, vectors=False):
+    """The certificate of every fit of a fitted BLMLBinnedBatch at once: lambda_max(D^1/2 S D^1/2) per fit
+    (blml_binned.py:501-518), D = sum_k |e_k|^2 / w on occupied bins, by float64 Lanczos with full
+    reorthogonalisation, all fits in lockstep: one grouped mat-vec, segmented inner products and linear combinations
+    per step, each fit's tridiagonal problem on the host (every third step), restarts from the Ritz vector until
+    every fit's Ritz residual |beta_j y_j| <= tol |theta|. Returns (theta (F,), dh, v): dh the per-bin scaling and v
+    the top Ritz vectors (float64 per bin over all fits, None unless vectors) -- d = dh v is the direction of a new
+    mode."""
+    from scipy.linalg import eigh_tridiagonal
+    from .sweep import _Group, _Seg
+    F, dev, st, B = batch.F, batch.device, batch.st, batch.Btot
+    code = _lib.F64
+    segs1 = (_Seg * F)(*[_Seg(int(batch.boff[f]), int(batch.boff[f]), int(batch.B[f]), 1, 0) for f in range(F)])
+    segs1_t = torch.frombuffer(bytearray(segs1), dtype=torch.uint8).to(dev)
+    dh = torch.empty(B, dtype=torch.float64, device=dev)
+    call('blml_seg_cert_weights', batch.code, F, batch.segs_t.data_ptr(), batch.E_t.data_ptr(), batch.w.data_ptr(),
+         dh.data_ptr(), st)
+    tmp = torch.empty(B, dtype=torch.float64, device=dev)
+    sv = torch.empty(B, dtype=torch.float64, device=dev)
+    grp = _Group(batch.p64, tmp, batch.boff[:-1], sv, batch.boff[:-1], False)
+
+    def dots(pairs):
+        call('blml_seg_dots', code, F, segs1_t.data_ptr(), 0, len(pairs), ptrs([p[0] for p in pairs]),
+             ptrs([p[1] for p in pairs]), batch.part.data_ptr(), batch.out.data_ptr(), st)
+        return batch._read(len(pairs))
+
+    def lin(out, coef, vecs):
+        cf = torch.as_tensor(np.ascontiguousarray(coef, np.float64)).to(dev, non_blocking=True)
+        call('blml_seg_lincomb', code, F, segs1_t.data_ptr(), 0, out.data_ptr(), len(vecs), cf.data_ptr(),
+             ptrs(vecs), st)
+
+    def op(x, out):                                  # out = dh * S (dh * x), every fit at once
+        call('blml_mul_bins', code, 1, B, 0, x.data_ptr(), dh.data_ptr(), tmp.data_ptr(), st)
+        grp(st)
+        call('blml_mul_bins', code, 1, B, 0, sv.data_ptr(), dh.data_ptr(), out.data_ptr(), st)
+
+    nb = max_basis
+    V = torch.empty((nb + 1, B), dtype=torch.float64, device=dev)
+    V[0].copy_(torch.as_tensor(np.random.default_rng(seed).standard_normal(B)))
+    nrm = dots([(V[0], V[0])])[:, 0]
+    lin(V[0], (1.0 / np.sqrt(np.maximum(nrm, 1e-300)))[:, None], [V[0]])
+    theta = np.zeros(F); done = np.zeros(F, bool)
+    wv = torch.empty(B, dtype=torch.float64, device=dev)
+    vec = torch.zeros(B, dtype=torch.float64, device=dev) if vectors else None
+    R = torch.empty(B, dtype=torch.float64, device=dev)
+    for _ in range(max_restarts + 1):
+        alphas = np.zeros((F, nb)); betas = np.zeros((F, nb))
+        conv = np.zeros(F, bool); yr = [None] * F
+        j_end = nb
+        for j in range(nb):
+            op(V[j], wv)
+            alpha = None
+            for ps in range(2):                                   # full reorthogonalisation, twice
+                for c0 in range(0, j + 1, 47):
+                    idx = list(range(c0, min(j + 1, c0 + 47)))
+                    cs = dots([(V[i], wv) for i in idx])
+                    if ps == 0 and c0 <= j < c0 + 47:
+                        alpha = cs[:, j - c0].copy()
+                    lin(wv, np.concatenate([np.ones((F, 1)), -cs], 1), [wv] + [V[i] for i in idx])
+            alphas[:, j] = alpha
+            beta = np.sqrt(np.maximum(dots([(wv, wv)])[:, 0], 0.0))
+            open_ = ~(done | conv)
+            check = j == nb - 1 or (j >= 5 and j % 3 == 2) or bool(np.any(beta[open_] <= 1e-300))
+            if check:
+                for f in np.where(open_)[0]:
+                    ev, evec = eigh_tridiagonal(alphas[f, :j + 1], betas[f, :j], select='i', select_range=(j, j))
+                    th = float(ev[0]); y = evec[:, 0]
+                    theta[f] = th; yr[f] = y
+                    if abs(beta[f] * y[-1]) <= tol * max(abs(th), 1e-300) or beta[f] <= 1e-14 * max(abs(th), 1e-300):
+                        conv[f] = True
+                if np.all(done | conv):
+                    j_end = j + 1
+                    break
+            betas[:, j] = beta
+            lin(V[j + 1], np.where(beta > 0, 1.0 / np.maximum(beta, 1e-300), 0.0)[:, None], [wv])
+        # the Ritz vector of every fit still open this round: R = sum_i y_i V[i]
+        act = ~done
+        R.zero_()
+        for c0 in range(0, j_end, 47):
+            idx = list(range(c0, min(j_end, c0 + 47)))
+            cf = np.zeros((F, 1 + len(idx))); cf[:, 0] = 1.0
+            for f in np.where(act)[0]:
+                y = yr[f]
+                if y is None:
+                    continue
+                for t, i in enumerate(idx):
+                    if i < len(y):
+                        cf[f, 1 + t] = y[i]
+            lin(R, cf, [R] + [V[i] for i in idx])
+        if vectors:                                               # keep the vectors of the fits converging now
+            keep = (act & conv).astype(float)
+            lin(vec, np.stack([keep, 1.0 - keep], 1), [R, vec])
+        done |= conv
+        if np.all(done):
+            break
+        rn = dots([(R, R)])[:, 0]
+        lin(V[0], np.where(done, 1.0, 1.0 / np.sqrt(np.maximum(rn, 1e-300)))[:, None], [R])
+    if vectors:
+        nv = dots([(vec, vec)])[:, 0]
+        lin(vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
+    return theta, dh, vec

@@ -121,7 +121,7 @@ class BLMLBinnedBatch:
         self.code = _lib.F32 if f32 else _lib.F64
         self.rt = torch.float32 if f32 else torch.float64
         self.ct = torch.complex64 if f32 else torch.complex128
-        shapes, specs, parts = [], [], []
+        shapes, specs, parts, Ks = [], [], [], []
         for counts, modes in zip(counts_list, modes_list):
             if isinstance(counts, torch.Tensor):            # counts already on the device stay there
                 ct = counts.to(dev, torch.float64)
@@ -130,9 +130,9 @@ class BLMLBinnedBatch:
             if ct.ndim != 2:
                 raise ValueError("counts: non-negative finite 2-D arrays")
             sp, dep = parse_modes(modes, 2)
-            if dep is not None or len(sp) != 1:
-                raise ValueError("BLMLBinnedBatch fits one mode per lattice (shared kernel)")
-            shapes.append(tuple(ct.shape)); specs.append(sp[0]); parts.append(ct.reshape(-1))
+            if dep is not None or len(sp) < 1 or any(spec_key(x) != spec_key(sp[0]) for x in sp):
+                raise ValueError("BLMLBinnedBatch fits K modes of one shared kernel per lattice")
+            shapes.append(tuple(ct.shape)); specs.append(sp[0]); Ks.append(len(sp)); parts.append(ct.reshape(-1))
         w64 = torch.cat(parts)
         if bool(((w64 < 0) | ~torch.isfinite(w64)).any()):
             raise ValueError("counts: non-negative finite 2-D arrays")
@@ -140,10 +140,14 @@ class BLMLBinnedBatch:
         if not np.all(self.n > 0):
             raise ValueError("counts: no observations")
         self.shapes, self.specs = shapes, specs
+        self.Kf = np.array(Ks, np.int64)
         self.B = np.array([a * b for a, b in shapes], np.int64)
         boff = np.concatenate([[0], np.cumsum(self.B)])
         self.boff = boff
-        self.segs_all = [_Seg(int(boff[f]), int(boff[f]), int(self.B[f]), 1, 0) for f in range(F)]
+        moff = np.concatenate([[0], np.cumsum(self.Kf * self.B)])     # mode arrays: fit f owns K_f lattices
+        self.moff = moff
+        self.Mtot = int(moff[-1])
+        self.segs_all = [_Seg(int(moff[f]), int(boff[f]), int(self.B[f]), int(self.Kf[f]), 0) for f in range(F)]
         segs = (_Seg * F)(*self.segs_all)
         self.segs_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
         self.Btot = int(boff[-1])
@@ -384,14 +388,16 @@ class BLMLBinnedBatch:
             if len(init) != F:
                 raise ValueError("init: one start per fit")
             parts = []
-            for e0, shape in zip(init, self.shapes):
+            for e0, shape, K in zip(init, self.shapes, self.Kf):
                 t = e0 if isinstance(e0, torch.Tensor) else torch.as_tensor(np.asarray(e0, complex))
-                if tuple(t.shape) != tuple(shape):
-                    raise ValueError("init: each start has its counts' shape")
+                if tuple(t.shape) not in ((int(K),) + tuple(shape),) + ((tuple(shape),) if K == 1 else ()):
+                    raise ValueError("init: each start has its counts' shape, (K,) + shape for K modes")
                 parts.append(t.to(dev, self.ct).reshape(-1))
             E = torch.cat(parts)
             self.start_sweeps_ = np.zeros(F, np.int64)
         else:
+            if np.any(self.Kf != 1):
+                raise ValueError("fits of K > 1 modes start from init (e.g. a lower-rank fit and a new direction)")
             er = self._start_device() if self.control == 'device' else self._start()
             # complex start: the real root with the seeded phases exp(i pn N(0,1)) (blml_binned.py:429-436)
             E = torch.zeros(self.Btot, dtype=self.ct, device=dev)
@@ -421,10 +427,10 @@ class BLMLBinnedBatch:
         F, code, dev, n, m_ = self.F, self.code, self.device, self.n, self.lbfgs_m
         U, g, gn, q, Sq, V, SV = (torch.zeros_like(E) for _ in range(7))
         Sh = [torch.zeros_like(E) for _ in range(m_)]; Yh = [torch.zeros_like(E) for _ in range(m_)]
-        off = self.boff[:-1]
-        g_EU = _Group(self.pfit, E, off, U, off, True)
-        g_q = _Group(self.pfit, q, off, Sq, off, True)
-        g_V = _Group(self.pfit, V, off, SV, off, True)
+        off = self.moff[:-1]
+        g_EU = _Group(self.pfit, E, off, U, off, True, self.Kf)
+        g_q = _Group(self.pfit, q, off, Sq, off, True, self.Kf)
+        g_V = _Group(self.pfit, V, off, SV, off, True, self.Kf)
         segs = self.segs_t.data_ptr()
 
         def Qdot(E_, U_):
@@ -563,7 +569,7 @@ class BLMLBinnedBatch:
         stop = np.array(stop, dtype=object)
         stop[(stop == 'tol') & (res >= self.tol)] = 'max_sweeps'
         V, SV, tmp = (torch.zeros_like(E) for _ in range(3))
-        g_V = _Group(self.pfit, V, self.boff[:-1], SV, self.boff[:-1], True)
+        g_V = _Group(self.pfit, V, self.moff[:-1], SV, self.moff[:-1], True, self.Kf)
 
         def Qdot(E_, U_):
             return self._dots(code, True, [(E_, U_)])[:, 0]
@@ -601,13 +607,95 @@ class BLMLBinnedBatch:
         return self.results_
 
     def field(self, f):
-        """u = S e / n of fit f on the device (complex, the counts' shape): |u|^2 is the density."""
-        a, b = self.boff[f], self.boff[f + 1]
-        return (self.U_t[a:b] / float(self.n[f])).reshape(self.shapes[f])
+        """u = S e / n of fit f on the device (complex, the counts' shape; (K,) + shape for K modes): sum_k |u_k|^2
+        is the density."""
+        a, b = self.moff[f], self.moff[f + 1]
+        shp = self.shapes[f] if self.Kf[f] == 1 else (int(self.Kf[f]),) + self.shapes[f]
+        return (self.U_t[a:b] / float(self.n[f])).reshape(shp)
+
+    def e_hat(self, f):
+        """The coefficients of fit f on the device, (K,) + the counts' shape (blml_binned.py e_hat_)."""
+        a, b = self.moff[f], self.moff[f + 1]
+        return self.E_t[a:b].reshape((int(self.Kf[f]),) + self.shapes[f])
 
     def density(self, f):
         a, b = self.boff[f], self.boff[f + 1]
         return self.dens_t[a:b].cpu().numpy().reshape(self.shapes[f])
+
+    # ---------------------------------------------------------------- certificate and certified fits
+    def certificate(self, tol=1e-6, vectors=False):
+        """lambda_max(D^1/2 S D^1/2) / n of every fit (blml_binned.py:501-518; D = sum_k |e_k|^2 / w on occupied
+        bins), by float64 Lanczos over all fits at once. <= 1 (up to the solver's tolerance) when the fit is the
+        optimum of the convex lift. With vectors: (certificates, dh, v), v the top eigenvectors (per bin)."""
+        from .certificate import lanczos_max_batched
+        theta, dh, v = lanczos_max_batched(self, tol=tol, seed=self.seed, vectors=vectors)
+        cert = theta / self.n
+        return (cert, dh, v) if vectors else cert
+
+    def _grown_starts(self, grow, dh, v, step):
+        """Starts of rank K_f + 1 for the fits `grow` (indices into this batch): the K_f modes, then
+        step * sqrt(sum |e|^2 / K_f) / |d| * d with d = dh v (device tensors, one (K_f + 1, M1, M2) start per fit)."""
+        F, code, dev = self.F, self.code, self.device
+        ee = self._dots(code, True, [(self.E_t, self.E_t)])[:, 0]
+        d = torch.empty(self.Btot, dtype=torch.float64, device=dev)
+        call('blml_mul_bins', _lib.F64, 1, self.Btot, 0, v.data_ptr(), dh.data_ptr(), d.data_ptr(), self.st)
+        segs1 = (_Seg * F)(*[_Seg(int(self.boff[f]), int(self.boff[f]), int(self.B[f]), 1, 0) for f in range(F)])
+        s1 = torch.frombuffer(bytearray(segs1), dtype=torch.uint8).to(dev)
+        call('blml_seg_dots', _lib.F64, F, s1.data_ptr(), 0, 1, ptrs([d]), ptrs([d]), self.part.data_ptr(),
+             self.out.data_ptr(), self.st)
+        dd = self._read(1)[:, 0]
+        scale = step * np.sqrt(ee / self.Kf) / np.sqrt(np.maximum(dd, 1e-300))
+        G = len(grow)
+        old = [self.segs_all[j] for j in grow]
+        nB = np.array([self.B[j] for j in grow], np.int64); nK = np.array([self.Kf[j] + 1 for j in grow], np.int64)
+        noff = np.concatenate([[0], np.cumsum(nB * nK)])
+        new = [_Seg(int(noff[t]), int(old[t].boff), int(nB[t]), int(nK[t]), 0) for t in range(G)]
+        o_t = torch.frombuffer(bytearray((_Seg * G)(*old)), dtype=torch.uint8).to(dev)
+        n_t = torch.frombuffer(bytearray((_Seg * G)(*new)), dtype=torch.uint8).to(dev)
+        En = torch.empty(int(noff[-1]), dtype=self.ct, device=dev)
+        sc = self._dev(scale[np.asarray(grow)])
+        call('blml_seg_append_mode', code, G, o_t.data_ptr(), n_t.data_ptr(), self.E_t.data_ptr(), dh.data_ptr(),
+             v.data_ptr(), sc.data_ptr(), En.data_ptr(), self.st)
+        return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
+
+    def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None):
+        """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then, for the fits
+        whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol, one more shared mode started along the
+        certificate's top eigenvector (every such fit of a round in one batch), until the certificate is met or K
+        reaches max_rank. The lift is convex: a fit that meets the certificate is at its unique optimum (the
+        reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results carry
+        rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations), ...]."""
+        F = len(counts_list)
+        self.fit(counts_list, modes_list, init=init)
+        final = [None] * F
+        paths = [[] for _ in range(F)]
+        cur, idx = self, np.arange(F)
+        self.certify_stats_ = dict(rounds=0, fits_per_round=[], lbfgs_iterations_max=[], seconds_certificate=0.0)
+        while True:
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+            ev[0].record()
+            cert, dh, v = cur.certificate(vectors=True)
+            ev[1].record(); ev[1].synchronize()
+            self.certify_stats_['seconds_certificate'] += ev[0].elapsed_time(ev[1]) / 1e3
+            self.certify_stats_['rounds'] += 1
+            self.certify_stats_['fits_per_round'].append(len(idx))
+            self.certify_stats_['lbfgs_iterations_max'].append(int(max(r.n_sweeps_ for r in cur.results_)))
+            for j, i in enumerate(idx):
+                r = cur.results_[j]
+                paths[i].append((int(cur.Kf[j]), float(r.loglik_), float(cert[j]), int(r.n_sweeps_)))
+                r.certificate_, r.rank_, r.rank_path_ = float(cert[j]), int(cur.Kf[j]), paths[i]
+                final[i] = r
+            grow = [j for j in range(len(idx)) if not cert[j] <= 1.0 + cert_tol and cur.Kf[j] < max_rank]
+            if not grow:
+                return final
+            starts = cur._grown_starts(grow, dh, v, step)
+            nxt = BLMLBinnedBatch(tol=self.tol, max_sweeps=self.max_sweeps, anderson=self.anderson, dtype=self.dtype,
+                                  phase_noise=self.phase_noise, seed=self.seed, stall=self.stall, ll_tol=self.ll_tol,
+                                  ll_window=self.ll_window, lbfgs_m=self.lbfgs_m, device=self.device,
+                                  verbose=self.verbose, control=self.control)
+            mds = [[modes_list[idx[j]][0]] * int(starts[t].shape[0]) for t, j in enumerate(grow)]
+            nxt.fit([counts_list[idx[j]] for j in grow], mds, init=starts)
+            cur, idx = nxt, idx[np.asarray(grow)]
 
     def val_score(self, counts_list):
         """Per fit: the mean log-probability of the counts (validation counts on the fit's lattice) with bin

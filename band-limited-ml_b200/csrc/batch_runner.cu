@@ -1055,9 +1055,11 @@ struct blml_start_batch_s : Runner {
   }
 };
 
-static int make_group(int F, const blml_plan* plans, int xc, const void* x, void* y, const std::vector<int64_t>& off,
-                      blml_group* out) {
-  std::vector<int> nb(F, 1);
+// one grouped mat-vec over every fit's K modes (the K lattices of fit f from off[f], one plan per fit)
+static int make_group(int F, const blml_plan* plans, const blml_seg* segs, int xc, const void* x, void* y,
+                      const std::vector<int64_t>& off, blml_group* out) {
+  std::vector<int> nb(F);
+  for (int f = 0; f < F; f++) nb[f] = segs[f].K;
   return blml_group_create(F, plans, nb.data(), xc, x, off.data(), y, off.data(), out);
 }
 
@@ -1074,10 +1076,12 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
   int64_t tot = 0;
   std::vector<int64_t> off(F);
   for (int f = 0; f < F; f++) {
-    if (segs[f].K != 1 || segs[f].B < 1) { set_error("blml_lbfgs_batch_create: one mode per fit"); return BLML_ERR_ARG; }
+    if (segs[f].K < 1 || segs[f].K > 64 || segs[f].B < 1) {
+      set_error("blml_lbfgs_batch_create: 1 to 64 modes (one shared kernel) per fit"); return BLML_ERR_ARG;
+    }
     if (!plans[f] || plans[f]->dtype != dtype) { set_error("blml_lbfgs_batch_create: plan dtype"); return BLML_ERR_ARG; }
     off[f] = segs[f].off;
-    tot = std::max<int64_t>(tot, segs[f].off + segs[f].B);
+    tot = std::max<int64_t>(tot, segs[f].off + (int64_t)segs[f].K * segs[f].B);
   }
   blml_lbfgs_batch_s* r = new blml_lbfgs_batch_s();
   r->m = m; r->dtype = dtype; r->tol = tol; r->ftol = ll_tol; r->cap = max_iters < 0 ? LLONG_MAX : max_iters;
@@ -1125,9 +1129,9 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
       if (!rc) rc = cuda_status(cudaStreamSynchronize(r->st), "lbfgs create");
     }
   }
-  if (!rc) rc = make_group(F, plans, 1, E, U, off, &r->gEU);
-  if (!rc) rc = make_group(F, plans, 1, r->q, r->Sq, off, &r->gq);
-  if (!rc) rc = make_group(F, plans, 1, r->V, r->SV, off, &r->gV);
+  if (!rc) rc = make_group(F, plans, segs, 1, E, U, off, &r->gEU);
+  if (!rc) rc = make_group(F, plans, segs, 1, r->q, r->Sq, off, &r->gq);
+  if (!rc) rc = make_group(F, plans, segs, 1, r->V, r->SV, off, &r->gV);
   if (rc) { r->release(); delete r; return rc; }
   *out = r;
   return BLML_OK;
@@ -1228,9 +1232,9 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
       if (!rc) rc = cuda_status(cudaStreamSynchronize(r->st), "start create");
     }
   }
-  if (!rc) rc = make_group(F, plans, 0, E, r->U, off, &r->gEU);
-  if (!rc) rc = make_group(F, plans, 0, r->EJ, r->UJ, off, &r->gJ);
-  if (!rc) rc = make_group(F, plans, 0, r->EA, r->UA, off, &r->gA);
+  if (!rc) rc = make_group(F, plans, segs, 0, E, r->U, off, &r->gEU);
+  if (!rc) rc = make_group(F, plans, segs, 0, r->EJ, r->UJ, off, &r->gJ);
+  if (!rc) rc = make_group(F, plans, segs, 0, r->EA, r->UA, off, &r->gA);
   if (rc) { r->release(); delete r; return rc; }
   *out = r;
   return BLML_OK;

@@ -403,6 +403,36 @@ __global__ void k_seg_real_to_complex(const blml_seg* real_segs, const blml_seg*
   SEG_LOOP(b, S) SAcc<T, true>::put(E, C.off + b, (double)er[S.off + b], 0.0);
 }
 
+// the certificate's diagonal scaling of every fit: dh[boff + b] = sqrt(sum_k |E_kb|^2 / w_b) on occupied bins, 0 elsewhere
+template <typename T>
+__global__ void k_seg_cert_weights(const blml_seg* segs, const void* E, const T* w, double* dh) {
+  const blml_seg S = segs[blockIdx.y];
+  SEG_LOOP(b, S) {
+    const double wb = (double)w[S.boff + b];
+    double s = 0.0;
+    for (int k = 0; k < S.K; k++) {
+      double er, ei; SAcc<T, true>::get(E, S.off + (int64_t)k * S.B + b, er, ei); s += er * er + ei * ei;
+    }
+    dh[S.boff + b] = wb > 0 ? sqrt(s / wb) : 0.0;
+  }
+}
+
+// one more mode per fit: the K modes of E (old layout) copied to the first K of the new layout (K + 1 modes), the new
+// one set to scale_f dh v (real direction v per bin, the certificate's top Ritz vector in scaled coordinates)
+template <typename T>
+__global__ void k_seg_append_mode(const blml_seg* old_segs, const blml_seg* new_segs, const void* E, const double* dh,
+                                  const double* v, const double* scale, void* En) {
+  const blml_seg S = old_segs[blockIdx.y], N = new_segs[blockIdx.y];
+  const double sc = scale[blockIdx.y];
+  SEG_LOOP(b, S) {
+    for (int k = 0; k < S.K; k++) {
+      double er, ei; SAcc<T, true>::get(E, S.off + (int64_t)k * S.B + b, er, ei);
+      SAcc<T, true>::put(En, N.off + (int64_t)k * N.B + b, er, ei);
+    }
+    SAcc<T, true>::put(En, N.off + (int64_t)S.K * N.B + b, sc * dh[S.boff + b] * v[S.boff + b], 0.0);
+  }
+}
+
 static int seg_finish(const double* part, int F, int nq, unsigned maxmask, double* out, cudaStream_t st) {
   k_seg_finish<<<F, 256, 0, st>>>(part, nq, seg_blocks_for(F), maxmask, out);
   BLML_CHECK_LAUNCH("seg finish");
@@ -637,6 +667,25 @@ int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const 
   if (dtype == BLML_F64) k_seg_real_to_complex<double><<<SGRID(F), 256, 0, SST>>>(real_segs, cplx_segs, (const double*)er, E);
   else k_seg_real_to_complex<float><<<SGRID(F), 256, 0, SST>>>(real_segs, cplx_segs, (const float*)er, E);
   BLML_CHECK_LAUNCH("blml_seg_real_to_complex");
+  return BLML_OK;
+}
+
+int blml_seg_cert_weights(int dtype, int F, const blml_seg* segs, const void* E, const void* w, double* dh,
+                          void* stream) {
+  if (seg_args(dtype, F, segs, "blml_seg_cert_weights") || !E || !w || !dh) return BLML_ERR_ARG;
+  if (dtype == BLML_F64) k_seg_cert_weights<double><<<SGRID(F), 256, 0, SST>>>(segs, E, (const double*)w, dh);
+  else k_seg_cert_weights<float><<<SGRID(F), 256, 0, SST>>>(segs, E, (const float*)w, dh);
+  BLML_CHECK_LAUNCH("blml_seg_cert_weights");
+  return BLML_OK;
+}
+
+int blml_seg_append_mode(int dtype, int F, const blml_seg* old_segs, const blml_seg* new_segs, const void* E,
+                         const double* dh, const double* v, const double* scale, void* E_new, void* stream) {
+  if (seg_args(dtype, F, old_segs, "blml_seg_append_mode") || !new_segs || !E || !dh || !v || !scale || !E_new)
+    return BLML_ERR_ARG;
+  if (dtype == BLML_F64) k_seg_append_mode<double><<<SGRID(F), 256, 0, SST>>>(old_segs, new_segs, E, dh, v, scale, E_new);
+  else k_seg_append_mode<float><<<SGRID(F), 256, 0, SST>>>(old_segs, new_segs, E, dh, v, scale, E_new);
+  BLML_CHECK_LAUNCH("blml_seg_append_mode");
   return BLML_OK;
 }
 

@@ -249,8 +249,19 @@ int blml_seg_val_score(int dtype, int F, const blml_seg* segs, const void* densi
 int blml_seg_phases(int dtype, int F, const blml_seg* segs, double pn, const double* z, void* E, void* stream);
 int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const blml_seg* cplx_segs, const void* er,
                              void* E, void* stream);
+/* the certificate of every fit (BLMLBinned.certificate, blml_binned.py:501-518): the diagonal scaling
+ * dh = sqrt(sum_k |e_kb|^2 / w_b) of D^1/2 S D^1/2 on occupied bins, float64 per bin in the boff layout (E complex) */
+int blml_seg_cert_weights(int dtype, int F, const blml_seg* segs, const void* E, const void* w, double* dh,
+                          void* stream);
+/* rank growth towards a certified fit: the certificate lambda_max(D^1/2 S D^1/2) / n <= 1 (blml_binned.py:501-518)
+ * holds at the optimum of the convex lift, which a fit with enough shared modes reaches; the next fit starts from the
+ * current modes plus the top eigenvector's direction (the reference's fit with K shared modes and init=,
+ * blml_binned.py:403-408). E_new (K_f + 1 modes, new_segs layout) = E's K_f modes, then scale_f dh v as the new mode
+ * (v: float64 per bin, boff layout; scale: F device doubles). No single reference function does this step. */
+int blml_seg_append_mode(int dtype, int F, const blml_seg* old_segs, const blml_seg* new_segs, const void* E,
+                         const double* dh, const double* v, const double* scale, void* E_new, void* stream);
 
-/* ---- batched solver phases with device-side control (one-mode fits, K = 1): the per-fit decisions of every
+/* ---- batched solver phases with device-side control: the per-fit decisions of every
  *      iteration run as kernels, a ring of iterations is one CUDA graph replayed until every fit has stopped, the
  *      host reading one active mask per replay; the graph is captured again over the fits still iterating when
  *      they fall to three quarters of those it covers. Stop codes: 0 tol, 1 ll_tol, 2 stall. ----
@@ -258,7 +269,9 @@ int blml_seg_real_to_complex(int dtype, int F, const blml_seg* real_segs, const 
  * memory m <= 20, Armijo over t = 2^-j, j < 40, U = S E recomputed at accepted steps, stop at max|rho| < tol, at a
  * likelihood gain below ll_tol over 10 iterations, or after max_iters (< 0: none) -- blml_trivial.py:2590-2645
  * (lbfgs_psd) as BLMLBinned.fit runs it (blml_binned.py:278-355, 429-445) for each fit of a cut-off sweep
- * (selector.py:488-553). w, c: float of dtype per bin (counts / n and counts); n: F host doubles. */
+ * (selector.py:488-553). w, c: float of dtype per bin (counts / n and counts); n: F host doubles. Fit f has
+ * segs[f].K modes (1 to 64) of one shared kernel (plans[f]); its modes are K lattices from segs[f].off. The start
+ * runner below takes one mode per fit. */
 typedef struct blml_lbfgs_batch_s* blml_lbfgs_batch;
 int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_plan* plans, int m, double tol,
                             double ll_tol, int64_t max_iters, const double* n, const void* w, const void* c, void* E,

@@ -15,6 +15,8 @@ kernel classes of blml_trivial.py), written from its documented behaviour:
   * L-BFGS         two-loop recursion, Armijo, canonical form               blml_binned.py:278-355
   * start/finish   real rank-1 start, phases, density_/loglik_              blml_binned.py:383-445
   * certificate    lambda_max(D^1/2 S_0 D^1/2)/n via ARPACK                  blml_binned.py:501-518
+  * certified fit  rank growth until the certificate is <= 1 + tol           no reference function: the fit with K
+                                                                            shared modes and init=, :383-413
 
 Parity pin: tests/golden/*.npz were produced by the reference itself (tests/golden/make_golden.py imports it
 read-only) and tests/test_oracle_golden.py checks this module against them.
@@ -576,6 +578,16 @@ class BinnedFit:
                     return_eigenvectors=False)
         return float(np.max(lam)) / self.n
 
+    def certificate_vector(self, tol=1e-8):
+        """(lambda_max / n, d): the certificate and its top eigenvector v mapped back to coefficients, d = D^1/2 v
+        (the direction a new shared mode takes when the fit grows its rank; shared kernel only)."""
+        from scipy.sparse.linalg import LinearOperator, eigsh
+        D = np.where(self.occ, (np.abs(self.e_hat) ** 2).sum(0) / np.where(self.occ, self.w, 1.0), 0.0)
+        dh = np.sqrt(D); B = int(np.prod(self.shape))
+        op = lambda x: (dh * self.op.S(0, dh * x.reshape(self.shape))).ravel()
+        lam, v = eigsh(LinearOperator((B, B), matvec=op, dtype=np.float64), k=1, which='LA', tol=tol)
+        return float(lam[0]) / self.n, dh * v[:, 0].reshape(self.shape)
+
     def certificate_dense(self):
         """The same lambda_max from the dense exact Gram (small lattices): the reference's own check
         (results/binned_checks.py:50-53)."""
@@ -583,6 +595,34 @@ class BinnedFit:
         D = np.where(self.occ, (np.abs(self.e_hat) ** 2).sum(0) / np.where(self.occ, self.w, 1.0), 0.0).ravel()
         dh = np.sqrt(D)
         return float(np.linalg.eigvalsh(dh[:, None] * G * dh[None, :]).max()) / self.n
+
+
+class _Start:
+    """An init= object: e_hat and shape (what BLMLBinned.fit reads from a previous fit, blml_binned.py:403-408)."""
+
+    def __init__(self, e_hat, shape):
+        self.e_hat, self.shape = e_hat, shape
+
+
+def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-4, max_rank=8, max_sweeps=20000, step=0.1):
+    """A certified fit of one shared kernel: the complex L-BFGS fit at rank K = 1, 2, ... until the certificate
+    lambda_max(D^1/2 S D^1/2) / n <= 1 + cert_tol (blml_binned.py:501-518), each rank started from the previous fit's
+    modes plus a new mode step * (rms mode norm) along d = D^1/2 v, v the certificate's top eigenvector (an ascent
+    direction of the convex lift while the certificate exceeds 1). The lift is convex, so the certified loglik is
+    that of its unique optimum, whatever the path. Returns (fit, [(K, loglik, certificate, iterations), ...])."""
+    K = 1
+    fit = BinnedFit(tol=tol, solver='lbfgs', max_sweeps=max_sweeps).fit(counts, [spec], complex_g=True)
+    path = []
+    while True:
+        cert, d = fit.certificate_vector()
+        path.append((K, float(fit.loglik), cert, int(fit.n_sweeps)))
+        if cert <= 1.0 + cert_tol or K >= max_rank:
+            return fit, path
+        scale = step * np.sqrt((np.abs(fit.e_hat) ** 2).sum() / K) / max(np.linalg.norm(d), 1e-300)
+        init = _Start(np.concatenate([fit.e_hat, (scale * d)[None].astype(complex)], 0), fit.shape)
+        K += 1
+        fit = BinnedFit(tol=tol, solver='lbfgs', max_sweeps=max_sweeps).fit(counts, [spec] * K, complex_g=True,
+                                                                           init=init)
 
 
 def anderson_mix(hX, hF, f):

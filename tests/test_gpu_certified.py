@@ -1,0 +1,66 @@
+"""Certified fits on the batched engine: the certificate of every fit at once (float64 Lanczos in lockstep) against the
+oracle's ARPACK certificate at the same coefficients (blml_binned.py:501-518); fits of K shared modes from a given
+start against the oracle's fit from the same start; rank growth until the certificate holds, whose loglik is the
+convex lift's unique optimum and so must equal the oracle's certified loglik (oracle.certified_fit)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+CASES = [((48, 48), 0.3, 2e4, 1), ((32, 64), 0.2, 1e4, 2), ((64, 48), 0.12, 3e4, 3), ((40, 40), 0.4, 5e3, 4)]
+
+
+def _fits():
+    from blml_b200 import workloads
+    return [(workloads.two_disk_field(shape, fc=fc, N=N, seed=seed), workloads.pball_modes(shape, fc))
+            for shape, fc, N, seed in CASES]
+
+
+def test_batched_certificate_matches_oracle(cuda_device):
+    import blml_oracle as bo
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _fits()
+    b = BLMLBinnedBatch(tol=1e-6, device='cuda')
+    b.fit([c for c, _ in fits], [m for _, m in fits])
+    cert = b.certificate()
+    for f, (counts, modes) in enumerate(fits):
+        o = bo.BinnedFit(tol=1e-6, solver='lbfgs', max_sweeps=0).fit(counts, modes, complex_g=True)
+        o.e_hat = b.e_hat(f).cpu().numpy()
+        ref = o.certificate(tol=1e-10)
+        assert abs(cert[f] - ref) <= 1e-5 * ref, (f, cert[f], ref)
+
+
+def test_rank_two_fit_from_a_start_matches_oracle(cuda_device):
+    """K = 2 shared modes from the same start (the rank-1 fit plus a small second mode): the engine and the oracle run
+    the same L-BFGS from the same point and reach the same loglik."""
+    import blml_oracle as bo
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _fits()[:2]
+    starts, mods = [], []
+    for counts, modes in fits:
+        o = bo.BinnedFit(tol=1e-6, solver='lbfgs').fit(counts, modes, complex_g=True)
+        _, d = o.certificate_vector()
+        sc = 0.1 * np.sqrt((np.abs(o.e_hat) ** 2).sum()) / np.linalg.norm(d)
+        starts.append(np.concatenate([o.e_hat, (sc * d)[None].astype(complex)], 0))
+        mods.append([modes[0]] * 2)
+    b = BLMLBinnedBatch(tol=1e-6, device='cuda')
+    res = b.fit([c for c, _ in fits], mods, init=starts)
+    for f, (counts, _) in enumerate(fits):
+        o = bo.BinnedFit(tol=1e-6, solver='lbfgs').fit(counts, mods[f], complex_g=True,
+                                                       init=bo._Start(starts[f], counts.shape))
+        assert abs(res[f].loglik_ - o.loglik) <= 1e-6 * abs(o.loglik), (f, res[f].loglik_, o.loglik)
+
+
+def test_certified_fits_reach_the_oracle_optimum(cuda_device):
+    import blml_oracle as bo
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _fits()
+    b = BLMLBinnedBatch(tol=1e-6, device='cuda')
+    res = b.fit_certified([c for c, _ in fits], [m for _, m in fits], cert_tol=1e-4)
+    for f, (counts, modes) in enumerate(fits):
+        r = res[f]
+        assert r.certificate_ <= 1 + 1e-4, (f, r.rank_path_)
+        _, path = bo.certified_fit(counts, modes[0], cert_tol=1e-4)
+        ll = path[-1][1]
+        assert abs(r.loglik_ - ll) <= 1e-6 * abs(ll), (f, r.rank_path_, path)
+        assert r.density_.shape == counts.shape
