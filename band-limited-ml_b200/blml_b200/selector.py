@@ -309,316 +309,50 @@ def select_counts_batched(train, val, kinds=('sinc', 'sinc'), periods=None, fc0=
     return (out, stats) if return_stats else out
 
 
-# ---------------------------------------------------------------------------------------------------- entry points
-# The selector's public entry points (selector.py:617-732): select on points and select_counts on counts on a fixed
-# lattice, both fitting BLMLQuick (here the GPU point / lattice fit of blml_b200.quick, real rank 1).
-
-def _estimator_class(engine):
-    """The point estimator for engine 'cpu' | 'gpu' (selector.py:113-118); this engine fits on the GPU for both."""
-    if engine not in ('cpu', 'gpu'):
-        raise ValueError(f"engine must be 'cpu' or 'gpu', got {engine}")
-    from .quick import BLMLQuick
-    return BLMLQuick
-
-
+# ---------------------------------------------------------------------------------------------------- counts entry
 def _lattice_estimator(tol):
-    """The fixed-lattice estimator of select_counts (selector.py:706-708), float64 state."""
-    return _estimator_class('gpu')(dtype=np.float64, tol=tol)
-
-
-def _wmean(v, w):
-    return float(np.mean(v)) if w is None else float(np.average(v, weights=w))
-
-
-def _wquantile(X, q, w):
-    """Per-column quantiles q (%) of X weighted by w (selector.py:39-51): np.percentile's linear rule on the points
-    repeated w times; constant or no weights: np.percentile itself."""
-    if w is None or np.all(w == w[0]):
-        return np.percentile(X, q, axis=0)
-    out = np.empty((len(q), X.shape[1]))
-    qs = np.asarray(q, float) / 100.0
-    for j in range(X.shape[1]):
-        o = np.argsort(X[:, j], kind='stable')
-        xs = X[o, j]
-        cw = np.cumsum(w[o])
-        N = cw[-1]
-        pos = qs * (N - 1)
-        lo = np.floor(pos)
-        hi = np.minimum(lo + 1, np.floor(N - 1))
-        at = lambda k: xs[np.minimum(np.searchsorted(cw, k, side='right'), len(xs) - 1)]
-        out[:, j] = at(lo) + (pos - lo) * (at(hi) - at(lo))
-    return out
-
-
-def _radial_groups(kinds):
-    """[(name, [columns])] of the ball / pball groups in order of first appearance (blml_trivial.py:251-261)."""
-    groups = {}
-    for j, k in enumerate(kinds or []):
-        if is_group(k):
-            name, tag = split_kind(k)
-            groups.setdefault(tag, (name, []))[1].append(j)
-    return list(groups.values())
-
-
-def _template(modes, d):
-    """kinds, periods, dep, rank and fc (K, d; NaN where missing) of a modes template (selector.py:54-61)."""
-    from .spec import parse_modes, modes_fc
-    specs, dep = parse_modes(modes, d, need_fc=False)
-    if any(sp['kinds'] != specs[0]['kinds'] or sp['periods'] != specs[0]['periods'] for sp in specs):
-        raise ValueError("selector: modes must share kind, period and group per column (fc may differ)")
-    return specs[0]['kinds'], specs[0]['periods'], dep, len(specs), modes_fc(modes)
-
-
-def _start_free(start, free, iqr, d):
-    """Scaled start (NaN where none), the trainable mask and the columns a shared bracket grows (selector.py:75-82)."""
-    st = np.full(d, np.nan) if start is None else np.asarray(start, float) * iqr
-    fr = np.ones(d, bool) if free is None else np.asarray(free, bool)
-    if start is not None and np.any(~fr & ~np.isfinite(st)):
-        raise ValueError("a fixed (non-trainable) fc needs a value")
-    return st, fr, fr & ~np.isfinite(st)
-
-
-def _tie(fc, kinds):
-    """fc equalised within each radial group (geometric mean, selector.py:89-94)."""
-    fc = np.array(fc, dtype=float)
-    for _, dims in _radial_groups(kinds):
-        fc[dims] = np.exp(np.log(fc[dims]).mean())
-    return fc
-
-
-def _split(Xtr, iqr, seed, X_val, sw=None, sw_val=None):
-    """Training / validation points in scaled units (selector.py:126-135): X_val scaled by the training IQR, or a
-    seeded 80/20 permutation split of the training points (their weights follow)."""
-    if X_val is not None:
-        return Xtr, np.asarray(X_val, dtype=float) / iqr, sw, sw_val
-    rng = np.random.default_rng(seed)
-    n = len(Xtr)
-    idx = rng.permutation(n)
-    n2 = int(0.8 * n)
-    sub = lambda a, i: None if a is None else a[i]
-    return Xtr[idx[:n2]], Xtr[idx[n2:]], sub(sw, idx[:n2]), sub(sw, idx[n2:])
-
-
-def _scale_data(X, kinds, periods, sw=None):
-    """(scaled points, scaled periods, IQR) (selector.py:137-159): each column divided by its (weighted) IQR, a radial
-    group by its columns' geometric-mean IQR; dirichlet / pball periods scaled with their columns."""
-    q75, q25 = _wquantile(np.asarray(X, float), [75, 25], sw)
-    iqr = np.maximum(q75 - q25, 1e-10)
-    for _, dims in _radial_groups(kinds):
-        iqr[dims] = np.exp(np.log(iqr[dims]).mean())
-    Xs = X / iqr
-    per = None
-    if periods is not None:
-        per = [p / iqr[k] if (p is not None and kinds is not None and k < len(kinds) and
-                              split_kind(kinds[k])[0] in ('dirichlet', 'pball')) else p
-               for k, p in enumerate(periods)]
-    return Xs, per, iqr
-
-
-def _shared_step(shared_step, d):
-    return 2.0 ** (1.0 / d) if shared_step == 'volume' else float(shared_step) if not isinstance(shared_step, str) \
-        else 2.0
-
-
-def _fit(Est, X, fc, kinds, periods, rank=1, complex_g=False, sw=None):
-    """One fit at cut-offs fc with the template's kinds / periods (selector.py:30-34)."""
-    kw = {} if sw is None else dict(sample_weight=sw)
-    return Est().fit(X, make_modes(fc, kinds, periods, rank, d=X.shape[1]), complex_g=complex_g, **kw)
-
-
-def _vll_fn(Est, Xa, Xb, kinds, periods_scaled, rank, complex_g, wa, wb, jac):
-    def vll(fc):
-        m = _fit(Est, Xa, fc, kinds, periods_scaled, rank, complex_g, sw=wa)
-        return _wmean(np.log(np.maximum(m.predict(Xb).ravel(), 1e-300)), wb) - jac
-    return vll
-
-
-def _cond_vll_fn(Est, Xa, Xb, kinds, periods_scaled, dep, iqr, rank, complex_g, wa, wb):
-    """The conditional validation score (selector.py:318-357, method 'ratio' with separate fits): the mean of
-    log p_joint - log p_marginal over the validation points, the marginal fitted on the other columns with the same
-    fc, less the dep columns' log IQR (original units)."""
-    d = Xa.shape[1]
-    dep_idx = sorted(set(int(i) for i in np.atleast_1d(dep)))
-    if not dep_idx or any(i < 0 or i >= d for i in dep_idx):
-        raise ValueError(f"dep indices {dep_idx} out of range for {d} dims")
-    keep = [k for k in range(d) if k not in dep_idx]
-    if not keep:
-        raise ValueError("dep covers all dims; need at least one conditioning dim for the marginal")
-    kinds_m = [kinds[k] for k in keep] if kinds else None
-    per_m = [periods_scaled[k] for k in keep] if periods_scaled else None
-    jac = np.log(iqr[dep_idx]).sum()
-
-    def cvll(fc):
-        fc = list(fc)
-        mj = _fit(Est, Xa, fc, kinds, periods_scaled, rank, complex_g, sw=wa)
-        mm = _fit(Est, Xa[:, keep], [fc[k] for k in keep], kinds_m, per_m, rank, complex_g, sw=wa)
-        lj = np.log(np.maximum(mj.predict(Xb).ravel(), 1e-300))
-        lm = np.log(np.maximum(mm.predict(Xb[:, keep]).ravel(), 1e-300))
-        return _wmean(lj - lm, wb) - jac
-    return cvll
-
-
-def _objective(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep):
-    if dep is None:
-        return _vll_fn(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, np.log(iqr).sum())
-    return _cond_vll_fn(Est, Xa, Xb, kinds, per, dep, iqr, rank, complex_g, wa, wb)
-
-
-def _select_shared(X, kinds, periods, seed=0, engine='cpu', X_val=None, shared_step='double', complex_g=False,
-                   rank=1, start=None, free=None, sw=None, sw_val=None, dep=None):
-    """One fc for every growing scaled column, doubled from 0.2 until the validation score first drops; the peak
-    (selector.py:162-195; conditional, dep given: :360-392). Returns (fc in data units, best)."""
-    Est = _estimator_class(engine)
-    Xs, per, iqr = _scale_data(X, kinds, periods, sw)
-    Xa, Xb, wa, wb = _split(Xs, iqr, seed, X_val, sw, sw_val)
-    step = _shared_step(shared_step, Xa.shape[1])
-    vll = _objective(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep)
-    st, fr, grow = _start_free(start, free, iqr, Xa.shape[1])
-    vec = lambda c: np.where(grow, c, st)
-    fc = 0.2
-    best = vll(vec(fc))
-    if not grow.any():
-        return vec(fc) / iqr, best
-    prev = best
-    while True:
-        fc *= step
-        v = vll(vec(fc))
-        if v < prev:
-            fc /= step
-            break
-        if v > best:
-            best = v
-        prev = v
-    return vec(fc) / iqr, best
-
-
-def _select_hillclimb(X, kinds, periods, seed=0, init_fc=None, engine='cpu', X_val=None, complex_g=False, rank=1,
-                      start=None, free=None, sw=None, sw_val=None, dep=None):
-    """Per-block doubling (x2 while it improves, else x0.5 while it improves), full sweeps until none moves
-    (selector.py:197-247; conditional: :394-440, started at 0.2 in every scaled column). Returns (fc in data
-    units, best)."""
-    Est = _estimator_class(engine)
-    Xs, per, iqr = _scale_data(X, kinds, periods, sw)
-    Xa, Xb, wa, wb = _split(Xs, iqr, seed, X_val, sw, sw_val)
-    n2, d = Xa.shape
-    vll = _objective(Est, Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep)
-    if init_fc is not None:
-        fc = np.array(init_fc, dtype=float)
-    elif dep is not None:
-        fc = np.full(d, 0.2)
-    else:
-        ranges = np.maximum(Xa.max(axis=0) - Xa.min(axis=0), 1e-10)
-        fc = 0.5 * 0.1 * (n2 ** -0.25) / ranges
-    st, fr, _ = _start_free(start, free, iqr, d)
-    fc = _tie(np.where(np.isfinite(st), st, fc), kinds)
-    best = vll(fc)
-    while True:
-        moved = False
-        for k in free_blocks(kinds, d, fr):
-            improved = False
-            for factor, tried_up in ((2.0, False), (0.5, True)):
-                if tried_up and improved:
-                    break
-                while True:
-                    cand = fc.copy()
-                    cand[k] *= factor
-                    v = vll(cand)
-                    if v > best:
-                        best, fc, improved = v, cand, True
-                    else:
-                        break
-            moved = moved or improved
-        if not moved:
-            break
-    return fc / iqr, best
-
-
-def _select_auto(X, kinds, periods, seed=0, engine='cpu', X_val=None, fc0=0.2, complex_g=False, rank=1,
-                 factors=(SQRT2,), start=None, free=None, sw=None, sw_val=None, dep=None):
-    """The volume-grid shared search and the harmonic-aware refinement (search) on the validation score, joint or
-    conditional (selector.py:554-613, rank 1 / shared modes). Returns (fc in data units, best)."""
-    X = np.asarray(X, dtype=float)
-    Xs, per, iqr = _scale_data(X, kinds, periods, sw)
-    Xa, Xb, wa, wb = _split(Xs, iqr, seed, X_val, sw, sw_val)
-    d = Xa.shape[1]
-    obj = _objective(_estimator_class(engine), Xa, Xb, kinds, per, rank, complex_g, wa, wb, iqr, dep)
-    st = None if start is None else np.asarray(start, float) * iqr
-    fc, best = search(obj, d, kinds, per, fc0=fc0, factors=factors, start=st, free=free)
-    return fc / iqr, best
-
-
-def select(Xtr_raw, modes, search='shared_hillclimb', seed=0, init_fc=None, engine='cpu', cond_method='ratio',
-           X_val=None, shared_step='double', signs=None, complex_g=False, factors=(SQRT2,), separate_modes=False,
-           sample_weight=None, val_weight=None):
-    """fc for a modes template on points (selector.py:617-666): IQR-scaled columns, a validation split (or X_val), the
-    search pattern 'shared_hillclimb' (default), 'shared', 'hillclimb' or 'auto', each candidate a BLMLQuick fit
-    scored by the mean log density of the validation points (in data units); dep columns in the modes give the
-    conditional score, mean log(p_joint / p_marginal), the marginal a second fit on the other columns with the same
-    fc. Returns (modes with the selected fc, best). The GPU fits are real rank 1: signs, complex_g, rank > 1 and
-    separate_modes raise NotImplementedError."""
-    if search not in ('shared_hillclimb', 'shared', 'hillclimb', 'auto'):
-        raise ValueError(f"search must be 'shared_hillclimb', 'shared', 'hillclimb' or 'auto', got {search}")
-    if cond_method != 'ratio':
-        raise ValueError(f"cond_method must be 'ratio', got {cond_method}")
-    Xtr_raw = np.asarray(Xtr_raw, dtype=float)
-    sw = None if sample_weight is None else np.asarray(sample_weight, float)
-    sw_val = None if val_weight is None else np.asarray(val_weight, float)
-    kinds, periods, dep, K, F = _template(modes, Xtr_raw.shape[1])
-    if signs is not None and dep is not None:
-        raise ValueError("signs with dep=... (the marginal's g has its own signs)")
-    if signs is not None or complex_g or K > 1 or separate_modes:
-        raise NotImplementedError("select on the GPU: real rank-1 fits (no signs, complex_g, rank > 1)")
-    from .spec import modes_trainable, with_fc
-    T = modes_trainable(modes)
-    start, free = F[0], T[0]
-    start = None if np.all(np.isnan(start)) else start
-    free = None if np.all(free) else free
-    sf = dict(start=start, free=free, sw=sw, sw_val=sw_val, dep=dep)
-    if search == 'auto':
-        fc, best = _select_auto(Xtr_raw, kinds, periods, seed, engine, X_val, factors=factors, **sf)
-    elif search == 'shared':
-        fc, best = _select_shared(Xtr_raw, kinds, periods, seed, engine, X_val, shared_step, **sf)
-    elif search == 'hillclimb':
-        fc, best = _select_hillclimb(Xtr_raw, kinds, periods, seed, init_fc, engine, X_val, **sf)
-    else:
-        fc_shared, _ = _select_shared(Xtr_raw, kinds, periods, seed, engine, X_val, shared_step, **sf)
-        _, _, iqr = _scale_data(Xtr_raw, kinds, periods, sw)
-        fc, best = _select_hillclimb(Xtr_raw, kinds, periods, seed, fc_shared * iqr, engine, X_val, free=free, sw=sw,
-                                     sw_val=sw_val, dep=dep)
-    return with_fc(modes, fc), best
+    """The fixed-lattice fit that scores a select_counts candidate: blml_b200.quick.BLMLQuick on the GPU, float64."""
+    from .quick import BLMLQuick
+    return BLMLQuick(dtype=np.float64, tol=tol)
 
 
 def select_counts(Z, w_tr, w_va, h, modes, complex_g=False, separate_modes=False, fc0=None, fc_max=None, tag='counts',
                   factors=(SQRT2,), engine='cpu', **fit_kw):
-    """fc for counts on a fixed lattice (selector.py:670-732): fit (Z, w_tr) with the modes on the lattice h, score
-    the mean log-probability of the validation counts w_va with bin probabilities f(z_b) normalised over the bins
-    given (Z should be the full grid, empty bins included); the search of `search` from fc0 (default 0.1 fc_max),
-    fc capped at fc_max (default 1 / h per column). Returns (modes with the selected fc, best). Real rank 1 on the
-    GPU: dep, complex_g, rank > 1 and separate_modes raise NotImplementedError."""
-    from .spec import modes_trainable, with_fc, with_lattice
-    Z = np.atleast_2d(np.asarray(Z, float))
-    d = Z.shape[1]
-    kinds, periods, dep, K, F = _template(modes, d)
-    if dep is not None or complex_g or K > 1 or separate_modes:
+    """fc of a one-mode template for counts on a fixed lattice (the reference's entry, selector.py:716-732): the
+    search of `search` over fc, each candidate a fit of the training counts w_tr at the lattice points Z (step h)
+    scored by the mean log-probability of the validation counts w_va, bin probabilities being the fitted density
+    normalised over the points given (so Z should hold the whole grid, empty bins included). The template's fc
+    values start the search (NaN: from fc0, default a tenth of the cap) and its non-trainable columns stay fixed;
+    no column goes above fc_max (default 1 / h). Returns (modes with the selected fc, best score). Real rank-1
+    joint fits only: dep columns, complex_g, K > 1 and separate_modes raise NotImplementedError. `engine` is
+    accepted for the reference's signature; the fits run on the GPU."""
+    from .spec import parse_modes, modes_fc, modes_trainable, with_fc, with_lattice
+    pts = np.atleast_2d(np.asarray(Z, float))
+    d = pts.shape[1]
+    specs, dep = parse_modes(modes, d, need_fc=False)
+    if dep is not None or complex_g or len(specs) != 1 or separate_modes:
         raise NotImplementedError("select_counts on the GPU: real rank-1 joint fits (no dep, complex_g, rank > 1)")
-    T = modes_trainable(modes)
-    start = None if np.all(np.isnan(F[0])) else np.asarray(F[0], float).ravel()
-    free = None if np.all(T[0]) else np.asarray(T[0], bool).ravel()
-    periods = list(periods) if periods is not None else [None] * d
-    h_vec = np.broadcast_to(np.asarray(h, float), (d,)).copy()
-    cap = np.broadcast_to(np.asarray(fc_max if fc_max is not None else 1.0 / h_vec, float), (d,))
-    w_tr = np.asarray(w_tr, float).ravel()
-    w_va = np.asarray(w_va, float).ravel()
+    kinds, periods = specs[0]['kinds'], specs[0]['periods']
+    fc_tpl = np.asarray(modes_fc(modes), float).reshape(-1, d)[0]
+    train_mask = np.asarray(modes_trainable(modes), bool).reshape(-1, d)[0]
+    step = np.ones(d) * np.asarray(h, float)
+    ceiling = np.ones(d) * np.asarray(1.0 / step if fc_max is None else fc_max, float)
+    train = np.asarray(w_tr, float).ravel()
+    held = np.asarray(w_va, float).ravel()
+    held_n = held.sum()
+    tol = fit_kw.get('tol', 1e-5)
 
-    def obj(fcv):
-        Fv = np.asarray(fcv, float).reshape(1, d)
-        if np.any(Fv > cap[None] * (1 + 1e-9)):
+    def held_out_score(fc):
+        fc = np.asarray(fc, float).ravel()
+        if np.any(fc > ceiling * (1 + 1e-9)):
             return -np.inf
-        m = _lattice_estimator(fit_kw.get('tol', 1e-5))
-        m.fit(Z, with_lattice(make_modes(Fv[0], kinds, periods, 1, d=d), h_vec), sample_weight=w_tr)
-        P = np.maximum(m.predict(Z), 1e-300)
-        P = P / P.sum()
-        return float(w_va @ np.log(P) / w_va.sum())
-    f0 = float(fc0) if fc0 is not None else 0.1 * float(cap.min())
-    fc, best = search(obj, d, kinds, periods, fc0=f0, tag=tag, factors=factors, start=start, free=free)
+        est = _lattice_estimator(tol)
+        est.fit(pts, with_lattice(make_modes(fc, kinds, periods, 1, d=d), step), sample_weight=train)
+        p = np.maximum(est.predict(pts), 1e-300)
+        return float(held @ np.log(p / p.sum()) / held_n)
+
+    first = 0.1 * float(ceiling.min()) if fc0 is None else float(fc0)
+    fc, best = search(held_out_score, d, kinds, list(periods), fc0=first, tag=tag, factors=factors,
+                      start=None if np.all(np.isnan(fc_tpl)) else fc_tpl,
+                      free=None if np.all(train_mask) else train_mask)
     return with_fc(modes, fc), best

@@ -1,7 +1,7 @@
 """Generate the golden fixtures of the binned path by running the reference implementation itself
 (rahuljhu/band-limited-ml, imported read-only from its checkout) on seeded inputs.
 
-    NUMBA_CACHE_DIR=/tmp/nb python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 Writes tests/golden/*.npz. The fixtures pin the CPU oracle (oracle/) and the GPU path's parity tests; the
 reference is never needed at test time.
@@ -11,11 +11,12 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_checkout   # noqa: E402
+REF = reference_checkout()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.join(HERE, '..', '..', 'band-limited-ml_b200'))
-os.environ.setdefault('NUMBA_CACHE_DIR', '/tmp/nb')
 
 import blml_trivial as bt                       # noqa: E402  (the reference)
 from blml_binned import BLMLBinned              # noqa: E402

@@ -3,18 +3,19 @@ blml_binned.py:520-628: fc_grad, param_grad, implicit_grad; imported read-only f
 tests/golden_cases.py GRAD_SPECS. Per case: the training and validation counts, the reference's fitted coefficients
 e_hat, fc_grad(), param_grad(val, eps), implicit_grad(val, eps) (K x units, NaN for integer units) and eps.
 
-    NUMBA_CACHE_DIR=/tmp/nb python tests/golden/make_grad_golden.py /root/reference
+    python tests/golden/make_grad_golden.py <reference checkout>
 """
 import os
 import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_checkout   # noqa: E402
+REF = reference_checkout()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.join(HERE, '..'))
-os.environ.setdefault('NUMBA_CACHE_DIR', '/tmp/nb')
 
 from blml_binned import BLMLBinned              # noqa: E402  (the reference)
 from golden_cases import GRAD_SPECS, grad_density, hist   # noqa: E402

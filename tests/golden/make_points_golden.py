@@ -3,18 +3,19 @@ blml_trivial.py:2705-2800 with engine='cpu', float64; imported read-only from it
 tests/golden_cases.py POINT_SPECS. Per case: the points (and weights), the reference's bins Z_ in its order, counts
 w_, steps, coefficients e_hat_, its predict and sqrt_density at query points.
 
-    NUMBA_CACHE_DIR=/tmp/nb python tests/golden/make_points_golden.py /root/reference
+    python tests/golden/make_points_golden.py <reference checkout>
 """
 import os
 import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_checkout   # noqa: E402
+REF = reference_checkout()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.join(HERE, '..'))
-os.environ.setdefault('NUMBA_CACHE_DIR', '/tmp/nb')
 
 from blml_trivial import BLMLQuick              # noqa: E402  (the reference)
 from golden_cases import POINT_SPECS, point_cloud   # noqa: E402

@@ -2,7 +2,7 @@
 (rahuljhu/band-limited-ml selector.py:488-553 `_search`, imported read-only from its checkout) on the deterministic
 objectives of tests/selector_cases.py, recording every candidate it scores, in order, and its result.
 
-    NUMBA_CACHE_DIR=/tmp/nb python tests/golden/make_selector_golden.py /root/reference
+    python tests/golden/make_selector_golden.py <reference checkout>
 """
 import contextlib
 import io
@@ -12,11 +12,12 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_checkout   # noqa: E402
+REF = reference_checkout()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.join(HERE, '..'))
-os.environ.setdefault('NUMBA_CACHE_DIR', '/tmp/nb')
 
 import selector as sel                          # noqa: E402  (the reference)
 from selector_cases import CASES                # noqa: E402

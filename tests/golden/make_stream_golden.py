@@ -3,7 +3,7 @@ blml_binned.py:648-1112: BLMLBinnedStreaming with its _KernelLearner; imported r
 of tests/golden_cases.py STREAM_SPECS. Per case: the batches, preq_ (NaN for burn-in entries), the fc of every
 history entry (entries x modes x columns), the number of parameter moves per entry and the final loglik_.
 
-    NUMBA_CACHE_DIR=/tmp/nb python tests/golden/make_stream_golden.py /root/reference
+    python tests/golden/make_stream_golden.py <reference checkout>
 """
 import contextlib
 import io
@@ -12,11 +12,12 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_checkout   # noqa: E402
+REF = reference_checkout()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.join(HERE, '..'))
-os.environ.setdefault('NUMBA_CACHE_DIR', '/tmp/nb')
 
 from blml_binned import BLMLBinnedStreaming     # noqa: E402  (the reference)
 from golden_cases import STREAM_SPECS, grad_density, hist   # noqa: E402

@@ -3,7 +3,7 @@ blml_maps.py:19-36 adam_step on a 'scale' parameter with dlog gradients, blml_bi
 imported read-only from its checkout): Adam trajectories of log fc for seeded gradient sequences of three magnitudes,
 and batch orders with and without groups.
 
-    NUMBA_CACHE_DIR=/tmp/nb python tests/golden/make_stream_helpers_golden.py /root/reference
+    python tests/golden/make_stream_helpers_golden.py <reference checkout>
 """
 import json
 import os
@@ -11,10 +11,11 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from _refpath import reference_checkout   # noqa: E402
+REF = reference_checkout()
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
-os.environ.setdefault('NUMBA_CACHE_DIR', '/tmp/nb')
 
 from blml_maps import adam_step                 # noqa: E402  (the reference)
 from blml_binned import _batch_order            # noqa: E402

@@ -90,34 +90,7 @@ class StubQuick:
         return (k @ self.sw) / self.sw.sum()
 
 
-def select_points(n, seed, d=2):
-    rng = np.random.default_rng(seed)
-    comp = rng.uniform(size=n) < 0.55
-    X = np.where(comp[:, None], rng.normal(0.3, 0.07, (n, d)), rng.normal(0.65, 0.12, (n, d)))
-    X[:, -1] *= 3.0                                         # columns on different scales (the IQR scaling matters)
-    return X
-
-
 SINC2 = [{0: dict(kind='sinc'), 1: dict(kind='sinc')}]
-# name: (points n, seed, modes template, select keywords, with X_val, with weights)
-SELECT_CASES = {
-    'shared': (240, 1, SINC2, dict(search='shared'), False, False),
-    'shared_volume': (240, 2, SINC2, dict(search='shared', shared_step='volume'), False, False),
-    'hillclimb': (240, 3, SINC2, dict(search='hillclimb'), False, False),
-    'shared_hillclimb': (240, 4, SINC2, dict(), False, False),
-    'auto': (240, 5, SINC2, dict(search='auto', factors=(2 ** 0.5, 2 ** 0.25)), False, False),
-    'auto_val_weights': (200, 6, SINC2, dict(search='auto'), True, True),
-    'auto_fixed_column': (240, 7, [{0: dict(kind='sinc', fc=dict(value=4.0, trainable=False)), 1: dict(kind='sinc')}],
-                          dict(search='auto'), False, False),
-    'ball_group': (240, 8, [{(0, 1): dict(kind='ball')}], dict(), False, False),
-    'cond_shared': (240, 9, [{0: dict(kind='sinc', dep=True), 1: dict(kind='sinc')}], dict(search='shared'), False,
-                    False),
-    'cond_hillclimb': (240, 10, [{0: dict(kind='sinc'), 1: dict(kind='sinc', dep=True)}], dict(search='hillclimb'),
-                       False, False),
-    'cond_shared_hillclimb': (240, 11, [{0: dict(kind='sinc', dep=True), 1: dict(kind='sinc')}], dict(), False, True),
-    'cond_auto_val': (200, 12, [{0: dict(kind='sinc'), 1: dict(kind='sinc', dep=True)}], dict(search='auto'), True,
-                      False),
-}
 # name: (lattice shape, seed, modes template, select_counts keywords)
 COUNTS_CASES = {
     'counts_default': ((24, 24), 11, SINC2, dict()),
