@@ -52,7 +52,7 @@ class BLMLBinned:
 
     def __init__(self, tol=1e-5, max_sweeps=None, anderson=5, engine='gpu', dtype=np.float64, phase_noise=0.1,
                  seed=0, workers=-1, verbose=False, stall=1000, ll_tol=None, ll_window=100, solver='cd', lbfgs_m=20,
-                 device=None, matvec_engine='simt'):
+                 device=None, matvec_engine='simt', matvec_route=0):
         if solver not in ('cd', 'lbfgs'):
             raise ValueError("solver: 'cd' (coordinate / Jacobi updates with Anderson mixing) or 'lbfgs'")
         if int(lbfgs_m) > 20:
@@ -70,6 +70,10 @@ class BLMLBinned:
         if matvec_engine == 'tc' and self.dtype != np.float32:
             raise ValueError("matvec_engine='tc' stores float32: use dtype=np.float32")
         self.matvec_engine = matvec_engine
+        if matvec_route not in (_lib.ROUTE_AUTO, _lib.ROUTE_CONTRACT, _lib.ROUTE_FFT):
+            raise ValueError("matvec_route: 0 (auto: FFTs where the kernel is a DFT mask), 1 (restricted transforms) "
+                             "or 2 (FFTs)")
+        self.matvec_route = matvec_route
 
     # ---------------------------------------------------------------- setup
     def _setup(self, counts, modes, h, origin):
@@ -122,6 +126,8 @@ class BLMLBinned:
                 hit = (plan, kernel_at_zero(sp, self.d_), (freqs, W))
             _PLANS[key] = hit                         # most recent last
             mine.add(key)
+            if eng == _lib.ENGINE_SIMT:
+                hit[0].route = self.matvec_route          # a cached plan takes this fit's route
             self.kern_.append(hit)
         while len(_PLANS) > _PLAN_CACHE_SIZE:
             _PLANS.popitem(last=False)
