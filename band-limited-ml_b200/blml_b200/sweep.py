@@ -722,3 +722,19 @@ class BLMLBinnedBatch:
              self._dev(1.0 / Q).data_ptr(), float(eps), self.part.data_ptr(), self.out.data_ptr(), self.st)
         r = self._read(2)
         return r[:, 0] / r[:, 1]
+
+
+def certified_log_density(results, counts_list, eps=0.0):
+    """Per fit of BLMLBinnedBatch.fit_certified's results: the mean log density of counts_list[i] (held-out counts on
+    fit i's lattice) under fit i (blml_binned.py:630-645); one launch per batch that holds a final fit."""
+    groups = {}
+    for i, r in enumerate(results):
+        groups.setdefault(id(r._batch), (r._batch, []))[1].append(i)
+    out = np.full(len(results), np.nan)
+    for b, idx in groups.values():
+        mine = {r._f: i for i, r in ((i, results[i]) for i in idx)}
+        full = [counts_list[mine[f]] if f in mine else np.zeros(b.shapes[f]) for f in range(b.F)]
+        sc = b.log_density(full, eps)
+        for f, i in mine.items():
+            out[i] = sc[f]
+    return out
