@@ -364,9 +364,9 @@ typedef struct {
 int blml_rows(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
               int grad, double* s, double* ds, void* stream);
 /* ---- blml_rows without any allocation: no counterpart in the reference ----
- * For callers that cannot allocate device memory themselves or let the library do it: code that runs while a
- * stream is being captured into a CUDA graph (where cudaMalloc breaks the capture), processes whose device memory
- * is reserved up front by another allocator, and embedded hosts that forbid allocation after start-up.
+ * For callers that cannot allocate device memory themselves or let the library do it: processes whose device
+ * memory is reserved up front by another allocator (a cudaMalloc would fail or fragment that pool), and embedded
+ * hosts that forbid allocation after start-up.
  * blml_rows allocates its column-slice partial sums and its extent-check buffer stream-ordered on every call; this
  * entry point keeps them in a fixed 4 MiB device array inside the library instead (every GPU that loads the library
  * holds it until the process exits), so it takes at most 524,224 rows (R), and larger R is rejected with

@@ -1,8 +1,7 @@
 """blml_rows_noalloc, the pair-accumulation entry point that allocates nothing.
 
-Some callers of this library cannot allocate device memory: code running while a stream is captured into a CUDA
-graph (a cudaMalloc there breaks the capture), processes whose device memory another allocator reserves up front,
-and embedded hosts that forbid allocation after start-up. For them blml_rows_noalloc keeps its scratch in a fixed
+Some callers of this library cannot allocate device memory: processes whose device memory another allocator
+reserves up front, and embedded hosts that forbid allocation after start-up. For them blml_rows_noalloc keeps its scratch in a fixed
 device array inside the library. This test calls it through the C ABI and checks it against blml_rows on the same
 inputs (the same deterministic arithmetic: equal to 1e-12 of the largest sum), on two calls in a row, since every
 call reuses the one array. The file is named to run last."""
