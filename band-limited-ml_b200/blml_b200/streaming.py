@@ -1,20 +1,22 @@
-"""Counts arriving in batches on one fixed lattice, with kernel-parameter learning (rahuljhu/band-limited-ml,
-blml_binned.py:648-1112: _KernelLearner and BLMLBinnedStreaming), on the GPU engine of blml_b200.binned.
+"""Counts arriving in batches on one fixed lattice, with cut-off learning, on the GPU engine of blml_b200.binned.
 
-The state between batches is the fit's coefficients and S e in device memory. A batch is scored by the current model
-(its prequential score, log_density), then its gradient of that score in log fc (implicit_grad / param_grad: the
-derivative plans and Hessian-vector products of blml_b200.binned) is pooled, then it is added (held counts times
-decay plus the batch) and the coefficients are warm-refitted. Every param_every learning batches the trainable
-cut-offs take one Adam step on log fc (sinc / slits / ball) or one hill-climb step (dirichlet / pball harmonics, once
-the pooled paired gain of the candidate on the batches exceeds z_se standard errors). fit(batches, epochs) revisits
-held batches with leave-batch-out scores. An fc left out of the modes (NaN) is selected at the burn-in by the
-selector's search (blml_b200.selector.search) on an 80/20 split of the held counts.
+Behaviour (rahuljhu/band-limited-ml, blml_binned.py:648-1112, _KernelLearner and BLMLBinnedStreaming): each batch is
+scored by the current model before it is used (its prequential score), its gradient of that score in log fc is
+pooled, then it joins the held counts (old counts times `decay`) and the coefficients are warm-refitted. Every
+`param_every` learning batches the trainable cut-offs move: an Adam step on log fc for continuous bands (sinc,
+slits, ball), or a one-harmonic hill-climb step (dirichlet, pball) once the pooled paired gain of a neighbouring
+value exceeds z_se standard errors. `fit(batches, epochs)` revisits the held batches, scored with their own share left
+out. An fc left out of the modes (NaN) is chosen at the burn-in by the selector's search (blml_b200.selector.search)
+on an 80/20 split of the held counts.
 
-Every array operation runs in libblml_b200.so (the fit's kernels plus the bin-wise streaming kernels
-blml_counts_axpy, blml_bin_ratio, blml_new_bins and blml_gain_sums); the host keeps the control flow, the pooled
-gradients and the Adam / hill-climb state.
+Structure. The learner is its own object (`CutoffLearner`): a table of the trainable units and, per unit, array
+state -- Adam moments, pooled gradient rows, paired-gain sums of the two neighbouring candidates -- so the fit object
+never has to be snapshotted. Every what-if fit (a candidate cut-off, a batch left out) runs on a `probe`: a shallow
+fork of the streaming fit with its own kernels and coefficients that shares the device counts and the learner, then
+is dropped, so the stream's own state is never rewound. Every array operation runs in libblml_b200.so (the fit's
+kernels and the bin-wise kernels blml_counts_axpy, blml_bin_ratio, blml_new_bins, blml_gain_sums).
 """
-import contextlib
+import copy
 
 import numpy as np
 import torch
@@ -24,37 +26,136 @@ from .binned import BLMLBinned
 from .spec import parse_modes, modes_fc, units_of, split_kind, with_fc
 from . import selector as _sel
 
-INTEGER_KINDS = ('dirichlet', 'pball')       # fc moves in whole harmonics: hill-climb, no gradient
+HARMONIC_KINDS = ('dirichlet', 'pball')      # fc moves in whole harmonics: hill-climb, no gradient
 
 
 def adam_log_step(value, grad, state, lr, betas):
-    """One Adam ascent step on log(value) from grad = d/dlog value; state = [m, v, t] updated in place
-    (blml_maps.py:19-36, the 'scale' parameter type)."""
+    """One Adam ascent step on log(value) from grad = d/dlog value; state = [m, v, t] updated in place (the 'scale'
+    parameter rule of blml_maps.py:19-36). Returns the new value."""
     b1, b2 = betas
     state[2] += 1
-    t = state[2]
     state[0] = b1 * state[0] + (1 - b1) * grad
     state[1] = b2 * state[1] + (1 - b2) * grad * grad
-    step = lr * (state[0] / (1 - b1 ** t)) / (np.sqrt(state[1] / (1 - b2 ** t)) + 1e-12)
-    return value * np.exp(step)
+    m_hat = state[0] / (1 - b1 ** state[2])
+    v_hat = state[1] / (1 - b2 ** state[2])
+    return value * np.exp(lr * m_hat / (np.sqrt(v_hat) + 1e-12))
 
 
 def batch_order(nb, groups, rng):
-    """Batch indices in random group order (no groups: a random permutation), whole groups together
-    (blml_binned.py:1022-1031)."""
+    """The visiting order of nb batches: a random permutation, or (with group labels) the groups in random order,
+    each group's batches together in their given order (blml_binned.py:1022-1031)."""
     if groups is None:
         return list(rng.permutation(nb))
-    u, inv = np.unique(np.asarray(groups), return_inverse=True)
-    members = [[] for _ in u]
-    for i, k in enumerate(np.ravel(inv)):
-        members[k].append(i)
-    return [i for k in rng.permutation(len(u)) for i in members[k]]
+    labels = np.asarray(groups)
+    uniq, which = np.unique(labels, return_inverse=True)
+    order = rng.permutation(len(uniq))
+    return [int(i) for g in order for i in np.flatnonzero(np.ravel(which) == g)]
 
 
-def _fill(F, free, v):
-    F = F.copy()
-    F[free] = np.asarray(v, float)
-    return F
+def _welford_free(s, ss, W):
+    """(mean, standard error) of a weighted sample from its sums: sum x, sum x^2, total weight W > 1."""
+    mu = s / W
+    return mu, np.sqrt(max(ss / W - mu * mu, 0.0) / (W - 1))
+
+
+class CutoffLearner:
+    """The learning state of a stream. units: one row per trainable unit (mode k, unit u, its dims, whether fc moves
+    by Adam or by hill-climb); per unit the Adam moments, and for hill-climb units the pooled paired-gain sums
+    [s, ss, W] and candidate value of its two neighbours (index 0: up, 1: down). Gradients of the Adam units are
+    pooled per batch (count weight, one value per unit) until the next move, and kept for the epoch's stationarity
+    test."""
+
+    def __init__(self, specs, fc_update):
+        self.units = []
+        if fc_update is not None:
+            for k, sp in enumerate(specs):
+                for u, (kind, dims) in enumerate(units_of(sp['kinds'])):
+                    if bool(sp['fc_trainable'][dims[0]]):
+                        harmonic = split_kind(kind)[0] in HARMONIC_KINDS
+                        rule = 'adam' if (not harmonic and fc_update == 'adam') else 'hill'
+                        self.units.append(dict(k=k, u=u, dims=tuple(dims), harmonic=harmonic, rule=rule))
+        self.adam_idx = [i for i, e in enumerate(self.units) if e['rule'] == 'adam']
+        self.hill_idx = [i for i, e in enumerate(self.units) if e['rule'] == 'hill']
+        self.moments = np.zeros((len(self.units), 3))                 # Adam m, v, t
+        self.gains = np.zeros((len(self.units), 2, 3))                 # hill-climb s, ss, W per neighbour
+        self.cands = np.full((len(self.units), 2), np.nan)
+        self.pool_w, self.pool_g = [], []                               # since the last move
+        self.epoch_w, self.epoch_g = [], []                             # since the epoch began
+        self.n_learned = 0
+
+    def pool(self, weight, grads):
+        self.pool_w.append(float(weight)); self.pool_g.append(np.asarray(grads, float))
+        self.epoch_w.append(float(weight)); self.epoch_g.append(np.asarray(grads, float))
+
+    def add_gain(self, i, side, s, ss, W, cand):
+        self.gains[i, side] += (s, ss, W)
+        self.cands[i, side] = cand
+
+    def new_epoch(self):
+        self.epoch_w, self.epoch_g = [], []
+
+    def adam_moves(self, fc_of, cap_of, lr, betas):
+        """New values of the Adam units from the pooled count-weighted mean gradient, capped at their Nyquist
+        limit; clears the pool. Returns [(unit index, old, new)]."""
+        if not self.adam_idx or not self.pool_w:
+            self.pool_w, self.pool_g = [], []
+            return []
+        w = np.asarray(self.pool_w)
+        G = (w[:, None] * np.stack(self.pool_g)).sum(0) / w.sum()
+        self.pool_w, self.pool_g = [], []
+        if not np.all(np.isfinite(G)):
+            raise FloatingPointError(f"streaming: non-finite gradient {G}")
+        out = []
+        for q, i in enumerate(self.adam_idx):
+            old = fc_of(i)
+            new = min(float(adam_log_step(old, G[q], self.moments[i], lr, betas)), cap_of(i))
+            out.append((i, old, new))
+        return out
+
+    def hill_moves(self, z_se):
+        """The hill-climb units whose up or down neighbour's pooled gain is positive and beyond z_se standard
+        errors (the up side looked at first); their gain sums restart. Returns [(unit index, side, value)]."""
+        out = []
+        for i in self.hill_idx:
+            for side in (0, 1):
+                s, ss, W = self.gains[i, side]
+                if W <= 1:
+                    continue
+                mu, se = _welford_free(s, ss, W)
+                if mu > 0 and mu > z_se * se:
+                    out.append((i, side, float(self.cands[i, side])))
+                    self.gains[i] = 0.0; self.cands[i] = np.nan
+                    break
+        return out
+
+    def stationary(self, fc_of, cap_of, z_se):
+        """Whether the epoch's parameters are stationary (blml_binned.py:817-842): every Adam unit's count-weighted
+        mean gradient within z_se standard errors of zero (or positive at its cap) and no hill-climb move pending.
+        Returns (bool, the largest |mean| / se among the units that fail)."""
+        ok, zmax = True, 0.0
+        if self.adam_idx:
+            if not self.epoch_w:
+                ok = False
+            else:
+                w = np.asarray(self.epoch_w)
+                if len(w) < 2:
+                    return False, np.inf
+                G = np.stack([np.ravel(g) for g in self.epoch_g])
+                mu = (w[:, None] * G).sum(0) / w.sum()
+                se = np.sqrt((w[:, None] * (G - mu) ** 2).sum(0) / w.sum() / (len(w) - 1))
+                for q, i in enumerate(self.adam_idx):
+                    z = abs(mu[q]) / se[q] if se[q] > 0 else (0.0 if mu[q] == 0 else np.inf)
+                    at_cap = fc_of(i) >= cap_of(i) - 1e-12
+                    if not (z <= z_se or (at_cap and mu[q] > 0)):
+                        ok = False; zmax = max(zmax, z)
+        for i in self.hill_idx:
+            for side in (0, 1):
+                s, ss, W = self.gains[i, side]
+                if W > 1:
+                    mu, se = _welford_free(s, ss, W)
+                    if mu > 0 and mu > z_se * se:
+                        ok = False
+        return ok, zmax
 
 
 class BLMLBinnedStreaming(BLMLBinned):
@@ -70,387 +171,326 @@ class BLMLBinnedStreaming(BLMLBinned):
         if 'implicit' in kw:
             implicit_grad = kw.pop('implicit')
         super().__init__(**kw)
-        self._base_kw = dict(kw)
-        self.decay, self.batch_sweeps, self.loo_sweeps = decay, batch_sweeps, loo_sweeps
+        self._fit_kw = dict(kw)
         if fc_update not in (None, 'adam', 'hillclimb'):
             raise ValueError("fc_update: 'adam', 'hillclimb' or None")
         if search not in ('shared', 'refine'):
             raise ValueError("search: 'shared' or 'refine'")
         if not (0.0 < bcd_frac <= 1.0 and 0.0 <= freeze_frac < 1.0):
             raise ValueError("bcd_frac in (0, 1], freeze_frac in [0, 1)")
-        self.burn_in, self.fc_update, self.lr, self.betas, self.step, self.z_se = \
-            burn_in, fc_update, lr, betas, step, z_se
+        self.decay, self.batch_sweeps, self.loo_sweeps, self.burn_in = decay, batch_sweeps, loo_sweeps, burn_in
+        self.fc_update, self.lr, self.betas, self.step, self.z_se = fc_update, lr, betas, step, z_se
         self.param_every, self.grad_eps, self._implicit = max(1, int(param_every)), grad_eps, bool(implicit_grad)
         self.search, self.bcd_frac, self.freeze_frac = search, float(bcd_frac), float(freeze_frac)
         self.trace_trainable = trace_trainable
         self.preq_, self.history_ = [], []
-        self._n_learn, self._pool, self._hc, self._adam, self._epoch_g = 0, [], {}, {}, []
-        self._held, self._held_groups, self.n_batches_ = None, [], 0
+        self.learner_ = None
+        self._buffer = None                   # burn-in: (held sum, list of batches, their group labels, fit args)
+        self.n_batches_ = 0
         self.converged_ = self.epochs_ = self.residual_ = None
 
     @property
     def implicit(self):
         return self._implicit
 
-    def _base(self):
-        return BLMLBinned(**self._base_kw)
+    # ---------------------------------------------------------------- probes and device state
+    def _probe(self):
+        """A what-if copy of the fit: rebinding its attributes (kernels, specs, counts, coefficients) leaves this
+        fit untouched; it shares the device counts, the reduction buffers and the learner."""
+        return copy.copy(self)
 
-    # ---------------------------------------------------------------- device state
-    def _set_weights(self, w):
-        """The held counts w (device, fit dtype): n, c = n w and the occupied mask follow."""
+    def _hold_weights(self, w):
+        """The held counts w (device, fit dtype) with n, c = n w and the occupancy that follow."""
         self.w_t_ = w
         self.n_ = float(w.sum(dtype=torch.float64))
         self.c_t_ = self._lin([(self.n_, w)])
         self._occ_t = None
 
-    def _axpy(self, a, w, b, m, clamp=False):
+    def _blend(self, a, w, b, m, clamp=False):
+        """a w + b m per bin (clamped at 0), a new device array."""
         out = torch.empty_like(w)
         call('blml_counts_axpy', self._code, self.B_, float(a), w.data_ptr(), float(b), m.data_ptr(), int(clamp),
              out.data_ptr(), self._st)
         return out
 
-    def _refresh(self):
-        E = self.e_hat_t_.clone()
-        U = self._Sall(E)
-        E, U = self._rescale(E, U)
+    def _refit(self, E, sweeps):
+        E, U = self._solve(E, sweeps)
         self._finish(E, U)
 
-    def _residual(self):
-        return self._resid(self.e_hat_t_, self.Se_t_)
-
-    def _hill_sweeps(self):
+    def _what_if_sweeps(self):
         return self.loo_sweeps if self.loo_sweeps is not None else self.max_sweeps
 
-    def _candidate_refit(self):
-        E, U = self._solve(self.e_hat_t_, self._hill_sweeps())
-        self._finish(E, U)
+    def _without(self, counts):
+        """The probe with a batch's share taken out of the held counts (blml_binned.py:1068-1080): each bin's
+        coefficients scaled by its remaining share (w - m) / w, then a warm refit (loo_sweeps caps it). The held
+        counts unchanged when nothing would remain."""
+        p = self._probe()
+        m = p._counts_t(counts)
+        rest = p._blend(1.0, p.w_t_, -1.0, m, clamp=True)
+        if not float(rest.sum(dtype=torch.float64)) > 0:
+            return p
+        share = torch.empty_like(rest)
+        call('blml_bin_ratio', p._code, p.B_, rest.data_ptr(), p.w_t_.data_ptr(), share.data_ptr(), p._st)
+        p._hold_weights(rest)
+        E = torch.empty_like(p.e_hat_t_)
+        call('blml_mul_bins', p._code, E.shape[0], p.B_, int(E.is_complex()), p.e_hat_t_.data_ptr(), share.data_ptr(),
+             E.data_ptr(), p._st)
+        p._refit(E, p._what_if_sweeps())
+        return p
 
-    def _loo_enter(self, m):
-        """The fit with batch m left out (blml_binned.py:1068-1080): each bin's coefficient scaled by its remaining
-        share (w - m) / w, then a warm refit on the held counts less m (loo_sweeps: a cap on its sweeps)."""
-        mt = self._counts_t(m)
-        w = self._axpy(1.0, self.w_t_, -1.0, mt, clamp=True)
-        if not float(w.sum(dtype=torch.float64)) > 0:
-            return
-        f = torch.empty_like(w)
-        call('blml_bin_ratio', self._code, self.B_, w.data_ptr(), self.w_t_.data_ptr(), f.data_ptr(), self._st)
-        self._set_weights(w)
-        E = self.e_hat_t_
-        Ef = torch.empty_like(E)
-        call('blml_mul_bins', self._code, E.shape[0], self.B_, int(E.is_complex()), E.data_ptr(), f.data_ptr(),
-             Ef.data_ptr(), self._st)
-        E, U = self._solve(Ef, self._hill_sweeps())
-        self._finish(E, U)
+    def _with_fc(self, k, dims, value):
+        """The probe with mode k's fc on dims set to value, its kernels rebuilt and refitted warm."""
+        p = self._probe()
+        p._set_fc(k, dims, value)
+        p._build_kernels()
+        p._refit(p.e_hat_t_.clone(), p._what_if_sweeps())
+        return p
 
-    # ---------------------------------------------------------------- parameters
-    def _registry(self):
-        reg = []
-        if self.fc_update is None:
-            return reg
-        for k, sp in enumerate(self.specs_):
-            for u, (kind, dims) in enumerate(units_of(sp['kinds'])):
-                if not bool(sp['fc_trainable'][dims[0]]):
-                    continue
-                ptype = 'integer' if split_kind(kind)[0] in INTEGER_KINDS else 'scale'
-                rule = 'adam' if ptype == 'scale' and self.fc_update == 'adam' else 'hill'
-                reg.append(dict(mode=k, unit=u, dims=tuple(dims), ptype=ptype, rule=rule))
-        return reg
-
-    def _fc_now(self):
-        return [np.array(sp['fc'], float) for sp in self.specs_]
-
-    def _trainable_now(self):
-        return {k: {'fc': [float(v) for v, t in zip(sp['fc'], sp['fc_trainable']) if t]}
-                for k, sp in enumerate(self.specs_)}
-
+    # ---------------------------------------------------------------- cut-off values
     def _set_fc(self, k, dims, value):
         fc = np.array(self.specs_[k]['fc'], float)
         fc[list(dims)] = value
         self.specs_ = [dict(sp, fc=fc) if j == k else sp for j, sp in enumerate(self.specs_)]
 
-    def _nyq(self, e):
-        """The largest identifiable value: fc <= 0.5 / h (the lattice's Nyquist limit, blml_binned.py:772-775)."""
-        return 0.5 / float(self.h_[e['dims'][0]])
+    def _fc_of(self, i):
+        e = self.learner_.units[i]
+        return float(self.specs_[e['k']]['fc'][e['dims'][0]])
 
-    def _in_range(self, e, value):
-        return 0.0 < value <= self._nyq(e) + 1e-12
+    def _cap_of(self, i):
+        """The largest identifiable cut-off of a unit: 0.5 / h, the lattice's Nyquist limit (blml_binned.py:772-775)."""
+        return 0.5 / float(self.h_[self.learner_.units[i]['dims'][0]])
 
-    def _keep_pools(self, saved):
-        pools = (self._pool, self._hc, self._adam, self._epoch_g)
-        self.__dict__.clear()
-        self.__dict__.update(saved)
-        self._pool, self._hc, self._adam, self._epoch_g = pools
+    def _neighbour(self, i, side):
+        """The hill-climb candidate of unit i on one side (0 up, 1 down): one harmonic more / less, at the middle of
+        its fc interval (N = floor(fc P / 2) +- 1, fc = (N + 1/2) 2 / P), or fc times step^+-1; None off range."""
+        e = self.learner_.units[i]
+        v = self._fc_of(i)
+        sgn = 1 if side == 0 else -1
+        if e['harmonic']:
+            P = float(self.specs_[e['k']]['periods'][e['dims'][0]])
+            N = int(np.floor(v * P / 2.0)) + sgn
+            if N < 0:
+                return None
+            cand = (N + 0.5) * 2.0 / P
+        else:
+            cand = v * self.step ** sgn
+        return cand if 0.0 < cand <= self._cap_of(i) + 1e-12 else None
 
-    def _candidate_fit(self, e, cand):
-        """(density, scale) of the fit with e's parameter at cand: the kernel swapped and a warm refit of the held
-        counts (blml_binned.py:777-789); F / Z = density * scale."""
-        saved = dict(self.__dict__)
-        try:
-            self._set_fc(e['mode'], e['dims'], cand)
-            self._build_kernels()
-            self._candidate_refit()
-            Z = self._Q(self.e_hat_t_, self.Se_t_)
-            return self.density_t_, self.n_ ** 2 / Z
-        finally:
-            self._keep_pools(saved)
+    def _trainable_values(self):
+        return {k: {'fc': [float(v) for v, t in zip(sp['fc'], sp['fc_trainable']) if t]}
+                for k, sp in enumerate(self.specs_)}
 
-    def _learn(self, counts):
-        """The batch's gradient (pooled) and hill-climb gains before it is added (blml_binned.py:737-770)."""
+    # ---------------------------------------------------------------- learning from one batch
+    def _gather(self, counts):
+        """The batch's contribution to the learner before it joins the held counts (blml_binned.py:737-770): the
+        Adam units' score gradient (implicit or at fixed coefficients) pooled with the batch's count as weight, and
+        for each hill-climb unit the paired gain of both neighbours' refits on the batch."""
+        L = self.learner_
         m = np.asarray(counts, float)
-        occ = m.ravel() > 0
+        on = m.ravel() > 0
         Z0 = self._Q(self.e_hat_t_, self.Se_t_)
-        n2 = self.n_ ** 2
-        eps = self.grad_eps * n2 * float(np.median(self.density_.ravel()[occ])) / Z0 if occ.any() else 0.0
-        reg = self._registry()
-        adam = [e for e in reg if e['rule'] == 'adam']
-        if adam:
+        nn = self.n_ ** 2
+        eps = self.grad_eps * nn * float(np.median(self.density_.ravel()[on])) / Z0 if on.any() else 0.0
+        if L.adam_idx:
             G = self.implicit_grad(m, eps) if self._implicit else self.param_grad(m, eps)
-            self._pool.append((float(m.sum()), [G[e['mode']][e['unit']] for e in adam]))
-            self._epoch_g.append(self._pool[-1])
-        hill = [e for e in reg if e['rule'] == 'hill']
-        if not hill:
+            L.pool(m.sum(), [G[L.units[i]['k']][L.units[i]['u']] for i in L.adam_idx])
+        if not L.hill_idx:
             return
         mt = self._counts_t(m)
-        d0, s0 = self.density_t_, n2 / Z0
-        for e in hill:
-            k, dims = e['mode'], list(e['dims'])
-            v = float(self.specs_[k]['fc'][dims[0]])
-            for sgn in (+1, -1):
-                if e['ptype'] == 'integer':       # one harmonic, N = floor(fc P / 2) +- 1, at its interval's middle
-                    P = float(self.specs_[k]['periods'][dims[0]])
-                    N = int(np.floor(v * P / 2.0)) + sgn
-                    if N < 0:
-                        continue
-                    cand = (N + 0.5) * 2.0 / P
-                else:
-                    cand = v * self.step ** sgn
-                if not self._in_range(e, cand):
+        for i in L.hill_idx:
+            e = L.units[i]
+            for side in (0, 1):
+                cand = self._neighbour(i, side)
+                if cand is None:
                     continue
-                dc, sc = self._candidate_fit(e, cand)
-                call('blml_gain_sums', self._code, self.B_, dc.data_ptr(), float(sc), d0.data_ptr(), float(s0),
-                     mt.data_ptr(), float(eps), self._red.part.data_ptr(), self._red.out.data_ptr(), self._st)
-                s, ss, W = self._red.read(3)
-                acc = self._hc.setdefault((k, e['unit'], sgn), dict(s=0.0, ss=0.0, W=0.0, cand=cand))
-                acc['s'] += s; acc['ss'] += ss; acc['W'] += W; acc['cand'] = cand
+                p = self._with_fc(e['k'], e['dims'], cand)
+                zp = p._Q(p.e_hat_t_, p.Se_t_)
+                call('blml_gain_sums', self._code, self.B_, p.density_t_.data_ptr(), float(p.n_ ** 2 / zp),
+                     self.density_t_.data_ptr(), float(nn / Z0), mt.data_ptr(), float(eps), self._red.part.data_ptr(),
+                     self._red.out.data_ptr(), self._st)
+                L.add_gain(i, side, *self._red.read(3), cand)
 
-    def _param_step(self):
-        """Every param_every learning batches (blml_binned.py:791-815): Adam on the pooled, count-weighted
-        gradients; a hill-climb move once its pooled gain exceeds z_se standard errors. Returns what moved."""
-        reg = self._registry()
+    def _move(self):
+        """A parameter step (blml_binned.py:791-815): the Adam units' new values, then at most one hill-climb move
+        per unit; the kernels rebuilt and the fit refreshed when anything moved. Returns the moves as
+        (mode, unit, log ratio) for Adam and (mode, unit, +-1) for hill-climb."""
+        L = self.learner_
         moved = []
-        adam = [e for e in reg if e['rule'] == 'adam']
-        if adam and self._pool:
-            Wt = sum(p[0] for p in self._pool)
-            G = sum(p[0] * np.asarray(p[1], float) for p in self._pool) / Wt
-            if not np.all(np.isfinite(G)):
-                raise FloatingPointError(f"streaming: non-finite gradient {G}")
-            for q, e in enumerate(adam):
-                k, dims = e['mode'], e['dims']
-                old = float(self.specs_[k]['fc'][dims[0]])
-                st = self._adam.setdefault((k, e['unit']), [0.0, 0.0, 0])
-                new = min(float(adam_log_step(old, G[q], st, self.lr, self.betas)), self._nyq(e))
-                self._set_fc(k, dims, new)
-                moved.append((k, e['unit'], round(float(np.log(new / old)), 5)))
-        self._pool = []
-        for e in (e for e in reg if e['rule'] == 'hill'):
-            for sgn in (+1, -1):
-                acc = self._hc.get((e['mode'], e['unit'], sgn))
-                if not acc or acc['W'] <= 1:
-                    continue
-                mu = acc['s'] / acc['W']
-                se = np.sqrt(max(acc['ss'] / acc['W'] - mu * mu, 0.0) / (acc['W'] - 1))
-                if mu > 0 and mu > self.z_se * se:
-                    self._set_fc(e['mode'], e['dims'], acc['cand'])
-                    moved.append((e['mode'], e['unit'], sgn))
-                    self._hc = {kk: v for kk, v in self._hc.items() if kk[:2] != (e['mode'], e['unit'])}
-                    break
+        for i, old, new in L.adam_moves(self._fc_of, self._cap_of, self.lr, self.betas):
+            e = L.units[i]
+            self._set_fc(e['k'], e['dims'], new)
+            moved.append((e['k'], e['u'], round(float(np.log(new / old)), 5)))
+        for i, side, value in L.hill_moves(self.z_se):
+            e = L.units[i]
+            self._set_fc(e['k'], e['dims'], value)
+            moved.append((e['k'], e['u'], 1 if side == 0 else -1))
         if moved:
             self._build_kernels()
-            self._refresh()
+            E = self.e_hat_t_.clone()
+            E, U = self._rescale(E, self._Sall(E))
+            self._finish(E, U)
         return moved
 
-    def _param_stationary(self):
-        """Whether the epoch's parameters are stationary (blml_binned.py:817-842): each Adam parameter's
-        count-weighted mean gradient within z_se standard errors of 0, or > 0 at the Nyquist cap, and no pending
-        hill-climb move. Returns (bool, max |mean| / se)."""
-        reg = self._registry()
-        adam = [e for e in reg if e['rule'] == 'adam']
-        zmax = 0.0
-        if adam and self._epoch_g:
-            W = np.array([p[0] for p in self._epoch_g])
-            G = np.array([np.ravel(np.asarray(p[1], float)) for p in self._epoch_g])
-            if len(W) < 2:
-                return False, np.inf
-            mu = (W[:, None] * G).sum(0) / W.sum()
-            var = (W[:, None] * (G - mu) ** 2).sum(0) / W.sum()
-            se = np.sqrt(var / (len(W) - 1))
-            ok = True
-            for q, e in enumerate(adam):
-                at_cap = float(self.specs_[e['mode']]['fc'][e['dims'][0]]) >= self._nyq(e) - 1e-12
-                z = abs(mu[q]) / se[q] if se[q] > 0 else (0.0 if mu[q] == 0 else np.inf)
-                if not (z <= self.z_se or (at_cap and mu[q] > 0)):
-                    ok = False
-                    zmax = max(zmax, z)
-        else:
-            ok = not adam
-        for acc in self._hc.values():
-            if acc['W'] > 1:
-                mu = acc['s'] / acc['W']
-                se = np.sqrt(max(acc['ss'] / acc['W'] - mu * mu, 0.0) / (acc['W'] - 1))
-                if mu > 0 and mu > self.z_se * se:
-                    ok = False
-        return ok, zmax
-
-    # ---------------------------------------------------------------- one batch
-    def _left_out(self, counts):
-        """Context: the fit with counts' share of the held counts removed (None: unchanged), restored after; the
-        gradients and gains gathered inside are kept (blml_binned.py:871-888)."""
-        @contextlib.contextmanager
-        def ctx():
-            if counts is None:
-                yield
-                return
-            saved = dict(self.__dict__)
-            try:
-                self._loo_enter(np.asarray(counts, float))
-                yield
-            finally:
-                self._keep_pools(saved)
-        return ctx()
-
-    def _stream_step(self, counts, absorb, revisit=False, learn=True):
-        """Score (leave-batch-out on a revisit) and learn after the burn-in, absorb, then a parameter step every
-        param_every learning batches (blml_binned.py:850-868)."""
-        burned = self.n_ >= self.burn_in
-        do_learn = learn and burned and self.fc_update is not None
-        with self._left_out(counts if revisit else None):
-            preq = self.log_density(counts)
-            if do_learn:
-                self._learn(counts)
-        if absorb is not None:
-            absorb(burned)
-        moved = []
-        if do_learn:
-            self._n_learn += 1
-            if self._n_learn % self.param_every == 0:
-                moved = self._param_step()
+    def _record(self, preq, moved, revisit):
         self.preq_.append(preq)
-        h = dict(n=self.n_, preq=preq, fc=[f.tolist() for f in self._fc_now()], moved=moved, revisit=bool(revisit))
+        entry = dict(n=self.n_, preq=preq, fc=[np.array(sp['fc'], float).tolist() for sp in self.specs_], moved=moved,
+                     revisit=bool(revisit))
         if self.trace_trainable:
-            h['trainable'] = self._trainable_now()
-        self.history_.append(h)
+            entry['trainable'] = self._trainable_values()
+        self.history_.append(entry)
+
+    def _visit(self, counts, join, revisit=False, learn=True):
+        """One batch after the burn-in (blml_binned.py:850-868): scored -- on a revisit by the fit without its own
+        share -- and gathered for learning, then joined (join(burned) changes the fit), then a parameter step every
+        param_every learning batches."""
+        burned = self.n_ >= self.burn_in
+        learning = learn and burned and self.fc_update is not None
+        judge = self._without(counts) if revisit else self
+        preq = judge.log_density(counts)
+        if learning:
+            judge._gather(counts)
+        if join is not None:
+            join(burned)
+        moved = []
+        if learning:
+            self.learner_.n_learned += 1
+            if self.learner_.n_learned % self.param_every == 0:
+                moved = self._move()
+        self._record(preq, moved, revisit)
+
+    def _sweeps(self, burned):
+        return self.batch_sweeps if (self.batch_sweeps is not None and burned) else self.max_sweeps
+
+    def _join_new(self, counts):
+        """Add a batch: held counts times decay plus the batch, the same roots rescaled to the new n, newly occupied
+        bins given their own coordinate root, then the warm refit."""
+        def join(burned):
+            mt = self._counts_t(counts)
+            n_was = self.n_
+            self._hold_weights(self._blend(self.decay, self.w_t_, 1.0, mt))
+            E = self._mask_(self._lin([(self.n_ / n_was, self.e_hat_t_)]))
+            Eu = self._update(E, self._Sall(E))
+            call('blml_new_bins', self._code, E.shape[0], self.B_, int(E.is_complex()), E.data_ptr(), Eu.data_ptr(),
+                 self.w_t_.data_ptr(), E.data_ptr(), self._st)
+            self._refit(E, self._sweeps(burned))
+        return join
+
+    def _join_again(self):
+        """A held batch revisited: the coefficients swept again on the unchanged held counts."""
+        def join(burned):
+            self._refit(self.e_hat_t_, self._sweeps(burned))
+        return join
 
     # ---------------------------------------------------------------- burn-in
-    def _hold(self, counts, modes, h, origin, complex_g, group):
-        if self._held is None:
+    def _buffer_batch(self, counts, modes, h, origin, complex_g, group):
+        """Keep a burn-in batch; True once the held counts reach burn_in."""
+        if self._buffer is None:
             if modes is None:
                 raise ValueError("partial_fit: modes on the first call")
-            self._modes_args = (modes, h, origin, complex_g)
-            self._held = counts.copy()
-            self._held_list = [counts]
+            self._buffer = dict(total=counts.copy(), batches=[counts], groups=[group],
+                                args=(modes, h, origin, complex_g))
         else:
-            if counts.shape != self._held.shape:
+            if counts.shape != self._buffer['total'].shape:
                 raise ValueError("partial_fit: the batch must be on the lattice of the first one")
-            self._held = self._held + counts
-            self._held_list.append(counts)
-        self._held_groups.append(group)
-        return float(self._held.sum()) >= self.burn_in
+            self._buffer['total'] = self._buffer['total'] + counts
+            self._buffer['batches'].append(counts); self._buffer['groups'].append(group)
+        return float(self._buffer['total'].sum()) >= self.burn_in
 
-    def _select(self):
-        """The selector's search for the fc entries the modes leave out (NaN), on the held counts: an 80/20 binomial
-        split, or 20% of whole groups for validation (blml_binned.py:904-940)."""
-        modes, h, origin, cg = self._modes_args
-        F = modes_fc(modes)
-        free = ~np.isfinite(F)
-        if not free.any():
+    def _choose_missing_fc(self):
+        """The selector's search for the fc entries the modes leave out (NaN) on the held counts (blml_binned.py:
+        904-940): trained on 80% of them (a binomial split, or 80% of whole groups when every batch has a group) and
+        scored on the rest."""
+        buf = self._buffer
+        modes, h, origin, cg = buf['args']
+        fc_all = modes_fc(modes)
+        missing = ~np.isfinite(fc_all)
+        if not missing.any():
             return modes
-        specs = parse_modes(modes, self._held.ndim, need_fc=False)[0]
+        total = buf['total']
+        specs = parse_modes(modes, total.ndim, need_fc=False)[0]
         rng = np.random.default_rng(self.seed)
-        groups = list(self._held_groups)
+        groups = buf['groups']
         if all(g is not None for g in groups):
-            u = np.unique(groups)
-            V = rng.choice(u, max(1, int(round(0.2 * len(u)))), replace=False)
-            tr = sum((b for b, g in zip(self._held_list, groups) if g not in V), np.zeros(self._held.shape))
-            va = sum((b for b, g in zip(self._held_list, groups) if g in V), np.zeros(self._held.shape))
+            labels = np.unique(groups)
+            held_out = rng.choice(labels, max(1, int(round(0.2 * len(labels)))), replace=False)
+            train = np.zeros(total.shape); valid = np.zeros(total.shape)
+            for b, g in zip(buf['batches'], groups):
+                if g in held_out:
+                    valid = valid + b
+                else:
+                    train = train + b
         else:
-            if not np.allclose(self._held, np.round(self._held)):
+            if not np.allclose(total, np.round(total)):
                 raise ValueError("burn-in selection: integer counts for the binomial split (or pass split_groups)")
-            tr = rng.binomial(np.round(self._held).astype(np.int64), 0.8).astype(float)
-            va = self._held - tr
-        idx = np.argwhere(free)
-        kinds = [specs[k]['kinds'][j].split(':')[0] for k, j in idx]
-        hh = np.broadcast_to(np.asarray(h, float), (self._held.ndim,))
-        periods = [None if specs[k]['periods'][j] is None else specs[k]['periods'][j] / hh[j] for k, j in idx]
+            train = rng.binomial(np.round(total).astype(np.int64), 0.8).astype(float)
+            valid = total - train
+        where = np.argwhere(missing)
+        kinds = [specs[k]['kinds'][j].split(':')[0] for k, j in where]
+        hv = np.broadcast_to(np.asarray(h, float), (total.ndim,))
+        periods = [None if specs[k]['periods'][j] is None else specs[k]['periods'][j] / hv[j] for k, j in where]
+        caps = 0.5 / hv[where[:, 1]] + 1e-12
 
-        def obj(v):
-            if np.any(np.asarray(v) > 0.5 / hh[idx[:, 1]] + 1e-12):
+        def filled(v):
+            out = fc_all.copy()
+            out[missing] = np.asarray(v, float)
+            return out
+
+        def score(v):
+            if np.any(np.asarray(v) > caps):
                 return -np.inf
             try:
-                mm = self._base().fit(tr, with_fc(modes, _fill(F, free, v)), h=h, origin=origin, complex_g=cg)
+                f = BLMLBinned(**self._fit_kw).fit(train, with_fc(modes, filled(v)), h=h, origin=origin, complex_g=cg)
             except (ValueError, FloatingPointError, np.linalg.LinAlgError):
                 return -np.inf
-            return mm._val_score(va)
-        fc0 = 2.0 / (max(self._held.shape) * float(np.max(hh)))
-        v, _ = _sel.search(obj, len(idx), kinds, periods, fc0=fc0, max_sweeps=0 if self.search == 'shared' else 6,
+            return f._val_score(valid)
+
+        start = 2.0 / (max(total.shape) * float(np.max(hv)))
+        v, _ = _sel.search(score, len(where), kinds, periods, fc0=start, max_sweeps=0 if self.search == 'shared' else 6,
                            tag='burn-in', factors=(np.sqrt(2.0), 2.0 ** 0.25, 2.0 ** 0.125))
-        return with_fc(modes, _fill(F, free, v))
+        return with_fc(modes, filled(v))
+
+    def _first_fit(self):
+        """The burn-in's end: the missing fc chosen, the fit of the held counts (capped at batch_sweeps when there
+        is no burn-in), the learner set up on its modes."""
+        modes = self._choose_missing_fc()
+        _, h, origin, complex_g = self._buffer['args']
+        cap, self.max_sweeps = self.max_sweeps, (self.batch_sweeps if (self.batch_sweeps is not None and
+                                                                        not self.burn_in) else self.max_sweeps)
+        try:
+            BLMLBinned.fit(self, self._buffer['total'], modes, h, origin, complex_g)
+        finally:
+            self.max_sweeps = cap
+        self.learner_ = CutoffLearner(self.specs_, self.fc_update)
+        self._buffer = dict(args=self._buffer['args'])
+        self.n_batches_ = 1
+        self.history_.append(dict(n=self.n_, preq=np.nan, fc=[np.array(sp['fc'], float).tolist()
+                                                              for sp in self.specs_], moved=[], burn_in=True))
+        self.preq_.append(np.nan)
 
     # ---------------------------------------------------------------- public
     def partial_fit(self, counts, modes=None, h=1.0, origin=0.0, complex_g=False, split_groups=None, _learn=True):
         counts = np.asarray(counts, float)
         if self.n_batches_ == 0:
-            if not self._hold(counts, modes, h, origin, complex_g, split_groups):
-                return self
-            modes = self._select()
-            _, h, origin, complex_g = self._modes_args
-            cap = self.max_sweeps
-            if self.batch_sweeps is not None and not self.burn_in:
-                self.max_sweeps = self.batch_sweeps
-            BLMLBinned.fit(self, self._held, modes, h, origin, complex_g)
-            self.max_sweeps = cap
-            self.n_batches_ = 1
-            self._held_list = None
-            self.history_.append(dict(n=self.n_, preq=np.nan, fc=[f.tolist() for f in self._fc_now()], moved=[],
-                                      burn_in=True))
-            self.preq_.append(np.nan)
+            if self._buffer_batch(counts, modes, h, origin, complex_g, split_groups):
+                self._first_fit()
             return self
         if counts.shape != self.shape_:
             raise ValueError("partial_fit: the batch must be on the lattice of the first one")
-
-        def absorb(burned):
-            mt = self._counts_t(counts)
-            n_old = self.n_
-            self._set_weights(self._axpy(self.decay, self.w_t_, 1.0, mt))
-            E = self._mask_(self._lin([(self.n_ / n_old, self.e_hat_t_)]))     # same g; _solve rescales Q = n^2
-            U = self._Sall(E)
-            Eu = self._update(E, U)
-            call('blml_new_bins', self._code, E.shape[0], self.B_, int(E.is_complex()), E.data_ptr(), Eu.data_ptr(),
-                 self.w_t_.data_ptr(), E.data_ptr(), self._st)                 # newly occupied bins: their own root
-            sweeps = self.batch_sweeps if (self.batch_sweeps is not None and burned) else self.max_sweeps
-            E, U = self._solve(E, sweeps)
-            self._finish(E, U)
-
-        self._stream_step(counts, absorb, learn=_learn)
+        self._visit(counts, self._join_new(counts), learn=_learn)
         self.n_batches_ += 1
         return self
-
-    def _again(self, counts, learn=True):
-        """A held batch revisited: scored leave-batch-out, its gradient pooled, the coefficients swept (not added)."""
-        def absorb(burned):
-            sweeps = self.batch_sweeps if (self.batch_sweeps is not None and burned) else self.max_sweeps
-            E, U = self._solve(self.e_hat_t_, sweeps)
-            self._finish(E, U)
-        self._stream_step(counts, absorb, revisit=True, learn=learn)
 
     def fit(self, batches, modes=None, epochs=2, h=1.0, origin=0.0, complex_g=False, split_groups=None, on_epoch=None,
             tol=None, tol_check='running'):
         """batches: count arrays on one lattice. Epoch 1 adds them in random group order; later epochs revisit them
         (scored leave-batch-out, the coefficients swept, the parameters moving); tol stops after the first epoch
-        whose fit meets the solver's residual test with the parameters stationary (blml_binned.py:942-1011)."""
+        whose fit meets the solver's residual test with the parameters stationary (blml_binned.py:942-1011).
+        bcd_frac < 1 keeps a binomial 1 - bcd_frac share of each batch for learning only (scored and gathered, not
+        joined) until freeze_frac of the visits are done, when the shares join the fit."""
         batches = [np.asarray(b, float) for b in batches]
         nb = len(batches)
-        grp = None if split_groups is None else list(np.asarray(split_groups).tolist())
-        if grp is not None and len(grp) != nb:
+        labels = None if split_groups is None else list(np.asarray(split_groups).tolist())
+        if labels is not None and len(labels) != nb:
             raise ValueError("split_groups: one label per batch")
         if tol is not None and not tol > 0:
             raise ValueError("tol: None (fixed epochs) or > 0")
@@ -462,41 +502,45 @@ class BLMLBinnedStreaming(BLMLBinned):
         if split:
             if not all(np.allclose(b, np.round(b)) for b in batches):
                 raise ValueError("bcd_frac < 1: integer counts (the learn share is a binomial thinning)")
-            r0 = np.random.default_rng([self.seed, 11])
-            L = [r0.binomial(np.round(b).astype(np.int64), 1.0 - self.bcd_frac).astype(float) for b in batches]
-        held, joined = [False] * nb, [False] * nb
-        T_learn = int(round((1.0 - self.freeze_frac) * epochs * nb))
-        t = 0
+            rs = np.random.default_rng([self.seed, 11])
+            learn_part = [rs.binomial(np.round(b).astype(np.int64), 1.0 - self.bcd_frac).astype(float) for b in batches]
+        added = np.zeros(nb, bool); shares_in = np.zeros(nb, bool)
+        learn_visits = int(round((1.0 - self.freeze_frac) * epochs * nb))
+        visit = 0
         self.converged_, self.epochs_, self.residual_ = None, 0, None
-        first = dict(modes=modes, h=h, origin=origin, complex_g=complex_g)
+        first_args = dict(modes=modes, h=h, origin=origin, complex_g=complex_g)
         for ep in range(epochs):
-            run_max = 0.0
-            self._epoch_g = []
-            for i in batch_order(nb, grp, np.random.default_rng(self.seed + ep)):
-                frozen = t >= T_learn
-                t += 1
-                both = not split and not frozen
-                Fi = batches[i] if (not split or frozen) else batches[i] - L[i]
-                if not held[i]:
-                    self.partial_fit(Fi, split_groups=None if grp is None else grp[i], _learn=both and not frozen,
-                                     **first)
-                    held[i] = True
-                    first = {}
+            worst = 0.0
+            if self.learner_ is not None:
+                self.learner_.new_epoch()
+            for i in batch_order(nb, labels, np.random.default_rng(self.seed + ep)):
+                frozen = visit >= learn_visits
+                visit += 1
+                whole = not split and not frozen
+                part = batches[i] if (not split or frozen) else batches[i] - learn_part[i]
+                if not added[i]:
+                    self.partial_fit(part, split_groups=None if labels is None else labels[i],
+                                     _learn=whole, **first_args)
+                    added[i] = True
+                    first_args = {}
                 elif self.n_batches_ > 0:
-                    run_max = max(run_max, self._residual())
-                    self._again(Fi, learn=both)
+                    worst = max(worst, self._resid(self.e_hat_t_, self.Se_t_))
+                    self._visit(part, self._join_again(), revisit=True, learn=whole)
                 if split and not frozen and self.n_batches_ > 0:
-                    self._stream_step(L[i], None, learn=True)            # scored, gradient pooled, not added
-                if split and frozen and not joined[i] and self.n_batches_ > 0:
-                    self.partial_fit(L[i], _learn=False)
-                    joined[i] = True
+                    self._visit(learn_part[i], None, learn=True)             # scored and gathered, not joined
+                if split and frozen and not shares_in[i] and self.n_batches_ > 0:
+                    self.partial_fit(learn_part[i], _learn=False)
+                    shares_in[i] = True
             if self.n_batches_ == 0:
                 raise ValueError(f"fit: burn_in = {self.burn_in} exceeds the counts given "
                                  f"({sum(float(b.sum()) for b in batches):g})")
             self.epochs_ = ep + 1
             if tol is not None and (tol_check == 'exact' or ep > 0):
-                self.residual_ = self._residual() if tol_check == 'exact' else run_max
-                still, z = self._param_stationary() if self.fc_update is not None else (True, 0.0)
+                self.residual_ = self._resid(self.e_hat_t_, self.Se_t_) if tol_check == 'exact' else worst
+                if self.fc_update is not None:
+                    still, z = self.learner_.stationary(self._fc_of, self._cap_of, self.z_se)
+                else:
+                    still, z = True, 0.0
                 self.converged_ = bool(self.residual_ < tol and still)
                 self.history_.append(dict(epoch=ep + 1, residual=self.residual_, params_stationary=still, grad_z=z))
             if on_epoch is not None:
