@@ -16,6 +16,7 @@
 // rounds like an FFT (~1e-16 log M relative), so the route changes no result beyond rounding.
 #include <vector>
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include "plan.cuh"
 
@@ -241,16 +242,70 @@ __device__ __forceinline__ void rows_inv_body(const FftDesc& D, int cta, unsigne
   }
 }
 
-#define FFT_STAGE(NAME, BODY, NCTAS)                                                                              \
+// The grouped launches cover only the work of the problems taking part: k_fft_schedule (one block) lists the
+// problems of the launch (subset[i], or i), drops those with live == 0, and writes the exclusive prefix sums of
+// their CTA counts for stages A / C and B; CTA x of a stage finds its problem by binary search over those sums
+// and returns at once when x is past the total. The grid is the host's bound: the sum of the n largest counts.
+constexpr int kSchedMax = 2048;          // problems a schedule takes (a launch over more runs in chunks of 2048)
+
+struct FftSched {
+  int n;                                 // problems in the schedule
+  int prob[kSchedMax];                   // their indices
+  int offA[kSchedMax + 1], offB[kSchedMax + 1];
+};
+
+__global__ void k_fft_schedule(const FftDesc* __restrict__ descs, const int* __restrict__ subset, int n0, int n,
+                               const int* __restrict__ live, FftSched* sch) {
+  __shared__ int cA[kSchedMax], cB[kSchedMax], pr[kSchedMax];
+  __shared__ int wsA[32], wsB[32];
+  const int tid = threadIdx.x;
+  for (int i = tid; i < n; i += blockDim.x) {
+    const int g = subset ? subset[n0 + i] : n0 + i;
+    const bool on = !live || live[g];
+    pr[i] = g; cA[i] = on ? descs[g].ctasA : 0; cB[i] = on ? descs[g].ctasB : 0;
+  }
+  __syncthreads();
+  if (tid < 32) {                        // one warp: a serial scan per lane chunk, then a warp scan of the chunk sums
+    const int per = (n + 31) / 32, lo = tid * per, hi = min(n, lo + per);
+    int sa = 0, sb = 0;
+    for (int i = lo; i < hi; i++) { sa += cA[i]; sb += cB[i]; }
+    int xa = sa, xb = sb;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ya = __shfl_up_sync(0xffffffffu, xa, o), yb = __shfl_up_sync(0xffffffffu, xb, o);
+      if (tid >= o) { xa += ya; xb += yb; }
+    }
+    wsA[tid] = xa - sa; wsB[tid] = xb - sb;
+    int ra = wsA[tid], rb = wsB[tid];
+    for (int i = lo; i < hi; i++) {
+      sch->offA[i] = ra; sch->offB[i] = rb; sch->prob[i] = pr[i];
+      ra += cA[i]; rb += cB[i];
+    }
+    if (tid == 31) { sch->offA[n] = xa; sch->offB[n] = xb; sch->n = n; }
+  }
+}
+
+// the problem and local CTA index of CTA x in a schedule (offsets off[0 .. n]), or -1 past the total
+__device__ __forceinline__ int sched_find(const int* off, int n, int x, int& local) {
+  if (x >= off[n]) return -1;
+  int lo = 0, hi = n - 1;                // the last i with off[i] <= x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= x) lo = mid; else hi = mid - 1;
+  }
+  local = x - off[lo];
+  return lo;
+}
+
+#define FFT_STAGE(NAME, BODY, OFF)                                                                                \
   template <typename T>                                                                                          \
   __global__ void __launch_bounds__(kFT) NAME##_grp(const FftDesc* __restrict__ descs,                           \
-                                                    const int* __restrict__ subset, const int* __restrict__ live) { \
+                                                    const FftSched* __restrict__ sch) {                          \
     extern __shared__ __align__(16) unsigned char fft_smem[];                                                    \
-    const int gi = subset ? subset[blockIdx.z] : (int)blockIdx.z;                                                \
-    if (live && !live[gi]) return;                                                                               \
-    const FftDesc D = descs[gi];                                                                                 \
-    if ((int)blockIdx.x >= D.NCTAS) return;                                                                      \
-    BODY<T>(D, blockIdx.x, fft_smem);                                                                            \
+    int local = 0;                                                                                               \
+    const int i = sched_find(sch->OFF, sch->n, (int)blockIdx.x, local);                                          \
+    if (i < 0) return;                                                                                           \
+    const FftDesc D = descs[sch->prob[i]];                                                                       \
+    BODY<T>(D, local, fft_smem);                                                                                 \
   }                                                                                                              \
   template <typename T>                                                                                          \
   __global__ void __launch_bounds__(kFT) NAME##_one(const FftDesc D) {                                           \
@@ -258,9 +313,9 @@ __device__ __forceinline__ void rows_inv_body(const FftDesc& D, int cta, unsigne
     BODY<T>(D, blockIdx.x, fft_smem);                                                                            \
   }
 
-FFT_STAGE(k_fft_rows_fwd, rows_fwd_body, ctasA)
-FFT_STAGE(k_fft_cols, cols_body, ctasB)
-FFT_STAGE(k_fft_rows_inv, rows_inv_body, ctasA)
+FFT_STAGE(k_fft_rows_fwd, rows_fwd_body, offA)
+FFT_STAGE(k_fft_cols, cols_body, offB)
+FFT_STAGE(k_fft_rows_inv, rows_inv_body, offA)
 
 // ------------------------------------------------------------------------------------------------- host side
 // radices of an N = 2^a 3^b point FFT: 8s, then a 4 or 2, then 3s, a 2 and a 3 merged into a 6 (fewest passes); 0
@@ -366,7 +421,8 @@ static FftDesc make_desc(const blml_plan_s* p, const void* x, void* y, void* z, 
 
 struct FftGroup {
   FftDesc* dev;                  // G descriptors
-  int maxA, maxB;                // largest CTA count of a problem in stages A / C and B
+  FftSched* sch;                 // the schedule of the current launch (written by k_fft_schedule)
+  std::vector<int> boundA, boundB;   // [n]: the sum of the n largest CTA counts (grid bounds), n <= kSchedMax
   size_t smemA, smemB;           // largest dynamic shared memory of a problem's stage
 };
 
@@ -399,14 +455,22 @@ static int fft_smem_once() {
 }
 
 template <typename T>
-static int launch_fft_grp(const FftDesc* dev, dim3 gA, dim3 gB, size_t smA, size_t smB, const int* subset,
-                          const int* live, cudaStream_t st) {
-  k_fft_rows_fwd_grp<T><<<gA, kFT, smA, st>>>(dev, subset, live);
-  BLML_CHECK_LAUNCH("FFT route: rows");
-  k_fft_cols_grp<T><<<gB, kFT, smB, st>>>(dev, subset, live);
-  BLML_CHECK_LAUNCH("FFT route: columns");
-  k_fft_rows_inv_grp<T><<<gA, kFT, smA, st>>>(dev, subset, live);
-  BLML_CHECK_LAUNCH("FFT route: inverse rows");
+static int launch_fft_grp(const FftGroup* fg, const int* subset, int n0, int n, const int* live, cudaStream_t st) {
+  k_fft_schedule<<<1, 256, 0, st>>>(fg->dev, subset, n0, n, live, fg->sch);
+  BLML_CHECK_LAUNCH("FFT route: schedule");
+  const int gA = fg->boundA[n], gB = fg->boundB[n];
+  if (gA > 0) {
+    k_fft_rows_fwd_grp<T><<<gA, kFT, fg->smemA, st>>>(fg->dev, fg->sch);
+    BLML_CHECK_LAUNCH("FFT route: rows");
+  }
+  if (gB > 0) {
+    k_fft_cols_grp<T><<<gB, kFT, fg->smemB, st>>>(fg->dev, fg->sch);
+    BLML_CHECK_LAUNCH("FFT route: columns");
+  }
+  if (gA > 0) {
+    k_fft_rows_inv_grp<T><<<gA, kFT, fg->smemA, st>>>(fg->dev, fg->sch);
+    BLML_CHECK_LAUNCH("FFT route: inverse rows");
+  }
   return BLML_OK;
 }
 
@@ -428,34 +492,45 @@ int fft_group_init(void** out, int G, const blml_plan* plans, const int* nbatch,
     if (!plans[g]->fft) return BLML_OK;
   const size_t esz = plans[0]->dtype == BLML_F64 ? 16 : 8;
   std::vector<FftDesc> h(G);
-  FftGroup fg{};
+  FftGroup* fg = new FftGroup();
+  fg->dev = nullptr; fg->sch = nullptr; fg->smemA = fg->smemB = 0;
+  std::vector<int> cA(G), cB(G);
   for (int g = 0; g < G; g++) {
     h[g] = make_desc(plans[g], x[g], y[g], z[g], nbatch[g], xc);
-    fg.maxA = std::max(fg.maxA, h[g].ctasA); fg.maxB = std::max(fg.maxB, h[g].ctasB);
-    fg.smemA = std::max(fg.smemA, stage_smem(h[g].rows, h[g].M2, esz));
-    fg.smemB = std::max(fg.smemB, stage_smem(h[g].cols, h[g].M1, esz));
+    cA[g] = h[g].ctasA; cB[g] = h[g].ctasB;
+    fg->smemA = std::max(fg->smemA, stage_smem(h[g].rows, h[g].M2, esz));
+    fg->smemB = std::max(fg->smemB, stage_smem(h[g].cols, h[g].M1, esz));
   }
+  std::sort(cA.begin(), cA.end(), std::greater<int>()); std::sort(cB.begin(), cB.end(), std::greater<int>());
+  const int nmax = std::min(G, kSchedMax);
+  fg->boundA.assign(nmax + 1, 0); fg->boundB.assign(nmax + 1, 0);
+  for (int i = 0; i < nmax; i++) { fg->boundA[i + 1] = fg->boundA[i] + cA[i]; fg->boundB[i + 1] = fg->boundB[i] + cB[i]; }
   int e = fft_smem_once();
-  if (e) return e;
-  if (cudaMalloc(&fg.dev, G * sizeof(FftDesc)) != cudaSuccess) { set_error("FFT route: allocation"); return BLML_ERR_CUDA; }
-  e = cuda_status(cudaMemcpy(fg.dev, h.data(), G * sizeof(FftDesc), cudaMemcpyHostToDevice), "FFT route");
-  if (e) { cudaFree(fg.dev); return e; }
-  *out = new FftGroup(fg);
+  if (!e && cudaMalloc(&fg->dev, G * sizeof(FftDesc)) != cudaSuccess) { set_error("FFT route: allocation"); e = BLML_ERR_CUDA; }
+  if (!e && cudaMalloc(&fg->sch, sizeof(FftSched)) != cudaSuccess) { set_error("FFT route: allocation"); e = BLML_ERR_CUDA; }
+  if (!e) e = cuda_status(cudaMemcpy(fg->dev, h.data(), G * sizeof(FftDesc), cudaMemcpyHostToDevice), "FFT route");
+  if (e) { fft_group_free(fg); return e; }
+  *out = fg;
   return BLML_OK;
 }
 
 void fft_group_free(void* fgv) {
   FftGroup* fg = reinterpret_cast<FftGroup*>(fgv);
   if (!fg) return;
-  cudaFree(fg->dev);
+  cudaFree(fg->dev); cudaFree(fg->sch);
   delete fg;
 }
 
+// problems of the launch in chunks of kSchedMax (one schedule buffer: the chunks run one after another on st)
 int fft_group_launch(void* fgv, int dtype, const int* subset, int n, const int* live, cudaStream_t st) {
   const FftGroup* fg = reinterpret_cast<const FftGroup*>(fgv);
-  const dim3 gA((unsigned)fg->maxA, 1, (unsigned)n), gB((unsigned)fg->maxB, 1, (unsigned)n);
-  return dtype == BLML_F64 ? launch_fft_grp<double>(fg->dev, gA, gB, fg->smemA, fg->smemB, subset, live, st)
-                           : launch_fft_grp<float>(fg->dev, gA, gB, fg->smemA, fg->smemB, subset, live, st);
+  for (int n0 = 0; n0 < n; n0 += kSchedMax) {
+    const int nc = std::min(kSchedMax, n - n0);
+    const int e = dtype == BLML_F64 ? launch_fft_grp<double>(fg, subset, n0, nc, live, st)
+                                    : launch_fft_grp<float>(fg, subset, n0, nc, live, st);
+    if (e) return e;
+  }
+  return BLML_OK;
 }
 
 // one plan over nb lattices: Z (nb, H2, M1) in the caller's workspace, the descriptor passed by value
