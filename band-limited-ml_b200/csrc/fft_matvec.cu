@@ -10,7 +10,7 @@
 //   B  columns: FFT of every Z column (length M1), times W over the band (zero elsewhere), inverse FFT -> Z
 //   C  rows:    scatter each row's H2 harmonics into a zero spectrum, inverse FFT (length M2) -> the lattice row
 // The FFTs are mixed-radix (2, 3, 4, 6, 8) Stockham passes: sides 2^a 3^b (the benchmark sweep's {64, ..., 384}).
-// Each CTA holds two buffers of up to kFE complex values (several rows or columns, one padded row per transform;
+// Each CTA holds two buffers of up to kCtaBytes / 2 (several rows or columns, one padded row per transform;
 // a single transform when the side is longer) and the length's twiddle table; passes run out of place between them.
 // Versus the restricted transforms (matvec.cu) this costs O(M log M) per row instead of O(M H), and in float64 it
 // rounds like an FFT (~1e-16 log M relative), so the route changes no result beyond rounding.
@@ -23,18 +23,39 @@
 namespace blml {
 
 constexpr int kFT = 256;                 // threads per CTA
-constexpr int kFE = 2048;                // complex values per CTA buffer (transforms x length); one transform when longer
+constexpr int kCtaBytes = 72 * 1024;     // shared memory a CTA aims for (3 CTAs per SM); one transform when longer
 constexpr int kMaxSide = 4096;           // longest side of the route
 constexpr int kMaxRad = 12;
+
+// Shared-memory index of point i of a transform: one pad slot after every 8 points, so the first pass's stores at
+// stride R (and the row gathers) spread over the banks; a transform occupies ld(N) slots, an odd count, so that
+// transforms side by side start on different banks.
+__host__ __device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+__host__ __device__ __forceinline__ int pld(int N) { return N + (N >> 3) + 1; }
+
+// x / d for 0 <= x < 2^16 and 1 <= d < 2^16 by a multiply and a shift: m = floor((2^32 - 1) / d) + 1 (0 for d = 1)
+__host__ __device__ __forceinline__ unsigned magic_of(unsigned d) { return d <= 1 ? 0u : 0xFFFFFFFFu / d + 1u; }
+__device__ __forceinline__ int div_m(int x, unsigned m) { return m ? (int)__umulhi((unsigned)x, m) : x; }
 
 static int fft_smem_once();
 
 // per-plan data of the route (host struct holding device pointers)
+// The passes of one axis's transform: radix, sub-transform length Ns before the pass, the magic numbers of the
+// divisions by N / R and by Ns, and where the pass's twiddles start in the axis's table. The table holds, pass after
+// pass (Ns > 1), w^(r k N / (Ns R)) for k < Ns, 1 <= r < R at [k (R - 1) + r - 1], w = exp(-2 pi i / N): N - R_0
+// values in all, read with consecutive k by consecutive threads.
+struct FftAxis {
+  int N, npass, ntw;
+  int8_t rad[kMaxRad];
+  int ns[kMaxRad], twoff[kMaxRad];
+  unsigned mnbt[kMaxRad], mns[kMaxRad];
+};
+
+// per-plan data of the route (host struct holding device pointers)
 struct FftPlan {
   int M1, M2, H1, H2;
-  int nrad1, nrad2;
-  int8_t rad1[kMaxRad], rad2[kMaxRad];
-  void* tw1; void* tw2;                  // exp(-2 pi i t / M) for t < M, complex of the plan's dtype
+  FftAxis ax1, ax2;                      // axis 0 (columns, length M1) and axis 1 (rows, length M2)
+  void* tw1; void* tw2;                  // the axes' pass twiddle tables, complex of the plan's dtype
   int* k2;                               // the H2 harmonics of axis 1 as DFT indices (k mod M2)
   int* map1;                             // per DFT index of axis 0: its position in the band's axis-0 list, or -1
 };
@@ -45,8 +66,7 @@ struct FftDesc {
   int M1, M2, H1, H2, nb, flags;         // flags: 1 real input, 4 real output
   int rows, cols;                        // transforms per CTA: rows (stages A, C), columns (stage B)
   int ctasA, ctasB;                      // CTAs of this problem in stages A / C and B
-  int nrad1, nrad2;
-  int8_t rad1[kMaxRad], rad2[kMaxRad];
+  FftAxis ax1, ax2;
 };
 
 // ------------------------------------------------------------------------------------------------- butterflies
@@ -104,50 +124,52 @@ template <typename T, int R, bool INV> __device__ __forceinline__ void butterfly
 }
 
 // One Stockham pass of radix R over ntr transforms of length N, from src to dst in shared memory (transform t at
-// + t * ld in both), after Ns points of each sub-transform are done: butterfly j (of N / R) reads src[j + r N / R]
-// times w^(r (j mod Ns) N / (Ns R)) and writes its R outputs to dst[(j - j mod Ns) R + j mod Ns + s Ns]. A thread
-// holds one butterfly's R values at a time; one barrier per pass.
+// + t * ld, point i at pidx(i), in both), after Ns points of each sub-transform are done: butterfly j (of N / R)
+// reads src[j + r N / R] times w^(r (j mod Ns) N / (Ns R)) and writes its R outputs to dst[(j - j mod Ns) R +
+// j mod Ns + s Ns]. A thread holds one butterfly's R values at a time; one barrier per pass.
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void fft_pass(const cpx<T>* src, cpx<T>* dst, const cpx<T>* tw, int N, int ld, int ntr,
-                                         int Ns) {
-  const int nbt = N / R, total = nbt * ntr, stride = N / (Ns * R);
+                                         int Ns, unsigned mnbt, unsigned mns) {
+  const int nbt = N / R, total = nbt * ntr;
   for (int b = threadIdx.x; b < total; b += kFT) {
-    const int t = b / nbt, j = b - t * nbt, k = j % Ns;
-    const cpx<T>* s = src + t * ld + j;
+    const int t = div_m(b, mnbt), j = b - t * nbt;
+    const int k = j - div_m(j, mns) * Ns;
+    const cpx<T>* s = src + t * ld;
     cpx<T> v[R];
 #pragma unroll
-    for (int r = 0; r < R; r++) v[r] = s[r * nbt];
+    for (int r = 0; r < R; r++) v[r] = s[pidx(j + r * nbt)];
     if (Ns > 1) {
+      const cpx<T>* w = tw + k * (R - 1);
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        cpx<T> w = tw[r * k * stride];
-        if (INV) w.im = -w.im;
-        v[r] = cmul(v[r], w);
+        cpx<T> ww = w[r - 1];
+        if (INV) ww.im = -ww.im;
+        v[r] = cmul(v[r], ww);
       }
     }
     butterfly<T, R, INV>(v);
-    cpx<T>* d = dst + t * ld + (j - k) * R + k;
+    cpx<T>* d = dst + t * ld;
+    const int o = (j - k) * R + k;
 #pragma unroll
-    for (int r = 0; r < R; r++) d[r * Ns] = v[r];
+    for (int r = 0; r < R; r++) d[pidx(o + r * Ns)] = v[r];
   }
   __syncthreads();
 }
 
 // All passes of the transform, alternating between the two buffers; returns the one holding the result.
 template <typename T, bool INV>
-__device__ cpx<T>* smem_fft(cpx<T>* a, cpx<T>* b, const cpx<T>* tw, int N, int ld, int ntr, const int8_t* rad,
-                            int nrad) {
-  int Ns = 1;
-  for (int p = 0; p < nrad; p++) {
-    const int R = rad[p];
-    switch (R) {
-      case 8: fft_pass<T, 8, INV>(a, b, tw, N, ld, ntr, Ns); break;
-      case 6: fft_pass<T, 6, INV>(a, b, tw, N, ld, ntr, Ns); break;
-      case 4: fft_pass<T, 4, INV>(a, b, tw, N, ld, ntr, Ns); break;
-      case 3: fft_pass<T, 3, INV>(a, b, tw, N, ld, ntr, Ns); break;
-      default: fft_pass<T, 2, INV>(a, b, tw, N, ld, ntr, Ns); break;
+__device__ cpx<T>* smem_fft(cpx<T>* a, cpx<T>* b, const cpx<T>* tw, int ld, int ntr, const FftAxis& ax) {
+  for (int p = 0; p < ax.npass; p++) {
+    const cpx<T>* twp = tw + ax.twoff[p];
+    const int N = ax.N, Ns = ax.ns[p];
+    const unsigned m1 = ax.mnbt[p], m2 = ax.mns[p];
+    switch (ax.rad[p]) {
+      case 8: fft_pass<T, 8, INV>(a, b, twp, N, ld, ntr, Ns, m1, m2); break;
+      case 6: fft_pass<T, 6, INV>(a, b, twp, N, ld, ntr, Ns, m1, m2); break;
+      case 4: fft_pass<T, 4, INV>(a, b, twp, N, ld, ntr, Ns, m1, m2); break;
+      case 3: fft_pass<T, 3, INV>(a, b, twp, N, ld, ntr, Ns, m1, m2); break;
+      default: fft_pass<T, 2, INV>(a, b, twp, N, ld, ntr, Ns, m1, m2); break;
     }
-    Ns *= R;
     cpx<T>* t = a; a = b; b = t;
   }
   return a;
@@ -161,84 +183,84 @@ __device__ cpx<T>* smem_fft(cpx<T>* a, cpx<T>* b, const cpx<T>* tw, int N, int l
 template <typename T>
 __device__ __forceinline__ void rows_fwd_body(const FftDesc& D, int cta, unsigned char* smem) {
   const int tid = threadIdx.x;
-  const int N = D.M2, ld = N + 1, rows_tot = D.nb * D.M1;
+  const int N = D.M2, ld = pld(N), rows_tot = D.nb * D.M1;
   const int r0 = cta * D.rows, nr = min(D.rows, rows_tot - r0);
   cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem);
   cpx<T>* alt = buf + D.rows * ld;
   cpx<T>* tw = alt + D.rows * ld;
-  for (int i = tid; i < N; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
+  for (int i = tid; i < D.ax2.ntw; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
   const int64_t base = (int64_t)r0 * N;
   if (D.flags & 1) {
     const T* X = reinterpret_cast<const T*>(D.X) + base;
-    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + (i - t * N)] = cpx<T>{X[i], T(0)}; }
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + pidx(i - t * N)] = cpx<T>{X[i], T(0)}; }
   } else {
     const cpx<T>* X = reinterpret_cast<const cpx<T>*>(D.X) + base;
-    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + (i - t * N)] = X[i]; }
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + pidx(i - t * N)] = X[i]; }
   }
   __syncthreads();
-  buf = smem_fft<T, false>(buf, alt, tw, N, ld, nr, D.rad2, D.nrad2);
+  buf = smem_fft<T, false>(buf, alt, tw, ld, nr, D.ax2);
   cpx<T>* Z = reinterpret_cast<cpx<T>*>(D.Z);
   for (int i = tid; i < nr * D.H2; i += kFT) {
     const int q2 = i / nr, t = i - q2 * nr;
     const int row = r0 + t, b = row / D.M1, r = row - b * D.M1;
-    Z[((int64_t)b * D.H2 + q2) * D.M1 + r] = buf[t * ld + __ldg(D.k2 + q2)];
+    Z[((int64_t)b * D.H2 + q2) * D.M1 + r] = buf[t * ld + pidx(__ldg(D.k2 + q2))];
   }
 }
 
 template <typename T>
 __device__ __forceinline__ void cols_body(const FftDesc& D, int cta, unsigned char* smem) {
   const int tid = threadIdx.x;
-  const int N = D.M1, ld = N + 1, cols_tot = D.nb * D.H2;
+  const int N = D.M1, ld = pld(N), cols_tot = D.nb * D.H2;
   const int c0 = cta * D.cols, nc = min(D.cols, cols_tot - c0);
   cpx<T>* base = reinterpret_cast<cpx<T>*>(smem);
   cpx<T>* buf = base;
   cpx<T>* alt = base + D.cols * ld;
   cpx<T>* tw = alt + D.cols * ld;
-  for (int i = tid; i < N; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw1)[i];
+  for (int i = tid; i < D.ax1.ntw; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw1)[i];
   cpx<T>* Z = reinterpret_cast<cpx<T>*>(D.Z) + (int64_t)c0 * N;
-  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; buf[t * ld + (i - t * N)] = Z[i]; }
+  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; buf[t * ld + pidx(i - t * N)] = Z[i]; }
   __syncthreads();
-  buf = smem_fft<T, false>(buf, alt, tw, N, ld, nc, D.rad1, D.nrad1);
+  buf = smem_fft<T, false>(buf, alt, tw, ld, nc, D.ax1);
   alt = buf == base ? base + D.cols * ld : base;
   const T* W = reinterpret_cast<const T*>(D.W);
   for (int i = tid; i < nc * N; i += kFT) {
     const int t = i / N, k1 = i - t * N;
     const int q1 = __ldg(D.map1 + k1), q2 = (c0 + t) % D.H2;
     const T w = q1 >= 0 ? W[(int64_t)q1 * D.H2 + q2] : T(0);
-    cpx<T>& v = buf[t * ld + k1];
+    cpx<T>& v = buf[t * ld + pidx(k1)];
     v.re *= w; v.im *= w;
   }
   __syncthreads();
-  buf = smem_fft<T, true>(buf, alt, tw, N, ld, nc, D.rad1, D.nrad1);
-  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; Z[i] = buf[t * ld + (i - t * N)]; }
+  buf = smem_fft<T, true>(buf, alt, tw, ld, nc, D.ax1);
+  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; Z[i] = buf[t * ld + pidx(i - t * N)]; }
 }
 
 template <typename T>
 __device__ __forceinline__ void rows_inv_body(const FftDesc& D, int cta, unsigned char* smem) {
   const int tid = threadIdx.x;
-  const int N = D.M2, ld = N + 1, rows_tot = D.nb * D.M1;
+  const int N = D.M2, ld = pld(N), rows_tot = D.nb * D.M1;
   const int r0 = cta * D.rows, nr = min(D.rows, rows_tot - r0);
   cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem);
   cpx<T>* alt = buf + D.rows * ld;
   cpx<T>* tw = alt + D.rows * ld;
-  for (int i = tid; i < N; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
+  for (int i = tid; i < D.ax2.ntw; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
   for (int i = tid; i < nr * ld; i += kFT) buf[i] = cpx<T>{T(0), T(0)};
   __syncthreads();
   const cpx<T>* Z = reinterpret_cast<const cpx<T>*>(D.Z);
   for (int i = tid; i < nr * D.H2; i += kFT) {
     const int q2 = i / nr, t = i - q2 * nr;
     const int row = r0 + t, b = row / D.M1, r = row - b * D.M1;
-    buf[t * ld + __ldg(D.k2 + q2)] = Z[((int64_t)b * D.H2 + q2) * D.M1 + r];
+    buf[t * ld + pidx(__ldg(D.k2 + q2))] = Z[((int64_t)b * D.H2 + q2) * D.M1 + r];
   }
   __syncthreads();
-  buf = smem_fft<T, true>(buf, alt, tw, N, ld, nr, D.rad2, D.nrad2);
+  buf = smem_fft<T, true>(buf, alt, tw, ld, nr, D.ax2);
   const int64_t base = (int64_t)r0 * N;
   if (D.flags & 4) {
     T* Y = reinterpret_cast<T*>(D.Y) + base;
-    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; Y[i] = buf[t * ld + (i - t * N)].re; }
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; Y[i] = buf[t * ld + pidx(i - t * N)].re; }
   } else {
     cpx<T>* Y = reinterpret_cast<cpx<T>*>(D.Y) + base;
-    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; Y[i] = buf[t * ld + (i - t * N)]; }
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; Y[i] = buf[t * ld + pidx(i - t * N)]; }
   }
 }
 
@@ -298,17 +320,23 @@ __device__ __forceinline__ int sched_find(const int* off, int n, int x, int& loc
 
 #define FFT_STAGE(NAME, BODY, OFF)                                                                                \
   template <typename T>                                                                                          \
-  __global__ void __launch_bounds__(kFT) NAME##_grp(const FftDesc* __restrict__ descs,                           \
+  __global__ void __launch_bounds__(kFT, 3) NAME##_grp(const FftDesc* __restrict__ descs,                           \
                                                     const FftSched* __restrict__ sch) {                          \
     extern __shared__ __align__(16) unsigned char fft_smem[];                                                    \
+    __shared__ __align__(16) FftDesc Ds;                                                                         \
     int local = 0;                                                                                               \
     const int i = sched_find(sch->OFF, sch->n, (int)blockIdx.x, local);                                          \
     if (i < 0) return;                                                                                           \
-    const FftDesc D = descs[sch->prob[i]];                                                                       \
-    BODY<T>(D, local, fft_smem);                                                                                 \
+    {                                   /* the problem's descriptor, staged once per CTA */                     \
+      const int* src = reinterpret_cast<const int*>(descs + sch->prob[i]);                                       \
+      int* dst = reinterpret_cast<int*>(&Ds);                                                                    \
+      for (int q = threadIdx.x; q < (int)(sizeof(FftDesc) / 4); q += kFT) dst[q] = src[q];                       \
+    }                                                                                                            \
+    __syncthreads();                                                                                             \
+    BODY<T>(Ds, local, fft_smem);                                                                                \
   }                                                                                                              \
   template <typename T>                                                                                          \
-  __global__ void __launch_bounds__(kFT) NAME##_one(const FftDesc D) {                                           \
+  __global__ void __launch_bounds__(kFT, 3) NAME##_one(const FftDesc D) {                                           \
     extern __shared__ __align__(16) unsigned char fft_smem[];                                                    \
     BODY<T>(D, blockIdx.x, fft_smem);                                                                            \
   }
@@ -340,10 +368,42 @@ static int radix_plan(int N, int8_t* rad) {
   return (int)r.size();
 }
 
-static int transforms_per_cta(int N) { return std::max(1, kFE / N); }
+// an axis's passes and its twiddle table (float64 host values, interleaved complex); false when N has no plan
+static bool axis_plan(int N, FftAxis& ax, std::vector<double>& tw) {
+  ax = FftAxis{};
+  ax.N = N;
+  ax.npass = radix_plan(N, ax.rad);
+  if (!ax.npass) return false;
+  tw.clear();
+  int Ns = 1;
+  for (int p = 0; p < ax.npass; p++) {
+    const int R = ax.rad[p];
+    ax.ns[p] = Ns; ax.mnbt[p] = magic_of((unsigned)(N / R)); ax.mns[p] = magic_of((unsigned)Ns);
+    ax.twoff[p] = (int)(tw.size() / 2);
+    if (Ns > 1) {
+      const int stride = N / (Ns * R);
+      for (int k = 0; k < Ns; k++)
+        for (int r = 1; r < R; r++) {
+          const long long e = (long long)r * k * stride % N;
+          const double ph = 2.0 * M_PI * (double)e / (double)N;
+          tw.push_back(std::cos(ph)); tw.push_back(-std::sin(ph));
+        }
+    }
+    Ns *= R;
+  }
+  ax.ntw = std::max(1, (int)(tw.size() / 2));
+  if (tw.empty()) { tw.push_back(1.0); tw.push_back(0.0); }
+  return true;
+}
 
-// two buffers of ntr padded transforms, then the twiddle table
-static size_t stage_smem(int ntr, int N, size_t esz) { return (2 * (size_t)ntr * (N + 1) + N) * esz; }
+// transforms of length N per CTA: as many as two padded buffers and the twiddles hold within kCtaBytes, at least one
+static int transforms_per_cta(int N, size_t esz) {
+  const long long room = (long long)(kCtaBytes / esz) - N;
+  return (int)std::max<long long>(1, room / (2LL * pld(N)));
+}
+
+// two buffers of ntr padded transforms, then the twiddle table (N values at most)
+static size_t stage_smem(int ntr, int N, size_t esz) { return (2 * (size_t)ntr * pld(N) + N) * esz; }
 
 int fft_plan_init(blml_plan_s* p, const double* freqs) {
   p->fft = nullptr;
@@ -352,8 +412,8 @@ int fft_plan_init(blml_plan_s* p, const double* freqs) {
   if (M1 > kMaxSide || M2 > kMaxSide || H1 > M1 || H2 > M2) return BLML_OK;
   FftPlan fp{};
   fp.M1 = M1; fp.M2 = M2; fp.H1 = H1; fp.H2 = H2;
-  fp.nrad1 = radix_plan(M1, fp.rad1); fp.nrad2 = radix_plan(M2, fp.rad2);
-  if (!fp.nrad1 || !fp.nrad2) return BLML_OK;
+  std::vector<double> tws1, tws2;
+  if (!axis_plan(M1, fp.ax1, tws1) || !axis_plan(M2, fp.ax2, tws2)) return BLML_OK;
   // integer harmonics, distinct modulo the side: then S is exactly the DFT mask
   std::vector<int> k2(H2), map1(M1, -1), seen2(M2, 0);
   for (int q = 0; q < H1 + H2; q++) {
@@ -371,19 +431,15 @@ int fft_plan_init(blml_plan_s* p, const double* freqs) {
   }
   const bool f64 = p->dtype == BLML_F64;
   const size_t esz = f64 ? 16 : 8;
-  auto table = [&](int M, void** dst) -> int {
-    std::vector<double> t(2 * (size_t)M);
-    for (int i = 0; i < M; i++) {
-      const double ph = 2.0 * M_PI * (double)i / (double)M;
-      t[2 * i] = std::cos(ph); t[2 * i + 1] = -std::sin(ph);
-    }
-    if (cudaMalloc(dst, M * esz) != cudaSuccess) { set_error("FFT plan: device allocation"); return BLML_ERR_CUDA; }
-    if (f64) return cuda_status(cudaMemcpy(*dst, t.data(), M * esz, cudaMemcpyHostToDevice), "FFT plan twiddles");
+  auto table = [&](const std::vector<double>& t, void** dst) -> int {
+    const size_t n = t.size() / 2;
+    if (cudaMalloc(dst, n * esz) != cudaSuccess) { set_error("FFT plan: device allocation"); return BLML_ERR_CUDA; }
+    if (f64) return cuda_status(cudaMemcpy(*dst, t.data(), n * esz, cudaMemcpyHostToDevice), "FFT plan twiddles");
     std::vector<float> t32(t.begin(), t.end());
-    return cuda_status(cudaMemcpy(*dst, t32.data(), M * esz, cudaMemcpyHostToDevice), "FFT plan twiddles");
+    return cuda_status(cudaMemcpy(*dst, t32.data(), n * esz, cudaMemcpyHostToDevice), "FFT plan twiddles");
   };
-  int rc = table(M1, &fp.tw1);
-  if (!rc) rc = table(M2, &fp.tw2);
+  int rc = table(tws1, &fp.tw1);
+  if (!rc) rc = table(tws2, &fp.tw2);
   if (!rc && cudaMalloc(&fp.k2, H2 * sizeof(int)) != cudaSuccess) { set_error("FFT plan: device allocation"); rc = BLML_ERR_CUDA; }
   if (!rc) rc = cuda_status(cudaMemcpy(fp.k2, k2.data(), H2 * sizeof(int), cudaMemcpyHostToDevice), "FFT plan");
   if (!rc && cudaMalloc(&fp.map1, M1 * sizeof(int)) != cudaSuccess) { set_error("FFT plan: device allocation"); rc = BLML_ERR_CUDA; }
@@ -411,11 +467,11 @@ static FftDesc make_desc(const blml_plan_s* p, const void* x, void* y, void* z, 
   D.tw1 = fp->tw1; D.tw2 = fp->tw2; D.k2 = fp->k2; D.map1 = fp->map1;
   D.M1 = fp->M1; D.M2 = fp->M2; D.H1 = fp->H1; D.H2 = fp->H2; D.nb = nb;
   D.flags = xc ? 0 : (1 | 4);
-  D.rows = transforms_per_cta(fp->M2); D.cols = transforms_per_cta(fp->M1);
+  const size_t esz = p->dtype == BLML_F64 ? 16 : 8;
+  D.rows = transforms_per_cta(fp->M2, esz); D.cols = transforms_per_cta(fp->M1, esz);
   D.ctasA = (nb * fp->M1 + D.rows - 1) / D.rows;
   D.ctasB = (nb * fp->H2 + D.cols - 1) / D.cols;
-  D.nrad1 = fp->nrad1; D.nrad2 = fp->nrad2;
-  std::copy(fp->rad1, fp->rad1 + kMaxRad, D.rad1); std::copy(fp->rad2, fp->rad2 + kMaxRad, D.rad2);
+  D.ax1 = fp->ax1; D.ax2 = fp->ax2;
   return D;
 }
 
@@ -426,9 +482,9 @@ struct FftGroup {
   size_t smemA, smemB;           // largest dynamic shared memory of a problem's stage
 };
 
-// the largest dynamic shared memory any stage asks for: two buffers of one kMaxSide-point transform (the longest
-// transform that has a CTA to itself) and its twiddles, in float64; shorter transforms fill kFE values per buffer
-constexpr size_t kMaxSmem = (size_t)(3 * kMaxSide + 2) * 16;
+// the largest dynamic shared memory any stage asks for: two padded buffers of one kMaxSide-point transform and its
+// twiddles, in float64 (shorter transforms stay within kCtaBytes)
+constexpr size_t kMaxSmem = (size_t)(2 * (kMaxSide + kMaxSide / 8 + 1) + kMaxSide) * 16;
 
 // the six kernels' dynamic shared-memory limit, set once per device (outside any stream capture: at plan creation)
 template <typename T>
