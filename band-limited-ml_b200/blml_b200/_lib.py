@@ -52,6 +52,9 @@ _SIGS = {
     'blml_group_create': (_I, [_I, _P, _P, _I, _P, _P, _P, _P, C.POINTER(_P)]),
     'blml_group_matvec': (_I, [_P, _P]),
     'blml_group_destroy': (_I, [_P]),
+    'blml_spectrum_workspace': (_L, [_P, _I]),
+    'blml_spectrum': (_I, [_P, _P, _P, _I, _I, _P, _L, _P]),
+    'blml_planewave_points': (_I, [_I, _I, _P, _P, _P, _L, _P, _P, _P]),
     'blml_plan_set_route': (_I, [_P, _I]),
     'blml_plan_route': (_I, [_P]),
     'blml_group_set_route': (_I, [_P, _I]),

@@ -598,14 +598,90 @@ class BLMLBinned:
             self._p64 = Plan(freqs, W, self.shape_, _lib.F64, _lib.ENGINE_SIMT)
         return self._p64
 
-    def predict(self, X):
-        raise NotImplementedError("predict at arbitrary points is outside this engine's path; use density_")
+    # ---------------------------------------------------------------- at arbitrary points
+    def _mode_at_points(self, k, X):
+        """sum_b e_kb K_k(x - z_b) at the points X (m, d) on the device, complex128 (m,). Columns of sinc / slits /
+        dirichlet kind: the exact one-column kernels per (point, bin) pair over the occupied bins (blml_point_rows).
+        Harmonic kernels (pball groups with dirichlet columns): the band's spectrum C = W (v^H e) and the plane-wave
+        sum over it (blml_spectrum, blml_planewave_points), exact since the kernel is that sum. ball: unsupported."""
+        from .spec import split_kind, dirichlet_N, dirichlet_inner_M
+        import ctypes as C
+        sp = self.specs_[k]
+        names = [split_kind(kd)[0] for kd, _ in units_of(sp['kinds'])]
+        e = self.e_hat_t_[k].to(torch.complex128 if self.e_hat_t_.is_complex() else torch.float64).contiguous()
+        Xt = torch.as_tensor(np.ascontiguousarray(X, np.float64)).to(self.dev_)
+        m = len(X)
+        if all(n in ('sinc', 'slits', 'dirichlet') for n in names):
+            cols = (_lib.PointCol * self.d_)()
+            for j, kind in enumerate(sp['kinds']):
+                name, tag = split_kind(kind)
+                c = cols[j]
+                c.kind = {'sinc': _lib.PT_SINC, 'slits': _lib.PT_SLITS, 'dirichlet': _lib.PT_DIRICHLET}[name]
+                c.f = float(sp['fc'][j])
+                if name == 'slits':
+                    c.fi = (1.0 - float(tag)) * c.f
+                if name == 'dirichlet':
+                    c.P = float(sp['periods'][j]); c.M = 2 * dirichlet_N(c.f, c.P) + 1
+                    c.Mi = dirichlet_inner_M(c.f, c.P, float(tag) if tag else None)
+            occ = self.w_t_ > 0
+            Z = torch.as_tensor(self.centres()).to(self.dev_)[occ].contiguous()
+            parts = [e.real, e.imag] if e.is_complex() else [e]
+            outs = []
+            for part in parts:
+                w = part[occ].contiguous()
+                g = torch.empty(m, dtype=torch.float64, device=self.dev_)
+                call('blml_point_rows', m, self.d_, Xt.data_ptr(), int(Z.shape[0]), Z.data_ptr(), w.data_ptr(),
+                     C.cast(cols, C.c_void_p), g.data_ptr(), self._st)
+                outs.append(g)
+            return torch.complex(outs[0], outs[1]) if len(outs) == 2 else torch.complex(outs[0], torch.zeros_like(outs[0]))
+        if not all(n in ('pball', 'dirichlet') for n in names) or self.d_ > 2:
+            raise NotImplementedError("sqrt_density at arbitrary points: sinc / slits / dirichlet columns, or pball groups "
+                                      "with dirichlet columns in 1-D / 2-D (ball kernels are not sums of harmonics)")
+        freqs, W = mode_transform(sp, self.shape_, self.h_, self.pad_)
+        plan = Plan(freqs, W, self.shape_, _lib.F64, _lib.ENGINE_SIMT)
+        ws = torch.empty(int(_lib.lib().blml_spectrum_workspace(plan._h, 1)), dtype=torch.uint8, device=self.dev_)
+        spec = torch.empty(int(np.prod([len(f) for f in freqs])), dtype=torch.complex128, device=self.dev_)
+        x = e if e.is_complex() else e.to(torch.complex128)
+        call('blml_spectrum', plan._h, x.data_ptr(), spec.data_ptr(), 1, 1, ws.data_ptr(), ws.numel(), self._st)
+        U = (np.asarray(X, float) - self.origin_[None, :]) / self.h_[None, :]
+        if self.d_ == 1:
+            f1, f2, U2 = np.zeros(1), np.asarray(freqs[0], float), np.stack([np.zeros(m), U[:, 0]], 1)
+        else:
+            f1, f2, U2 = np.asarray(freqs[0], float), np.asarray(freqs[1], float), U
+        dev = self.dev_
+        f1t, f2t = torch.as_tensor(f1).to(dev), torch.as_tensor(f2).to(dev)
+        Ut = torch.as_tensor(np.ascontiguousarray(U2, np.float64)).to(dev)
+        g = torch.empty(m, dtype=torch.complex128, device=dev)
+        call('blml_planewave_points', len(f1), len(f2), f1t.data_ptr(), f2t.data_ptr(), spec.data_ptr(), m,
+             Ut.data_ptr(), g.data_ptr(), self._st)
+        return g
 
-    def sqrt_density(self, X, chunk=4096):
-        raise NotImplementedError("sqrt_density at arbitrary points is outside this engine's path; use Se_ / n")
+    def sqrt_density(self, X, chunk=65536):
+        """g_k(x) = (1/n) sum_b e_bk K_k(x - z_b) at arbitrary points X (m, d) (blml_binned.py:451-465): (m,) for
+        rank 1, else (m, K); complex for complex_g."""
+        X = np.atleast_2d(np.asarray(X, float))
+        if X.shape[1] != self.d_:
+            X = X.reshape(-1, self.d_)
+        out = np.zeros((len(X), self.K_), dtype=complex if self.complex_g_ else float)
+        for i in range(0, len(X), chunk):
+            for k in range(self.K_):
+                g = self._mode_at_points(k, X[i:i + chunk]).cpu().numpy() / self.n_
+                out[i:i + chunk, k] = g if self.complex_g_ else g.real
+        return out[:, 0] if self.K_ == 1 else out
+
+    def predict(self, X):
+        """f(x) = sum_k |g_k(x)|^2 at arbitrary points (blml_binned.py:467-469)."""
+        G = self.sqrt_density(X)
+        return np.abs(G) ** 2 if G.ndim == 1 else (np.abs(G) ** 2).sum(1)
 
     def predict_grid(self, r):
-        raise NotImplementedError("predict_grid is outside this engine's path")
+        """f on the lattice refined r times per dim (from the origin in steps h / r; the last fine point is the last
+        bin): shape ((m_j - 1) r + 1, ...) (blml_binned.py:471-500)."""
+        r = int(r)
+        fine = tuple((m - 1) * r + 1 for m in self.shape_)
+        g = np.meshgrid(*[self.origin_[j] + (self.h_[j] / r) * np.arange(n) for j, n in enumerate(fine)], indexing='ij')
+        X = np.stack([x.ravel() for x in g], 1)
+        return self.predict(X).reshape(fine)
 
     # ---------------------------------------------------------------- fc gradients
     def _dplans(self):

@@ -10,7 +10,7 @@ CSRC = os.path.join(ROOT, 'csrc')
 INCLUDE = os.path.join(REPO, 'include')
 LIB = os.path.join(PKG, 'libblml_b200.so')
 SOURCES = ['capi.cu', 'matvec.cu', 'fft_matvec.cu', 'tc_matvec.cu', 'solver_ops.cu', 'pairs.cu', 'batched.cu', 'batch_runner.cu', 'unet.cu',
-           'points.cu']
+           'points.cu', 'predict.cu']
 NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 FLAGS = ['-O3', '-std=c++17', '-gencode', 'arch=compute_100a,code=sm_100a', '-lineinfo', '-Xcompiler', '-fPIC',
          '-Xcompiler', '-O3', '--expt-relaxed-constexpr', '-I', INCLUDE, '-I', CSRC]

@@ -161,6 +161,29 @@ static int launch_stage(const void* X, bool xreal, const void* Tw, const void* W
   return BLML_OK;
 }
 
+// the d forward stages alone, the weight in the last one's epilogue: spec = W (v^H x), (nb, H_1 ... H_d) natural order
+template <typename T>
+static int simt_forward(blml_plan_s* p, const void* x, void* spec, int nb, int xc, void* ws, cudaStream_t st) {
+  const int d = p->d;
+  std::vector<int64_t> dims(p->shape, p->shape + d);
+  const size_t esz = sizeof(cpx<T>);
+  char* buf[2] = {reinterpret_cast<char*>(ws), reinterpret_cast<char*>(ws) + (size_t)nb * p->max_elems * esz};
+  const void* cur = x; bool cur_real = !xc; int which = 0;
+  for (int s = 0; s < d; s++) {
+    const int a = d - 1 - s;
+    const int64_t M = dims.back();
+    int64_t tot = 1; for (auto v : dims) tot *= v;
+    const int64_t R = tot / M, N = p->nfreq[a];
+    void* out = s == d - 1 ? spec : buf[which];
+    int rc = launch_stage<T>(cur, cur_real, p->tf[a], s == d - 1 ? p->W : nullptr, out, false, R, (int)M, (int)N, nb,
+                             st);
+    if (rc) return rc;
+    dims.pop_back(); dims.insert(dims.begin(), N);
+    cur = out; cur_real = false; which ^= 1;
+  }
+  return BLML_OK;
+}
+
 template <typename T>
 static int simt_matvec(blml_plan_s* p, const void* x, void* y, int nb, int xc, void* ws, cudaStream_t st) {
   const int d = p->d;
@@ -640,5 +663,23 @@ int blml_group_set_route(blml_group grp, int route) {
 }
 
 int blml_group_route(blml_group grp) { return grp ? grp->route : BLML_ERR_ARG; }
+
+int blml_spectrum(blml_plan p, const void* x, void* spec, int nb, int xc, void* ws, int64_t wsb, void* stream) {
+  if (!p || !x || !spec || nb < 1) { set_error("blml_spectrum: bad arguments"); return BLML_ERR_ARG; }
+  if (p->engine != BLML_ENGINE_SIMT) { set_error("blml_spectrum: SIMT plans only"); return BLML_ERR_UNSUPPORTED; }
+  const int64_t need = 2 * (int64_t)nb * p->max_elems * (p->dtype == BLML_F64 ? 16 : 8);
+  if (wsb < need || !ws) {
+    set_error("blml_spectrum: workspace of %lld bytes, need %lld", (long long)wsb, (long long)need);
+    return BLML_ERR_WORKSPACE;
+  }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  return p->dtype == BLML_F64 ? simt_forward<double>(p, x, spec, nb, xc, ws, st)
+                              : simt_forward<float>(p, x, spec, nb, xc, ws, st);
+}
+
+int64_t blml_spectrum_workspace(blml_plan p, int nb) {
+  if (!p || nb < 1) return -1;
+  return 2 * (int64_t)nb * p->max_elems * (p->dtype == BLML_F64 ? 16 : 8);
+}
 
 }

@@ -172,6 +172,20 @@ typedef struct { blml_point_col c[8]; } blml_point_cols;
 int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* e,
                     const blml_point_col* cols, double* g, void* stream);
 
+/* ---- the binned fit at arbitrary points for harmonic kernels (BLMLBinned.sqrt_density / predict / predict_grid,
+ *      blml_binned.py:451-500) ----
+ * spectrum: spec (nbatch x prod nfreq, complex of the plan's dtype, natural order) = W (v^H x), the forward half of
+ * blml_matvec (SIMT plans); workspace blml_spectrum_workspace bytes.
+ * planewave: g[i] = sum_{q1, q2} spec[q1 H2 + q2] exp(2 pi i (f1[q1] U[i, 0] + f2[q2] U[i, 1])) for m points U (m x 2,
+ * lattice coordinates (x - origin) / h), frequencies in cycles per lattice index, spec and g complex128; a 1-D
+ * kernel is H1 = 1, f1 = {0}, U[i, 0] = 0. Exact for pball groups and dirichlet columns, whose kernels are sums of
+ * harmonics (the reference evaluates the same sums, blml_trivial.py:632-665). */
+int64_t blml_spectrum_workspace(blml_plan plan, int nbatch);
+int blml_spectrum(blml_plan plan, const void* x, void* spec, int nbatch, int x_complex, void* ws, int64_t ws_bytes,
+                  void* stream);
+int blml_planewave_points(int H1, int H2, const double* f1, const double* f2, const double* spec, int64_t m,
+                          const double* U, double* g, void* stream);
+
 /* ---- one Armijo trial of the L-BFGS line search (BLMLBinned._solve_lbfgs, blml_binned.py:316-321) ----
  * En = E + t q and Un = U + t Sq (S linear: U + t S q = S(E + t q)), both written; out[0] = sum_occ w log F(Un),
  * out[1] = Re <En, Un>, from which L(En) = out[0] - n log out[1]. nq = 2. */
