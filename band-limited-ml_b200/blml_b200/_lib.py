@@ -96,6 +96,7 @@ _SIGS = {
     'blml_nn_adam': (_I, [_P, _P, _P, _P, _L, C.c_float, C.c_float, C.c_float, C.c_float, _I, _P, _P, _I, _I, _P]),
     'blml_nn_to_bf16': (_I, [_P, _L, _P, _P, _I, _I, _P]),
     'blml_lbfgs_batch_create': (_I, [_I, _I, _P, _P, _I, _D, _D, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
+    'blml_lbfgs_batch_set_caps': (_I, [_P, _P]),
     'blml_lbfgs_batch_run': (_I, [_P, _P]),
     'blml_lbfgs_batch_result': (_I, [_P, _P, _P, _P, _P, _P]),
     'blml_lbfgs_batch_stats': (_I, [_P, _P]),
@@ -134,6 +135,7 @@ _SIGS = {
     'blml_cert_weights': (_I, [_I, _I, _L, _I, _P, _P, _P, _P]),
     'blml_rows': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P, _P, _P]),
     'blml_cols': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P]),
+    'blml_cols_dep': (_I, [_P, _P, _L, _P, _L, _L, _P, _P, _I, _P]),
     'blml_lattice_coords': (_I, [_P, _L, _I, _P, _P, _P]),
     'blml_rows_noalloc': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _P, _P]),
 }

@@ -115,12 +115,14 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     wv = torch.empty(B, dtype=torch.float64, device=dev)
     vec = torch.zeros(B, dtype=torch.float64, device=dev) if vectors else None
     R = torch.empty(B, dtype=torch.float64, device=dev)
-    for _ in range(max_restarts + 1):
+    steps = 0
+    for rnd in range(max_restarts + 1):
         alphas = np.zeros((F, nb)); betas = np.zeros((F, nb))
         conv = np.zeros(F, bool); yr = [None] * F
         j_end = nb
         for j in range(nb):
             op(V[j], wv)
+            steps += 1
             alpha = None
             for ps in range(2):                                   # full reorthogonalisation, twice
                 for c0 in range(0, j + 1, 47):
@@ -170,4 +172,5 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     if vectors:
         nv = dots([(vec, vec)])[:, 0]
         lin(vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
+    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()))
     return theta, dh, vec

@@ -244,9 +244,10 @@ def rows(ZA, ZB, w, tab, grad=False, f32=False, device=None):
 
 def cols(ZA_dev, ZB_dev, tab, out, out_m=None, depmask=0, f32=False):
     """The explicit block S(ZA_r, ZB_j) into out (R, M) on the device; ZA_dev, ZB_dev are rank coordinates (torch
-    int64 on the device). out float64 or float32."""
-    if depmask or out_m is not None:
-        raise NotImplementedError("cols: the joint + marginal (depmask) pass is outside this engine's path")
+    int64 on the device). out float64 or float32. With depmask (a bit per column), out_m receives the marginal: the
+    product over the units none of whose columns is in depmask (blml_local_gpu.py:320-361)."""
+    if depmask and out_m is None:
+        raise ValueError("cols: depmask needs out_m")
     device = out.device
     t = dev_tab(tab, device)
     A = _coords_dev(ZA_dev, tab, device); Bz = _coords_dev(ZB_dev, tab, device)
@@ -254,6 +255,12 @@ def cols(ZA_dev, ZB_dev, tab, out, out_m=None, depmask=0, f32=False):
     if tuple(out.shape) != (R, M) or not out.is_contiguous():
         raise ValueError(f"cols: out must be a contiguous ({R}, {M}) array")
     st = _struct(tab, t, False, f32)
+    if out_m is not None:
+        if tuple(out_m.shape) != (R, M) or not out_m.is_contiguous() or out_m.dtype != out.dtype:
+            raise ValueError(f"cols: out_m must be a contiguous ({R}, {M}) array of out's dtype")
+        call('blml_cols_dep', st, A.data_ptr(), R, Bz.data_ptr(), M, int(depmask), out.data_ptr(), out_m.data_ptr(),
+             int(out.dtype == torch.float32), torch.cuda.current_stream(device).cuda_stream)
+        return out
     call('blml_cols', st, A.data_ptr(), R, Bz.data_ptr(), M, out.data_ptr(), int(out.dtype == torch.float32),
          torch.cuda.current_stream(device).cuda_stream)
     return out

@@ -365,6 +365,9 @@ class BLMLBinnedBatch:
              n.ctypes.data_as(C.c_void_p), self.w.data_ptr(), self.c.data_ptr(), E.data_ptr(), U.data_ptr(),
              C.byref(h))
         try:
+            if getattr(self, '_caps', None) is not None:
+                caps = np.ascontiguousarray(self._caps, np.int64)
+                call('blml_lbfgs_batch_set_caps', h, caps.ctypes.data_as(C.c_void_p))
             call('blml_lbfgs_batch_run', h, self.st)
             it = np.zeros(F, np.int64); stop = np.zeros(F, np.int32); L = np.zeros(F); res = np.zeros(F)
             call('blml_lbfgs_batch_result', h, it.ctypes.data_as(C.c_void_p), stop.ctypes.data_as(C.c_void_p),
@@ -377,9 +380,11 @@ class BLMLBinnedBatch:
         return U, it, np.array(STOP_CODES, dtype=object)[stop], L, res
 
     # ---------------------------------------------------------------- fit
-    def fit(self, counts_list, modes_list, init=None):
+    def fit(self, counts_list, modes_list, init=None, caps=None):
         """init: None (the seeded start), or one complex start E0 per fit (arrays of the counts' shapes, host or
-        device), e.g. from blml_b200.warmstart; the start phase is then skipped (blml_binned.py:403-408)."""
+        device), e.g. from blml_b200.warmstart; the start phase is then skipped (blml_binned.py:403-408). caps: per-fit
+        L-BFGS iteration caps (< 0: none) in place of max_sweeps (device-side control)."""
+        self._caps = caps
         self._prepare(counts_list, modes_list)
         F, code, dev = self.F, self.code, self.device
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
@@ -658,44 +663,58 @@ class BLMLBinnedBatch:
              v.data_ptr(), sc.data_ptr(), En.data_ptr(), self.st)
         return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
 
-    def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None):
-        """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then, for the fits
-        whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol, one more shared mode started along the
-        certificate's top eigenvector (every such fit of a round in one batch), until the certificate is met or K
-        reaches max_rank. The lift is convex: a fit that meets the certificate is at its unique optimum (the
-        reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results carry
-        rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations), ...]."""
+    def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300):
+        """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
+        batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
+        mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
+        to tol at the same rank and checked again. Rounds before the last rank are capped at grow_iters L-BFGS
+        iterations: at too low a rank the solver crawls along the lift's boundary, so those fits only have to show that
+        they need another mode. The lift is convex: a fit that meets the certificate at tol is at its unique optimum
+        (the reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results
+        carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...]."""
         F = len(counts_list)
-        self.fit(counts_list, modes_list, init=init)
+        first_caps = np.full(F, grow_iters if max_rank > 1 else -1, np.int64)
+        self.fit(counts_list, modes_list, init=init, caps=first_caps)
         final = [None] * F
         paths = [[] for _ in range(F)]
-        cur, idx = self, np.arange(F)
+        cur, idx, capped = self, np.arange(F), first_caps >= 0
         self.certify_stats_ = dict(rounds=0, fits_per_round=[], lbfgs_iterations_max=[], seconds_certificate=0.0)
         while True:
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record()
             cert, dh, v = cur.certificate(vectors=True)
             ev[1].record(); ev[1].synchronize()
-            self.certify_stats_['seconds_certificate'] += ev[0].elapsed_time(ev[1]) / 1e3
-            self.certify_stats_['rounds'] += 1
-            self.certify_stats_['fits_per_round'].append(len(idx))
-            self.certify_stats_['lbfgs_iterations_max'].append(int(max(r.n_sweeps_ for r in cur.results_)))
+            st = self.certify_stats_
+            st['seconds_certificate'] += ev[0].elapsed_time(ev[1]) / 1e3
+            st['rounds'] += 1; st['fits_per_round'].append(len(idx))
+            st['lbfgs_iterations_max'].append(int(max(r.n_sweeps_ for r in cur.results_)))
+            st.setdefault('lanczos', []).append(cur.lanczos_stats_)
+            nxt_fits, nxt_starts, nxt_caps = [], [], []
             for j, i in enumerate(idx):
                 r = cur.results_[j]
-                paths[i].append((int(cur.Kf[j]), float(r.loglik_), float(cert[j]), int(r.n_sweeps_)))
-                r.certificate_, r.rank_, r.rank_path_ = float(cert[j]), int(cur.Kf[j]), paths[i]
+                K = int(cur.Kf[j])
+                was_capped = bool(capped[j]) and r.stop_reason_ == 'max_sweeps'
+                paths[i].append((K, float(r.loglik_), float(cert[j]), int(r.n_sweeps_), was_capped))
+                r.certificate_, r.rank_, r.rank_path_ = float(cert[j]), K, paths[i]
                 final[i] = r
-            grow = [j for j in range(len(idx)) if not cert[j] <= 1.0 + cert_tol and cur.Kf[j] < max_rank]
-            if not grow:
+                ok = cert[j] <= 1.0 + cert_tol
+                if was_capped and (ok or K >= max_rank):
+                    nxt_fits.append((j, i, K)); nxt_caps.append(-1)            # run on to tol at this rank
+                elif not ok and K < max_rank:
+                    nxt_fits.append((j, i, K + 1)); nxt_caps.append(grow_iters if K + 1 < max_rank else -1)
+            if not nxt_fits:
                 return final
-            starts = cur._grown_starts(grow, dh, v, step)
+            grow = [j for j, _, K1 in nxt_fits if K1 > int(cur.Kf[j])]
+            grown = dict(zip(grow, cur._grown_starts(grow, dh, v, step))) if grow else {}
+            starts = [grown[j] if j in grown else cur.e_hat(j) for j, _, _ in nxt_fits]
             nxt = BLMLBinnedBatch(tol=self.tol, max_sweeps=self.max_sweeps, anderson=self.anderson, dtype=self.dtype,
                                   phase_noise=self.phase_noise, seed=self.seed, stall=self.stall, ll_tol=self.ll_tol,
                                   ll_window=self.ll_window, lbfgs_m=self.lbfgs_m, device=self.device,
                                   verbose=self.verbose, control=self.control)
-            mds = [[modes_list[idx[j]][0]] * int(starts[t].shape[0]) for t, j in enumerate(grow)]
-            nxt.fit([counts_list[idx[j]] for j in grow], mds, init=starts)
-            cur, idx = nxt, idx[np.asarray(grow)]
+            mds = [[modes_list[i][0]] * K1 for _, i, K1 in nxt_fits]
+            caps = np.array(nxt_caps, np.int64)
+            nxt.fit([counts_list[i] for _, i, _ in nxt_fits], mds, init=starts, caps=caps)
+            cur, idx, capped = nxt, np.array([i for _, i, _ in nxt_fits]), caps >= 0
 
     def val_score(self, counts_list):
         """Per fit: the mean log-probability of the counts (validation counts on the fit's lattice) with bin

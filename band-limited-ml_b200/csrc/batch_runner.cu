@@ -66,6 +66,7 @@ __global__ void k_finish_flagged(const double* part, int nq, int nblk, const int
 struct LbState {
   double *L, *Q, *Qn, *n, *res, *slope, *qq, *mh, *SY, *YY;
   int *active, *it, *stop, *reset, *nh, *ok, *stamp, *step;
+  const long long* caps;                 // per-fit iteration caps (null: the runner's one cap for every fit)
 };
 
 // the compact L-BFGS direction of fit f (one warp): q = gam g + S p - gam Y t over the fit's pairs in the order they
@@ -334,7 +335,7 @@ __global__ void k_lb_post(int Fa, int m, int p, double tol, double ftol, long lo
   }
   int a = s.active[f];
   if (a && s.nh[f] > LB_FWIN && h[LB_FWIN] - h[0] < ftol) { s.stop[f] = STOP_LLTOL; a = 0; }
-  if (a && s.it[f] >= cap) a = 0;
+  if (a && s.it[f] >= (s.caps ? s.caps[f] : cap)) a = 0;
   if (a) s.it[f]++;
   s.active[f] = a;
   set_live(j, f, a, live, segs_c, segs_eff);
@@ -372,7 +373,7 @@ __global__ void k_lbi_state(int Fa, int m, double tol, long long cap, const int*
   h[LB_FWIN] = s.L[f] / nf;
   s.nh[f] = 1; s.reset[f] = 0; s.stop[f] = STOP_TOL; s.ok[f] = 0; s.it[f] = 0;
   int a = r >= tol;
-  if (a && 0 >= cap) a = 0;
+  if (a && 0 >= (s.caps ? s.caps[f] : cap)) a = 0;
   if (a) s.it[f] = 1;
   s.active[f] = a;
   set_live(j, f, a, live, segs_c, segs_eff);
@@ -831,6 +832,7 @@ struct blml_lbfgs_batch_s : Runner {
          *ones = nullptr, *sc = nullptr;
   int* need2 = nullptr;
   LbState s{};
+  long long* d_caps = nullptr;
 
   // the history scan: H1 = [S_q . y_p, S_q . g, y_p . y_p, g . g, E . E], H2 = [Y_q . y_p, Y_q . g, ...]
   int hist(int Fa_, const blml_seg* S, int p) {
@@ -1135,6 +1137,21 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
   if (rc) { r->release(); delete r; return rc; }
   *out = r;
   return BLML_OK;
+}
+
+int blml_lbfgs_batch_set_caps(blml_lbfgs_batch r, const int64_t* caps) {
+  if (!r || !caps) { set_error("blml_lbfgs_batch_set_caps: null argument"); return BLML_ERR_ARG; }
+  if (!r->d_caps) {
+    r->d_caps = (long long*)r->dalloc(sizeof(long long) * (size_t)r->F);
+    if (!r->d_caps) { set_error("blml_lbfgs_batch_set_caps: allocation"); return BLML_ERR_CUDA; }
+  }
+  std::vector<long long> c(r->F);
+  for (int f = 0; f < r->F; f++) c[f] = caps[f] < 0 ? LLONG_MAX : (long long)caps[f];
+  int rc = cuda_status(cudaMemcpyAsync(r->d_caps, c.data(), sizeof(long long) * r->F, cudaMemcpyHostToDevice, r->st),
+                       "blml_lbfgs_batch_set_caps");
+  if (!rc) rc = cuda_status(cudaStreamSynchronize(r->st), "blml_lbfgs_batch_set_caps");
+  if (!rc) r->s.caps = r->d_caps;
+  return rc;
 }
 
 int blml_lbfgs_batch_run(blml_lbfgs_batch r, void* stream) {

@@ -468,7 +468,8 @@ static FftDesc make_desc(const blml_plan_s* p, const void* x, void* y, void* z, 
   D.M1 = fp->M1; D.M2 = fp->M2; D.H1 = fp->H1; D.H2 = fp->H2; D.nb = nb;
   D.flags = xc ? 0 : (1 | 4);
   const size_t esz = p->dtype == BLML_F64 ? 16 : 8;
-  D.rows = transforms_per_cta(fp->M2, esz); D.cols = transforms_per_cta(fp->M1, esz);
+  // the column stage has few transforms (H2 per lattice): at most 2 per CTA, so its launch still fills the GPU
+  D.rows = transforms_per_cta(fp->M2, esz); D.cols = std::min(2, transforms_per_cta(fp->M1, esz));
   D.ctasA = (nb * fp->M1 + D.rows - 1) / D.rows;
   D.ctasB = (nb * fp->H2 + D.cols - 1) / D.cols;
   D.ax1 = fp->ax1; D.ax2 = fp->ax2;

@@ -196,9 +196,11 @@ __global__ void k_sum_slices(const double* part, int nsl, int64_t n, double* out
   }
 }
 
+// out[r, j] = S(ZA_r, ZB_j); with out_m, also the product over the units whose bit in dep_units is clear (the
+// marginal of the columns outside the dep mask, from the same lookups)
 template <typename REAL, typename OUT>
 __global__ void k_cols(ColMeta cm, const REAL* T, const REAL* RT, const int64_t* ZA, int64_t R, const int64_t* ZB,
-                       int64_t M, OUT* out) {
+                       int64_t M, OUT* out, OUT* out_m, unsigned dep_units) {
   for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < R * M;
        idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = idx / M, j = idx % M;
@@ -207,9 +209,13 @@ __global__ void k_cols(ColMeta cm, const REAL* T, const REAL* RT, const int64_t*
     for (int u = 0; u < MAXU; u++) fac[u] = REAL(1);
     for (int k = 0; k < cm.d; k++) { za[k] = ZA[r * cm.d + k]; zb[k] = ZB[j * cm.d + k]; }
     pair_factors<REAL>(cm, T, RT, za, zb, fac, r2, tor);
-    REAL v = REAL(1);
-    for (int u = 0; u < cm.U; u++) v *= fac[u];
-    out[idx] = (OUT)v;
+    REAL v = REAL(1), vdep = REAL(1);
+    for (int u = 0; u < cm.U; u++) {
+      if ((dep_units >> u) & 1u) vdep *= fac[u];
+      else v *= fac[u];
+    }
+    out[idx] = (OUT)(v * vdep);
+    if (out_m) out_m[idx] = (OUT)v;
   }
 }
 
@@ -548,26 +554,41 @@ int blml_lattice_coords(const double* Z, int64_t n, int d, const double* h, int6
   return cuda_status(cudaGetLastError(), "blml_lattice_coords");
 }
 
-int blml_cols(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
-              int out_f32, void* stream) {
+static int cols_launch(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
+                       void* out_m, int64_t depmask, int out_f32, void* stream, const char* who) {
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   ColMeta cm;
   int e = read_meta(tb, cm, st);
   if (e) return e;
+  if (depmask < 0 || (cm.d < 63 && (depmask >> cm.d) != 0)) { set_error("%s: depmask has bits past column d", who); return BLML_ERR_ARG; }
   if (R == 0 || M == 0) return BLML_OK;
   e = check_extents(cm, ZA, R, ZB, M, st);
   if (e) return e;
+  unsigned dep_units = 0;                        // a unit (column or radial group) is dep when one of its columns is
+  for (int k = 0; k < cm.d; k++)
+    if ((depmask >> k) & 1) dep_units |= 1u << cm.dim_unit[k];
   const int64_t n = R * M;
   const int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 32);
   if (tb->f32) {
-    if (out_f32) k_cols<float, float><<<g, 256, 0, st>>>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, (float*)out);
-    else k_cols<float, double><<<g, 256, 0, st>>>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, (double*)out);
+    if (out_f32) k_cols<float, float><<<g, 256, 0, st>>>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, (float*)out, (float*)out_m, dep_units);
+    else k_cols<float, double><<<g, 256, 0, st>>>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, (double*)out, (double*)out_m, dep_units);
   } else {
-    if (out_f32) k_cols<double, float><<<g, 256, 0, st>>>(cm, tb->T, tb->RT, ZA, R, ZB, M, (float*)out);
-    else k_cols<double, double><<<g, 256, 0, st>>>(cm, tb->T, tb->RT, ZA, R, ZB, M, (double*)out);
+    if (out_f32) k_cols<double, float><<<g, 256, 0, st>>>(cm, tb->T, tb->RT, ZA, R, ZB, M, (float*)out, (float*)out_m, dep_units);
+    else k_cols<double, double><<<g, 256, 0, st>>>(cm, tb->T, tb->RT, ZA, R, ZB, M, (double*)out, (double*)out_m, dep_units);
   }
   count_launches(1);
-  return cuda_status(cudaGetLastError(), "blml_cols");
+  return cuda_status(cudaGetLastError(), who);
+}
+
+int blml_cols(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
+              int out_f32, void* stream) {
+  return cols_launch(tb, ZA, R, ZB, M, out, nullptr, 0, out_f32, stream, "blml_cols");
+}
+
+int blml_cols_dep(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, int64_t depmask,
+                  void* out, void* out_m, int out_f32, void* stream) {
+  if (!out_m) { set_error("blml_cols_dep: out_m"); return BLML_ERR_ARG; }
+  return cols_launch(tb, ZA, R, ZB, M, out, out_m, depmask, out_f32, stream, "blml_cols_dep");
 }
 
 }

@@ -290,6 +290,9 @@ typedef struct blml_lbfgs_batch_s* blml_lbfgs_batch;
 int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_plan* plans, int m, double tol,
                             double ll_tol, int64_t max_iters, const double* n, const void* w, const void* c, void* E,
                             void* U, blml_lbfgs_batch* runner);
+/* per-fit iteration caps (F host values, < 0: none) in place of max_iters, before blml_lbfgs_batch_run: rounds of a
+   certified fit cap the fits still growing their rank and let the final ones run to tol */
+int blml_lbfgs_batch_set_caps(blml_lbfgs_batch runner, const int64_t* caps);
 int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);
 /* per fit (host arrays of F, any may be null): iterations, stop code, L, Q, max|rho| */
 int blml_lbfgs_batch_result(blml_lbfgs_batch runner, int64_t* iters, int32_t* stop, double* L, double* Q,
@@ -399,6 +402,11 @@ int blml_lattice_coords(const double* Z, int64_t n, int d, const double* h, int6
 /* out (R, M) row-major = S(ZA_r, ZB_j), float64 (out_f32 = 0) or float32 */
 int blml_cols(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, void* out,
               int out_f32, void* stream);
+/* the joint and marginal blocks of a conditional fit (cols_kernel with depmask, blml_local_gpu.py:320-361): out as
+ * blml_cols, out_m (R, M) = the product over the units (columns, or whole radial groups) none of whose columns has
+ * its bit set in depmask -- the marginal kernel of the other columns -- from the same table lookups */
+int blml_cols_dep(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, int64_t depmask,
+                  void* out, void* out_m, int out_f32, void* stream);
 
 #ifdef __cplusplus
 }

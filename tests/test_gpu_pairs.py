@@ -71,3 +71,29 @@ def test_empty_inputs(cuda_device):
     assert np.array_equal(s, np.zeros(2))
     s, _ = rows(Z[:0], Z, np.ones(2), tab)
     assert s.shape == (0,)
+
+
+@pytest.mark.parametrize('case,masks', [('p5', (0b00101, 0b10000)), ('pt', (0b100, 0b001))])
+def test_cols_joint_and_marginal(cuda_device, case, masks):
+    """cols with depmask (blml_local_gpu.py:320-361): out = the joint block, out_m = the block of the product kernel
+    over the columns outside the mask (a radial group dep when one of its columns is), both against the reference's
+    own CPU blocks (tests/golden/cols_dep.npz); the pball group case masks the sinc column, then the group."""
+    from blml_b200.local_gpu import ProductKernel, cols, rank_coords
+    c = golden('cols_dep.npz')[case]
+    p = golden('pairs.npz')[case]
+    if case == 'p5':
+        ZA, ZB = p['bins'][:300], p['bins'][:200]
+        kinds, per, fc, h = ['sinc'] * 5, [None] * 5, p['fc'], p['h']
+    else:
+        ZA, ZB = p['ZA'], p['ZB']
+        kinds, per = ['pball:0-1', 'pball:0-1', 'sinc'], [31.0, 31.0, None]
+        fc, h = np.array([0.33, 0.33, 0.2]), np.array([1.0, 1.0, 0.7])
+    pk = ProductKernel(kinds, per, fold=[True] * len(kinds))
+    tab = pk.tables(fc, per, h, np.r_[ZA, ZB])
+    A = torch.as_tensor(rank_coords(ZA, tab)).cuda(); B = torch.as_tensor(rank_coords(ZB, tab)).cuda()
+    for mask in masks:
+        out = torch.empty((len(ZA), len(ZB)), dtype=torch.float64, device='cuda')
+        out_m = torch.empty_like(out)
+        cols(A, B, tab, out, out_m=out_m, depmask=mask)
+        assert np.abs(out.cpu().numpy() - c['joint']).max() <= 1e-12
+        assert np.abs(out_m.cpu().numpy() - c[f'marg{mask}']).max() <= 1e-12, mask
