@@ -500,7 +500,8 @@ class BinnedFit:
 
     def solve(self, E, cap):
         if self.solver == 'lbfgs' and self.psd:
-            return self.solve_lbfgs(E, cap)
+            lc = getattr(self, 'lbfgs_cap', None)           # a cap on the L-BFGS alone (the start keeps max_sweeps)
+            return self.solve_lbfgs(E, cap if lc is None else lc)
         return self.solve_cd(E, cap)
 
     # ---------------------------------------------------------------- fit
@@ -604,25 +605,38 @@ class _Start:
         self.e_hat, self.shape = e_hat, shape
 
 
-def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-4, max_rank=8, max_sweeps=20000, step=0.1):
+def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-3, max_rank=8, grow_iters=300, step=0.1):
     """A certified fit of one shared kernel: the complex L-BFGS fit at rank K = 1, 2, ... until the certificate
     lambda_max(D^1/2 S D^1/2) / n <= 1 + cert_tol (blml_binned.py:501-518), each rank started from the previous fit's
     modes plus a new mode step * (rms mode norm) along d = D^1/2 v, v the certificate's top eigenvector (an ascent
-    direction of the convex lift while the certificate exceeds 1). The lift is convex, so the certified loglik is
-    that of its unique optimum, whatever the path. Returns (fit, [(K, loglik, certificate, iterations), ...])."""
-    K = 1
-    fit = BinnedFit(tol=tol, solver='lbfgs', max_sweeps=max_sweeps).fit(counts, [spec], complex_g=True)
+    direction of the convex lift while the certificate exceeds 1). Ranks below max_rank run at most grow_iters
+    L-BFGS iterations (at too low a rank the solver crawls); a capped fit that meets the certificate, and the fit at
+    max_rank, run on to tol. The lift is convex, so the certified loglik is that of its unique optimum, whatever the
+    path. Returns (fit, [(K, loglik, certificate, iterations, capped), ...])."""
+    def run(K, cap, init=None):
+        f = BinnedFit(tol=tol, solver='lbfgs')
+        f.lbfgs_cap = cap
+        return f.fit(counts, [spec] * K, complex_g=True, init=init)
+
+    K, cap = 1, (grow_iters if max_rank > 1 else None)
+    fit = run(1, cap)
     path = []
     while True:
         cert, d = fit.certificate_vector()
-        path.append((K, float(fit.loglik), cert, int(fit.n_sweeps)))
-        if cert <= 1.0 + cert_tol or K >= max_rank:
+        capped = cap is not None and fit.stop_reason == 'max_sweeps'
+        path.append((K, float(fit.loglik), cert, int(fit.n_sweeps), capped))
+        ok = cert <= 1.0 + cert_tol
+        if capped and (ok or K >= max_rank):
+            cap = None
+            fit = run(K, None, _Start(fit.e_hat.copy(), fit.shape))
+            continue
+        if ok or K >= max_rank:
             return fit, path
         scale = step * np.sqrt((np.abs(fit.e_hat) ** 2).sum() / K) / max(np.linalg.norm(d), 1e-300)
         init = _Start(np.concatenate([fit.e_hat, (scale * d)[None].astype(complex)], 0), fit.shape)
         K += 1
-        fit = BinnedFit(tol=tol, solver='lbfgs', max_sweeps=max_sweeps).fit(counts, [spec] * K, complex_g=True,
-                                                                           init=init)
+        cap = grow_iters if K < max_rank else None
+        fit = run(K, cap, init)
 
 
 def anderson_mix(hX, hF, f):
