@@ -18,7 +18,7 @@ from . import _lib
 from ._lib import call, ptrs, dbl
 from .binned import BLMLBinned, _Red, _device
 from .spec import parse_modes, modes_lattice, with_lattice, split_kind, dirichlet_N, dirichlet_inner_M
-from .local_gpu import ProductKernel, rows_dev
+from .local_gpu import ProductKernel, rows_dev, dev_tab, _struct
 
 
 def lattice_coords(Z, h, device=None):
@@ -123,11 +123,26 @@ class BLMLQuickLattice(BLMLBinned):
         d = torch.empty(Bs, dtype=torch.float64, device=dev)
         Zb = torch.empty((Bs, D), dtype=torch.int64, device=dev)
         q = torch.empty(65, dtype=torch.float64, device=dev)
+        v = torch.empty(B, dtype=torch.float64, device=dev)
         steps = 0.5 ** np.arange(31)
         rng = np.random.default_rng(self.seed)
+        # every pass is bins against bins of the same coordinate set: the tables and extents are checked once here,
+        # and the passes run with no host synchronisation or allocation
+        import ctypes as C
+        tstruct = _struct(self.tab_, dev_tab(self.tab_, dev), False, f32)
+        rplan = C.c_void_p()
+        call('blml_rows_plan_create', tstruct, self._Z.data_ptr(), B, st, C.byref(rplan))
+        wsb = max(int(_lib.lib().blml_rows_plan_workspace(rplan, B, Bs)),
+                  int(_lib.lib().blml_rows_plan_workspace(rplan, B, B)))
+        rws = torch.empty(max(wsb, 8), dtype=torch.uint8, device=dev)
+
+        def pass_rows(ZB, M, w, out):
+            call('blml_rows_plan_run', rplan, self._Z.data_ptr(), B, ZB.data_ptr(), M, w.data_ptr(), out.data_ptr(),
+                 rws.data_ptr(), rws.numel(), st)
+            return out
 
         def exact_Se(e):
-            return rows_dev(self._Z, self._Z, e, self.tab_, grad=False, f32=f32)[0]
+            return pass_rows(self._Z, B, e, torch.empty(B, dtype=torch.float64, device=dev))
 
         def phi(e, Se):
             call('blml_merit_terms', _lib.F64, 1, B, 0, 0, e.data_ptr(), Se.data_ptr(), c64.data_ptr(),
@@ -149,7 +164,7 @@ class BLMLQuickLattice(BLMLBinned):
                 call('blml_block_root', m, I.data_ptr(), B, e.data_ptr(), Se.data_ptr(), c64.data_ptr(), sbb,
                      d.data_ptr(), st)
                 call('blml_gather_rows_i64', m, D, self._Z.data_ptr(), I.data_ptr(), B, Zb.data_ptr(), st)
-                v = rows_dev(self._Z, Zb[:m], d[:m], self.tab_, grad=False, f32=f32)[0]
+                pass_rows(Zb, m, d, v)
                 t = 1.0
                 if safeguard:
                     call('blml_block_search', m, I.data_ptr(), B, e.data_ptr(), d.data_ptr(), Se.data_ptr(),
@@ -211,6 +226,7 @@ class BLMLQuickLattice(BLMLBinned):
             res = resid(e, Se)
             conv = res < self.tol
             hist.append(res)
+        _lib.lib().blml_rows_plan_destroy(rplan)
         self.n_sweeps_, self.residual_, self.converged_ = it, res, conv
         self.rho_history_ = hist
         self.safeguard_ = safeguard

@@ -349,21 +349,31 @@ static int check_extents(const ColMeta& cm, const int64_t* ZA, int64_t R, const 
   return BLML_OK;
 }
 
+// column slices of a rows launch: so that the grid covers the GPU about four times
+static void rows_slices(int64_t R, int64_t M, int64_t& nsl, int64_t& slice) {
+  const int64_t rblocks = (R + PR_THREADS - 1) / PR_THREADS;
+  nsl = std::max<int64_t>(1, std::min<int64_t>((4 * 148 + rblocks - 1) / rblocks, (M + 1023) / 1024));
+  nsl = std::min<int64_t>(nsl, 65535);
+  slice = (M + nsl - 1) / nsl;
+  nsl = (M + slice - 1) / slice;
+}
+
+// ws: the slice partials (nsl R (1 + nW) doubles) when the caller provides them, else a stream-ordered allocation
 template <typename REAL>
 static int rows_impl(const blml_tables* tb, const ColMeta& cm, const REAL* T, const REAL* RT, const REAL* dT,
                      const REAL* dR, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
-                     int grad, double* s, double* ds, cudaStream_t st) {
+                     int grad, double* s, double* ds, cudaStream_t st, double* ws = nullptr) {
   const int64_t rblocks = (R + PR_THREADS - 1) / PR_THREADS;
-  // column slices so that the grid covers the GPU about four times
-  int64_t nsl = std::max<int64_t>(1, std::min<int64_t>((4 * 148 + rblocks - 1) / rblocks, (M + 1023) / 1024));
-  nsl = std::min<int64_t>(nsl, 65535);
-  const int64_t slice = (M + nsl - 1) / nsl;
-  nsl = (M + slice - 1) / slice;
+  int64_t nsl, slice;
+  rows_slices(R, M, nsl, slice);
   const int nW = grad ? cm.nW : 0;
-  double* part = nullptr;
+  double* part = ws;
   const size_t pbytes = (size_t)nsl * R * (1 + nW) * sizeof(double);
-  int e = cuda_status(cudaMallocAsync((void**)&part, std::max<size_t>(pbytes, 8), st), "blml_rows workspace");
-  if (e) return e;
+  int e = BLML_OK;
+  if (!part) {
+    e = cuda_status(cudaMallocAsync((void**)&part, std::max<size_t>(pbytes, 8), st), "blml_rows workspace");
+    if (e) return e;
+  }
   double* dpart = part + (size_t)nsl * R;
   bool offset_only = cm.G == 0 && !grad;
   for (int k = 0; k < cm.d; k++) offset_only = offset_only && cm.code[k] == 0;
@@ -371,7 +381,7 @@ static int rows_impl(const blml_tables* tb, const ColMeta& cm, const REAL* T, co
   dim3 grid((unsigned)rblocks, (unsigned)nsl);
   if (offset_only) {
     const size_t sm = offset_smem_bytes<REAL>(cm.Tn, cm.d);
-    if (sm > 200 * 1024) { cudaFreeAsync(part, st); set_error("blml_rows: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+    if (sm > 200 * 1024) { if (!ws) cudaFreeAsync(part, st); set_error("blml_rows: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
 #define ROWS_OFF(DD) case DD: \
       cudaFuncSetAttribute(k_rows_offset<REAL, DD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm); \
       k_rows_offset<REAL, DD><<<grid, PR_THREADS, sm, st>>>(cm, T, ZA, R, ZB, w, slice, M, part); break;
@@ -379,7 +389,7 @@ static int rows_impl(const blml_tables* tb, const ColMeta& cm, const REAL* T, co
 #undef ROWS_OFF
   } else {
     const size_t sm = tsz + (size_t)cm.G * cm.LR * sizeof(REAL);
-    if (sm > 200 * 1024) { cudaFreeAsync(part, st); set_error("blml_rows: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+    if (sm > 200 * 1024) { if (!ws) cudaFreeAsync(part, st); set_error("blml_rows: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
     if (grad) {
       cudaFuncSetAttribute(k_rows_general<REAL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
       k_rows_general<REAL, true><<<grid, PR_THREADS, sm, st>>>(cm, T, RT, dT, dR, ZA, R, ZB, w, 0, slice, M, part, dpart);
@@ -398,11 +408,64 @@ static int rows_impl(const blml_tables* tb, const ColMeta& cm, const REAL* T, co
     }
     e = cuda_status(cudaGetLastError(), "blml_rows finish");
   }
-  cudaFreeAsync(part, st);
+  if (!ws) cudaFreeAsync(part, st);
   return e;
 }
 
 extern "C" {
+
+// a rows plan: the tables' metadata read and the coordinates' extents checked once, for many value-row passes over
+// rows of the same coordinate set (the block coordinate descent's passes of every bin against a block)
+struct blml_rows_plan_s {
+  blml_tables tb;
+  ColMeta cm;
+};
+
+int blml_rows_plan_create(const blml_tables* tb, const int64_t* Z, int64_t n, void* stream, blml_rows_plan* out) {
+  if (!tb || !out || n < 0 || (n > 0 && !Z)) { set_error("blml_rows_plan_create: bad arguments"); return BLML_ERR_ARG; }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  blml_rows_plan_s* p = new blml_rows_plan_s();
+  p->tb = *tb;
+  int e = read_meta(tb, p->cm, st);
+  if (!e && n > 0) e = check_extents(p->cm, Z, n, Z, n, st);          // every pair within Z: min / max per column
+  if (!e && (tb->f32 ? (!tb->T32 || (p->cm.G && !tb->RT32)) : (!tb->T || (p->cm.G && !tb->RT)))) {
+    set_error("blml_rows_plan_create: value tables missing"); e = BLML_ERR_ARG;
+  }
+  if (e) { delete p; return e; }
+  *out = p;
+  return BLML_OK;
+}
+
+int64_t blml_rows_plan_workspace(blml_rows_plan p, int64_t R, int64_t M) {
+  if (!p || R < 0 || M < 1) return -1;
+  int64_t nsl, slice;
+  rows_slices(R, M, nsl, slice);
+  return nsl * R * (int64_t)sizeof(double);
+}
+
+int blml_rows_plan_run(blml_rows_plan p, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
+                       double* s, void* ws, int64_t ws_bytes, void* stream) {
+  if (!p || R < 0 || M < 0) { set_error("blml_rows_plan_run: bad arguments"); return BLML_ERR_ARG; }
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (R == 0) return BLML_OK;
+  if (M == 0) return cuda_status(cudaMemsetAsync(s, 0, R * sizeof(double), st), "blml_rows_plan_run");
+  const int64_t need = blml_rows_plan_workspace(p, R, M);
+  if (!ws || ws_bytes < need) {
+    set_error("blml_rows_plan_run: workspace of %lld bytes, need %lld", (long long)ws_bytes, (long long)need);
+    return BLML_ERR_WORKSPACE;
+  }
+  const blml_tables* tb = &p->tb;
+  if (tb->f32)
+    return rows_impl<float>(tb, p->cm, tb->T32, tb->RT32, nullptr, nullptr, ZA, R, ZB, M, w, 0, s, nullptr, st,
+                            reinterpret_cast<double*>(ws));
+  return rows_impl<double>(tb, p->cm, tb->T, tb->RT, nullptr, nullptr, ZA, R, ZB, M, w, 0, s, nullptr, st,
+                           reinterpret_cast<double*>(ws));
+}
+
+int blml_rows_plan_destroy(blml_rows_plan p) {
+  delete p;
+  return BLML_OK;
+}
 
 int blml_rows(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
               int grad, double* s, double* ds, void* stream) {

@@ -380,6 +380,19 @@ typedef struct {
 } blml_tables;
 int blml_rows(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
               int grad, double* s, double* ds, void* stream);
+/* ---- value rows over one coordinate set, validated once (the block coordinate descent of BLMLQuick,
+ *      blml_trivial.py:2860-3035 / blml_gpu.py:340-373, whose passes run every bin against a block of bins) ----
+ * plan_create reads the tables' metadata and checks that every pair of rows of Z (n x d rank coordinates, device)
+ * lies in the tables' extents; plan_run then computes s = rows(ZA, ZB, w) (value rows, as blml_rows) for ZA and ZB made
+ * of rows of that Z -- the caller's promise, not re-checked -- with no host synchronisation and no allocation:
+ * ws holds blml_rows_plan_workspace(plan, R, M) bytes. The plan copies the table struct; the device tables it points
+ * to must outlive it. */
+typedef struct blml_rows_plan_s* blml_rows_plan;
+int blml_rows_plan_create(const blml_tables* tab, const int64_t* Z, int64_t n, void* stream, blml_rows_plan* plan);
+int64_t blml_rows_plan_workspace(blml_rows_plan plan, int64_t R, int64_t M);
+int blml_rows_plan_run(blml_rows_plan plan, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                       const double* w, double* s, void* ws, int64_t ws_bytes, void* stream);
+int blml_rows_plan_destroy(blml_rows_plan plan);
 /* ---- blml_rows without any allocation: no counterpart in the reference ----
  * For callers that cannot allocate device memory themselves or let the library do it: processes whose device
  * memory is reserved up front by another allocator (a cudaMalloc would fail or fragment that pool), and embedded

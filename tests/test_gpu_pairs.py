@@ -97,3 +97,34 @@ def test_cols_joint_and_marginal(cuda_device, case, masks):
         cols(A, B, tab, out, out_m=out_m, depmask=mask)
         assert np.abs(out.cpu().numpy() - c['joint']).max() <= 1e-12
         assert np.abs(out_m.cpu().numpy() - c[f'marg{mask}']).max() <= 1e-12, mask
+
+
+def test_rows_plan_equals_rows(cuda_device):
+    """The validated-once rows plan (the block coordinate descent's passes) gives blml_rows' sums, bit for bit, on
+    the 5-D bins against a block of them and against all of them."""
+    import ctypes as C
+    from blml_b200.local_gpu import ProductKernel, rows_dev, rank_coords, dev_tab, _struct
+    from blml_b200 import _lib
+    from blml_b200._lib import call
+    p = golden('pairs.npz')['p5']
+    u, cnt = p['bins'], p['counts']
+    pk = ProductKernel(['sinc'] * 5, [None] * 5)
+    tab = pk.tables(p['fc'], [None] * 5, p['h'], u)
+    Z = torch.as_tensor(rank_coords(u, tab)).cuda()
+    B = Z.shape[0]
+    st = torch.cuda.current_stream().cuda_stream
+    plan = C.c_void_p()
+    call('blml_rows_plan_create', _struct(tab, dev_tab(tab, 'cuda'), False, False), Z.data_ptr(), B, st, C.byref(plan))
+    try:
+        idx = torch.as_tensor(np.random.default_rng(1).permutation(B)[:257]).cuda()
+        for ZB in (Z[idx].contiguous(), Z):
+            w = torch.as_tensor(np.random.default_rng(2).standard_normal(ZB.shape[0])).cuda()
+            ref = rows_dev(Z, ZB, w, tab)[0]
+            ws = torch.empty(int(_lib.lib().blml_rows_plan_workspace(plan, B, ZB.shape[0])), dtype=torch.uint8,
+                             device='cuda')
+            out = torch.empty(B, dtype=torch.float64, device='cuda')
+            call('blml_rows_plan_run', plan, Z.data_ptr(), B, ZB.data_ptr(), ZB.shape[0], w.data_ptr(), out.data_ptr(),
+                 ws.data_ptr(), ws.numel(), st)
+            assert torch.equal(out, ref)
+    finally:
+        _lib.lib().blml_rows_plan_destroy(plan)
