@@ -70,12 +70,16 @@ def lanczos_max(plan, dh, red, stream, tol=1e-6, seed=0, max_basis=96, max_resta
     return theta
 
 
-def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, vectors=False):
+def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, vectors=False, above=None):
     """The certificate of every fit of a fitted BLMLBinnedBatch at once: lambda_max(D^1/2 S D^1/2) per fit
     (blml_binned.py:501-518), D = sum_k |e_k|^2 / w on occupied bins, by float64 Lanczos with full
     reorthogonalisation, all fits in lockstep: one grouped mat-vec, segmented inner products and linear combinations
     per step, each fit's tridiagonal problem on the host (every third step), restarts from the Ritz vector until
-    every fit's Ritz residual |beta_j y_j| <= tol |theta|. Returns (theta (F,), dh, v): dh the per-bin scaling and v
+    every fit's Ritz residual |beta_j y_j| <= tol |theta|, or its Ritz value moved by less than 1e-9 relative between
+    two checks (at a certified optimum the top eigenvalue is K-fold, so the residual of its Ritz vector converges far
+    more slowly than the value). above: per-fit thresholds; a Ritz value is a lower bound of lambda_max, so a fit
+    whose Ritz value exceeds its threshold is decided there (its Ritz vector then has a Rayleigh quotient above the
+    threshold: the direction a new mode takes). Returns (theta (F,), dh, v): dh the per-bin scaling and v
     the top Ritz vectors (float64 per bin over all fits, None unless vectors) -- d = dh v is the direction of a new
     mode."""
     from scipy.linalg import eigh_tridiagonal
@@ -111,7 +115,8 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     V[0].copy_(torch.as_tensor(np.random.default_rng(seed).standard_normal(B)))
     nrm = dots([(V[0], V[0])])[:, 0]
     lin(V[0], (1.0 / np.sqrt(np.maximum(nrm, 1e-300)))[:, None], [V[0]])
-    theta = np.zeros(F); done = np.zeros(F, bool)
+    theta = np.zeros(F); done = np.zeros(F, bool); prev = np.full(F, np.nan)
+    above = np.full(F, np.inf) if above is None else np.asarray(above, float)
     wv = torch.empty(B, dtype=torch.float64, device=dev)
     vec = torch.zeros(B, dtype=torch.float64, device=dev) if vectors else None
     R = torch.empty(B, dtype=torch.float64, device=dev)
@@ -140,8 +145,10 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                     ev, evec = eigh_tridiagonal(alphas[f, :j + 1], betas[f, :j], select='i', select_range=(j, j))
                     th = float(ev[0]); y = evec[:, 0]
                     theta[f] = th; yr[f] = y
-                    if abs(beta[f] * y[-1]) <= tol * max(abs(th), 1e-300) or beta[f] <= 1e-14 * max(abs(th), 1e-300):
+                    if (abs(beta[f] * y[-1]) <= tol * max(abs(th), 1e-300) or beta[f] <= 1e-14 * max(abs(th), 1e-300)
+                            or th > above[f] or abs(th - prev[f]) <= 1e-9 * abs(th)):
                         conv[f] = True
+                    prev[f] = th
                 if np.all(done | conv):
                     j_end = j + 1
                     break

@@ -628,12 +628,15 @@ class BLMLBinnedBatch:
         return self.dens_t[a:b].cpu().numpy().reshape(self.shapes[f])
 
     # ---------------------------------------------------------------- certificate and certified fits
-    def certificate(self, tol=1e-6, vectors=False):
+    def certificate(self, tol=1e-6, vectors=False, decide_above=None):
         """lambda_max(D^1/2 S D^1/2) / n of every fit (blml_binned.py:501-518; D = sum_k |e_k|^2 / w on occupied
         bins), by float64 Lanczos over all fits at once. <= 1 (up to the solver's tolerance) when the fit is the
-        optimum of the convex lift. With vectors: (certificates, dh, v), v the top eigenvectors (per bin)."""
+        optimum of the convex lift. With vectors: (certificates, dh, v), v the top eigenvectors (per bin).
+        decide_above: a level (e.g. 1 + cert_tol) past which a fit's value need not be refined -- the Lanczos value is
+        a lower bound, so the returned value is then a lower bound above that level."""
         from .certificate import lanczos_max_batched
-        theta, dh, v = lanczos_max_batched(self, tol=tol, seed=self.seed, vectors=vectors)
+        above = None if decide_above is None else decide_above * self.n
+        theta, dh, v = lanczos_max_batched(self, tol=tol, seed=self.seed, vectors=vectors, above=above)
         cert = theta / self.n
         return (cert, dh, v) if vectors else cert
 
@@ -682,12 +685,13 @@ class BLMLBinnedBatch:
         while True:
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record()
-            cert, dh, v = cur.certificate(vectors=True)
+            cert, dh, v = cur.certificate(vectors=True, decide_above=1.0 + cert_tol)
             ev[1].record(); ev[1].synchronize()
             st = self.certify_stats_
             st['seconds_certificate'] += ev[0].elapsed_time(ev[1]) / 1e3
             st['rounds'] += 1; st['fits_per_round'].append(len(idx))
             st['lbfgs_iterations_max'].append(int(max(r.n_sweeps_ for r in cur.results_)))
+            st.setdefault('lbfgs_seconds', []).append(round(cur.timing_['lbfgs_s'] + cur.timing_['start_s'], 4))
             st.setdefault('lanczos', []).append(cur.lanczos_stats_)
             nxt_fits, nxt_starts, nxt_caps = [], [], []
             for j, i in enumerate(idx):

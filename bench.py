@@ -326,6 +326,35 @@ def pairs_bench(dev, reps=3):
     return out
 
 
+def quick5d_bench(dev, solvers=('block', 'jacobi')):
+    """The 5-D fixed-lattice fit at size (n = 2e5 points of an 8-component mixture, bins at 1/64, B ~ 1.84e5 occupied
+    bins, sinc fc = 0.1 cycles per bin per column; blml_trivial.py:2860-3035 through BLMLQuickLattice): float32 pair
+    tables, float64 state and loglik, tol 1e-4 (BLMLQuick's default); wall time of the public fit call, sweeps, the
+    final max|rho| (S e recomputed exactly at the stop) and the loglik. The objective is convex (real rank 1), so a fit
+    that meets tol is at the unique optimum; solvers: the block coordinate descent and the Jacobi / Anderson sweep."""
+    import torch
+    from blml_b200 import workloads
+    from blml_b200.quick import BLMLQuickLattice, bin_points
+    from blml_b200.spec import make_modes, with_lattice
+    X = workloads.points_5d_mixture(seed=0)
+    u, cnt = bin_points(X, 1 / 64, device=dev)
+    Zc = u.cpu().numpy() / 64.0
+    w = cnt.cpu().numpy()
+    modes = with_lattice(make_modes(np.full(5, 0.1 * 64), ['sinc'] * 5), 1 / 64)
+    out = {'workload': '5-D fixed-lattice fit: n = 2e5 points, 8-component mixture, bins at 1/64, sinc fc 0.1 / bin',
+           'bins': int(len(w))}
+    for solver in solvers:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m = BLMLQuickLattice(tol=1e-4, dtype=np.float32, device=dev, solver=solver).fit(Zc, modes, sample_weight=w)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        out[solver] = {'seconds': t, 'sweeps': int(m.n_sweeps_), 'residual': float(m.residual_),
+                       'converged': bool(m.converged_), 'loglik': float(m.loglik_), 'stop': m.stop_reason_,
+                       'seconds_per_sweep': t / max(m.n_sweeps_, 1)}
+    return out
+
+
 def select_bench(dev, n_search=16, seq_sample=2, batch=256):
     """The cut-off search over many lattices (selector.py:488-553 `_search`, run on binned counts as
     dslit_job.py:158-171 does): 16 lattices of 64 x 64 from two-disk fields (band fc geomspace(0.08, 0.4, 16),
@@ -483,6 +512,8 @@ def main():
                     help='one certified sweep (rank growth) with its per-round statistics, and exit')
     ap.add_argument('--pairs', action='store_true',
                     help='the 5-D pair path: one full rows pass over all bin pairs, GPU and a CPU-oracle sample')
+    ap.add_argument('--quick5d', action='store_true',
+                    help='the 5-D fixed-lattice fit at size (B ~ 1.84e5 bins): block CD and Jacobi sweeps')
     ap.add_argument('--select', action='store_true',
                     help='the batched cut-off search over 16 lattices beside the sequential single-fit search')
     ap.add_argument('--extras', action='store_true',
@@ -507,6 +538,9 @@ def main():
         return
     if args.select:
         print(json.dumps(select_bench(dev)), flush=True)
+        return
+    if args.quick5d:
+        print(json.dumps(quick5d_bench(dev)), flush=True)
         return
     if args.extras:
         print(json.dumps(extras_bench(dev)), flush=True)
