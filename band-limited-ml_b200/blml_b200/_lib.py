@@ -59,6 +59,8 @@ _SIGS = {
     'blml_plan_route': (_I, [_P]),
     'blml_group_set_route': (_I, [_P, _I]),
     'blml_group_route': (_I, [_P]),
+    'blml_fft_set_shape': (_I, [_I, _I]),
+    'blml_fft_get_shape': (_I, [_P, _P]),
     'blml_seg_blocks': (_I, []),
     'blml_seg_start_root': (_I, [_I, _I, _P, _P, _P, _P, _P, _P]),
     'blml_seg_update_real1': (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -160,7 +162,20 @@ def lib():
             f.restype = res
             f.argtypes = args
         _lib = L
+        _apply_tuning(L)
     return _lib
+
+
+TUNING_PATH = os.path.join(_HERE, 'fft_tuning.json')
+
+
+def _apply_tuning(L):
+    """The FFT route's launch shape from the autotuner's table (bench.py --tune writes it), if the package has one."""
+    if os.path.exists(TUNING_PATH):
+        import json
+        t = json.load(open(TUNING_PATH))
+        if L.blml_fft_set_shape(int(t['cta_bytes']), int(t['max_cols'])) != 0:
+            raise BLMLError(f'{TUNING_PATH}: {L.blml_last_error().decode(errors="replace")}')
 
 
 def check(rc, what):

@@ -23,7 +23,13 @@
 namespace blml {
 
 constexpr int kFT = 256;                 // threads per CTA
-constexpr int kCtaBytes = 72 * 1024;     // shared memory a CTA aims for (3 CTAs per SM); one transform when longer
+constexpr int kCtaBytesMax = 72 * 1024;  // the largest shared-memory budget a CTA may aim for (3 CTAs per SM)
+
+// launch shape of the route, chosen by blml_fft_set_shape (the project's autotuner writes a table the package applies)
+// and read when a plan's descriptor is made: the shared memory a CTA aims for (several transforms per CTA; one when
+// longer) and the most columns a CTA of the column stage takes
+static int g_cta_bytes = kCtaBytesMax;
+static int g_max_cols = 2;
 constexpr int kMaxSide = 4096;           // longest side of the route
 constexpr int kMaxRad = 12;
 
@@ -398,7 +404,7 @@ static bool axis_plan(int N, FftAxis& ax, std::vector<double>& tw) {
 
 // transforms of length N per CTA: as many as two padded buffers and the twiddles hold within kCtaBytes, at least one
 static int transforms_per_cta(int N, size_t esz) {
-  const long long room = (long long)(kCtaBytes / esz) - N;
+  const long long room = (long long)(g_cta_bytes / esz) - N;
   return (int)std::max<long long>(1, room / (2LL * pld(N)));
 }
 
@@ -469,7 +475,7 @@ static FftDesc make_desc(const blml_plan_s* p, const void* x, void* y, void* z, 
   D.flags = xc ? 0 : (1 | 4);
   const size_t esz = p->dtype == BLML_F64 ? 16 : 8;
   // the column stage has few transforms (H2 per lattice): at most 2 per CTA, so its launch still fills the GPU
-  D.rows = transforms_per_cta(fp->M2, esz); D.cols = std::min(2, transforms_per_cta(fp->M1, esz));
+  D.rows = transforms_per_cta(fp->M2, esz); D.cols = std::min(g_max_cols, transforms_per_cta(fp->M1, esz));
   D.ctasA = (nb * fp->M1 + D.rows - 1) / D.rows;
   D.ctasB = (nb * fp->H2 + D.cols - 1) / D.cols;
   D.ax1 = fp->ax1; D.ax2 = fp->ax2;
@@ -484,7 +490,7 @@ struct FftGroup {
 };
 
 // the largest dynamic shared memory any stage asks for: two padded buffers of one kMaxSide-point transform and its
-// twiddles, in float64 (shorter transforms stay within kCtaBytes)
+// twiddles, in float64 (shorter transforms stay within the CTA budget)
 constexpr size_t kMaxSmem = (size_t)(2 * (kMaxSide + kMaxSide / 8 + 1) + kMaxSide) * 16;
 
 // the six kernels' dynamic shared-memory limit, set once per device (outside any stream capture: at plan creation)
@@ -605,3 +611,22 @@ int fft_matvec(blml_plan_s* p, const void* x, void* y, int nb, int xc, void* ws,
 }
 
 }  // namespace blml
+
+extern "C" {
+
+int blml_fft_set_shape(int cta_bytes, int max_cols) {
+  if (cta_bytes < 8 * 1024 || cta_bytes > blml::kCtaBytesMax || max_cols < 1 || max_cols > 64) {
+    blml::set_error("blml_fft_set_shape: 8 KiB <= cta_bytes <= %d, 1 <= max_cols <= 64", blml::kCtaBytesMax);
+    return BLML_ERR_ARG;
+  }
+  blml::g_cta_bytes = cta_bytes; blml::g_max_cols = max_cols;
+  return BLML_OK;
+}
+
+int blml_fft_get_shape(int* cta_bytes, int* max_cols) {
+  if (!cta_bytes || !max_cols) { blml::set_error("blml_fft_get_shape: null argument"); return BLML_ERR_ARG; }
+  *cta_bytes = blml::g_cta_bytes; *max_cols = blml::g_max_cols;
+  return BLML_OK;
+}
+
+}

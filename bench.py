@@ -326,6 +326,53 @@ def pairs_bench(dev, reps=3):
     return out
 
 
+def tune_fft(dev, cta_kib=(24, 32, 48, 64, 72), max_cols=(1, 2, 4), reps=20):
+    """The project's autotuner for the FFT route's launch shape: the grouped mat-vec over the 64 sweep lattices
+    (complex float64, and real float64 as the start phase runs it) timed with CUDA events for every shared-memory
+    budget per CTA and column-stage width; the fastest total is written to the package's fft_tuning.json, which the
+    library applies at load. Returns every measurement."""
+    import torch
+    from blml_b200 import _lib
+    from blml_b200.sweep import BLMLBinnedBatch, _Group
+    import ctypes as C
+    sweep, modes = workload(0)
+    b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
+    b._prepare([f['train'] for f in sweep], modes)
+    st = torch.cuda.current_stream(dev)
+    off = b.boff[:-1]
+    xc = torch.randn(b.Btot, dtype=torch.complex128, device=dev); yc = torch.empty_like(xc)
+    xr = torch.randn(b.Btot, dtype=torch.float64, device=dev); yr = torch.empty_like(xr)
+    L = _lib.lib()
+    c0, m0 = C.c_int(), C.c_int()
+    L.blml_fft_get_shape(C.byref(c0), C.byref(m0))
+    rows = []
+    try:
+        for kib in cta_kib:
+            for mc in max_cols:
+                _lib.call('blml_fft_set_shape', kib * 1024, mc)
+                t = {}
+                for name, x, y, xcp in (('complex', xc, yc, True), ('real', xr, yr, False)):
+                    g = _Group(b.p64, x, off, y, off, xcp)
+                    for _ in range(3):
+                        g(st.cuda_stream)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    for _ in range(reps):
+                        g(st.cuda_stream)
+                    e1.record(st); torch.cuda.synchronize()
+                    t[name] = e0.elapsed_time(e1) * 1e3 / reps
+                    del g
+                rows.append({'cta_bytes': kib * 1024, 'max_cols': mc, 'us_complex': t['complex'], 'us_real': t['real']})
+    finally:
+        L.blml_fft_set_shape(c0.value, m0.value)
+    best = min(rows, key=lambda r: 2 * r['us_complex'] + r['us_real'])      # the L-BFGS runs two complex per real
+    out = {'best': best, 'candidates': rows,
+           'what': 'grouped FFT mat-vec over the 64 sweep lattices, float64, CUDA events, 20 launches each'}
+    with open(os.path.join(ROOT, 'band-limited-ml_b200', 'blml_b200', 'fft_tuning.json'), 'w') as fh:
+        json.dump({'cta_bytes': best['cta_bytes'], 'max_cols': best['max_cols'], 'measured': out}, fh, indent=1)
+    return out
+
+
 def quick5d_bench(dev, solvers=('block', 'jacobi')):
     """The 5-D fixed-lattice fit at size (n = 2e5 points of an 8-component mixture, bins at 1/64, B ~ 1.84e5 occupied
     bins, sinc fc = 0.1 cycles per bin per column; blml_trivial.py:2860-3035 through BLMLQuickLattice): float32 pair
@@ -512,6 +559,8 @@ def main():
                     help='one certified sweep (rank growth) with its per-round statistics, and exit')
     ap.add_argument('--pairs', action='store_true',
                     help='the 5-D pair path: one full rows pass over all bin pairs, GPU and a CPU-oracle sample')
+    ap.add_argument('--tune', action='store_true',
+                    help="the FFT route's autotuner: time its launch shapes on the sweep, write the package's table")
     ap.add_argument('--quick5d', action='store_true',
                     help='the 5-D fixed-lattice fit at size (B ~ 1.84e5 bins): block CD and Jacobi sweeps')
     ap.add_argument('--select', action='store_true',
@@ -541,6 +590,9 @@ def main():
         return
     if args.quick5d:
         print(json.dumps(quick5d_bench(dev)), flush=True)
+        return
+    if args.tune:
+        print(json.dumps(tune_fft(dev)), flush=True)
         return
     if args.extras:
         print(json.dumps(extras_bench(dev)), flush=True)

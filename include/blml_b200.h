@@ -77,6 +77,11 @@ int blml_group_destroy(blml_group group);
    FFT, inverse row FFTs) when every plan has one and BLML_ROUTE_AUTO, else the 2 d restricted-transform stages */
 int blml_group_set_route(blml_group group, int route);
 int blml_group_route(blml_group group);
+/* the FFT route's launch shape for descriptors made from now on (plans' single mat-vecs, groups created later): the
+   shared memory a CTA aims for (8 KiB .. 72 KiB; several rows per CTA up to it) and the most columns per CTA of the
+   column stage. The package sets the shape its autotuner measured fastest (bench.py --tune) at import. */
+int blml_fft_set_shape(int cta_bytes, int max_cols);
+int blml_fft_get_shape(int* cta_bytes, int* max_cols);
 
 /* ---- coordinate (Jacobi) update of every bin (BLMLBinned._update / _secular / _cd_root,
  *      blml_binned.py:184-206, 1549-1573; cd_root blml_trivial.py:84-89) ----
