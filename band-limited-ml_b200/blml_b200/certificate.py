@@ -75,9 +75,9 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     (blml_binned.py:501-518), D = sum_k |e_k|^2 / w on occupied bins, by float64 Lanczos with full
     reorthogonalisation, all fits in lockstep: one grouped mat-vec, segmented inner products and linear combinations
     per step, each fit's tridiagonal problem on the host (every third step), restarts from the Ritz vector until
-    every fit's Ritz residual |beta_j y_j| <= tol |theta|, or its Ritz value moved by less than 1e-9 relative between
+    every fit's Ritz residual |beta_j y_j| <= tol |theta|, or its Ritz value moved by less than 1e-8 relative between
     two checks (at a certified optimum the top eigenvalue is K-fold, so the residual of its Ritz vector converges far
-    more slowly than the value). above: per-fit thresholds; a Ritz value is a lower bound of lambda_max, so a fit
+    more slowly than the value; 1e-8 is far below any certification bar). above: per-fit thresholds; a Ritz value is a lower bound of lambda_max, so a fit
     whose Ritz value exceeds its threshold is decided there (its Ritz vector then has a Rayleigh quotient above the
     threshold: the direction a new mode takes). Returns (theta (F,), dh, v): dh the per-bin scaling and v
     the top Ritz vectors (float64 per bin over all fits, None unless vectors) -- d = dh v is the direction of a new
@@ -146,7 +146,7 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                     th = float(ev[0]); y = evec[:, 0]
                     theta[f] = th; yr[f] = y
                     if (abs(beta[f] * y[-1]) <= tol * max(abs(th), 1e-300) or beta[f] <= 1e-14 * max(abs(th), 1e-300)
-                            or th > above[f] or abs(th - prev[f]) <= 1e-9 * abs(th)):
+                            or th > above[f] or abs(th - prev[f]) <= 1e-8 * abs(th)):
                         conv[f] = True
                     prev[f] = th
                 if np.all(done | conv):

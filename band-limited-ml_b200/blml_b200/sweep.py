@@ -666,13 +666,15 @@ class BLMLBinnedBatch:
              v.data_ptr(), sc.data_ptr(), En.data_ptr(), self.st)
         return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
 
-    def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300):
+    def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300,
+                      grow_margin=10.0):
         """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
         batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
         mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
         to tol at the same rank and checked again. Rounds before the last rank are capped at grow_iters L-BFGS
         iterations: at too low a rank the solver crawls along the lift's boundary, so those fits only have to show that
-        they need another mode. The lift is convex: a fit that meets the certificate at tol is at its unique optimum
+        they need another mode. A capped fit whose certificate is above the bar by less than grow_margin times
+        cert_tol is run on to tol at its rank before it may grow (its excess may be the cap's, not the rank's). The lift is convex: a fit that meets the certificate at tol is at its unique optimum
         (the reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results
         carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...]."""
         F = len(counts_list)
@@ -702,7 +704,8 @@ class BLMLBinnedBatch:
                 r.certificate_, r.rank_, r.rank_path_ = float(cert[j]), K, paths[i]
                 final[i] = r
                 ok = cert[j] <= 1.0 + cert_tol
-                if was_capped and (ok or K >= max_rank):
+                near = cert[j] <= 1.0 + grow_margin * cert_tol
+                if was_capped and (near or K >= max_rank):
                     nxt_fits.append((j, i, K)); nxt_caps.append(-1)            # run on to tol at this rank
                 elif not ok and K < max_rank:
                     nxt_fits.append((j, i, K + 1)); nxt_caps.append(grow_iters if K + 1 < max_rank else -1)

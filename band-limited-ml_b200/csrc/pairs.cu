@@ -628,8 +628,8 @@ static int cols_launch(const blml_tables* tb, const int64_t* ZA, int64_t R, cons
   e = check_extents(cm, ZA, R, ZB, M, st);
   if (e) return e;
   unsigned dep_units = 0;                        // a unit (column or radial group) is dep when one of its columns is
-  for (int k = 0; k < cm.d; k++)
-    if ((depmask >> k) & 1) dep_units |= 1u << cm.dim_unit[k];
+  for (int k = 0; k < cm.d; k++)              // a group column's unit is its group's
+    if ((depmask >> k) & 1) dep_units |= 1u << ((cm.code[k] == 2 || cm.code[k] == 4) ? cm.grp_unit[cm.grp[k]] : cm.dim_unit[k]);
   const int64_t n = R * M;
   const int g = (int)std::min<int64_t>((n + 255) / 256, 148 * 32);
   if (tb->f32) {
