@@ -373,6 +373,69 @@ def tune_fft(dev, cta_kib=(24, 32, 48, 64, 72), max_cols=(1, 2, 4), reps=20):
     return out
 
 
+def config2_bench(dev, reps=50):
+    """The 256 x 256 complex two-mode pball workload (pball 0.33 + background pball 3/256, L-BFGS tol 1e-6, float64,
+    the reference's seeded start) through the public fit call, against the reference's own fit of the same counts
+    (tests/golden/config2_256.npz holds its loglik, iterations and CPU seconds); and one mat-vec of each mode on every
+    route: FFT float64, restricted transforms float64, tcgen05 split-TF32 float32 -- CUDA events, mat-vecs/s, GB/s of
+    the algorithmic bytes (read E + write U, complex of the storage type) and the error against the FFT float64
+    result."""
+    import torch
+    from blml_b200 import workloads, _lib
+    from blml_b200.binned import BLMLBinned
+    from blml_b200.operator import Plan, mode_transform, pad_rule
+    from blml_b200.spec import parse_modes
+    shape = (256, 256)
+    counts = workloads.two_disk_field(shape, fc=0.33, N=1e6, seed=0)
+    modes = workloads.pball_modes(shape, 0.33, bg_fc=3.0 / 256)
+    g = np.load(os.path.join(ROOT, 'tests', 'golden', 'config2_256.npz'))
+    out = {'workload': '256 x 256 complex pball 0.33 + background pball 3/256, L-BFGS tol 1e-6, float64'}
+    BLMLBinned(dtype=np.float64, solver='lbfgs', tol=1e-6, device=dev).fit(counts, modes, complex_g=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m = BLMLBinned(dtype=np.float64, solver='lbfgs', tol=1e-6, device=dev).fit(counts, modes, complex_g=True)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    ll_ref = float(g['loglik'])
+    out['fit'] = {'seconds': t, 'iterations': int(m.n_sweeps_), 'loglik': float(m.loglik_),
+                  'rel_dloglik_vs_reference': (float(m.loglik_) - ll_ref) / abs(ll_ref),
+                  'reference_cpu_seconds': float(g['seconds']), 'reference_iterations': int(g['n_sweeps']),
+                  'reference_cores': int(g['cores'])}
+    specs, _ = parse_modes(modes, 2)
+    h = np.ones(2)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    rng = np.random.default_rng(3)
+    for k, sp in enumerate(specs):
+        tr = mode_transform(sp, shape, h, pad_rule(shape, h, specs))
+        e = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+        ref = None
+        row = {}
+        for name, code, eng, route in (('fft_f64', _lib.F64, _lib.ENGINE_SIMT, _lib.ROUTE_FFT),
+                                       ('contract_f64', _lib.F64, _lib.ENGINE_SIMT, _lib.ROUTE_CONTRACT),
+                                       ('tcgen05_split_tf32_f32', _lib.F32, _lib.ENGINE_TC, None)):
+            p = Plan(*tr, shape, code, eng)
+            if route is not None:
+                p.route = route
+            x = torch.as_tensor(e).to(dev, torch.complex128 if code == _lib.F64 else torch.complex64)
+            y = torch.empty_like(x)
+            for _ in range(3):
+                p.apply(x, y, 1, True, st)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                p.apply(x, y, 1, True, st)
+            e1.record(); torch.cuda.synchronize()
+            tm = e0.elapsed_time(e1) / 1e3 / reps
+            yy = y.cpu().numpy().astype(np.complex128)
+            if ref is None:
+                ref = yy
+            nbytes = 2 * x.numel() * x.element_size()
+            row[name] = {'us': tm * 1e6, 'matvecs_per_s': 1.0 / tm, 'GB_per_s': nbytes / tm / 1e9,
+                         'rel_err_vs_fft_f64': float(np.abs(yy - ref).max() / np.abs(ref).max())}
+        out[f'mode{k}_matvec'] = row
+    return out
+
+
 def quick5d_bench(dev, solvers=('block', 'jacobi')):
     """The 5-D fixed-lattice fit at size (n = 2e5 points of an 8-component mixture, bins at 1/64, B ~ 1.84e5 occupied
     bins, sinc fc = 0.1 cycles per bin per column; blml_trivial.py:2860-3035 through BLMLQuickLattice): float32 pair
@@ -561,6 +624,8 @@ def main():
                     help='the 5-D pair path: one full rows pass over all bin pairs, GPU and a CPU-oracle sample')
     ap.add_argument('--tune', action='store_true',
                     help="the FFT route's autotuner: time its launch shapes on the sweep, write the package's table")
+    ap.add_argument('--config2', action='store_true',
+                    help='the 256 x 256 complex two-mode pball fit and its mat-vec routes')
     ap.add_argument('--quick5d', action='store_true',
                     help='the 5-D fixed-lattice fit at size (B ~ 1.84e5 bins): block CD and Jacobi sweeps')
     ap.add_argument('--select', action='store_true',
@@ -590,6 +655,9 @@ def main():
         return
     if args.quick5d:
         print(json.dumps(quick5d_bench(dev)), flush=True)
+        return
+    if args.config2:
+        print(json.dumps(config2_bench(dev)), flush=True)
         return
     if args.tune:
         print(json.dumps(tune_fft(dev)), flush=True)
