@@ -764,3 +764,45 @@ def certified_log_density(results, counts_list, eps=0.0):
         for f, i in mine.items():
             out[i] = sc[f]
     return out
+
+
+class BLMLBinnedRolling:
+    """Rolling-window refits of many sequences at once (blml_rolling.py:40-155: BLMLRolling refits one estimator per
+    window, each fit warm-started from the previous window's through init=). Each update(windows) takes the next count
+    window of every sequence (one lattice per sequence), fits them all in one BLMLBinnedBatch call, each started from
+    its sequence's previous fit (the first window from the seeded start), and keeps the new coefficients on the
+    device for the next call. Complex one-mode fits (L-BFGS), as BLMLBinnedBatch runs them.
+
+        roll = BLMLBinnedRolling([pball_modes(shape, fc) for shape, fc in zip(shapes, fcs)], tol=1e-6)
+        for windows in stream_of_windows:            # one count array per sequence
+            fits = roll.update(windows)              # FitResults, one per sequence
+    """
+
+    def __init__(self, modes_list, **batch_kw):
+        self.modes_list = list(modes_list)
+        self.batch_kw = dict(batch_kw)
+        self.prev_ = None                             # per sequence: its last coefficients (device)
+        self.n_updates_ = 0
+        self.history_ = []
+
+    def update(self, windows):
+        if len(windows) != len(self.modes_list):
+            raise ValueError("update: one window per sequence")
+        batch = BLMLBinnedBatch(**self.batch_kw)
+        init = None
+        if self.prev_ is not None:
+            init = []
+            for e, w in zip(self.prev_, windows):
+                if tuple(e.shape[-2:]) != tuple(np.shape(w)):
+                    raise ValueError("update: a sequence's windows share its lattice")
+                init.append(e)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        res = batch.fit(list(windows), self.modes_list, init=init)
+        ev[1].record(); ev[1].synchronize()
+        self.prev_ = [batch.e_hat(f).clone() for f in range(batch.F)]
+        self.n_updates_ += 1
+        self.history_.append(dict(seconds=ev[0].elapsed_time(ev[1]) / 1e3,
+                                  iterations=[r.n_sweeps_ for r in res], warm=init is not None))
+        self.batch_ = batch
+        return res
