@@ -1,0 +1,36 @@
+"""What the trained warm start gains (the network shipped with the package, blml_b200/warmstart_weights.npz, trained
+on fits of other seeds): on fresh 128 x 128 two-disk / two-slit fits, the batched engine started from the network's
+roots needs fewer solver iterations (start sweeps + L-BFGS) than from the reference's seeded start, and certifying
+both (rank growth until the certificate is met) reaches the same optimum -- the lift is convex -- so the warm start
+loses no certified fit."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_warm_start_cuts_iterations_and_keeps_certification(cuda_device):
+    from blml_b200 import workloads, warmstart_job
+    from blml_b200.sweep import BLMLBinnedBatch
+    path = os.path.join(os.path.dirname(warmstart_job.__file__), 'warmstart_weights.npz')
+    net = warmstart_job.load(path, device='cuda')
+    fits = workloads.warm_start_set(12, seed=70_000)
+    counts = [f['counts'] for f in fits]; modes = [f['modes'] for f in fits]
+    fcs = [f['fc'] for f in fits]; kinds = [f['kind'] for f in fits]
+    cold = BLMLBinnedBatch(tol=1e-6, max_sweeps=5000, device='cuda').fit(counts, modes)
+    warm = BLMLBinnedBatch(tol=1e-6, max_sweeps=5000, device='cuda').fit(counts, modes,
+                                                                         init=net.start(counts, fcs, kinds))
+    it_cold = sum(r.n_sweeps_ + r.start_sweeps_ for r in cold)
+    it_warm = sum(r.n_sweeps_ + r.start_sweeps_ for r in warm)
+    assert it_warm <= 0.75 * it_cold, (it_warm, it_cold)
+    cc = BLMLBinnedBatch(tol=1e-6, device='cuda').fit_certified(counts, modes, cert_tol=1e-3)
+    cw = BLMLBinnedBatch(tol=1e-6, device='cuda').fit_certified(counts, modes, cert_tol=1e-3,
+                                                                init=net.start(counts, fcs, kinds))
+    ok_c = [r.certificate_ <= 1 + 1e-3 for r in cc]
+    ok_w = [r.certificate_ <= 1 + 1e-3 for r in cw]
+    assert sum(ok_w) >= sum(ok_c), (ok_c, ok_w)
+    for a, b, oa, ob in zip(cc, cw, ok_c, ok_w):
+        if oa and ob:
+            assert abs(a.loglik_ - b.loglik_) <= 1e-6 * abs(a.loglik_), (a.rank_path_, b.rank_path_)
