@@ -310,21 +310,10 @@ static int read_meta(const blml_tables* tb, ColMeta& cm, cudaStream_t st) {
   return BLML_OK;
 }
 
-// the coordinates must lie in the tables' extents: offsets within +-J (offset rows), ranks within the rank table,
-// folded coordinates within the period (circular / torus), radii within the radial row
-static int check_extents(const ColMeta& cm, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
-                         cudaStream_t st) {
-  if (R == 0 || M == 0) return BLML_OK;
-  long long* dr = nullptr;
-  long long hr[4 * MAXD];
-  int e = cuda_status(cudaMallocAsync((void**)&dr, 4 * cm.d * sizeof(long long), st), "pair extents");
-  if (e) return e;
-  k_coord_range<<<cm.d, 256, 0, st>>>(ZA, R, ZB, M, cm.d, dr);
-  count_launches(1);
-  e = cuda_status(cudaMemcpyAsync(hr, dr, 4 * cm.d * sizeof(long long), cudaMemcpyDeviceToHost, st), "pair extents");
-  cudaFreeAsync(dr, st);
-  if (!e) e = cuda_status(cudaStreamSynchronize(st), "pair extents");
-  if (e) return e;
+// the per-column coordinate ranges hr[4 k + (0..3)] = min / max of ZA, min / max of ZB against the tables' extents:
+// offsets within +-J (offset rows), ranks within the rank table, folded coordinates within the period (circular /
+// torus), radii within the radial row
+static int extents_ok(const ColMeta& cm, const long long* hr) {
   double rad[MAXG] = {0, 0, 0, 0};
   for (int k = 0; k < cm.d; k++) {
     const long long mnA = hr[4 * k], mxA = hr[4 * k + 1], mnB = hr[4 * k + 2], mxB = hr[4 * k + 3];
@@ -347,6 +336,24 @@ static int check_extents(const ColMeta& cm, const int64_t* ZA, int64_t R, const 
       return BLML_ERR_ARG;
     }
   return BLML_OK;
+}
+
+// the coordinates must lie in the tables' extents: offsets within +-J (offset rows), ranks within the rank table,
+// folded coordinates within the period (circular / torus), radii within the radial row
+static int check_extents(const ColMeta& cm, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                         cudaStream_t st) {
+  if (R == 0 || M == 0) return BLML_OK;
+  long long* dr = nullptr;
+  long long hr[4 * MAXD];
+  int e = cuda_status(cudaMallocAsync((void**)&dr, 4 * cm.d * sizeof(long long), st), "pair extents");
+  if (e) return e;
+  k_coord_range<<<cm.d, 256, 0, st>>>(ZA, R, ZB, M, cm.d, dr);
+  count_launches(1);
+  e = cuda_status(cudaMemcpyAsync(hr, dr, 4 * cm.d * sizeof(long long), cudaMemcpyDeviceToHost, st), "pair extents");
+  cudaFreeAsync(dr, st);
+  if (!e) e = cuda_status(cudaStreamSynchronize(st), "pair extents");
+  if (e) return e;
+  return extents_ok(cm, hr);
 }
 
 // column slices of a rows launch: so that the grid covers the GPU about four times
@@ -578,27 +585,8 @@ int blml_rows_noalloc(const blml_tables* tb, const int64_t* ZA, int64_t R, const
                   "blml_rows_noalloc extents");
   if (!e) e = cuda_status(cudaStreamSynchronize(st), "blml_rows_noalloc extents");
   if (e) return e;
-  double rad[MAXG] = {0, 0, 0, 0};
-  for (int k = 0; k < cm.d; k++) {
-    const long long mnA = hr[4 * k], mxA = hr[4 * k + 1], mnB = hr[4 * k + 2], mxB = hr[4 * k + 3];
-    const long long span = std::max(mxA - mnB, mxB - mnA);
-    bool ok = true;
-    switch (cm.code[k]) {
-      case 0: ok = span <= cm.J[k]; break;
-      case 3: ok = mnA >= 0 && mnB >= 0 && mxA < cm.mk[k] && mxB < cm.mk[k]; break;
-      case 1: case 4: ok = mnA >= 0 && mnB >= 0 && mxA < cm.nb[k] && mxB < cm.nb[k]; break;
-      case 2: rad[cm.grp[k]] += (double)span * (double)span; break;
-    }
-    if (!ok) {
-      set_error("pair tables: column %d coordinates outside the tables' span (stale tables)", k);
-      return BLML_ERR_ARG;
-    }
-  }
-  for (int k = 0; k < cm.d; k++)
-    if (cm.code[k] == 2 && sqrt(rad[cm.grp[k]]) * RQ + 1 >= cm.LR) {
-      set_error("pair tables: radial group %d radius outside its row (stale tables)", cm.grp[k]);
-      return BLML_ERR_ARG;
-    }
+  e = extents_ok(cm, hr);
+  if (e) return e;
   double* part = scratch + kRowsScratchRangeSlots;
   if (tb->f32) {
     if (!tb->T32 || (cm.G && !tb->RT32)) { set_error("blml_rows_noalloc: float32 tables missing"); return BLML_ERR_ARG; }
