@@ -8,6 +8,7 @@
 // Before any launch the coordinates are checked against the tables' extents on the device, so a stale table is an
 // error, never an out-of-range read.
 #include <mutex>
+#include <cuda.h>
 #include "common.cuh"
 
 namespace blml {
@@ -499,7 +500,8 @@ int blml_rows(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t
 // Its scratch (the per-column coordinate ranges of the extent check, then the column-slice partial sums) lives in
 // this file-scope device array: 4 MiB on every GPU that loads the library, held until the process exits. Host code
 // must not pass the symbol itself to a kernel (on the host it names a stand-in, not device memory): the device
-// address comes from cudaGetSymbolAddress, taken once per device with that device current, on the first call.
+// address comes from cudaGetSymbolAddress, taken once per device with that device current, on the first call (and
+// again if the device's context has changed since).
 constexpr int64_t kRowsScratchDoubles = (int64_t)1 << 19;       // 4 MiB
 constexpr int64_t kRowsScratchRangeSlots = 64;                   // 4 * d <= 32 range words, padded to 512 bytes
 constexpr int64_t kRowsNoAllocMaxR = kRowsScratchDoubles - kRowsScratchRangeSlots;
@@ -510,14 +512,19 @@ static int rows_scratch(double** out) {
   int e = cuda_status(cudaGetDevice(&dev), "blml_rows_noalloc");
   if (e) return e;
   if (dev < 0 || dev >= 64) { set_error("blml_rows_noalloc: device ordinal %d above 63", dev); return BLML_ERR_ARG; }
+  // the address belongs to the device's current context: taken again when that context is not the one it was
+  // taken in (after a cudaDeviceReset, or under another context)
+  CUcontext ctx = nullptr;
+  if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS) { set_error("blml_rows_noalloc: no current context"); return BLML_ERR_CUDA; }
   static std::mutex mu;
   static double* ptrs[64] = {nullptr};
+  static CUcontext ctxs[64] = {nullptr};
   std::lock_guard<std::mutex> lock(mu);
-  if (!ptrs[dev]) {
+  if (!ptrs[dev] || ctxs[dev] != ctx) {
     void* p = nullptr;
     e = cuda_status(cudaGetSymbolAddress(&p, g_rows_scratch), "blml_rows_noalloc scratch address");
     if (e) return e;
-    ptrs[dev] = reinterpret_cast<double*>(p);
+    ptrs[dev] = reinterpret_cast<double*>(p); ctxs[dev] = ctx;
   }
   *out = ptrs[dev];
   return BLML_OK;
