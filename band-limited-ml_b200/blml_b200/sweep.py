@@ -667,14 +667,15 @@ class BLMLBinnedBatch:
         return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
 
     def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300,
-                      grow_margin=10.0):
+                      grow_margin=1.0):
         """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
         batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
         mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
         to tol at the same rank and checked again. Rounds before the last rank are capped at grow_iters L-BFGS
         iterations: at too low a rank the solver crawls along the lift's boundary, so those fits only have to show that
         they need another mode. A capped fit whose certificate is above the bar by less than grow_margin times
-        cert_tol is run on to tol at its rank before it may grow (its excess may be the cap's, not the rank's). The lift is convex: a fit that meets the certificate at tol is at its unique optimum
+        cert_tol (default: none) is run on to tol at its rank before it may grow; on the benchmark sweep a margin of
+        10 doubled the time, the polished fits crawling at too low a rank. The lift is convex: a fit that meets the certificate at tol is at its unique optimum
         (the reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results
         carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...]."""
         F = len(counts_list)

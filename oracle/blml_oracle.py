@@ -605,7 +605,7 @@ class _Start:
         self.e_hat, self.shape = e_hat, shape
 
 
-def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-3, max_rank=8, grow_iters=300, step=0.1, grow_margin=10.0):
+def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-3, max_rank=8, grow_iters=300, step=0.1, grow_margin=1.0):
     """A certified fit of one shared kernel: the complex L-BFGS fit at rank K = 1, 2, ... until the certificate
     lambda_max(D^1/2 S D^1/2) / n <= 1 + cert_tol (blml_binned.py:501-518), each rank started from the previous fit's
     modes plus a new mode step * (rms mode norm) along d = D^1/2 v, v the certificate's top eigenvector (an ascent
