@@ -514,8 +514,21 @@ static int rows_scratch(double** out) {
   if (dev < 0 || dev >= 64) { set_error("blml_rows_noalloc: device ordinal %d above 63", dev); return BLML_ERR_ARG; }
   // the address belongs to the device's current context: taken again when that context is not the one it was
   // taken in (after a cudaDeviceReset, or under another context)
+  // cuCtxGetCurrent through the runtime's driver entry point, so that the library needs no link to libcuda and
+  // loads on a host without a driver
+  using CtxGetFn = CUresult (*)(CUcontext*);
+  static CtxGetFn ctx_get = []() -> CtxGetFn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      return reinterpret_cast<CtxGetFn>(p);
+    return nullptr;
+  }();
   CUcontext ctx = nullptr;
-  if (cuCtxGetCurrent(&ctx) != CUDA_SUCCESS) { set_error("blml_rows_noalloc: no current context"); return BLML_ERR_CUDA; }
+  if (!ctx_get || ctx_get(&ctx) != CUDA_SUCCESS) {
+    set_error("blml_rows_noalloc: no current context"); return BLML_ERR_CUDA;
+  }
   static std::mutex mu;
   static double* ptrs[64] = {nullptr};
   static CUcontext ctxs[64] = {nullptr};
