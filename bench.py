@@ -8,7 +8,8 @@ lambda_max(D^1/2 S D^1/2) / n (blml_binned.py:501-518), and, while it exceeds 1 
 along the certificate's top eigenvector and a refit (at most 8 modes), then the held-out scores. A fit is certified
 when its certificate is <= 1 + 1e-3 and its loglik is within 1e-6 (relative, either side) of the FP64 oracle's
 certified fit of the same counts (oracle/sweep64_certified.json): the convex lift has one optimum, so that loglik is
-unique. value = certified fits/s with the counts in device memory; e2e = the same through the public API from host
+unique. Where the oracle's rank growth stops at 8 modes with its certificate above 1 + 1e-4, its loglik is only a lower
+bound of the optimum, and the fit may not fall more than 1e-6 below it. value = certified fits/s with the counts in device memory; e2e = the same through the public API from host
 counts (host->device copy of the counts, device->host read of every density and score inside each timed step).
 plain_gpu = the same certification with one fit at a time (no batching, cold starts); learned = the learned warm
 start's rank-1 starts, then the same certification.
@@ -32,8 +33,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, 'band-limited-ml_b200'))
 
 N_FITS, TOL, CERT_TOL, MAX_RANK = 64, 1e-6, 1e-3, 8
-METRIC = ('certified fits/s (certificate <= 1 + 1e-3 and |dloglik| <= 1e-6 rel of the FP64 oracle\'s certified fit), '
-          '64-fit 2-D pball cut-off sweep')
+METRIC = ('certified fits/s (certificate <= 1 + 1e-3 and |dloglik| <= 1e-6 rel of the FP64 oracle\'s certified fit; '
+          'not below it where the oracle needs more than 8 modes), 64-fit 2-D pball cut-off sweep')
 CONFIG = {'workload': '64-fit batched 2-D complex pball cut-off sweep: sides {64..384}^2, fc geomspace(0.05, 0.45, '
                       '16), N log-uniform 1e4..1e6, 80/20 held-out split, L-BFGS tol 1e-6, float64 state, '
                       'certified by rank growth',
@@ -208,15 +209,14 @@ def port_sample():
     return sorted(range(N_FITS), key=lambda i: secs[i])[:REF_SAMPLE]
 
 
-def port_step(pool, sample, ll_ref):
+def port_step(pool, sample, ref):
     """One step of the CPU arm: every sample fit certified, one per worker process in parallel; returns (wall
     seconds, certified count) with the main arm's certification rule."""
     t0 = time.perf_counter()
     out = pool.map(_port_certified_fit, sample, chunksize=1)
     wall = time.perf_counter() - t0
     ll = np.array([o[0] for o in out]); cert = np.array([o[1] for o in out])
-    rel = (ll - ll_ref[sample]) / np.abs(ll_ref[sample])
-    return wall, int(np.sum((cert <= 1.0 + CERT_TOL) & (np.abs(rel) <= 1e-6)))
+    return wall, int(certified_mask(ll, cert, ref[sample])[0].sum())
 
 
 def port_pool():
@@ -239,12 +239,30 @@ def oracle_certified():
     return json.load(open(os.path.join(ROOT, 'oracle', 'sweep64_certified.json')))
 
 
-def certify(res, ll_ref):
+def oracle_ref():
+    """(64, 2): the oracle's loglik and certificate per sweep fit."""
+    return np.array([[c['loglik'], c['certificate']] for c in oracle_certified()])
+
+
+ORACLE_CERT_TOL = 1e-4               # the oracle's own bar (oracle/make_sweep_certified.py)
+
+
+def certified_mask(ll, cert, ref):
+    """The certification rule: certificate <= 1 + CERT_TOL, and the loglik within 1e-6 (relative) of the oracle's
+    where the oracle certified its fit within MAX_RANK modes (its loglik is then the lift's optimum); where it did
+    not, its loglik is only a lower bound of the optimum and the fit may not fall more than 1e-6 below it."""
+    ref, c_ref = ref[:, 0], ref[:, 1]
+    rel = (np.asarray(ll) - ref) / np.abs(ref)
+    pinned = c_ref <= 1.0 + ORACLE_CERT_TOL
+    ok = (np.asarray(cert) <= 1.0 + CERT_TOL) & np.where(pinned, np.abs(rel) <= 1e-6, rel >= -1e-6)
+    return ok, rel
+
+
+def certify(res, ref):
     """(certified count, relative loglik differences, certificates) of fit_certified's results against the oracle's
-    certified logliks."""
+    certified fits."""
     cert = np.array([r.certificate_ for r in res])
-    rel = (np.array([r.loglik_ for r in res]) - ll_ref) / np.abs(ll_ref)
-    ok = (cert <= 1.0 + CERT_TOL) & (np.abs(rel) <= 1e-6)
+    ok, rel = certified_mask([r.loglik_ for r in res], cert, ref[:len(res)])
     return int(ok.sum()), rel, cert
 
 
@@ -256,7 +274,7 @@ def certified_sweep(dev, train, val, modes, init=None):
     return b, res, certified_log_density(res, val)
 
 
-def learned_arm(dev, sweep, modes, train_dev, val_dev, ll_ref, flush, ws, steps=2):
+def learned_arm(dev, sweep, modes, train_dev, val_dev, ref, flush, ws, steps=2):
     """The learned warm start on the same sweep (the trained weights shipped with the package): network inference
     (one forward per lattice shape) for the rank-1 starts, then the same certification (rank growth, held-out
     scores), timed like the main arm. None when no weights ship."""
@@ -278,7 +296,7 @@ def learned_arm(dev, sweep, modes, train_dev, val_dev, ll_ref, flush, ws, steps=
         b, res, _ = certified_sweep(dev, train_dev, val_dev, modes, init=net.start(train_dev, fcs, kinds))
         e1.record(st); torch.cuda.synchronize()
         tot += e0.elapsed_time(e1) / 1e3
-        c1, rel, _ = certify(res, ll_ref)
+        c1, rel, _ = certify(res, ref)
         cert += c1; ranks = np.array([r.rank_ for r in res])
         its = np.array([r.rank_path_[0][3] for r in res])
     tmax = max_over_ranks(tot, ws)
@@ -396,9 +414,9 @@ def config2_bench(dev, reps=50):
     m = BLMLBinned(dtype=np.float64, solver='lbfgs', tol=1e-6, device=dev).fit(counts, modes, complex_g=True)
     torch.cuda.synchronize()
     t = time.perf_counter() - t0
-    ll_ref = float(g['loglik'])
+    ref = float(g['loglik'])
     out['fit'] = {'seconds': t, 'iterations': int(m.n_sweeps_), 'loglik': float(m.loglik_),
-                  'rel_dloglik_vs_reference': (float(m.loglik_) - ll_ref) / abs(ll_ref),
+                  'rel_dloglik_vs_reference': (float(m.loglik_) - ref) / abs(ref),
                   'reference_cpu_seconds': float(g['seconds']), 'reference_iterations': int(g['n_sweeps']),
                   'reference_cores': int(g['cores'])}
     specs, _ = parse_modes(modes, 2)
@@ -694,13 +712,13 @@ def main():
         out = {'seconds': time.perf_counter() - t0, 'stats': b.certify_stats_,
                'rank_path': [r.rank_path_ for r in res], 'scores': sc.tolist()}
         try:
-            out['certified'] = certify(res, np.array([c['loglik'] for c in oracle_certified()]))[0]
+            out['certified'] = certify(res, oracle_ref())[0]
         except FileNotFoundError:
             pass
         print(json.dumps(out), flush=True)
         return
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-    ll_ref = np.array([c['loglik'] for c in oracle_certified()])
+    ref = oracle_ref()
     # the plain engine: the same certification, one fit at a time (no batching), cold starts
     certified_sweep(dev, train_dev[:1], val_dev[:1], modes[:1])
     torch.cuda.synchronize()
@@ -710,7 +728,7 @@ def main():
         plain_res += certified_sweep(dev, train_dev[i:i + 1], val_dev[i:i + 1], modes[i:i + 1])[1]
     torch.cuda.synchronize()
     t_plain = time.perf_counter() - t0
-    plain_cert = certify(plain_res, ll_ref)[0]
+    plain_cert = certify(plain_res, ref)[0]
     del plain_res
     for _ in range(args.warmup):
         certified_sweep(dev, train_dev, val_dev, modes)
@@ -727,7 +745,7 @@ def main():
             b, res, scores = certified_sweep(dev, train_dev, val_dev, modes)
             e1.record(st); torch.cuda.synchronize()
             tot += e0.elapsed_time(e1) / 1e3
-            c1, rel, cert = certify(res, ll_ref)
+            c1, rel, cert = certify(res, ref)
             certified += c1
             ranks = np.array([r.rank_ for r in res]); stats = b.certify_stats_
     launches = _lib.lib().blml_launch_count() - l0
@@ -744,11 +762,11 @@ def main():
         dens = [r.density_ for r in res]
         torch.cuda.synchronize()
         e2e_t += time.perf_counter() - t0
-        e2e_cert += certify(res, ll_ref)[0]
+        e2e_cert += certify(res, ref)[0]
         d2h = int(sum(d.nbytes for d in dens) + sc.nbytes)
     e2e_t = max_over_ranks(e2e_t, ws)
     e2e_value = sum_over_ranks(e2e_cert, ws) / e2e_t if e2e_t > 0 else 0.0
-    learned = learned_arm(dev, sweep, modes, train_dev, val_dev, ll_ref, flush, ws)
+    learned = learned_arm(dev, sweep, modes, train_dev, val_dev, ref, flush, ws)
     b1 = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
     b1._prepare(train, modes)
     t_mv, mv_bytes, mv_flops = grouped_matvec_roofline(b1)
@@ -761,8 +779,8 @@ def main():
             sample = port_sample()
             pool, procs = port_pool()
             try:
-                port_step(pool, sample, ll_ref)                      # worker start-up and imports
-                wall, nc = port_step(pool, sample, ll_ref)
+                port_step(pool, sample, ref)                      # worker start-up and imports
+                wall, nc = port_step(pool, sample, ref)
             finally:
                 pool.terminate()
             cpu = {'value': nc / wall, 'unit': 'fits/s', 'cores': procs, 'kind': 'port',
@@ -804,13 +822,13 @@ def reference_arm(args, rank, ws):
     fits whole, one fit per process; value = certified fits / wall time of the sample."""
     if rank != 0:
         return
-    ll_ref = np.array([c['loglik'] for c in oracle_certified()])
+    ref = oracle_ref()
     sample = port_sample()
     pool, procs = port_pool()
     walls, ncs = [], []
     try:
         for i in range(args.warmup + args.steps):
-            wall, nc = port_step(pool, sample, ll_ref)
+            wall, nc = port_step(pool, sample, ref)
             if i >= args.warmup:
                 walls.append(wall); ncs.append(nc)
     finally:
