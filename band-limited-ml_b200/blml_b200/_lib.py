@@ -36,7 +36,7 @@ class PointCol(C.Structure):
                 ('P', C.c_double)]
 
 
-PT_SINC, PT_SLITS, PT_DIRICHLET = 0, 1, 2
+PT_SINC, PT_SLITS, PT_DIRICHLET, PT_BALL = 0, 1, 2, 3
 
 _P, _I, _L, _D = C.c_void_p, C.c_int, C.c_int64, C.c_double
 _SIGS = {

@@ -47,6 +47,37 @@ class _Red:
         return self.host[:nq].tolist()
 
 
+def point_cols(sp, d):
+    """One mode's kernel as blml_point_col per column (include/blml_b200.h): sinc, slits and dirichlet columns, and
+    ball groups (blml_trivial.py:580-591: prod fc p(||fc t||), p(0) the unit ball's volume pi^(D/2) (1/2)^D /
+    Gamma(D/2 + 1), :135-143). Other kinds raise NotImplementedError."""
+    from math import gamma, pi
+    from .spec import split_kind, dirichlet_N, dirichlet_inner_M
+    cols = (_lib.PointCol * d)()
+    for kind, dims in units_of(sp['kinds']):
+        name, tag = split_kind(kind)
+        if name == 'ball':
+            mask = sum(1 << j for j in dims)
+            for j in dims:
+                c = cols[j]
+                c.kind, c.M, c.f, c.fi = _lib.PT_BALL, mask, float(sp['fc'][j]), 0.0
+            lead, D = cols[min(dims)], len(dims)
+            lead.fi = float(np.prod([float(sp['fc'][j]) for j in dims])); lead.Mi = D
+            lead.P = pi ** (D / 2) * 0.5 ** D / gamma(D / 2 + 1)
+            continue
+        if name not in ('sinc', 'slits', 'dirichlet'):
+            raise NotImplementedError(f"kernel at arbitrary points: kind {name!r} (sinc, slits, dirichlet, ball)")
+        c = cols[dims[0]]
+        c.kind = {'sinc': _lib.PT_SINC, 'slits': _lib.PT_SLITS, 'dirichlet': _lib.PT_DIRICHLET}[name]
+        c.f = float(sp['fc'][dims[0]])
+        if name == 'slits':
+            c.fi = (1.0 - float(tag)) * c.f
+        if name == 'dirichlet':
+            c.P = float(sp['periods'][dims[0]]); c.M = 2 * dirichlet_N(c.f, c.P) + 1
+            c.Mi = dirichlet_inner_M(c.f, c.P, float(tag) if tag else None)
+    return cols
+
+
 class BLMLBinned:
     """BLML on counts on a full regular lattice, fitted on the GPU (see the module docstring)."""
 
@@ -600,29 +631,19 @@ class BLMLBinned:
 
     # ---------------------------------------------------------------- at arbitrary points
     def _mode_at_points(self, k, X):
-        """sum_b e_kb K_k(x - z_b) at the points X (m, d) on the device, complex128 (m,). Columns of sinc / slits /
-        dirichlet kind: the exact one-column kernels per (point, bin) pair over the occupied bins (blml_point_rows).
+        """sum_b e_kb K_k(x - z_b) at the points X (m, d) on the device, complex128 (m,). Units of sinc / slits /
+        dirichlet / ball kind: the exact kernels per (point, bin) pair over the occupied bins (blml_point_rows).
         Harmonic kernels (pball groups with dirichlet columns): the band's spectrum C = W (v^H e) and the plane-wave
-        sum over it (blml_spectrum, blml_planewave_points), exact since the kernel is that sum. ball: unsupported."""
-        from .spec import split_kind, dirichlet_N, dirichlet_inner_M
+        sum over it (blml_spectrum, blml_planewave_points), exact since the kernel is that sum."""
+        from .spec import split_kind
         import ctypes as C
         sp = self.specs_[k]
         names = [split_kind(kd)[0] for kd, _ in units_of(sp['kinds'])]
         e = self.e_hat_t_[k].to(torch.complex128 if self.e_hat_t_.is_complex() else torch.float64).contiguous()
         Xt = torch.as_tensor(np.ascontiguousarray(X, np.float64)).to(self.dev_)
         m = len(X)
-        if all(n in ('sinc', 'slits', 'dirichlet') for n in names):
-            cols = (_lib.PointCol * self.d_)()
-            for j, kind in enumerate(sp['kinds']):
-                name, tag = split_kind(kind)
-                c = cols[j]
-                c.kind = {'sinc': _lib.PT_SINC, 'slits': _lib.PT_SLITS, 'dirichlet': _lib.PT_DIRICHLET}[name]
-                c.f = float(sp['fc'][j])
-                if name == 'slits':
-                    c.fi = (1.0 - float(tag)) * c.f
-                if name == 'dirichlet':
-                    c.P = float(sp['periods'][j]); c.M = 2 * dirichlet_N(c.f, c.P) + 1
-                    c.Mi = dirichlet_inner_M(c.f, c.P, float(tag) if tag else None)
+        if all(n in ('sinc', 'slits', 'dirichlet', 'ball') for n in names):
+            cols = point_cols(sp, self.d_)
             occ = self.w_t_ > 0
             Z = torch.as_tensor(self.centres()).to(self.dev_)[occ].contiguous()
             parts = [e.real, e.imag] if e.is_complex() else [e]
@@ -635,8 +656,9 @@ class BLMLBinned:
                 outs.append(g)
             return torch.complex(outs[0], outs[1]) if len(outs) == 2 else torch.complex(outs[0], torch.zeros_like(outs[0]))
         if not all(n in ('pball', 'dirichlet') for n in names) or self.d_ > 2:
-            raise NotImplementedError("sqrt_density at arbitrary points: sinc / slits / dirichlet columns, or pball groups "
-                                      "with dirichlet columns in 1-D / 2-D (ball kernels are not sums of harmonics)")
+            raise NotImplementedError("sqrt_density at arbitrary points: sinc / slits / dirichlet / ball units, or pball "
+                                      "groups with dirichlet columns in 1-D / 2-D (a pball group times another unit "
+                                      "is neither)")
         freqs, W = mode_transform(sp, self.shape_, self.h_, self.pad_)
         plan = Plan(freqs, W, self.shape_, _lib.F64, _lib.ENGINE_SIMT)
         ws = torch.empty(int(_lib.lib().blml_spectrum_workspace(plan._h, 1)), dtype=torch.uint8, device=self.dev_)

@@ -16,8 +16,8 @@ import torch
 
 from . import _lib
 from ._lib import call, ptrs, dbl
-from .binned import BLMLBinned, _Red, _device
-from .spec import parse_modes, modes_lattice, with_lattice, split_kind, dirichlet_N, dirichlet_inner_M
+from .binned import BLMLBinned, _Red, _device, point_cols
+from .spec import parse_modes, modes_lattice, with_lattice, split_kind
 from .local_gpu import ProductKernel, rows_dev, dev_tab, _struct
 
 
@@ -292,7 +292,6 @@ def unique_bins(Xq, sample_weight=None):
     return Xq[idx], w, inv
 
 
-_PT_KIND = {'sinc': _lib.PT_SINC, 'slits': _lib.PT_SLITS, 'dirichlet': _lib.PT_DIRICHLET}
 
 
 class BLMLQuick(BLMLQuickLattice):
@@ -345,20 +344,7 @@ class BLMLQuick(BLMLQuickLattice):
     # ---------------------------------------------------------------- at arbitrary points
     def _point_cols(self):
         if self._pt_cols is None:
-            sp = self.specs_[0]
-            cols = (_lib.PointCol * self.d_)()
-            for j, kind in enumerate(sp['kinds']):
-                name, tag = split_kind(kind)
-                if name not in _PT_KIND:
-                    raise NotImplementedError(f"predict at points: column kind {name!r} (sinc, slits, dirichlet)")
-                c = cols[j]
-                c.kind = _PT_KIND[name]; c.f = float(sp['fc'][j])
-                if name == 'slits':
-                    c.fi = (1.0 - float(tag)) * c.f
-                if name == 'dirichlet':
-                    P = float(sp['periods'][j])
-                    c.P = P; c.M = 2 * dirichlet_N(c.f, P) + 1
-                    c.Mi = dirichlet_inner_M(c.f, P, float(tag) if tag else None)
+            cols = point_cols(self.specs_[0], self.d_)
             self._pt_cols = cols
         return self._pt_cols
 

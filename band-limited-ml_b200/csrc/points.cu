@@ -3,7 +3,10 @@
 // over the fit's B bin centres z_b, the kernel evaluated exactly (not from a lattice table: the query points are off
 // the lattice). One thread per query point; the bins are staged through shared memory in tiles shared by the block,
 // so each bin centre and coefficient is read from HBM once per block. Per pair: d kernel values (sinpi) and d + 1
-// multiplies in float64, summed in a fixed order.
+// multiplies in float64, summed in a fixed order. A ball unit over a group of D columns (blml_trivial.py:580-591,
+// 135-143) is one radial value per pair: prod fc p(s), s = ||fc (x - z)|| over the group, p(s) = (1/2)^(D/2)
+// J_(D/2)(pi s) / s^(D/2) -- CUDA's jn for whole orders; for half orders the power series below nu + 12 and, above,
+// upward recurrence from the closed forms of J_1/2 and J_3/2 (the standard methods).
 #include "common.cuh"
 
 namespace blml {
@@ -28,6 +31,38 @@ __device__ __forceinline__ double point_unit(const blml_point_col& c, double t) 
   return (sinpi(c.M * u / P) - sinpi(c.Mi * u / P)) / sinpi(u / P) / P;
 }
 
+// J_(twice_nu / 2)(x), x >= 0, twice_nu odd: the power series sum_k (-1)^k (x/2)^(2k+nu) / (k! Gamma(k+nu+1)) below
+// x = nu + 12 (upward recurrence loses accuracy below the order), above it J_{m+1} = (2m / x) J_m - J_{m-1} from
+// J_1/2 = c sin x and J_3/2 = c (sin x / x - cos x), c = sqrt(2 / (pi x))
+__device__ __noinline__ double bessel_half_order(int twice_nu, double x) {
+  const double nu = 0.5 * twice_nu;
+  if (x < nu + 12.0) {
+    const double xs = 0.5 * x;
+    double term = pow(xs, nu) / tgamma(nu + 1.0), acc = term;
+    for (int k = 1; k < 80; k++) {
+      term = -term * xs * xs / (k * (k + nu));
+      acc += term;
+    }
+    return acc;
+  }
+  const double c = sqrt(2.0 / (M_PI * x));
+  double jm = c * sin(x), jc = c * (sin(x) / x - cos(x)), m = 0.5;
+  if (twice_nu == 1) return jm;
+  while (m + 1.0 < nu - 1e-9) {
+    const double jn1 = (2.0 * (m + 1.0) / x) * jc - jm;
+    jm = jc; jc = jn1; m += 1.0;
+  }
+  return jc;
+}
+
+// the ball profile p(s) in D dims; p0 = p(0) = pi^(D/2) (1/2)^D / Gamma(D/2 + 1), the ball's volume
+__device__ __noinline__ double ball_profile(double s, int D, double p0) {
+  if (s == 0.0) return p0;
+  const double x = M_PI * s;
+  const double J = (D % 2 == 0) ? jn(D / 2, x) : bessel_half_order(D, x);
+  return pow(0.5, 0.5 * D) * J / pow(s, 0.5 * D);
+}
+
 __global__ void __launch_bounds__(kPtThreads) k_point_rows(int64_t m, int d, const double* __restrict__ X,
                                                           int64_t B, const double* __restrict__ Z,
                                                           const double* __restrict__ e, blml_point_cols cols,
@@ -47,7 +82,21 @@ __global__ void __launch_bounds__(kPtThreads) k_point_rows(int64_t m, int d, con
     if (i < m) {
       for (int j = 0; j < nt; j++) {
         double p = es[j];
-        for (int c = 0; c < d; c++) p *= point_unit(cols.c[c], x[c] - zs[j * d + c]);
+        for (int c = 0; c < d; c++) {
+          const blml_point_col& cc = cols.c[c];
+          if (cc.kind == BLML_PT_BALL) {
+            if (cc.fi == 0.0) continue;                   // a ball group's value sits on its first column
+            double s2 = 0.0;
+            for (int c2 = 0; c2 < d; c2++)
+              if ((cc.M >> c2) & 1) {
+                const double t = cols.c[c2].f * (x[c2] - zs[j * d + c2]);
+                s2 += t * t;
+              }
+            p *= cc.fi * ball_profile(sqrt(s2), cc.Mi, cc.P);
+          } else {
+            p *= point_unit(cc, x[c] - zs[j * d + c]);
+          }
+        }
         acc += p;
       }
     }
@@ -73,13 +122,30 @@ int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* 
   for (int c = 0; c < d; c++) {
     cc.c[c] = cols[c];
     const int k = cols[c].kind;
-    if (k != BLML_PT_SINC && k != BLML_PT_SLITS && k != BLML_PT_DIRICHLET) {
-      set_error("blml_point_rows: column %d: kind %d (sinc, slits or dirichlet)", c, k);
+    if (k != BLML_PT_SINC && k != BLML_PT_SLITS && k != BLML_PT_DIRICHLET && k != BLML_PT_BALL) {
+      set_error("blml_point_rows: column %d: kind %d (sinc, slits, dirichlet or ball)", c, k);
       return BLML_ERR_ARG;
     }
     if (k == BLML_PT_DIRICHLET && !(cols[c].P > 0)) {
       set_error("blml_point_rows: column %d: dirichlet period must be positive", c);
       return BLML_ERR_ARG;
+    }
+    if (k == BLML_PT_BALL) {
+      // the group mask holds this column and only ball columns; the first column of the group carries prod fc (fi),
+      // the group size (Mi) and p(0) (P), the others fi = 0
+      const int mask = cols[c].M;
+      int lead = -1, size = 0;
+      for (int c2 = 0; c2 < d; c2++)
+        if ((mask >> c2) & 1) { size++; if (lead < 0) lead = c2; }
+      bool ok = mask > 0 && mask < (1 << d) && ((mask >> c) & 1) && cols[c].f > 0;
+      for (int c2 = 0; c2 < d && ok; c2++)
+        if ((mask >> c2) & 1) ok = cols[c2].kind == BLML_PT_BALL && cols[c2].M == mask;
+      if (ok && c == lead) ok = cols[c].Mi == size && cols[c].fi > 0 && cols[c].P > 0;
+      if (ok && c != lead) ok = cols[c].fi == 0.0;
+      if (!ok) {
+        set_error("blml_point_rows: column %d: inconsistent ball group (mask %d)", c, mask);
+        return BLML_ERR_ARG;
+      }
     }
   }
   const int64_t blocks = (m + kPtThreads - 1) / kPtThreads;

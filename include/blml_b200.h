@@ -170,8 +170,11 @@ int blml_gather_rows_i64(int m, int d, const int64_t* src, const int64_t* I, int
 /* ---- the fitted amplitude at arbitrary points (BLMLQuick.sqrt_density / predict, blml_trivial.py:3288-3320) ----
    g[i] = sum_b e[b] prod_c K_c(X[i, c] - Z[b, c]) with the exact one-column kernels (X: m x d, Z: B x d row-major
    float64, d <= 8): sinc f sinc(f t); slits f sinc(f t) - fi sinc(fi t); dirichlet
-   (sin(pi M u / P) - sin(pi Mi u / P)) / (P sin(pi u / P)), u = |t| folded into [0, P / 2], (M - Mi) / P at u = 0 */
-enum { BLML_PT_SINC = 0, BLML_PT_SLITS = 1, BLML_PT_DIRICHLET = 2 };
+   (sin(pi M u / P) - sin(pi Mi u / P)) / (P sin(pi u / P)), u = |t| folded into [0, P / 2], (M - Mi) / P at u = 0;
+   ball (a radial unit over a group of columns, blml_trivial.py:580-591): every column of the group has kind ball,
+   f its fc and M the group's column bit mask; the group's first column holds fi = prod fc, Mi = D (the group size)
+   and P = p(0), the others fi = 0; the unit's value is fi p(||fc t||), p(s) = (1/2)^(D/2) J_(D/2)(pi s) / s^(D/2) */
+enum { BLML_PT_SINC = 0, BLML_PT_SLITS = 1, BLML_PT_DIRICHLET = 2, BLML_PT_BALL = 3 };
 typedef struct { int kind; int M, Mi; double f, fi, P; } blml_point_col;
 typedef struct { blml_point_col c[8]; } blml_point_cols;
 int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* e,

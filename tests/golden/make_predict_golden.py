@@ -2,8 +2,8 @@
 (rahuljhu/band-limited-ml blml_binned.py:451-500; imported read-only from its checkout) of its fits of the fit cases
 in tests/golden/fits.npz (counts and the fit settings of tests/golden_cases.py FIT_SPECS): per case the fitted
 coefficients e_hat, 300 query points inside the lattice's span (default_rng(7)), the amplitudes, densities and the
-refined grid. The ball case is left out (its kernel is not a sum of harmonics; the engine does not evaluate it off
-the lattice).
+refined grid; and two 3-D ball cases on seeded counts of their own (EXTRA: a ball over all three columns -- a
+half-integer Bessel order -- and a 2-D ball group times a sinc column).
 
     python tests/golden/make_predict_golden.py <reference checkout>
 """
@@ -21,10 +21,10 @@ sys.path.insert(0, os.path.join(HERE, '..'))
 sys.path.insert(0, os.path.join(HERE, '..', '..', 'band-limited-ml_b200'))
 
 from blml_binned import BLMLBinned              # noqa: E402  (the reference)
-from golden_cases import FIT_SPECS              # noqa: E402
+from golden_cases import FIT_SPECS, PREDICT_EXTRA, extra_counts     # noqa: E402
 
 CASES = ('d1_sinc_real', 'd1_sinc_complex', 'd1_sinc_rank2_permode', 'd1_dir_circ_real', 'd2_sinc_sinc_real',
-         'd2_pball_lbfgs', 'd2_pball_bg_lbfgs')
+         'd2_pball_lbfgs', 'd2_pball_bg_lbfgs', 'd2_ball_real') + tuple(PREDICT_EXTRA)
 
 
 def main():
@@ -32,8 +32,12 @@ def main():
     out = {}
     rng = np.random.default_rng(7)
     for name in CASES:
-        modes, fkw, ckw = FIT_SPECS[name]
-        counts = fits[f'{name}/counts']
+        if name in PREDICT_EXTRA:
+            _, modes, fkw, ckw = PREDICT_EXTRA[name]
+            counts = extra_counts(name)
+        else:
+            modes, fkw, ckw = FIT_SPECS[name]
+            counts = fits[f'{name}/counts']
         m = BLMLBinned(engine='cpu', dtype=np.float64, **ckw).fit(counts, modes, **fkw)
         X = np.stack([rng.uniform(0.0, s - 1.0, 300) for s in counts.shape], 1)
         out[f'{name}/counts'] = counts

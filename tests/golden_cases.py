@@ -51,6 +51,26 @@ FIT_SPECS = {
     'c1_sinc1024': (make_modes([0.05], ['sinc']), {}, dict(tol=1e-7)),
 }
 
+# point-prediction cases beyond FIT_SPECS (tests/golden/make_predict_golden.py): name -> (shape, modes, fit kwargs,
+# constructor kwargs), counts from extra_counts
+PREDICT_EXTRA = {
+    'd3_ball3_real': ((10, 10, 8), make_modes([0.45, 0.45, 0.45], ['ball', 'ball', 'ball']), {}, dict(tol=1e-9)),
+    'd3_ball2_sinc_complex': ((12, 12, 6), make_modes([0.4, 0.4, 0.3], ['ball', 'ball', 'sinc']), dict(complex_g=True),
+                              dict(tol=1e-8, solver='lbfgs', max_sweeps=3000)),
+}
+
+
+def extra_counts(name):
+    """Seeded counts of a PREDICT_EXTRA case: 4,000 draws from a two-bump density on its lattice."""
+    shape = PREDICT_EXTRA[name][0]
+
+    def f(*g):
+        c1 = [0.35 * m for m in shape]; c2 = [0.7 * m for m in shape]
+        r1 = sum((x - a) ** 2 for x, a in zip(g, c1)) / (0.2 * max(shape)) ** 2
+        r2 = sum((x - a) ** 2 for x, a in zip(g, c2)) / (0.15 * max(shape)) ** 2
+        return np.exp(-r1) + 0.6 * np.exp(-r2) + 0.02
+    return hist(np.random.default_rng(sum(shape)), shape, 4000, f)
+
 
 def hist(rng, shape, n, f):
     g = np.meshgrid(*[np.arange(m, dtype=float) for m in shape], indexing='ij')
