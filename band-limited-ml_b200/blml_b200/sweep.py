@@ -383,7 +383,10 @@ class BLMLBinnedBatch:
     def fit(self, counts_list, modes_list, init=None, caps=None):
         """init: None (the seeded start), or one complex start E0 per fit (arrays of the counts' shapes, host or
         device), e.g. from blml_b200.warmstart; the start phase is then skipped (blml_binned.py:403-408). caps: per-fit
-        L-BFGS iteration caps (< 0: none) in place of max_sweeps (device-side control)."""
+        L-BFGS iteration caps (< 0: none but max_sweeps) in place of max_sweeps (device-side control)."""
+        if caps is not None and self.max_sweeps is not None:
+            caps = np.asarray(caps, np.int64)
+            caps = np.where(caps < 0, int(self.max_sweeps), np.minimum(caps, int(self.max_sweeps)))
         self._caps = caps
         self._prepare(counts_list, modes_list)
         F, code, dev = self.F, self.code, self.device
@@ -399,6 +402,16 @@ class BLMLBinnedBatch:
                     raise ValueError("init: each start has its counts' shape, (K,) + shape for K modes")
                 parts.append(t.to(dev, self.ct).reshape(-1))
             E = torch.cat(parts)
+            # a start's coefficients on bins these counts leave empty are zeroed (blml_binned.py:403-408)
+            occm = (self.w > 0).to(self.rt)
+            if np.all(self.Kf == 1):
+                call('blml_mul_bins', code, 1, self.Btot, 1, E.data_ptr(), occm.data_ptr(), E.data_ptr(), self.st)
+            else:
+                for f in range(F):
+                    sg = self.segs_all[f]
+                    Ef, of = E[sg.off:sg.off + sg.K * sg.B], occm[sg.boff:sg.boff + sg.B]
+                    call('blml_mul_bins', code, int(sg.K), int(sg.B), 1, Ef.data_ptr(), of.data_ptr(), Ef.data_ptr(),
+                         self.st)
             self.start_sweeps_ = np.zeros(F, np.int64)
         else:
             if np.any(self.Kf != 1):
