@@ -77,44 +77,60 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     per step, each fit's tridiagonal problem on the host (every third step), restarts from the Ritz vector until
     every fit's Ritz residual |beta_j y_j| <= tol |theta|, or its Ritz value moved by less than 1e-8 relative between
     two checks (at a certified optimum the top eigenvalue is K-fold, so the residual of its Ritz vector converges far
-    more slowly than the value; 1e-8 is far below any certification bar). above: per-fit thresholds; a Ritz value is a lower bound of lambda_max, so a fit
-    whose Ritz value exceeds its threshold is decided there (its Ritz vector then has a Rayleigh quotient above the
-    threshold: the direction a new mode takes). Returns (theta (F,), dh, v): dh the per-bin scaling and v
-    the top Ritz vectors (float64 per bin over all fits, None unless vectors) -- d = dh v is the direction of a new
-    mode."""
+    more slowly than the value; 1e-8 is far below any certification bar). above: per-fit thresholds; a Ritz value is
+    a lower bound of lambda_max, so a fit whose Ritz value exceeds its threshold is decided there (its Ritz vector
+    then has a Rayleigh quotient above the threshold: the direction a new mode takes). The steps run over the fits
+    still open only: when they fall to 3/4 of the fits the steps cover, the segment list and the grouped mat-vec are
+    rebuilt over them (a fit's arithmetic does not depend on which other fits share the launch). Returns (theta (F,),
+    dh, v): dh the per-bin scaling and v the top Ritz vectors (float64 per bin over all fits, None unless vectors)
+    -- d = dh v is the direction of a new mode."""
     from scipy.linalg import eigh_tridiagonal
     from .sweep import _Group, _Seg
     F, dev, st, B = batch.F, batch.device, batch.st, batch.Btot
     code = _lib.F64
-    segs1 = (_Seg * F)(*[_Seg(int(batch.boff[f]), int(batch.boff[f]), int(batch.B[f]), 1, 0) for f in range(F)])
-    segs1_t = torch.frombuffer(bytearray(segs1), dtype=torch.uint8).to(dev)
     dh = torch.empty(B, dtype=torch.float64, device=dev)
     call('blml_seg_cert_weights', batch.code, F, batch.segs_t.data_ptr(), batch.E_t.data_ptr(), batch.w.data_ptr(),
          dh.data_ptr(), st)
     tmp = torch.empty(B, dtype=torch.float64, device=dev)
     sv = torch.empty(B, dtype=torch.float64, device=dev)
-    grp = _Group(batch.p64, tmp, batch.boff[:-1], sv, batch.boff[:-1], False)
 
-    def dots(pairs):
-        call('blml_seg_dots', code, F, segs1_t.data_ptr(), 0, len(pairs), ptrs([p[0] for p in pairs]),
+    class Subset:
+        """The fits a launch covers: their segment list (offsets into the full vectors) and grouped mat-vec."""
+
+        def __init__(self, idx):
+            self.idx = np.asarray(idx, np.int64)
+            segs = (_Seg * len(self.idx))(*[_Seg(int(batch.boff[f]), int(batch.boff[f]), int(batch.B[f]), 1, 0)
+                                            for f in self.idx])
+            self.segs_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
+            off = np.asarray(batch.boff[:-1])[self.idx]
+            self.grp = _Group([batch.p64[f] for f in self.idx], tmp, off, sv, off, False)
+
+    def dots(S, pairs):
+        n = len(S.idx)
+        call('blml_seg_dots', code, n, S.segs_t.data_ptr(), 0, len(pairs), ptrs([p[0] for p in pairs]),
              ptrs([p[1] for p in pairs]), batch.part.data_ptr(), batch.out.data_ptr(), st)
-        return batch._read(len(pairs))
+        batch.host[:len(pairs) * n].copy_(batch.out[:len(pairs) * n], non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        out = np.zeros((F, len(pairs)))
+        out[S.idx] = batch.host[:len(pairs) * n].numpy().reshape(n, len(pairs))
+        return out
 
-    def lin(out, coef, vecs):
-        cf = torch.as_tensor(np.ascontiguousarray(coef, np.float64)).to(dev, non_blocking=True)
-        call('blml_seg_lincomb', code, F, segs1_t.data_ptr(), 0, out.data_ptr(), len(vecs), cf.data_ptr(),
-             ptrs(vecs), st)
+    def lin(S, out, coef, vecs):                     # coef (F, nterms): the rows of S's fits are used
+        cf = torch.as_tensor(np.ascontiguousarray(np.asarray(coef, np.float64)[S.idx])).to(dev, non_blocking=True)
+        call('blml_seg_lincomb', code, len(S.idx), S.segs_t.data_ptr(), 0, out.data_ptr(), len(vecs),
+             cf.data_ptr(), ptrs(vecs), st)
 
-    def op(x, out):                                  # out = dh * S (dh * x), every fit at once
+    def op(S, x, out):                               # out = dh * S (dh * x) on S's fits
         call('blml_mul_bins', code, 1, B, 0, x.data_ptr(), dh.data_ptr(), tmp.data_ptr(), st)
-        grp(st)
+        S.grp(st)
         call('blml_mul_bins', code, 1, B, 0, sv.data_ptr(), dh.data_ptr(), out.data_ptr(), st)
 
+    every = Subset(np.arange(F))
     nb = max_basis
     V = torch.empty((nb + 1, B), dtype=torch.float64, device=dev)
     V[0].copy_(torch.as_tensor(np.random.default_rng(seed).standard_normal(B)))
-    nrm = dots([(V[0], V[0])])[:, 0]
-    lin(V[0], (1.0 / np.sqrt(np.maximum(nrm, 1e-300)))[:, None], [V[0]])
+    nrm = dots(every, [(V[0], V[0])])[:, 0]
+    lin(every, V[0], (1.0 / np.sqrt(np.maximum(nrm, 1e-300)))[:, None], [V[0]])
     theta = np.zeros(F); done = np.zeros(F, bool); prev = np.full(F, np.nan)
     above = np.full(F, np.inf) if above is None else np.asarray(above, float)
     wv = torch.empty(B, dtype=torch.float64, device=dev)
@@ -124,21 +140,23 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     for rnd in range(max_restarts + 1):
         alphas = np.zeros((F, nb)); betas = np.zeros((F, nb))
         conv = np.zeros(F, bool); yr = [None] * F
+        S = every if not done.any() else Subset(np.where(~done)[0])
         j_end = nb
         for j in range(nb):
-            op(V[j], wv)
+            op(S, V[j], wv)
             steps += 1
             alpha = None
             for ps in range(2):                                   # full reorthogonalisation, twice
                 for c0 in range(0, j + 1, 47):
                     idx = list(range(c0, min(j + 1, c0 + 47)))
-                    cs = dots([(V[i], wv) for i in idx])
+                    cs = dots(S, [(V[i], wv) for i in idx])
                     if ps == 0 and c0 <= j < c0 + 47:
                         alpha = cs[:, j - c0].copy()
-                    lin(wv, np.concatenate([np.ones((F, 1)), -cs], 1), [wv] + [V[i] for i in idx])
+                    lin(S, wv, np.concatenate([np.ones((F, 1)), -cs], 1), [wv] + [V[i] for i in idx])
             alphas[:, j] = alpha
-            beta = np.sqrt(np.maximum(dots([(wv, wv)])[:, 0], 0.0))
-            open_ = ~(done | conv)
+            beta = np.sqrt(np.maximum(dots(S, [(wv, wv)])[:, 0], 0.0))
+            open_ = np.zeros(F, bool); open_[S.idx] = True
+            open_ &= ~(done | conv)
             check = j == nb - 1 or (j >= 5 and j % 3 == 2) or bool(np.any(beta[open_] <= 1e-300))
             if check:
                 for f in np.where(open_)[0]:
@@ -153,9 +171,14 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                     j_end = j + 1
                     break
             betas[:, j] = beta
-            lin(V[j + 1], np.where(beta > 0, 1.0 / np.maximum(beta, 1e-300), 0.0)[:, None], [wv])
-        # the Ritz vector of every fit still open this round: R = sum_i y_i V[i]
+            lin(S, V[j + 1], np.where(beta > 0, 1.0 / np.maximum(beta, 1e-300), 0.0)[:, None], [wv])
+            still = np.where(~(done | conv))[0]
+            if check and j + 1 < nb and len(still) <= 0.75 * len(S.idx):
+                # the steps go on over the open fits only; the converged ones keep V[0..j], all their Ritz vectors use
+                S = Subset(still)
+        # the Ritz vector of every fit still open at the start of this round: R = sum_i y_i V[i]
         act = ~done
+        SA = Subset(np.where(act)[0])
         R.zero_()
         for c0 in range(0, j_end, 47):
             idx = list(range(c0, min(j_end, c0 + 47)))
@@ -167,17 +190,18 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                 for t, i in enumerate(idx):
                     if i < len(y):
                         cf[f, 1 + t] = y[i]
-            lin(R, cf, [R] + [V[i] for i in idx])
+            lin(SA, R, cf, [R] + [V[i] for i in idx])
         if vectors:                                               # keep the vectors of the fits converging now
             keep = (act & conv).astype(float)
-            lin(vec, np.stack([keep, 1.0 - keep], 1), [R, vec])
+            lin(SA, vec, np.stack([keep, 1.0 - keep], 1), [R, vec])
         done |= conv
         if np.all(done):
             break
-        rn = dots([(R, R)])[:, 0]
-        lin(V[0], np.where(done, 1.0, 1.0 / np.sqrt(np.maximum(rn, 1e-300)))[:, None], [R])
+        SO = Subset(np.where(~done)[0])
+        rn = dots(SO, [(R, R)])[:, 0]
+        lin(SO, V[0], (1.0 / np.sqrt(np.maximum(rn, 1e-300)))[:, None], [R])
     if vectors:
-        nv = dots([(vec, vec)])[:, 0]
-        lin(vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
+        nv = dots(every, [(vec, vec)])[:, 0]
+        lin(every, vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
     batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()))
     return theta, dh, vec
