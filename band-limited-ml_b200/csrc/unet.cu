@@ -9,8 +9,8 @@
 //   data grad      dCol[P x 9C]  = dPre[P x Cout] . Wt[9C x Cout]^T      (then col2im gathers the 9 taps)
 //   weight grad    dW[Cout x 9C] = dPreT[Cout x P] . ColT[9C x P]^T      (split over P, partials summed in order)
 // Every GEMM is C = A B^T with A (M x K) and B (N x K) K-major BF16 and FP32 output, on tcgen05: TMA loads of
-// 128-byte-swizzled 64-deep K slices, one elected thread issuing kind::f16 MMAs (M 128, N <= 256, K 16) into a TMEM
-// accumulator, tcgen05.ld epilogue. Waits are bounded: on timeout the kernel sets the caller's error word, gives
+// 128-byte-swizzled 64-deep K slices into a ring of up to 8 stages, one elected thread issuing kind::f16 MMAs (M 128,
+// N <= 256, K 16) into one of two TMEM accumulators, tcgen05.ld epilogue overlapping the next tile's MMAs. Waits are bounded: on timeout the kernel sets the caller's error word, gives
 // copies and MMAs in flight one more bounded wait, frees its tensor memory and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -20,7 +20,7 @@
 
 namespace blml {
 
-constexpr int NN_BM = 128, NN_BK = 64, NN_THREADS = 128;
+constexpr int NN_BM = 128, NN_BK = 64;
 
 __device__ __forceinline__ uint32_t nn_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void nn_mbar_init(uint64_t* bar, uint32_t count) {
@@ -58,113 +58,190 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(NN_BM >> 4) << 24);
 }
 
-// C[z][m][n] = sum_{k in split z} A[m][k] B[n][k]. Persistent: at most 2 CTAs per SM (their TMEM accumulators fit
-// the SM's 512 columns together), each allocating its accumulator once and walking the tiles (m tile, n tile, split)
-// t = blockIdx.x, blockIdx.x + gridDim.x, ...; between tiles the epilogue's reads finish before the next tile's
-// first MMA overwrites the accumulator.
-__global__ void __launch_bounds__(NN_THREADS) k_gemm_bf16(const __grid_constant__ CUtensorMap mA,
-                                                          const __grid_constant__ CUtensorMap mB, int M, int N,
-                                                          int NT, int tcols, int nkb, int kb_per_split, int splits,
-                                                          float* C, int* err) {
+// C[z][m][n] = sum_{k in split z} A[m][k] B[n][k]. Persistent, one CTA per SM (its shared memory keeps a second
+// one out), warp-specialised over a ring of `stages` shared-memory K slices and two TMEM accumulators:
+//   warp 4 lane 0   TMA producer: waits for a free slice (empty[s]), loads A and B of the next K slice (full[s])
+//   warp 5 lane 0   MMA issuer: waits for a loaded slice, issues its four K = 16 MMAs into the tile's accumulator and
+//                   commits to empty[s] (the slice is reusable once those MMAs have read it); after a tile's last
+//                   slice it commits to tfull[a]
+//   warps 0-3       epilogue: wait for tfull[a], tcgen05.ld their 32 TMEM lanes, store, arrive on tempty[a]
+// so the loads run `stages` slices ahead of the MMAs and a tile's epilogue overlaps the next tile's MMAs. Tiles are
+// walked t = blockIdx.x, blockIdx.x + gridDim.x, ... with the n tile fastest, so the CTAs that share an A tile run
+// at the same time and the second read of it comes from L2. Tiles whose split has an empty K range are written as
+// zeros by the epilogue and skipped by the other roles.
+constexpr int NN_PIPE_THREADS = 192, NN_MAX_STAGES = 8;
+
+struct NNPipeShared {
+  uint64_t full[NN_MAX_STAGES], empty[NN_MAX_STAGES], tfull[2], tempty[2];
+  uint32_t tslot;
+  int abort;
+  long long issued, consumed;           // K slices loaded by the producer / taken by the MMA issuer
+};
+
+__device__ __forceinline__ bool nn_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (long it = 0; it < (1L << 20); it++) {
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(nn_smem_u32(bar)), "r"(parity) : "memory");
+    if (done) return true;
+    if ((it & 63) == 63 && abort && *abort) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void nn_fail(volatile int* abort, int* err) {
+  *abort = 1;
+  atomicExch(err, 1);
+}
+
+__global__ void __launch_bounds__(NN_PIPE_THREADS, 1) k_gemm_bf16(const __grid_constant__ CUtensorMap mA,
+                                                                  const __grid_constant__ CUtensorMap mB, int M, int N,
+                                                                  int NT, int tcols, int nkb, int kb_per_split,
+                                                                  int splits, int stages, float* C, int* err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(base);
-  __nv_bfloat16* sB = sA + NN_BM * NN_BK;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sB + (size_t)NT * NN_BK);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+  const uint32_t a_bytes = NN_BM * NN_BK * 2, stage_bytes = a_bytes + (uint32_t)NT * NN_BK * 2;
+  NNPipeShared* sh = reinterpret_cast<NNPipeShared*>(base + (size_t)stages * stage_bytes);
+  volatile int* abort = &sh->abort;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int Mt = (M + NN_BM - 1) / NN_BM, Nt = (N + NT - 1) / NT;
   const long long tiles = (long long)Mt * Nt * splits;
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(nn_smem_u32(tslot)), "r"(tcols));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(nn_smem_u32(&sh->tslot)), "r"(2 * tcols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (tid == 0) {
-    nn_mbar_init(&bars[0], 1); nn_mbar_init(&bars[1], 1);
+  if (tid == 32) {
+    for (int s = 0; s < stages; s++) { nn_mbar_init(&sh->full[s], 1); nn_mbar_init(&sh->empty[s], 1); }
+    for (int a = 0; a < 2; a++) { nn_mbar_init(&sh->tfull[a], 1); nn_mbar_init(&sh->tempty[a], 4); }
+    sh->abort = 0; sh->issued = 0; sh->consumed = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t taddr = *tslot;
-  const uint32_t tx = (uint32_t)((NN_BM + NT) * NN_BK * 2);
-  const uint32_t idesc = idesc_bf16(NT);
-  bool ok = true;
-  uint32_t par_last = 0;
-  long long phase = 0;                         // mbarrier phases used so far (both barriers advance together)
-  for (long long t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-    const int z = (int)(t / ((long long)Mt * Nt));
-    const long long rem = t - (long long)z * Mt * Nt;
-    const int nt_i = (int)(rem / Mt), mt_i = (int)(rem - (long long)nt_i * Mt);
-    const int m0 = mt_i * NN_BM, n0 = nt_i * NT;
-    const int kb0 = z * kb_per_split, kb1 = min(nkb, kb0 + kb_per_split);
-    int done = 0;
-    for (int kb = kb0; kb < kb1 && ok; kb++, done++, phase++) {
-      const uint32_t par = (uint32_t)(phase & 1);
-      par_last = par;
-      if (tid == 0) {
-        nn_mbar_expect_tx(&bars[0], tx);
-        nn_tma_2d(sA, &mA, kb * NN_BK, m0, &bars[0]);
-        nn_tma_2d(sB, &mB, kb * NN_BK, n0, &bars[0]);
+  const uint32_t taddr = sh->tslot;
+
+  if (warp == 4 && lane == 0) {                                   // ---- TMA producer
+    const uint32_t tx = stage_bytes;
+    long long g = 0;
+    for (long long t = blockIdx.x; t < tiles && !*abort; t += gridDim.x) {
+      const int z = (int)(t / ((long long)Mt * Nt));
+      const long long rem = t - (long long)z * Mt * Nt;
+      const int mt_i = (int)(rem / Nt), nt_i = (int)(rem - (long long)mt_i * Nt);
+      const int kb0 = z * kb_per_split, kb1 = min(nkb, kb0 + kb_per_split);
+      for (int kb = kb0; kb < kb1; kb++, g++) {
+        const int s = (int)(g % stages);
+        const long long r = g / stages;
+        if (r > 0 && !nn_wait_or_abort(&sh->empty[s], (uint32_t)((r - 1) & 1), abort)) { nn_fail(abort, err); break; }
+        uint8_t* sa = base + (size_t)s * stage_bytes;
+        nn_mbar_expect_tx(&sh->full[s], tx);
+        nn_tma_2d(sa, &mA, kb * NN_BK, mt_i * NN_BM, &sh->full[s]);
+        nn_tma_2d(sa + a_bytes, &mB, kb * NN_BK, nt_i * NT, &sh->full[s]);
+        *(volatile long long*)&sh->issued = g + 1;
       }
-      ok = nn_mbar_wait(&bars[0], par);
-      if (!ok) break;
-      if (tid == 0) {
+    }
+  } else if (warp == 5 && lane == 0) {                            // ---- MMA issuer
+    const uint32_t idesc = idesc_bf16(NT);
+    long long g = 0, it = 0;
+    for (long long t = blockIdx.x; t < tiles && !*abort; t += gridDim.x) {
+      const int z = (int)(t / ((long long)Mt * Nt));
+      const int kb0 = z * kb_per_split, kb1 = min(nkb, kb0 + kb_per_split);
+      if (kb0 >= kb1) continue;
+      const int a = (int)(it & 1);
+      const long long u = it >> 1;
+      if (u > 0 && !nn_wait_or_abort(&sh->tempty[a], (uint32_t)((u - 1) & 1), abort)) { nn_fail(abort, err); break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t acc_addr = taddr + (uint32_t)(a * tcols);
+      bool ok = true;
+      for (int kb = kb0; kb < kb1; kb++, g++) {
+        const int s = (int)(g % stages);
+        if (!nn_wait_or_abort(&sh->full[s], (uint32_t)((g / stages) & 1), abort)) { ok = false; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const __nv_bfloat16* sa = reinterpret_cast<const __nv_bfloat16*>(base + (size_t)s * stage_bytes);
+        const __nv_bfloat16* sb = reinterpret_cast<const __nv_bfloat16*>(base + (size_t)s * stage_bytes + a_bytes);
 #pragma unroll
         for (int j = 0; j < NN_BK / 16; j++) {
-          const uint64_t ad = nn_desc(sA + j * 16), bd = nn_desc(sB + j * 16);
-          const uint32_t acc = (done > 0 || j > 0) ? 1u : 0u;
+          const uint64_t ad = nn_desc(sa + j * 16), bd = nn_desc(sb + j * 16);
+          const uint32_t acc = (kb > kb0 || j > 0) ? 1u : 0u;
           asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                       :: "r"(taddr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+                       :: "r"(acc_addr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                     :: "r"(nn_smem_u32(&bars[1])) : "memory");
+                     :: "r"(nn_smem_u32(&sh->empty[s])) : "memory");
+        *(volatile long long*)&sh->consumed = g + 1;
       }
-      ok = nn_mbar_wait(&bars[1], par);
+      if (!ok) { nn_fail(abort, err); break; }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(nn_smem_u32(&sh->tfull[a])) : "memory");
+      it++;
     }
-    if (!ok) break;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    float* Cz = C + (size_t)z * M * N;
-    const int row = m0 + 32 * warp + lane;
-    for (int c0 = 0; c0 < NT; c0 += 16) {
-      uint32_t v[16];
-      if (done > 0) {
+  } else if (warp < 4) {                                          // ---- epilogue
+    const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(C) & 15) == 0);
+    long long it = 0;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+      if (__any_sync(0xffffffffu, *abort != 0)) break;            // warp-uniform: the tcgen05.ld below are .aligned
+      const int z = (int)(t / ((long long)Mt * Nt));
+      const long long rem = t - (long long)z * Mt * Nt;
+      const int mt_i = (int)(rem / Nt), nt_i = (int)(rem - (long long)mt_i * Nt);
+      const int m0 = mt_i * NN_BM, n0 = nt_i * NT;
+      const int kb0 = z * kb_per_split, kb1 = min(nkb, kb0 + kb_per_split);
+      float* Cz = C + (size_t)z * M * N;
+      const int row = m0 + 32 * warp + lane;
+      if (kb0 >= kb1) {                                           // an empty K range: the partial is zero
+        if (row < M)
+          for (int col = n0; col < min(N, n0 + NT); col++) Cz[(size_t)row * N + col] = 0.f;
+        continue;
+      }
+      const int a = (int)(it & 1);
+      const long long u = it >> 1;
+      const bool got = nn_wait_or_abort(&sh->tfull[a], (uint32_t)(u & 1), abort);
+      if (!__all_sync(0xffffffffu, got)) { if (lane == 0) nn_fail(abort, err); break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int c0 = 0; c0 < NT; c0 += 16) {
+        uint32_t v[16];
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
                      "%13, %14, %15}, [%16];"
                      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
                        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
                        "=r"(v[15])
-                     : "r"(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0));
+                     : "r"(taddr + ((uint32_t)(32 * warp) << 16) + (uint32_t)(a * tcols + c0)));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      } else {
+        if (row < M) {
+          float* out = Cz + (size_t)row * N + n0 + c0;
+          const int nv = min(16, N - (n0 + c0));
+          if (vec && nv == 16) {
 #pragma unroll
-        for (int i = 0; i < 16; i++) v[i] = 0u;            // an empty K range: the partial is zero
-      }
-      if (row < M) {
+            for (int i = 0; i < 16; i += 4)
+              *reinterpret_cast<float4*>(out + i) = make_float4(__uint_as_float(v[i]), __uint_as_float(v[i + 1]),
+                                                                __uint_as_float(v[i + 2]), __uint_as_float(v[i + 3]));
+          } else {
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const int col = n0 + c0 + i;
-          if (col < N) Cz[(size_t)row * N + col] = __uint_as_float(v[i]);
+            for (int i = 0; i < 16; i++)
+              if (i < nv) out[i] = __uint_as_float(v[i]);
+          }
         }
       }
+      // this warp's accumulator reads are done: the MMA issuer may overwrite the accumulator
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(nn_smem_u32(&sh->tempty[a])) : "memory");
+      it++;
     }
-    // every warp's accumulator reads are done before thread 0 issues the next tile's first MMA
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
-  if (!ok) {
-    // a bounded wait gave up: record it, then give the copy and the MMAs in flight one more bounded wait before the
-    // tensor memory is released
-    if (tid == 0) atomicExch(err, 1);
-    nn_mbar_wait(&bars[0], par_last);
-    nn_mbar_wait(&bars[1], par_last);
+  __syncthreads();
+  if (*abort && tid == 0) {
+    // a bounded wait gave up: the slices still loading and the MMAs last committed get one more bounded wait each
+    // before the shared and tensor memory are released
+    const long long iss = *(volatile long long*)&sh->issued, con = *(volatile long long*)&sh->consumed;
+    for (long long g = con; g < iss; g++)
+      nn_wait_or_abort(&sh->full[g % stages], (uint32_t)((g / stages) & 1), nullptr);
+    if (con > 0) nn_wait_or_abort(&sh->empty[(con - 1) % stages], (uint32_t)(((con - 1) / stages) & 1), nullptr);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(tcols));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(2 * tcols));
 }
 
 // ---------------------------------------------------------------------------------------------- layout kernels
@@ -466,28 +543,35 @@ int blml_nn_gemm_bf16(const void* A, const void* B, float* C, int M, int N, int 
   if (!A || !B || !C || !err || M < 1 || N < 1 || K < 8 || splits < 1 || splits > 4096) {
     set_error("blml_nn_gemm_bf16: bad arguments"); return BLML_ERR_ARG;
   }
-  const int NT = N <= 256 ? (N + 15) / 16 * 16 : 256;
-  int tcols = 32; while (tcols < NT) tcols <<= 1;
+  // n tiles of equal width (a multiple of 16, at most 256: the MMA's N), so N = 288 is two tiles of 144, not 256 + 32
+  const int ntiles = (N + 255) / 256;
+  const int NT = ((N + ntiles - 1) / ntiles + 15) / 16 * 16;
+  int tcols = 32; while (tcols < NT) tcols <<= 1;                 // two accumulators: 2 tcols <= 512 TMEM columns
   CUtensorMap mA, mB;
   int e = nn_map(&mA, A, K, M, NN_BM);
   if (!e) e = nn_map(&mB, B, K, N, NT);
   if (e) return e;
   const int nkb = (K + NN_BK - 1) / NN_BK;
   const int per = (nkb + splits - 1) / splits;
-  // shared memory sized so at most 2 CTAs share an SM (their TMEM accumulators then always fit its 512 columns)
-  const size_t smem = std::max<size_t>(1024 + (size_t)(NN_BM + NT) * NN_BK * 2 + 64, 80 * 1024);
+  // as many K slices in flight as the shared memory holds (at most 8); more than half of it, so one CTA per SM
+  constexpr size_t kSmemMax = 227 * 1024;
+  const size_t stage_bytes = (size_t)(NN_BM + NT) * NN_BK * 2;
+  const size_t fixed = 1024 + sizeof(NNPipeShared);
+  const int stages = (int)std::min<size_t>(NN_MAX_STAGES, (kSmemMax - fixed) / stage_bytes);
+  const size_t smem = std::max<size_t>(fixed + (size_t)stages * stage_bytes, 120 * 1024);
   static bool attr = false;
   if (!attr) {
-    e = cuda_status(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 1024),
+    e = cuda_status(cudaFuncSetAttribute(k_gemm_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemMax),
                     "blml_nn_gemm_bf16");
     if (e) return e;
     attr = true;
   }
   const long long tiles = (long long)((M + NN_BM - 1) / NN_BM) * ((N + NT - 1) / NT) * splits;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-  const unsigned grid = (unsigned)std::min<long long>(tiles, 2LL * sms);    // 2 CTAs per SM: TMEM 2 x 256 columns
-  k_gemm_bf16<<<grid, NN_THREADS, smem, NST>>>(mA, mB, M, N, NT, tcols, nkb, per, splits, C, err);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const unsigned grid = (unsigned)std::min<long long>(tiles, sms);
+  k_gemm_bf16<<<grid, NN_PIPE_THREADS, smem, NST>>>(mA, mB, M, N, NT, tcols, nkb, per, splits, stages, C, err);
   BLML_CHECK_LAUNCH("blml_nn_gemm_bf16");
   return BLML_OK;
 }

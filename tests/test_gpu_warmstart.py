@@ -10,7 +10,8 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize('M,N,K,splits', [(128, 32, 72, 1), (300, 64, 200, 1), (1000, 256, 864, 1),
-                                          (64, 300, 512, 3), (32, 2304, 4096, 7), (513, 16, 8, 1)])
+                                          (64, 300, 512, 3), (32, 2304, 4096, 7), (513, 16, 8, 1),
+                                          (200, 48, 512, 7), (262144 // 16, 288, 864, 1)])
 def test_gemm_bf16_matches_fp32_product(cuda_device, M, N, K, splits):
     from blml_b200._lib import call
     g = torch.Generator(device='cuda').manual_seed(M + N + K)
