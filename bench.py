@@ -706,10 +706,12 @@ def main():
     train_dev = [torch.as_tensor(c).to(dev) for c in train]
     val_dev = [torch.as_tensor(c).to(dev) for c in val]
     if args.certify:
+        l0 = _lib.lib().blml_launch_count()
         t0 = time.perf_counter()
         b, res, sc = certified_sweep(dev, train_dev, val_dev, modes)
         torch.cuda.synchronize()
-        out = {'seconds': time.perf_counter() - t0, 'stats': b.certify_stats_,
+        out = {'seconds': time.perf_counter() - t0, 'launches': int(_lib.lib().blml_launch_count() - l0),
+               'stats': b.certify_stats_,
                'rank_path': [r.rank_path_ for r in res], 'scores': sc.tolist()}
         try:
             out['certified'] = certify(res, oracle_ref())[0]
