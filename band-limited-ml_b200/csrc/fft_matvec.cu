@@ -37,6 +37,17 @@ constexpr int kMaxRad = 12;
 // stride R (and the row gathers) spread over the banks; a transform occupies ld(N) slots, an odd count, so that
 // transforms side by side start on different banks.
 __host__ __device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+
+// one complex value global -> shared without a register round trip (cp.async: the loads of a stage's data are all
+// in flight at once; cp.async.wait_all and a barrier before the first pass)
+template <typename V>
+__device__ __forceinline__ void cp_async_el(V* dst, const V* src) {
+  static_assert(sizeof(V) == 16 || sizeof(V) == 8, "complex float64 or float32");
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  if (sizeof(V) == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(d), "l"(src) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 __host__ __device__ __forceinline__ int pld(int N) { return N + (N >> 3) + 1; }
 
 // x / d for 0 <= x < 2^16 and 1 <= d < 2^16 by a multiply and a shift: m = floor((2^32 - 1) / d) + 1 (0 for d = 1)
@@ -194,15 +205,16 @@ __device__ __forceinline__ void rows_fwd_body(const FftDesc& D, int cta, unsigne
   cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem);
   cpx<T>* alt = buf + D.rows * ld;
   cpx<T>* tw = alt + D.rows * ld;
-  for (int i = tid; i < D.ax2.ntw; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
+  for (int i = tid; i < D.ax2.ntw; i += kFT) cp_async_el(&tw[i], reinterpret_cast<const cpx<T>*>(D.tw2) + i);
   const int64_t base = (int64_t)r0 * N;
   if (D.flags & 1) {
     const T* X = reinterpret_cast<const T*>(D.X) + base;
     for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + pidx(i - t * N)] = cpx<T>{X[i], T(0)}; }
   } else {
     const cpx<T>* X = reinterpret_cast<const cpx<T>*>(D.X) + base;
-    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; buf[t * ld + pidx(i - t * N)] = X[i]; }
+    for (int i = tid; i < nr * N; i += kFT) { const int t = i / N; cp_async_el(&buf[t * ld + pidx(i - t * N)], X + i); }
   }
+  cp_async_wait_all();
   __syncthreads();
   buf = smem_fft<T, false>(buf, alt, tw, ld, nr, D.ax2);
   cpx<T>* Z = reinterpret_cast<cpx<T>*>(D.Z);
@@ -222,9 +234,10 @@ __device__ __forceinline__ void cols_body(const FftDesc& D, int cta, unsigned ch
   cpx<T>* buf = base;
   cpx<T>* alt = base + D.cols * ld;
   cpx<T>* tw = alt + D.cols * ld;
-  for (int i = tid; i < D.ax1.ntw; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw1)[i];
+  for (int i = tid; i < D.ax1.ntw; i += kFT) cp_async_el(&tw[i], reinterpret_cast<const cpx<T>*>(D.tw1) + i);
   cpx<T>* Z = reinterpret_cast<cpx<T>*>(D.Z) + (int64_t)c0 * N;
-  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; buf[t * ld + pidx(i - t * N)] = Z[i]; }
+  for (int i = tid; i < nc * N; i += kFT) { const int t = i / N; cp_async_el(&buf[t * ld + pidx(i - t * N)], Z + i); }
+  cp_async_wait_all();
   __syncthreads();
   buf = smem_fft<T, false>(buf, alt, tw, ld, nc, D.ax1);
   alt = buf == base ? base + D.cols * ld : base;
@@ -249,15 +262,16 @@ __device__ __forceinline__ void rows_inv_body(const FftDesc& D, int cta, unsigne
   cpx<T>* buf = reinterpret_cast<cpx<T>*>(smem);
   cpx<T>* alt = buf + D.rows * ld;
   cpx<T>* tw = alt + D.rows * ld;
-  for (int i = tid; i < D.ax2.ntw; i += kFT) tw[i] = reinterpret_cast<const cpx<T>*>(D.tw2)[i];
+  for (int i = tid; i < D.ax2.ntw; i += kFT) cp_async_el(&tw[i], reinterpret_cast<const cpx<T>*>(D.tw2) + i);
   for (int i = tid; i < nr * ld; i += kFT) buf[i] = cpx<T>{T(0), T(0)};
   __syncthreads();
   const cpx<T>* Z = reinterpret_cast<const cpx<T>*>(D.Z);
   for (int i = tid; i < nr * D.H2; i += kFT) {
     const int q2 = i / nr, t = i - q2 * nr;
     const int row = r0 + t, b = row / D.M1, r = row - b * D.M1;
-    buf[t * ld + pidx(__ldg(D.k2 + q2))] = Z[((int64_t)b * D.H2 + q2) * D.M1 + r];
+    cp_async_el(&buf[t * ld + pidx(__ldg(D.k2 + q2))], Z + ((int64_t)b * D.H2 + q2) * D.M1 + r);
   }
+  cp_async_wait_all();
   __syncthreads();
   buf = smem_fft<T, true>(buf, alt, tw, ld, nr, D.ax2);
   const int64_t base = (int64_t)r0 * N;
