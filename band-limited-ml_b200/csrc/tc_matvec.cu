@@ -28,6 +28,7 @@ constexpr int TC_THREADS = 128;
 struct TcB {
   int K, Nr, ldk;            // logical K, output real columns, padded row length (floats)
   float* hi; float* lo;
+  CUtensorMap mh, ml;        // their tensor maps, encoded once when the plan is built
 };
 struct TcPlan {
   TcB fwd[8], fwd_real[8], inv[8];
@@ -254,6 +255,9 @@ static int upload_B(TcB& b, const std::vector<double>& T, int Mc, int Nc, bool r
   }
   int e = cuda_status(cudaMemcpy(b.hi, hi.data(), bytes, cudaMemcpyHostToDevice), "tc twiddles");
   if (!e) e = cuda_status(cudaMemcpy(b.lo, lo.data(), bytes, cudaMemcpyHostToDevice), "tc twiddles");
+  const int nt = out_tile(b.Nr);
+  if (!e) e = make_map(&b.mh, b.hi, b.K, b.Nr, b.ldk, nt);
+  if (!e) e = make_map(&b.ml, b.lo, b.K, b.Nr, b.ldk, nt);
   return e;
 }
 
@@ -308,15 +312,19 @@ int64_t tc_workspace(const blml_plan_s* p, int nb) { return 2 * (int64_t)nb * tc
 template <bool W_, bool YR>
 static int launch_tc(const CUtensorMap& mA, const TcB& B, int64_t rows, int64_t Rs, int64_t ldout, const float* W,
                      void* Y, int* err, cudaStream_t st) {
-  CUtensorMap mBh, mBl;
   const int nt = out_tile(B.Nr);
-  int e = make_map(&mBh, B.hi, B.K, B.Nr, B.ldk, nt);
-  if (!e) e = make_map(&mBl, B.lo, B.K, B.Nr, B.ldk, nt);
-  if (e) return e;
   const size_t sm = tc_smem(nt);
-  cudaFuncSetAttribute(k_tc_stage<W_, YR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  static int attr_dev = -1;                     // the largest tile's shared memory, set once per device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    int e = cuda_status(cudaFuncSetAttribute(k_tc_stage<W_, YR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)tc_smem(256)), "tc stage");
+    if (e) return e;
+    attr_dev = dev;
+  }
   dim3 grid((unsigned)((rows + TC_BM - 1) / TC_BM), (unsigned)((B.Nr + nt - 1) / nt));
-  k_tc_stage<W_, YR><<<grid, TC_THREADS, sm, st>>>(mA, mBh, mBl, B.K, B.Nr, nt, tmem_cols(nt), rows, Rs, ldout, W,
+  k_tc_stage<W_, YR><<<grid, TC_THREADS, sm, st>>>(mA, B.mh, B.ml, B.K, B.Nr, nt, tmem_cols(nt), rows, Rs, ldout, W,
                                                   Y, err);
   BLML_CHECK_LAUNCH("tc stage");
   return BLML_OK;
