@@ -188,29 +188,61 @@ __global__ void __launch_bounds__(256) k_seg_dots2(const blml_seg* segs, int cpl
   seg_partials<43>(v, part);
 }
 
-// the same scan for float64 complex vectors, one 16-byte (re, im) load per element and vector
+// the same scan for float64 complex vectors, one 16-byte (re, im) load per element and vector. The block's 8 warps
+// split the stored vectors (warp w takes q = w, w + 8, w + 16) and walk the same 64-element tiles, so each thread
+// holds at most 6 accumulators (full occupancy, many loads in flight) and the two shared vectors are read from HBM
+// once per tile and from L1 by the other warps; the last warp also sums the three squared norms. Each quantity's
+// block partial comes from one warp (warp_sum, fixed order), in seg_partials' layout.
 __global__ void __launch_bounds__(256) k_seg_dots2_c128(const blml_seg* segs, int np, SegList al, const void* b0,
                                                         const void* b1, const void* x, double* part) {
   const blml_seg S = segs[blockIdx.y];
   const int64_t o = S.off, n = (int64_t)S.K * S.B;
-  double v[43];
-#pragma unroll
-  for (int q = 0; q < 43; q++) v[q] = 0.0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const double2* B0 = reinterpret_cast<const double2*>(b0) + o;
   const double2* B1 = reinterpret_cast<const double2*>(b1) + o;
   const double2* X = x ? reinterpret_cast<const double2*>(x) + o : nullptr;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double2 y0 = B0[i], y1 = B1[i];
+  const double2* A[3];
+  int na = 0;
 #pragma unroll
-    for (int q = 0; q < 20; q++)
-      if (q < np) {
-        const double2 a = reinterpret_cast<const double2*>(al.a[q])[o + i];
-        v[q] += a.x * y0.x + a.y * y0.y; v[20 + q] += a.x * y1.x + a.y * y1.y;
-      }
-    v[40] += y0.x * y0.x + y0.y * y0.y; v[41] += y1.x * y1.x + y1.y * y1.y;
-    if (X) { const double2 z = X[i]; v[42] += z.x * z.x + z.y * z.y; }
+  for (int j = 0; j < 3; j++) {
+    const int q = warp + nw * j;
+    A[j] = q < np ? reinterpret_cast<const double2*>(al.a[q]) + o : nullptr;
+    na += q < np;
   }
-  seg_partials<43>(v, part);
+  const bool norms = warp == nw - 1;
+  double a0[3] = {0.0, 0.0, 0.0}, a1[3] = {0.0, 0.0, 0.0}, n0 = 0.0, n1 = 0.0, nx = 0.0;
+  for (int64_t t = (int64_t)blockIdx.x * 64; t < n; t += (int64_t)gridDim.x * 64) {
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int64_t i = t + u * 32 + lane;
+      if (i < n) {
+        const double2 y0 = __ldg(B0 + i), y1 = __ldg(B1 + i);
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+          if (j < na) {
+            const double2 a = __ldg(A[j] + i);
+            a0[j] += a.x * y0.x + a.y * y0.y; a1[j] += a.x * y1.x + a.y * y1.y;
+          }
+        if (norms) {
+          n0 += y0.x * y0.x + y0.y * y0.y; n1 += y1.x * y1.x + y1.y * y1.y;
+          if (X) { const double2 z = __ldg(X + i); nx += z.x * z.x + z.y * z.y; }
+        }
+      }
+    }
+  }
+  const int64_t slot = (int64_t)blockIdx.y * gridDim.x + blockIdx.x, qs = (int64_t)gridDim.y * gridDim.x;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const double s0 = warp_sum(a0[j]), s1 = warp_sum(a1[j]);
+    if (j < na && lane == 0) {
+      const int q = warp + nw * j;
+      part[q * qs + slot] = s0; part[(20 + q) * qs + slot] = s1;
+    }
+  }
+  if (norms) {
+    n0 = warp_sum(n0); n1 = warp_sum(n1); nx = warp_sum(nx);
+    if (lane == 0) { part[40 * qs + slot] = n0; part[41 * qs + slot] = n1; part[42 * qs + slot] = nx; }
+  }
 }
 
 // out[f * (2 np + 3) + q] from the 43-quantity partials (quantities 20.. shifted down when np < 20)
@@ -228,20 +260,73 @@ __global__ void k_seg_finish_dots2(const double* part, int np, int nblk, double*
 
 struct SegTerms { const void* v[48]; };
 
-// out = sum_i coef[f * nt + i] v_i over each fit's slice
-template <typename T>
-__global__ void k_seg_lincomb(const blml_seg* segs, int cplx, T* out, int nt, const double* coef, SegTerms t) {
+// out = sum_i coef[f * nt + i] v_i over each fit's slice. The block lists the fit's nonzero terms (pointer, coefficient)
+// in shared memory once; each thread then takes two elements at a time and issues the loads of four terms together,
+// summing in term order (the sum of the terms in order, zero terms skipped, as a plain loop would). V is the element
+// type (double2 / float2: one (re, im) load per complex element). out may be one of the terms: every element is read
+// before the same thread writes it.
+template <typename T, typename V>
+__global__ void __launch_bounds__(256) k_seg_lincomb(const blml_seg* segs, int cplx, T* out, int nt,
+                                                     const double* coef, SegTerms t) {
+  __shared__ const V* sp[48];
+  __shared__ double sc[48];
+  __shared__ int snz;
   const blml_seg S = segs[blockIdx.y];
-  const int64_t w = cplx ? 2 : 1;
-  const int64_t o = S.off * w, n = (int64_t)S.K * S.B * w;
   const double* cf = coef + (int64_t)blockIdx.y * nt;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    double acc = 0.0;
+  if (threadIdx.x == 0) {
+    int c = 0;
     for (int q = 0; q < nt; q++) {
-      const double c = cf[q];
-      if (c != 0.0) acc += c * (double)reinterpret_cast<const T*>(t.v[q])[o + i];
+      const double v = cf[q];
+      if (v != 0.0) { sp[c] = reinterpret_cast<const V*>(t.v[q]); sc[c] = v; c++; }
     }
-    out[o + i] = (T)acc;
+    snz = c;
+  }
+  __syncthreads();
+  constexpr int W = sizeof(V) / sizeof(T);                  // reals per element: 2 for (re, im) pairs
+  const int64_t o = S.off * (cplx ? 2 : 1) / W, n = (int64_t)S.K * S.B * (cplx ? 2 : 1) / W;
+  const int nz = snz;
+  V* Y = reinterpret_cast<V*>(out);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
+    const int64_t i2 = i + stride;
+    const bool two = i2 < n;
+    double r0[W], r1[W];
+#pragma unroll
+    for (int w = 0; w < W; w++) { r0[w] = 0.0; r1[w] = 0.0; }
+    int k = 0;
+    for (; k + 4 <= nz; k += 4) {
+      V v0[4], v1[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) { v0[j] = sp[k + j][o + i]; if (two) v1[j] = sp[k + j][o + i2]; }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const double c = sc[k + j];
+        const T* a = reinterpret_cast<const T*>(&v0[j]);
+        const T* b = reinterpret_cast<const T*>(&v1[j]);
+#pragma unroll
+        for (int w = 0; w < W; w++) { r0[w] += c * (double)a[w]; if (two) r1[w] += c * (double)b[w]; }
+      }
+    }
+    for (; k < nz; k++) {
+      const double c = sc[k];
+      const V v0 = sp[k][o + i];
+      const T* a = reinterpret_cast<const T*>(&v0);
+#pragma unroll
+      for (int w = 0; w < W; w++) r0[w] += c * (double)a[w];
+      if (two) {
+        const V v1 = sp[k][o + i2];
+        const T* b = reinterpret_cast<const T*>(&v1);
+#pragma unroll
+        for (int w = 0; w < W; w++) r1[w] += c * (double)b[w];
+      }
+    }
+    V y0, y1;
+    T* p0 = reinterpret_cast<T*>(&y0);
+    T* p1 = reinterpret_cast<T*>(&y1);
+#pragma unroll
+    for (int w = 0; w < W; w++) { p0[w] = (T)r0[w]; p1[w] = (T)r1[w]; }
+    Y[o + i] = y0;
+    if (two) Y[o + i2] = y1;
   }
 }
 
@@ -559,8 +644,13 @@ int blml_seg_lincomb(int dtype, int F, const blml_seg* segs, int cplx, void* out
   if (nterms < 1 || nterms > 48) { set_error("blml_seg_lincomb: 1..48 terms"); return BLML_ERR_ARG; }
   SegTerms t;
   for (int q = 0; q < 48; q++) t.v[q] = q < nterms ? v[q] : nullptr;
-  if (dtype == BLML_F64) k_seg_lincomb<double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (double*)out, nterms, coef, t);
-  else k_seg_lincomb<float><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (float*)out, nterms, coef, t);
+  if (dtype == BLML_F64 && cplx)
+    k_seg_lincomb<double, double2><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (double*)out, nterms, coef, t);
+  else if (dtype == BLML_F64)
+    k_seg_lincomb<double, double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (double*)out, nterms, coef, t);
+  else if (cplx)
+    k_seg_lincomb<float, float2><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (float*)out, nterms, coef, t);
+  else k_seg_lincomb<float, float><<<SGRID(F), 256, 0, SST>>>(segs, cplx, (float*)out, nterms, coef, t);
   BLML_CHECK_LAUNCH("blml_seg_lincomb");
   return BLML_OK;
 }

@@ -344,6 +344,53 @@ def pairs_bench(dev, reps=3):
     return out
 
 
+def segscan_bench(dev, K=4, m=20, reps=20):
+    """The L-BFGS history kernels that dominate the certified sweep's GPU time, at its size: every sweep fit at K
+    shared modes (complex128 vectors of sum K B elements), the history scan (blml_seg_dots2: m stored vectors against
+    two shared ones) and the direction's linear combination (blml_seg_lincomb of 1 + 2 m vectors). CUDA events;
+    GB/s of the algorithmic bytes (each vector read once, the output written once)."""
+    import ctypes as C
+    import torch
+    from blml_b200 import _lib
+    from blml_b200._lib import call, ptrs
+    from blml_b200.sweep import _Seg
+    sweep, _ = workload(0)
+    B = np.array([f['train'].size for f in sweep], np.int64)
+    off = np.concatenate([[0], np.cumsum(K * B)]); boff = np.concatenate([[0], np.cumsum(B)])
+    F = len(B)
+    segs = (_Seg * F)(*[_Seg(int(off[f]), int(boff[f]), int(B[f]), K, 0) for f in range(F)])
+    st_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
+    n = int(off[-1])
+    g = torch.Generator(device=dev).manual_seed(0)
+    vecs = [torch.randn(n, dtype=torch.complex128, device=dev, generator=g) for _ in range(2 * m + 3)]
+    part = torch.empty(48 * 4096 + 64, dtype=torch.float64, device=dev)
+    out = torch.empty(48 * F + 64, dtype=torch.float64, device=dev)
+    q = torch.empty_like(vecs[0])
+    cf = torch.full((F, 1 + 2 * m), 0.5, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    vb = n * 16
+
+    def dots2():
+        call('blml_seg_dots2', _lib.F64, F, st_t.data_ptr(), 1, m, ptrs(vecs[:m]), vecs[2 * m].data_ptr(),
+             vecs[2 * m + 1].data_ptr(), vecs[2 * m + 2].data_ptr(), part.data_ptr(), out.data_ptr(), st)
+
+    def lincomb():
+        call('blml_seg_lincomb', _lib.F64, F, st_t.data_ptr(), 1, q.data_ptr(), 1 + 2 * m, cf.data_ptr(),
+             ptrs([vecs[2 * m]] + vecs[:2 * m]), st)
+    res = {'elements': n, 'vector_MB': vb / 1e6, 'K': K, 'm': m}
+    for name, fn, nbytes in (('dots2', dots2, (m + 3) * vb), ('lincomb', lincomb, (2 * m + 2) * vb)):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record(); torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        res[name] = {'us': t * 1e6, 'GB/s': nbytes / t / 1e9}
+    return res
+
+
 def tune_fft(dev, cta_kib=(24, 32, 48, 64, 72), max_cols=(1, 2, 4), reps=20):
     """The project's autotuner for the FFT route's launch shape: the grouped mat-vec over the 64 sweep lattices
     (complex float64, and real float64 as the start phase runs it) timed with CUDA events for every shared-memory
@@ -650,6 +697,8 @@ def main():
                     help='the batched cut-off search over 16 lattices beside the sequential single-fit search')
     ap.add_argument('--extras', action='store_true',
                     help='the gradients, point predictions and streaming refits, each beside a CPU-oracle sample')
+    ap.add_argument('--segscan', action='store_true',
+                    help="the L-BFGS history scan and direction kernels at the sweep's size (K = 4 modes per fit)")
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
@@ -682,6 +731,9 @@ def main():
         return
     if args.extras:
         print(json.dumps(extras_bench(dev)), flush=True)
+        return
+    if args.segscan:
+        print(json.dumps(segscan_bench(dev)), flush=True)
         return
     if args.matvec:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
