@@ -698,7 +698,8 @@ def main():
     ap.add_argument('--extras', action='store_true',
                     help='the gradients, point predictions and streaming refits, each beside a CPU-oracle sample')
     ap.add_argument('--segscan', action='store_true',
-                    help="the L-BFGS history scan and direction kernels at the sweep's size (K = 4 modes per fit)")
+                    help="the L-BFGS history scan and direction kernels at the sweep's size (--segscan-k modes per fit)")
+    ap.add_argument('--segscan-k', type=int, default=4)
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
@@ -733,7 +734,7 @@ def main():
         print(json.dumps(extras_bench(dev)), flush=True)
         return
     if args.segscan:
-        print(json.dumps(segscan_bench(dev)), flush=True)
+        print(json.dumps(segscan_bench(dev, K=args.segscan_k)), flush=True)
         return
     if args.matvec:
         b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
