@@ -44,6 +44,7 @@ CONFIG = {'workload': '64-fit batched 2-D complex pball cut-off sweep: sides {64
           'engine': 'batched lockstep, device-side control in CUDA-graph rings, grouped FFT mat-vecs',
           'l2': 'flushed between steps (256 MiB write)'}
 REF_SAMPLE = 8                       # fits of the sweep in the reference arm's bounded sample (the cheapest on CPU)
+LBFGS_M = 20                         # L-BFGS memory of the certified rounds (the certified optimum does not depend on it)
 
 
 def workload(seed=0):
@@ -269,7 +270,7 @@ def certify(res, ref):
 def certified_sweep(dev, train, val, modes, init=None):
     """One step: the sweep's certified fits (rank growth) and their held-out scores."""
     from blml_b200.sweep import BLMLBinnedBatch, certified_log_density
-    b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
+    b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev, lbfgs_m=LBFGS_M)
     res = b.fit_certified(train, modes, cert_tol=CERT_TOL, max_rank=MAX_RANK, init=init)
     return b, res, certified_log_density(res, val)
 
@@ -677,6 +678,7 @@ def flush_l2(buf):
 
 
 def main():
+    global LBFGS_M, MAX_RANK
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=3)
@@ -700,10 +702,13 @@ def main():
     ap.add_argument('--segscan', action='store_true',
                     help="the L-BFGS history scan and direction kernels at the sweep's size (--segscan-k modes per fit)")
     ap.add_argument('--segscan-k', type=int, default=4)
+    ap.add_argument('--lbfgs-m', type=int, default=20, help='L-BFGS memory of the certified rounds (1..20)')
+    ap.add_argument('--max-rank', type=int, default=MAX_RANK, help='most shared modes a certified fit grows to')
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
     args = ap.parse_args()
+    LBFGS_M, MAX_RANK = args.lbfgs_m, args.max_rank
     rank, ws, local = dist_init()
     if args.impl == 'reference':
         return reference_arm(args, rank, ws)
