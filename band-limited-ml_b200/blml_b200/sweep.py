@@ -774,7 +774,8 @@ def certified_log_density(results, counts_list, eps=0.0):
     for b, idx in groups.values():
         mine = {r._f: i for i, r in ((i, results[i]) for i in idx)}
         full = [counts_list[mine[f]] if f in mine else np.zeros(b.shapes[f]) for f in range(b.F)]
-        sc = b.log_density(full, eps)
+        with np.errstate(invalid='ignore', divide='ignore'):     # the batch's other fits score empty counts: 0 / 0
+            sc = b.log_density(full, eps)
         for f, i in mine.items():
             out[i] = sc[f]
     return out
