@@ -214,6 +214,9 @@ class BLMLBinnedStreaming(BLMLBinned):
         return out
 
     def _refit(self, E, sweeps):
+        if getattr(self, '_defer', None) is not None:        # BLMLBinnedStreamingBatch refits many streams at once
+            self._defer.append((E, sweeps))
+            return
         E, U = self._solve(E, sweeps)
         self._finish(E, U)
 
@@ -547,4 +550,68 @@ class BLMLBinnedStreaming(BLMLBinned):
                 on_epoch(ep, self)
             if tol is not None and self.converged_:
                 break
+        return self
+
+
+class BLMLBinnedStreamingBatch:
+    """Many count streams at once, each the reference's streaming fit with a fixed kernel (blml_binned.py:1034-1112
+    with fc_update=None; complex_g, L-BFGS): partial_fit(batches) takes the next batch of every stream. Each stream
+    scores and joins its batch as BLMLBinnedStreaming does (the prequential score under the current fit, the held
+    counts times decay plus the batch, the roots rescaled to the new n, newly occupied bins given their coordinate
+    root), then every stream's warm refit runs in one BLMLBinnedBatch lockstep from its joined coefficients, in place
+    of one L-BFGS fit per stream. The first batch of a stream (its burn-in and first fit) runs on the stream itself.
+
+        sb = BLMLBinnedStreamingBatch(len(streams), tol=1e-6, decay=0.95)
+        for batches in zip(*streams):                  # one count array per stream
+            sb.partial_fit(batches, modes_list)        # sb.streams[i].preq_, .loglik_, .e_hat_ ...
+    """
+
+    def __init__(self, n_streams, **kw):
+        if kw.get('fc_update', 'adam') is not None:
+            raise ValueError("BLMLBinnedStreamingBatch: fixed kernels (fc_update=None)")
+        if kw.setdefault('solver', 'lbfgs') != 'lbfgs':
+            raise ValueError("BLMLBinnedStreamingBatch: complex L-BFGS streams (solver='lbfgs')")
+        self.streams = [BLMLBinnedStreaming(**kw) for _ in range(int(n_streams))]
+        self.n_refits_ = 0
+
+    def partial_fit(self, batches, modes_list=None, h=1.0, origin=0.0):
+        from .sweep import BLMLBinnedBatch
+        if len(batches) != len(self.streams):
+            raise ValueError("partial_fit: one batch per stream")
+        pend = []
+        for i, (st, counts) in enumerate(zip(self.streams, batches)):
+            if st.n_batches_ == 0 and st._buffer is None:
+                if modes_list is None:
+                    raise ValueError("partial_fit: the first batches need modes_list")
+                st.partial_fit(counts, modes_list[i], h=h, origin=origin, complex_g=True)
+                continue
+            st._defer = []
+            try:
+                st.partial_fit(counts)
+            finally:
+                job, st._defer = st._defer, None
+            if job:
+                if st.d_ != 2 or not np.allclose(st.h_, 1.0):
+                    raise NotImplementedError("BLMLBinnedStreamingBatch: 2-D lattices with unit steps (h = 1)")
+                pend.append((st, job[-1]))
+        if not pend:
+            return self
+        ref = pend[0][0]
+        caps = np.array([-1 if sw is None else int(sw) for _, (_, sw) in pend], np.int64)
+        b = BLMLBinnedBatch(tol=ref.tol, max_sweeps=None, anderson=ref.anderson, dtype=ref.dtype,
+                            phase_noise=ref.phase_noise, seed=ref.seed, stall=ref.stall, ll_tol=ref.ll_tol,
+                            ll_window=ref.ll_window, lbfgs_m=ref.lbfgs_m, device=ref.dev_)
+        counts = [st.w_t_.reshape(st.shape_) for st, _ in pend]
+        modes = [st.modes_ for st, _ in pend]
+        init = [E.reshape((E.shape[0],) + tuple(st.shape_)) for st, (E, _) in pend]
+        res = b.fit(counts, modes, init=init, caps=caps)
+        for f, (st, _) in enumerate(pend):
+            E = b.e_hat(f).reshape(st.e_hat_t_.shape).clone()
+            a, z = b.moff[f], b.moff[f + 1]
+            U = b.U_t[a:z].reshape(E.shape).clone()
+            st._finish(E, U)
+            r = res[f]
+            st.n_sweeps_, st.stop_reason_, st.residual_, st.converged_ = (r.n_sweeps_, r.stop_reason_, r.residual_,
+                                                                         r.converged_)
+        self.n_refits_ += 1
         return self
