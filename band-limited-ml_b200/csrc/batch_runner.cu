@@ -1100,7 +1100,7 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
       r->Yh[i] = vec + (6 + (size_t)m + i) * tot * esz;
     }
     cudaMemsetAsync(vec, 0, (6 + 2 * (size_t)m) * tot * esz, r->st);
-    const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
+    const size_t pw = (size_t)SEG_PART_WIDTH(F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     const int nq = 48;                    // the widest reduction: blml_seg_dots' 48 accumulators
     const int hs = 2 * m + 3;
     double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F * (2 * hs + (LB_T1 + 4) + LB_T2 + 1 + 2 + 2 +
@@ -1220,7 +1220,7 @@ int blml_start_batch_create(int F, const blml_seg* segs, const blml_plan* plans,
     for (int i = 0; i < mA; i++) { r->DX[i] = vec + (10 + (size_t)i) * tot; r->DF[i] = vec + (10 + (size_t)mA + i) * tot; }
     cudaMemsetAsync(vec, 0, (10 + 2 * (size_t)mA) * tot * sizeof(double), r->st);
     const int nq = 3 * DAMP_NT;           // the widest reduction: the damping trials' 78 quantities
-    const size_t pw = (size_t)std::max(4096, 16 * F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
+    const size_t pw = (size_t)SEG_PART_WIDTH(F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F *
                                      (3 + 3 + 2 * AA_MMAX + 1 + 5 + nq + nq + (2 + 2 * AA_MMAX) + 2 + 3 + 1 + 1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (8 + (size_t)AA_MMAX * AA_MMAX));

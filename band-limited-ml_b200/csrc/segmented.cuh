@@ -6,12 +6,17 @@
 
 namespace blml {
 
-// blocks per fit (gridDim.x) of a segmented launch over F fits: ~4096 blocks in all, 16 to 256 per fit, so a few large
-// fits (or the last fits still iterating) still spread over every SM; the partials of a reduction over F fits take
-// nq * F * seg_blocks_for(F) <= nq * max(4096, 16 F) doubles
-constexpr int SEG_BLOCKS_MIN = 16, SEG_BLOCKS_MAX = 256;
+// blocks per fit (gridDim.x) of a segmented launch over F fits: ~16384 blocks in all, 16 to 256 per fit. Fits differ
+// in size by up to ~300x (lattice and mode count), and every fit gets the same blocks, so the block count is sized
+// for the largest: their blocks then still spread over every SM while the small fits' blocks find little or no work
+// and leave at once. The partials of a reduction over F fits take nq * F * seg_blocks_for(F) <= nq * SEG_PART_WIDTH(F)
+// doubles.
+constexpr int SEG_BLOCKS_MIN = 16, SEG_BLOCKS_MAX = 256, SEG_BLOCKS_TOTAL = 16384;
+__host__ __device__ constexpr int64_t SEG_PART_WIDTH(int F) {
+  return (int64_t)(SEG_BLOCKS_TOTAL > 16 * F ? SEG_BLOCKS_TOTAL : 16 * F);
+}
 __host__ __device__ inline int seg_blocks_for(int F) {
-  int x = 4096 / (F > 0 ? F : 1);
+  int x = SEG_BLOCKS_TOTAL / (F > 0 ? F : 1);
   return x < SEG_BLOCKS_MIN ? SEG_BLOCKS_MIN : (x > SEG_BLOCKS_MAX ? SEG_BLOCKS_MAX : x);
 }
 

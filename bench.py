@@ -364,7 +364,7 @@ def segscan_bench(dev, K=4, m=20, reps=20):
     n = int(off[-1])
     g = torch.Generator(device=dev).manual_seed(0)
     vecs = [torch.randn(n, dtype=torch.complex128, device=dev, generator=g) for _ in range(2 * m + 3)]
-    part = torch.empty(48 * 4096 + 64, dtype=torch.float64, device=dev)
+    part = torch.empty(48 * F * _lib.lib().blml_seg_blocks() + 64, dtype=torch.float64, device=dev)
     out = torch.empty(48 * F + 64, dtype=torch.float64, device=dev)
     q = torch.empty_like(vecs[0])
     cf = torch.full((F, 1 + 2 * m), 0.5, dtype=torch.float64, device=dev)
