@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(256) k_seg_dots2(const blml_seg* segs, int cpl
 // holds at most 6 accumulators (full occupancy, many loads in flight) and the two shared vectors are read from HBM
 // once per tile and from L1 by the other warps; the last warp also sums the three squared norms. Each quantity's
 // block partial comes from one warp (warp_sum, fixed order), in seg_partials' layout.
-__global__ void __launch_bounds__(256) k_seg_dots2_c128(const blml_seg* segs, int np, SegList al, const void* b0,
+__global__ void __launch_bounds__(256, 3) k_seg_dots2_c128(const blml_seg* segs, int np, SegList al, const void* b0,
                                                         const void* b1, const void* x, double* part) {
   const blml_seg S = segs[blockIdx.y];
   const int64_t o = S.off, n = (int64_t)S.K * S.B;
@@ -211,23 +211,31 @@ __global__ void __launch_bounds__(256) k_seg_dots2_c128(const blml_seg* segs, in
   }
   const bool norms = warp == nw - 1;
   double a0[3] = {0.0, 0.0, 0.0}, a1[3] = {0.0, 0.0, 0.0}, n0 = 0.0, n1 = 0.0, nx = 0.0;
+  const double2 zero = make_double2(0.0, 0.0);
   for (int64_t t = (int64_t)blockIdx.x * 64; t < n; t += (int64_t)gridDim.x * 64) {
+    // both elements' loads issued together: out-of-range lanes read element 0 and zero its shared values, so their
+    // products and norms add nothing
+    const int64_t i0 = t + lane, i1 = t + 32 + lane;
+    const bool v0 = i0 < n, v1 = i1 < n;
+    const int64_t j0 = v0 ? i0 : 0, j1 = v1 ? i1 : 0;
+    double2 y00 = __ldg(B0 + j0), y01 = __ldg(B0 + j1), y10 = __ldg(B1 + j0), y11 = __ldg(B1 + j1);
+    double2 a[3][2];
 #pragma unroll
-    for (int u = 0; u < 2; u++) {
-      const int64_t i = t + u * 32 + lane;
-      if (i < n) {
-        const double2 y0 = __ldg(B0 + i), y1 = __ldg(B1 + i);
+    for (int j = 0; j < 3; j++)
+      if (j < na) { a[j][0] = __ldg(A[j] + j0); a[j][1] = __ldg(A[j] + j1); }
+    double2 z0 = zero, z1 = zero;
+    if (norms && X) { z0 = __ldg(X + j0); z1 = __ldg(X + j1); }
+    if (!v0) { y00 = zero; y10 = zero; z0 = zero; }
+    if (!v1) { y01 = zero; y11 = zero; z1 = zero; }
 #pragma unroll
-        for (int j = 0; j < 3; j++)
-          if (j < na) {
-            const double2 a = __ldg(A[j] + i);
-            a0[j] += a.x * y0.x + a.y * y0.y; a1[j] += a.x * y1.x + a.y * y1.y;
-          }
-        if (norms) {
-          n0 += y0.x * y0.x + y0.y * y0.y; n1 += y1.x * y1.x + y1.y * y1.y;
-          if (X) { const double2 z = __ldg(X + i); nx += z.x * z.x + z.y * z.y; }
-        }
+    for (int j = 0; j < 3; j++)
+      if (j < na) {
+        a0[j] += a[j][0].x * y00.x + a[j][0].y * y00.y; a1[j] += a[j][0].x * y10.x + a[j][0].y * y10.y;
+        a0[j] += a[j][1].x * y01.x + a[j][1].y * y01.y; a1[j] += a[j][1].x * y11.x + a[j][1].y * y11.y;
       }
+    if (norms) {
+      n0 += y00.x * y00.x + y00.y * y00.y; n1 += y10.x * y10.x + y10.y * y10.y; nx += z0.x * z0.x + z0.y * z0.y;
+      n0 += y01.x * y01.x + y01.y * y01.y; n1 += y11.x * y11.x + y11.y * y11.y; nx += z1.x * z1.x + z1.y * z1.y;
     }
   }
   const int64_t slot = (int64_t)blockIdx.y * gridDim.x + blockIdx.x, qs = (int64_t)gridDim.y * gridDim.x;

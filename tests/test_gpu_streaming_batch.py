@@ -32,7 +32,8 @@ def test_streams_in_one_batch_equal_streams_one_by_one(cuda_device):
         for t in range(4):
             one.partial_fit(s[t], modes[i] if t == 0 else None, complex_g=True)
         got = sb.streams[i]
-        assert len(got.preq_) == len(one.preq_) == 3
-        for a, b in zip(got.preq_, one.preq_):
+        assert len(got.preq_) == len(one.preq_) == 4            # the first batch has no fit to score it: NaN
+        assert np.isnan(got.preq_[0]) and np.isnan(one.preq_[0])
+        for a, b in zip(got.preq_[1:], one.preq_[1:]):
             assert abs(a - b) <= 1e-6 * abs(b), (i, got.preq_, one.preq_)
         assert abs(got.loglik_ - one.loglik_) <= 1e-6 * abs(one.loglik_), (i, got.loglik_, one.loglik_)
