@@ -2,6 +2,8 @@
 where the reference calls ARPACK's eigsh(k=1, which='LA', tol)). Full reorthogonalisation against the stored
 basis (float64 multi-dot and linear-combination kernels), the tridiagonal eigenproblem on the host, restarts from the
 Ritz vector. Converged when the Ritz residual |beta_j y_j| <= tol |theta|."""
+import time
+
 import numpy as np
 import torch
 
@@ -84,8 +86,8 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     rebuilt over them (a fit's arithmetic does not depend on which other fits share the launch). Returns (theta (F,),
     dh, v): dh the per-bin scaling and v the top Ritz vectors (float64 per bin over all fits, None unless vectors)
     -- d = dh v is the direction of a new mode."""
-    from scipy.linalg import eigh_tridiagonal
     from .sweep import _Group, _Seg
+    clock = {'wait_s': 0.0, 'host_s': 0.0}
     F, dev, st, B = batch.F, batch.device, batch.st, batch.Btot
     code = _lib.F64
     dh = torch.empty(B, dtype=torch.float64, device=dev)
@@ -110,15 +112,31 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
         call('blml_seg_dots', code, n, S.segs_t.data_ptr(), 0, len(pairs), ptrs([p[0] for p in pairs]),
              ptrs([p[1] for p in pairs]), batch.part.data_ptr(), batch.out.data_ptr(), st)
         batch.host[:len(pairs) * n].copy_(batch.out[:len(pairs) * n], non_blocking=True)
+        t0 = time.perf_counter()
         torch.cuda.current_stream(dev).synchronize()
+        clock['wait_s'] += time.perf_counter() - t0
         out = np.zeros((F, len(pairs)))
         out[S.idx] = batch.host[:len(pairs) * n].numpy().reshape(n, len(pairs))
         return out
 
+    # coefficient uploads through a ring of pinned host slots, so a linear combination does not wait for the stream
+    # (a pageable copy would): a slot is reused only after the event recorded behind its copy has completed
+    nring, width = 32, F * 48 + 64
+    ring_h = torch.empty((nring, width), dtype=torch.float64, pin_memory=True)
+    ring_d = torch.empty((nring, width), dtype=torch.float64, device=dev)
+    ring_ev = [None] * nring
+    slot = [0]
+
     def lin(S, out, coef, vecs):                     # coef (F, nterms): the rows of S's fits are used
-        cf = torch.as_tensor(np.ascontiguousarray(np.asarray(coef, np.float64)[S.idx])).to(dev, non_blocking=True)
+        c = np.ascontiguousarray(np.asarray(coef, np.float64)[S.idx]).ravel()
+        k = slot[0]; slot[0] = (k + 1) % nring
+        if ring_ev[k] is not None:
+            ring_ev[k].synchronize()
+        ring_h[k, :c.size].numpy()[:] = c
+        ring_d[k, :c.size].copy_(ring_h[k, :c.size], non_blocking=True)
+        ev = torch.cuda.Event(); ev.record(torch.cuda.current_stream(dev)); ring_ev[k] = ev
         call('blml_seg_lincomb', code, len(S.idx), S.segs_t.data_ptr(), 0, out.data_ptr(), len(vecs),
-             cf.data_ptr(), ptrs(vecs), st)
+             ring_d[k].data_ptr(), ptrs(vecs), st)
 
     def op(S, x, out):                               # out = dh * S (dh * x) on S's fits
         call('blml_mul_bins', code, 1, B, 0, x.data_ptr(), dh.data_ptr(), tmp.data_ptr(), st)
@@ -159,14 +177,23 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
             open_ &= ~(done | conv)
             check = j == nb - 1 or (j >= 5 and j % 3 == 2) or bool(np.any(beta[open_] <= 1e-300))
             if check:
-                for f in np.where(open_)[0]:
-                    ev, evec = eigh_tridiagonal(alphas[f, :j + 1], betas[f, :j], select='i', select_range=(j, j))
-                    th = float(ev[0]); y = evec[:, 0]
+                t0 = time.perf_counter()
+                of = np.where(open_)[0]
+                # every open fit's tridiagonal problem at once: the largest eigenpair of T_f (j + 1 square)
+                T = np.zeros((len(of), j + 1, j + 1))
+                ii = np.arange(j + 1)
+                T[:, ii, ii] = alphas[of, :j + 1]
+                T[:, ii[:-1], ii[1:]] = betas[of, :j]
+                T[:, ii[1:], ii[:-1]] = betas[of, :j]
+                ev_all, evec_all = np.linalg.eigh(T)
+                for t_, f in enumerate(of):
+                    th = float(ev_all[t_, -1]); y = evec_all[t_, :, -1].copy()
                     theta[f] = th; yr[f] = y
                     if (abs(beta[f] * y[-1]) <= tol * max(abs(th), 1e-300) or beta[f] <= 1e-14 * max(abs(th), 1e-300)
                             or th > above[f] or abs(th - prev[f]) <= 1e-8 * abs(th)):
                         conv[f] = True
                     prev[f] = th
+                clock['host_s'] += time.perf_counter() - t0
                 if np.all(done | conv):
                     j_end = j + 1
                     break
@@ -203,5 +230,6 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     if vectors:
         nv = dots(every, [(vec, vec)])[:, 0]
         lin(every, vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
-    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()))
+    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()), wait_s=round(clock['wait_s'], 4),
+                                host_s=round(clock['host_s'], 4))
     return theta, dh, vec

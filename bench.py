@@ -193,6 +193,16 @@ def traffic_from_profiles():
         return None
 
 
+def scan_traffic(K):
+    """DRAM bytes of one history-scan launch at K modes per fit: the committed ncu capture (K = 1, the same 64 lattices)
+    scaled by K -- the scan streams K-times-longer vectors, so its traffic grows in proportion."""
+    try:
+        t = json.load(open(os.path.join(ROOT, 'profiles', 'history_scan_sweep64_traffic.json')))
+        return t['dram_bytes_per_launch'] * K / t['K']
+    except Exception:
+        return None
+
+
 def _port_certified_fit(i):
     """Sweep fit i certified by the FP64 NumPy / SciPy port of the reference's algorithm (oracle/blml_oracle.py) on
     one host core: the same rank growth and certificate bar as the engine. Runs in a spawned worker."""
@@ -830,6 +840,7 @@ def main():
     b1 = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev)
     b1._prepare(train, modes)
     t_mv, mv_bytes, mv_flops = grouped_matvec_roofline(b1)
+    scan = segscan_bench(dev, K=4)
     pk = peaks()
     peak = pk['hbm_gbs'] if pk else 6650.0
     achieved = mv_bytes / t_mv / 1e9
@@ -853,12 +864,24 @@ def main():
                        'h2d_bytes_per_step': int(sum(c.nbytes for c in train) + sum(c.nbytes for c in val)),
                        'd2h_bytes_per_step': d2h},
                'gpu_launches': int(launches),
-               'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
-                            'frac': achieved / peak, 'traffic': traffic_from_profiles(),
-                            'kernel': f'grouped mat-vec over the 64 fits (FFT route: 3 grouped launches, float64): '
-                                      f'{mv_bytes} algorithmic bytes (read E + write U, complex128), '
-                                      f'{t_mv * 1e6:.1f} us per chain',
+               'roofline': {'bound': 'hbm', 'achieved': scan['dots2']['GB/s'], 'peak': peak, 'unit': 'GB/s',
+                            'frac': scan['dots2']['GB/s'] / peak, 'traffic': scan_traffic(4),
+                            'kernel': f"k_seg_dots2_c128, the L-BFGS history scan (with the direction's linear "
+                                      f"combination, two thirds of the certified sweep's GPU time): the 20 stored "
+                                      f"vectors and 2 shared ones over the 64 sweep lattices at K = 4 modes, "
+                                      f"complex128, {scan['elements']} elements: "
+                                      f"{23 * 16 * scan['elements']} algorithmic bytes, {scan['dots2']['us']:.1f} us "
+                                      f"per launch",
                             'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if pk else 'fallback'},
+               'roofline_lincomb': {'bound': 'hbm', 'achieved': scan['lincomb']['GB/s'], 'peak': peak,
+                                    'unit': 'GB/s', 'frac': scan['lincomb']['GB/s'] / peak,
+                                    'kernel': f"k_seg_lincomb<double, double2>, the direction (41 vectors in, 1 out), "
+                                              f"{scan['lincomb']['us']:.1f} us per launch"},
+               'roofline_matvec': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                                   'frac': achieved / peak, 'traffic': traffic_from_profiles(),
+                                   'kernel': f'grouped mat-vec over the 64 fits (FFT route: 3 grouped launches, '
+                                             f'float64): {mv_bytes} algorithmic bytes (read E + write U, complex128), '
+                                             f'{t_mv * 1e6:.1f} us per chain; latency bound'},
                'cpu_baseline': cpu, 'clocks': clk.summary(),
                'plain_gpu': {'value': plain_cert / t_plain, 'unit': 'fits/s', 'certified': plain_cert,
                              'seconds': t_plain,
