@@ -99,6 +99,7 @@ _SIGS = {
     'blml_nn_to_bf16': (_I, [_P, _L, _P, _P, _I, _I, _P]),
     'blml_lbfgs_batch_create': (_I, [_I, _I, _P, _P, _I, _D, _D, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     'blml_lbfgs_batch_set_caps': (_I, [_P, _P]),
+    'blml_lbfgs_batch_set_history': (_I, [_P, _I]),
     'blml_lbfgs_batch_run': (_I, [_P, _P]),
     'blml_lbfgs_batch_result': (_I, [_P, _P, _P, _P, _P, _P]),
     'blml_lbfgs_batch_stats': (_I, [_P, _P]),

@@ -368,6 +368,8 @@ class BLMLBinnedBatch:
             if getattr(self, '_caps', None) is not None:
                 caps = np.ascontiguousarray(self._caps, np.int64)
                 call('blml_lbfgs_batch_set_caps', h, caps.ctypes.data_as(C.c_void_p))
+            if getattr(self, '_history_f32', False):
+                call('blml_lbfgs_batch_set_history', h, 1)
             call('blml_lbfgs_batch_run', h, self.st)
             it = np.zeros(F, np.int64); stop = np.zeros(F, np.int32); L = np.zeros(F); res = np.zeros(F)
             call('blml_lbfgs_batch_result', h, it.ctypes.data_as(C.c_void_p), stop.ctypes.data_as(C.c_void_p),
@@ -680,7 +682,7 @@ class BLMLBinnedBatch:
         return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
 
     def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300,
-                      grow_margin=1.0):
+                      grow_margin=1.0, history_f32=True):
         """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
         batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
         mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
@@ -690,10 +692,16 @@ class BLMLBinnedBatch:
         cert_tol (default: none) is run on to tol at its rank before it may grow; on the benchmark sweep a margin of
         10 doubled the time, the polished fits crawling at too low a rank. The lift is convex: a fit that meets the certificate at tol is at its unique optimum
         (the reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results
-        carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...]."""
+        carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...].
+        history_f32: the L-BFGS history of every round in complex64 storage (the iterate, gradient and line search
+        stay float64): the certified optimum does not depend on the path the solver takes to it."""
         F = len(counts_list)
         first_caps = np.full(F, grow_iters if max_rank > 1 else -1, np.int64)
-        self.fit(counts_list, modes_list, init=init, caps=first_caps)
+        self._history_f32 = bool(history_f32)
+        try:
+            self.fit(counts_list, modes_list, init=init, caps=first_caps)
+        finally:
+            self._history_f32 = False
         final = [None] * F
         paths = [[] for _ in range(F)]
         cur, idx, capped = self, np.arange(F), first_caps >= 0
@@ -734,7 +742,9 @@ class BLMLBinnedBatch:
                                   verbose=self.verbose, control=self.control)
             mds = [[modes_list[i][0]] * K1 for _, i, K1 in nxt_fits]
             caps = np.array(nxt_caps, np.int64)
+            nxt._history_f32 = bool(history_f32)
             nxt.fit([counts_list[i] for _, i, _ in nxt_fits], mds, init=starts, caps=caps)
+            nxt._history_f32 = False
             cur, idx, capped = nxt, np.array([i for _, i, _ in nxt_fits]), caps >= 0
 
     def val_score(self, counts_list):

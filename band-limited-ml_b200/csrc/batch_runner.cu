@@ -826,6 +826,9 @@ struct blml_lbfgs_batch_s : Runner {
   const void *w = nullptr, *c = nullptr;
   void *g = nullptr, *gn = nullptr, *q = nullptr, *Sq = nullptr, *V = nullptr, *SV = nullptr;
   void *Sh[LB_MMAX] = {}, *Yh[LB_MMAX] = {};
+  int h32 = 0;                           // the history (Sh, Yh) in complex64 storage (float64 state only)
+  int64_t tot = 0;                       // elements of every mode array (the fits' K B summed)
+  void* hvec = nullptr;                  // the history's allocation
   double *part = nullptr, *H1 = nullptr, *H2 = nullptr, *T1 = nullptr, *T2 = nullptr, *outC = nullptr,
          *outD = nullptr, *outE = nullptr;
   double *cq = nullptr, *tA = nullptr, *cS = nullptr, *cY = nullptr, *cG = nullptr, *nqA = nullptr, *scrA = nullptr,
@@ -838,8 +841,10 @@ struct blml_lbfgs_batch_s : Runner {
   int hist(int Fa_, const blml_seg* S, int p) {
     const void* a[LB_MMAX];
     for (int i = 0; i < m; i++) a[i] = Sh[i];
-    RC(blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, E, part, H1, st));
+    if (h32) RC(seg_dots2_h32(Fa_, S, m, a, Yh[p], g, E, part, H1, st));
+    else RC(blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, E, part, H1, st));
     for (int i = 0; i < m; i++) a[i] = Yh[i];
+    if (h32) return seg_dots2_h32(Fa_, S, m, a, Yh[p], g, nullptr, part, H2, st);
     return blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, nullptr, part, H2, st);
   }
 
@@ -882,7 +887,8 @@ struct blml_lbfgs_batch_s : Runner {
     const void* terms[48];
     terms[0] = g;
     for (int i = 0; i < m; i++) { terms[1 + i] = Sh[i]; terms[1 + m + i] = Yh[i]; }
-    RC(blml_seg_lincomb(dt, Fa_, S, 1, q, 1 + 2 * m, cq, terms, sv));
+    if (h32) RC(seg_lincomb_mixed(Fa_, S, q, 0, 1 + 2 * m, cq, terms, ((1ull << (2 * m)) - 1ull) << 1, st));
+    else RC(blml_seg_lincomb(dt, Fa_, S, 1, q, 1 + 2 * m, cq, terms, sv));
     RC(blml_group_matvec_masked(gq, d_fid, Fa_, d_live, sv));
     // every fit's Armijo search (8 trials, then 32 more for the fits that need them), the accepted steps, U = S E
     RC(dt == BLML_F64 ? trials<double>(Fa_, S) : trials<float>(Fa_, S));
@@ -897,9 +903,11 @@ struct blml_lbfgs_batch_s : Runner {
     RC(blml_group_matvec_masked(gV, d_fid, Fa_, d_live, sv));
     RC(blml_seg_lgrad_finish(dt, Fa_, S, 1, SV, U, w, nqA, gn, sv));
     terms[0] = q; terms[1] = Sh[p];
-    RC(blml_seg_lincomb(dt, Fa_, S, 1, Sh[p], 2, cS, terms, sv));
+    if (h32) RC(seg_lincomb_mixed(Fa_, S, Sh[p], 1, 2, cS, terms, 2ull, st));
+    else RC(blml_seg_lincomb(dt, Fa_, S, 1, Sh[p], 2, cS, terms, sv));
     terms[0] = g; terms[1] = gn; terms[2] = Yh[p];
-    RC(blml_seg_lincomb(dt, Fa_, S, 1, Yh[p], 3, cY, terms, sv));
+    if (h32) RC(seg_lincomb_mixed(Fa_, S, Yh[p], 1, 3, cY, terms, 4ull, st));
+    else RC(blml_seg_lincomb(dt, Fa_, S, 1, Yh[p], 3, cY, terms, sv));
     terms[0] = gn; terms[1] = g;
     RC(blml_seg_lincomb(dt, Fa_, S, 1, g, 2, cG, terms, sv));
     RC(blml_seg_resid(dt, Fa_, S, 1, E, U, c, scrA, part, outE, sv));
@@ -1090,16 +1098,19 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
   r->E = E; r->U = U; r->w = w; r->c = c;
   int rc = r->base_init(F, segs);
   const size_t esz = dtype == BLML_F64 ? 16 : 8;
-  char* vec = rc ? nullptr : (char*)r->dalloc((6 + 2 * (size_t)m) * tot * esz);
-  if (!rc && !vec) { set_error("blml_lbfgs_batch_create: vector allocation"); rc = BLML_ERR_CUDA; }
+  char* vec = rc ? nullptr : (char*)r->dalloc(6 * tot * esz);
+  char* hv = rc ? nullptr : (char*)r->dalloc(2 * (size_t)m * tot * esz);
+  if (!rc && (!vec || !hv)) { set_error("blml_lbfgs_batch_create: vector allocation"); rc = BLML_ERR_CUDA; }
   if (!rc) {
+    r->tot = tot; r->hvec = hv;
     void** v6[6] = {&r->g, &r->gn, &r->q, &r->Sq, &r->V, &r->SV};
     for (int i = 0; i < 6; i++) *v6[i] = vec + (size_t)i * tot * esz;
     for (int i = 0; i < m; i++) {
-      r->Sh[i] = vec + (6 + (size_t)i) * tot * esz;
-      r->Yh[i] = vec + (6 + (size_t)m + i) * tot * esz;
+      r->Sh[i] = hv + (size_t)i * tot * esz;
+      r->Yh[i] = hv + ((size_t)m + i) * tot * esz;
     }
-    cudaMemsetAsync(vec, 0, (6 + 2 * (size_t)m) * tot * esz, r->st);
+    cudaMemsetAsync(vec, 0, 6 * tot * esz, r->st);
+    cudaMemsetAsync(hv, 0, 2 * (size_t)m * tot * esz, r->st);
     const size_t pw = (size_t)SEG_PART_WIDTH(F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
     const int nq = 48;                    // the widest reduction: blml_seg_dots' 48 accumulators
     const int hs = 2 * m + 3;
@@ -1136,6 +1147,28 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
   if (!rc) rc = make_group(F, plans, segs, 1, r->V, r->SV, off, &r->gV);
   if (rc) { r->release(); delete r; return rc; }
   *out = r;
+  return BLML_OK;
+}
+
+int blml_lbfgs_batch_set_history(blml_lbfgs_batch r, int f32) {
+  if (!r) { set_error("blml_lbfgs_batch_set_history: null runner"); return BLML_ERR_ARG; }
+  if (!f32 || r->h32) return BLML_OK;
+  if (r->dtype != BLML_F64) return BLML_OK;          // float32 state: the history is float32 already
+  // a complex64 history in place of the complex128 one (half its size); the old allocation is released
+  const size_t bytes = 2 * (size_t)r->m * r->tot * 8;
+  void* hv = nullptr;
+  if (cudaMalloc(&hv, bytes) != cudaSuccess) { set_error("blml_lbfgs_batch_set_history: allocation"); return BLML_ERR_CUDA; }
+  int rc = cuda_status(cudaStreamSynchronize(r->st), "blml_lbfgs_batch_set_history");
+  if (!rc) rc = cuda_status(cudaMemsetAsync(hv, 0, bytes, r->st), "blml_lbfgs_batch_set_history");
+  if (rc) { cudaFree(hv); return rc; }
+  for (auto& p : r->allocs)
+    if (p == r->hvec) { cudaFree(p); p = hv; break; }
+  r->hvec = hv;
+  for (int i = 0; i < r->m; i++) {
+    r->Sh[i] = (char*)hv + (size_t)i * r->tot * 8;
+    r->Yh[i] = (char*)hv + ((size_t)r->m + i) * r->tot * 8;
+  }
+  r->h32 = 1;
   return BLML_OK;
 }
 

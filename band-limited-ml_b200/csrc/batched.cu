@@ -188,25 +188,34 @@ __global__ void __launch_bounds__(256) k_seg_dots2(const blml_seg* segs, int cpl
   seg_partials<43>(v, part);
 }
 
-// the same scan for float64 complex vectors, one 16-byte (re, im) load per element and vector. The block's 8 warps
+// the same scan for float64 complex vectors, one (re, im) load per element and vector -- the stored vectors (TA)
+// and the first shared one (TB0) complex128, or complex64 when the history is kept in float32. The block's 8 warps
 // split the stored vectors (warp w takes q = w, w + 8, w + 16) and walk the same 64-element tiles, so each thread
 // holds at most 6 accumulators (full occupancy, many loads in flight) and the two shared vectors are read from HBM
 // once per tile and from L1 by the other warps; the last warp also sums the three squared norms. Each quantity's
 // block partial comes from one warp (warp_sum, fixed order), in seg_partials' layout.
+// one complex element as (re, im) in float64, from complex128 or complex64 storage
+__device__ __forceinline__ double2 ld_c2(const double2* p) { return __ldg(p); }
+__device__ __forceinline__ double2 ld_c2(const float2* p) {
+  const float2 v = __ldg(p);
+  return make_double2((double)v.x, (double)v.y);
+}
+
+template <typename TA, typename TB0>
 __global__ void __launch_bounds__(256, 3) k_seg_dots2_c128(const blml_seg* segs, int np, SegList al, const void* b0,
-                                                        const void* b1, const void* x, double* part) {
+                                                           const void* b1, const void* x, double* part) {
   const blml_seg S = segs[blockIdx.y];
   const int64_t o = S.off, n = (int64_t)S.K * S.B;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const double2* B0 = reinterpret_cast<const double2*>(b0) + o;
+  const TB0* B0 = reinterpret_cast<const TB0*>(b0) + o;
   const double2* B1 = reinterpret_cast<const double2*>(b1) + o;
   const double2* X = x ? reinterpret_cast<const double2*>(x) + o : nullptr;
-  const double2* A[3];
+  const TA* A[3];
   int na = 0;
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     const int q = warp + nw * j;
-    A[j] = q < np ? reinterpret_cast<const double2*>(al.a[q]) + o : nullptr;
+    A[j] = q < np ? reinterpret_cast<const TA*>(al.a[q]) + o : nullptr;
     na += q < np;
   }
   const bool norms = warp == nw - 1;
@@ -218,11 +227,11 @@ __global__ void __launch_bounds__(256, 3) k_seg_dots2_c128(const blml_seg* segs,
     const int64_t i0 = t + lane, i1 = t + 32 + lane;
     const bool v0 = i0 < n, v1 = i1 < n;
     const int64_t j0 = v0 ? i0 : 0, j1 = v1 ? i1 : 0;
-    double2 y00 = __ldg(B0 + j0), y01 = __ldg(B0 + j1), y10 = __ldg(B1 + j0), y11 = __ldg(B1 + j1);
+    double2 y00 = ld_c2(B0 + j0), y01 = ld_c2(B0 + j1), y10 = __ldg(B1 + j0), y11 = __ldg(B1 + j1);
     double2 a[3][2];
 #pragma unroll
     for (int j = 0; j < 3; j++)
-      if (j < na) { a[j][0] = __ldg(A[j] + j0); a[j][1] = __ldg(A[j] + j1); }
+      if (j < na) { a[j][0] = ld_c2(A[j] + j0); a[j][1] = ld_c2(A[j] + j1); }
     double2 z0 = zero, z1 = zero;
     if (norms && X) { z0 = __ldg(X + j0); z1 = __ldg(X + j1); }
     if (!v0) { y00 = zero; y10 = zero; z0 = zero; }
@@ -335,6 +344,73 @@ __global__ void __launch_bounds__(256) k_seg_lincomb(const blml_seg* segs, int c
     for (int w = 0; w < W; w++) { p0[w] = (T)r0[w]; p1[w] = (T)r1[w]; }
     Y[o + i] = y0;
     if (two) Y[o + i2] = y1;
+  }
+}
+
+// out = sum_i coef[f * nt + i] v_i for complex float64 arithmetic over terms of two storage types: bit i of f32mask
+// marks term i as complex64 (a float32 history vector), the others complex128; out is complex64 (VO = float2) or
+// complex128. Same term order, listing and load batching as k_seg_lincomb.
+template <typename VO>
+__global__ void __launch_bounds__(256) k_seg_lincomb_mixed(const blml_seg* segs, VO* out, int nt, const double* coef,
+                                                           SegTerms t, unsigned long long f32mask) {
+  __shared__ const void* sp[48];
+  __shared__ double sc[48];
+  __shared__ int s32[48];
+  __shared__ int snz;
+  const blml_seg S = segs[blockIdx.y];
+  const double* cf = coef + (int64_t)blockIdx.y * nt;
+  if (threadIdx.x == 0) {
+    int c = 0;
+    for (int q = 0; q < nt; q++) {
+      const double v = cf[q];
+      if (v != 0.0) { sp[c] = t.v[q]; sc[c] = v; s32[c] = (int)((f32mask >> q) & 1ull); c++; }
+    }
+    snz = c;
+  }
+  __syncthreads();
+  const int64_t o = S.off, n = (int64_t)S.K * S.B;
+  const int nz = snz;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
+    const int64_t i2 = i + stride;
+    const bool two = i2 < n;
+    const int64_t j2 = two ? i2 : i;
+    double r0x = 0.0, r0y = 0.0, r1x = 0.0, r1y = 0.0;
+    int k = 0;
+    for (; k + 4 <= nz; k += 4) {
+      double2 v0[4], v1[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        if (s32[k + j]) {
+          const float2* p = reinterpret_cast<const float2*>(sp[k + j]) + o;
+          v0[j] = ld_c2(p + i); v1[j] = ld_c2(p + j2);
+        } else {
+          const double2* p = reinterpret_cast<const double2*>(sp[k + j]) + o;
+          v0[j] = ld_c2(p + i); v1[j] = ld_c2(p + j2);
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const double c = sc[k + j];
+        r0x += c * v0[j].x; r0y += c * v0[j].y; r1x += c * v1[j].x; r1y += c * v1[j].y;
+      }
+    }
+    for (; k < nz; k++) {
+      double2 v0, v1;
+      if (s32[k]) {
+        const float2* p = reinterpret_cast<const float2*>(sp[k]) + o;
+        v0 = ld_c2(p + i); v1 = ld_c2(p + j2);
+      } else {
+        const double2* p = reinterpret_cast<const double2*>(sp[k]) + o;
+        v0 = ld_c2(p + i); v1 = ld_c2(p + j2);
+      }
+      const double c = sc[k];
+      r0x += c * v0.x; r0y += c * v0.y; r1x += c * v1.x; r1y += c * v1.y;
+    }
+    VO y0, y1;
+    y0.x = r0x; y0.y = r0y; y1.x = r1x; y1.y = r1y;
+    out[o + i] = y0;
+    if (two) out[o + i2] = y1;
   }
 }
 
@@ -548,6 +624,35 @@ static void seg_dots_launch(dim3 g, const blml_seg* s, int cplx, int np, const S
 
 using namespace blml;
 #define SST reinterpret_cast<cudaStream_t>(stream)
+namespace blml {
+// the L-BFGS runner's history with float32 storage (internal to the library): the scan over complex64 stored vectors
+// and a complex64 first shared vector, and linear combinations over complex128 / complex64 terms
+int seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
+                  const void* x, double* part, double* out, cudaStream_t st) {
+  if (np < 1 || np > 20 || !a || !b0 || !b1) { set_error("history scan: 1..20 vectors, b0 and b1"); return BLML_ERR_ARG; }
+  SegList al;
+  for (int q = 0; q < 20; q++) al.a[q] = q < np ? a[q] : nullptr;
+  k_seg_dots2_c128<float2, float2><<<dim3((unsigned)seg_blocks_for(F), (unsigned)F), 256, 0, st>>>(segs, np, al, b0,
+                                                                                                 b1, x, part);
+  BLML_CHECK_LAUNCH("history scan (float32 history)");
+  k_seg_finish_dots2<<<F, 256, 0, st>>>(part, np, seg_blocks_for(F), out);
+  BLML_CHECK_LAUNCH("history scan finish");
+  return BLML_OK;
+}
+
+int seg_lincomb_mixed(int F, const blml_seg* segs, void* out, int out_f32, int nterms, const double* coef,
+                      const void* const* v, unsigned long long f32mask, cudaStream_t st) {
+  if (nterms < 1 || nterms > 48) { set_error("linear combination: 1..48 terms"); return BLML_ERR_ARG; }
+  SegTerms t;
+  for (int q = 0; q < 48; q++) t.v[q] = q < nterms ? v[q] : nullptr;
+  const dim3 grid((unsigned)seg_blocks_for(F), (unsigned)F);
+  if (out_f32) k_seg_lincomb_mixed<float2><<<grid, 256, 0, st>>>(segs, (float2*)out, nterms, coef, t, f32mask);
+  else k_seg_lincomb_mixed<double2><<<grid, 256, 0, st>>>(segs, (double2*)out, nterms, coef, t, f32mask);
+  BLML_CHECK_LAUNCH("linear combination (mixed storage)");
+  return BLML_OK;
+}
+}  // namespace blml
+
 #define SGRID(F) dim3((unsigned)seg_blocks_for(F), (unsigned)(F))
 #define TYPED(dtype, cplx, K, ...)                                          \
   do {                                                                      \
@@ -637,7 +742,8 @@ int blml_seg_dots2(int dtype, int F, const blml_seg* segs, int cplx, int np, con
   if (np < 1 || np > 20 || !a || !b0 || !b1) { set_error("blml_seg_dots2: 1..20 vectors, b0 and b1"); return BLML_ERR_ARG; }
   SegList al;
   for (int q = 0; q < 20; q++) al.a[q] = q < np ? a[q] : nullptr;
-  if (dtype == BLML_F64 && cplx) k_seg_dots2_c128<<<SGRID(F), 256, 0, SST>>>(segs, np, al, b0, b1, x, part);
+  if (dtype == BLML_F64 && cplx)
+    k_seg_dots2_c128<double2, double2><<<SGRID(F), 256, 0, SST>>>(segs, np, al, b0, b1, x, part);
   else if (dtype == BLML_F64) k_seg_dots2<double><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
   else k_seg_dots2<float><<<SGRID(F), 256, 0, SST>>>(segs, cplx, np, al, b0, b1, x, part);
   BLML_CHECK_LAUNCH("blml_seg_dots2");

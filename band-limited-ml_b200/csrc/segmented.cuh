@@ -20,6 +20,12 @@ __host__ __device__ inline int seg_blocks_for(int F) {
   return x < SEG_BLOCKS_MIN ? SEG_BLOCKS_MIN : (x > SEG_BLOCKS_MAX ? SEG_BLOCKS_MAX : x);
 }
 
+// the L-BFGS runner's float32 history (batched.cu)
+int seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
+                  const void* x, double* part, double* out, cudaStream_t st);
+int seg_lincomb_mixed(int F, const blml_seg* segs, void* out, int out_f32, int nterms, const double* coef,
+                      const void* const* v, unsigned long long f32mask, cudaStream_t st);
+
 template <typename T, bool CPLX>
 struct SAcc {
   static __device__ __forceinline__ void get(const void* p, int64_t i, double& re, double& im) {

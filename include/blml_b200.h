@@ -301,6 +301,11 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
 /* per-fit iteration caps (F host values, < 0: none) in place of max_iters, before blml_lbfgs_batch_run: rounds of a
    certified fit cap the fits still growing their rank and let the final ones run to tol */
 int blml_lbfgs_batch_set_caps(blml_lbfgs_batch runner, const int64_t* caps);
+/* The runner's L-BFGS history (its 2 m stored step and gradient-difference vectors) kept in complex64 storage when
+   f32 != 0 and the state is float64: the direction and the history scan read half the bytes, the iterate, gradient
+   and line search stay float64. No counterpart in the reference (its history is float64); for runs whose answer does
+   not depend on the path, e.g. certified fits. Call before the first run. */
+int blml_lbfgs_batch_set_history(blml_lbfgs_batch runner, int f32);
 int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);
 /* per fit (host arrays of F, any may be null): iterations, stop code, L, Q, max|rho| */
 int blml_lbfgs_batch_result(blml_lbfgs_batch runner, int64_t* iters, int32_t* stop, double* L, double* Q,

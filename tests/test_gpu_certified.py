@@ -66,3 +66,17 @@ def test_certified_fits_reach_the_oracle_optimum(cuda_device):
         ll = path[-1][1]
         assert abs(r.loglik_ - ll) <= 1e-6 * abs(ll), (f, r.rank_path_, path)
         assert r.density_.shape == counts.shape
+
+
+def test_float32_history_reaches_the_same_certified_optimum(cuda_device):
+    """The L-BFGS history in complex64 storage (fit_certified's default) changes the solver's path, not the certified
+    optimum: the same fits certified with a float64 history agree to 1e-6."""
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _fits()
+    counts, modes = [c for c, _ in fits], [m for _, m in fits]
+    r32 = BLMLBinnedBatch(tol=1e-6, device='cuda').fit_certified(counts, modes, cert_tol=1e-4, history_f32=True)
+    r64 = BLMLBinnedBatch(tol=1e-6, device='cuda').fit_certified(counts, modes, cert_tol=1e-4, history_f32=False)
+    for f in range(len(fits)):
+        assert r32[f].certificate_ <= 1 + 1e-4 and r64[f].certificate_ <= 1 + 1e-4
+        assert abs(r32[f].loglik_ - r64[f].loglik_) <= 1e-6 * abs(r64[f].loglik_), (f, r32[f].rank_path_,
+                                                                                      r64[f].rank_path_)
