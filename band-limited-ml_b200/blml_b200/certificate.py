@@ -154,7 +154,7 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     wv = torch.empty(B, dtype=torch.float64, device=dev)
     vec = torch.zeros(B, dtype=torch.float64, device=dev) if vectors else None
     R = torch.empty(B, dtype=torch.float64, device=dev)
-    steps = 0
+    steps = twice = 0
     for rnd in range(max_restarts + 1):
         alphas = np.zeros((F, nb)); betas = np.zeros((F, nb))
         conv = np.zeros(F, bool); yr = [None] * F
@@ -164,13 +164,27 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
             op(S, V[j], wv)
             steps += 1
             alpha = None
-            for ps in range(2):                                   # full reorthogonalisation, twice
+            # full reorthogonalisation against the basis; a second pass only where the first removed more than half
+            # of |w|^2 (the criterion of Daniel, Gragg, Kaufman and Stewart: then w' may have lost orthogonality)
+            w2 = proj = None
+            for ps in range(2):
+                if ps == 1 and not again:
+                    break
                 for c0 in range(0, j + 1, 47):
                     idx = list(range(c0, min(j + 1, c0 + 47)))
-                    cs = dots(S, [(V[i], wv) for i in idx])
+                    first = ps == 0 and c0 == 0
+                    got = dots(S, [(V[i], wv) for i in idx] + ([(wv, wv)] if first else []))
+                    cs = got[:, :len(idx)]
+                    if first:
+                        w2, proj = got[:, len(idx)], np.zeros(F)
+                    if ps == 0:
+                        proj += (cs * cs).sum(1)
                     if ps == 0 and c0 <= j < c0 + 47:
                         alpha = cs[:, j - c0].copy()
                     lin(S, wv, np.concatenate([np.ones((F, 1)), -cs], 1), [wv] + [V[i] for i in idx])
+                if ps == 0:
+                    again = bool(np.any((w2 - proj < 0.5 * w2)[S.idx]))
+                    twice += again
             alphas[:, j] = alpha
             beta = np.sqrt(np.maximum(dots(S, [(wv, wv)])[:, 0], 0.0))
             open_ = np.zeros(F, bool); open_[S.idx] = True
@@ -230,6 +244,7 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     if vectors:
         nv = dots(every, [(vec, vec)])[:, 0]
         lin(every, vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
-    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()), wait_s=round(clock['wait_s'], 4),
+    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()), second_passes=int(twice),
+                                wait_s=round(clock['wait_s'], 4),
                                 host_s=round(clock['host_s'], 4))
     return theta, dh, vec
