@@ -76,7 +76,8 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     """The certificate of every fit of a fitted BLMLBinnedBatch at once: lambda_max(D^1/2 S D^1/2) per fit
     (blml_binned.py:501-518), D = sum_k |e_k|^2 / w on occupied bins, by float64 Lanczos with full
     reorthogonalisation, all fits in lockstep: one grouped mat-vec, segmented inner products and linear combinations
-    per step, each fit's tridiagonal problem on the host (every third step), restarts from the Ritz vector until
+    per step with their coefficients formed on the device (no host round trip inside a step), each fit's tridiagonal
+    problem on the host (every third step, when alpha and beta are read back), restarts from the Ritz vector until
     every fit's Ritz residual |beta_j y_j| <= tol |theta|, or its Ritz value moved by less than 1e-8 relative between
     two checks (at a certified optimum the top eigenvalue is K-fold, so the residual of its Ritz vector converges far
     more slowly than the value; 1e-8 is far below any certification bar). above: per-fit thresholds; a Ritz value is
@@ -154,43 +155,54 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     wv = torch.empty(B, dtype=torch.float64, device=dev)
     vec = torch.zeros(B, dtype=torch.float64, device=dev) if vectors else None
     R = torch.empty(B, dtype=torch.float64, device=dev)
-    steps = twice = 0
+    # the steps themselves make no host round trip: the reorthogonalisation's coefficients and alpha / beta come from
+    # the inner products on the device (blml_lanczos_coef / _beta); the host reads alpha and beta at the checks
+    coef_d = torch.empty(F * 48 + 64, dtype=torch.float64, device=dev)
+    bcoef_d = torch.empty(F + 64, dtype=torch.float64, device=dev)
+    alpha_d = torch.zeros((nb, F), dtype=torch.float64, device=dev)
+    beta_d = torch.zeros((nb, F), dtype=torch.float64, device=dev)
+
+    def dots_dev(S, pairs):                          # inner products into batch.out (rows of S), no read
+        call('blml_seg_dots', code, len(S.idx), S.segs_t.data_ptr(), 0, len(pairs), ptrs([p[0] for p in pairs]),
+             ptrs([p[1] for p in pairs]), batch.part.data_ptr(), batch.out.data_ptr(), st)
+
+    def lin_dev(S, out, cptr, vecs):
+        call('blml_seg_lincomb', code, len(S.idx), S.segs_t.data_ptr(), 0, out.data_ptr(), len(vecs), cptr,
+             ptrs(vecs), st)
+
+    steps = 0
     for rnd in range(max_restarts + 1):
         alphas = np.zeros((F, nb)); betas = np.zeros((F, nb))
         conv = np.zeros(F, bool); yr = [None] * F
         S = every if not done.any() else Subset(np.where(~done)[0])
         j_end = nb
+        fetched = 0                                   # steps whose alpha / beta the host holds
         for j in range(nb):
             op(S, V[j], wv)
             steps += 1
-            alpha = None
-            # full reorthogonalisation against the basis; a second pass only where the first removed more than half
-            # of |w|^2 (the criterion of Daniel, Gragg, Kaufman and Stewart: then w' may have lost orthogonality)
-            w2 = proj = None
-            for ps in range(2):
-                if ps == 1 and not again:
-                    break
+            n = len(S.idx)
+            for ps in range(2):                       # full reorthogonalisation against the basis, twice
                 for c0 in range(0, j + 1, 47):
                     idx = list(range(c0, min(j + 1, c0 + 47)))
-                    first = ps == 0 and c0 == 0
-                    got = dots(S, [(V[i], wv) for i in idx] + ([(wv, wv)] if first else []))
-                    cs = got[:, :len(idx)]
-                    if first:
-                        w2, proj = got[:, len(idx)], np.zeros(F)
-                    if ps == 0:
-                        proj += (cs * cs).sum(1)
-                    if ps == 0 and c0 <= j < c0 + 47:
-                        alpha = cs[:, j - c0].copy()
-                    lin(S, wv, np.concatenate([np.ones((F, 1)), -cs], 1), [wv] + [V[i] for i in idx])
-                if ps == 0:
-                    again = bool(np.any((w2 - proj < 0.5 * w2)[S.idx]))
-                    twice += again
-            alphas[:, j] = alpha
-            beta = np.sqrt(np.maximum(dots(S, [(wv, wv)])[:, 0], 0.0))
+                    dots_dev(S, [(V[i], wv) for i in idx])
+                    acol = j - c0 if (ps == 0 and c0 <= j < c0 + 47) else -1
+                    call('blml_lanczos_coef', n, len(idx), batch.out.data_ptr(), coef_d.data_ptr(),
+                         alpha_d[j].data_ptr() if acol >= 0 else None, acol, st)
+                    lin_dev(S, wv, coef_d.data_ptr(), [wv] + [V[i] for i in idx])
+            dots_dev(S, [(wv, wv)])
+            call('blml_lanczos_beta', n, batch.out.data_ptr(), beta_d[j].data_ptr(), bcoef_d.data_ptr(), st)
             open_ = np.zeros(F, bool); open_[S.idx] = True
             open_ &= ~(done | conv)
-            check = j == nb - 1 or (j >= 5 and j % 3 == 2) or bool(np.any(beta[open_] <= 1e-300))
+            check = j == nb - 1 or (j >= 5 and j % 3 == 2)
             if check:
+                t0 = time.perf_counter()
+                a_h = alpha_d[fetched:j + 1, :n].cpu().numpy()
+                b_h = beta_d[fetched:j + 1, :n].cpu().numpy()
+                clock['wait_s'] += time.perf_counter() - t0
+                alphas[S.idx, fetched:j + 1] = a_h.T
+                betas[S.idx, fetched:j + 1] = b_h.T
+                fetched = j + 1
+                beta = betas[:, j]
                 t0 = time.perf_counter()
                 of = np.where(open_)[0]
                 # every open fit's tridiagonal problem at once: the largest eigenpair of T_f (j + 1 square)
@@ -211,8 +223,7 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                 if np.all(done | conv):
                     j_end = j + 1
                     break
-            betas[:, j] = beta
-            lin(S, V[j + 1], np.where(beta > 0, 1.0 / np.maximum(beta, 1e-300), 0.0)[:, None], [wv])
+            lin_dev(S, V[j + 1], bcoef_d.data_ptr(), [wv])
             still = np.where(~(done | conv))[0]
             if check and j + 1 < nb and len(still) <= 0.75 * len(S.idx):
                 # the steps go on over the open fits only; the converged ones keep V[0..j], all their Ritz vectors use
@@ -244,7 +255,6 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     if vectors:
         nv = dots(every, [(vec, vec)])[:, 0]
         lin(every, vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
-    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()), second_passes=int(twice),
-                                wait_s=round(clock['wait_s'], 4),
+    batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()), wait_s=round(clock['wait_s'], 4),
                                 host_s=round(clock['host_s'], 4))
     return theta, dh, vec

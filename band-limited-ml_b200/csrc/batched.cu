@@ -620,6 +620,26 @@ static void seg_dots_launch(dim3 g, const blml_seg* s, int cplx, int np, const S
   else k_seg_dots<T, 48><<<g, 256, 0, st>>>(s, cplx, np, pp, part);
 }
 
+// Lanczos steps of the batched certificate without a host round trip: the reorthogonalisation w -= V c takes its
+// coefficients [1, -c] straight from the inner products on the device (and keeps alpha, the one against the newest
+// basis vector); the next basis vector is w / beta with beta = |w|, 0 when w vanishes. d holds n rows of np values.
+__global__ void k_lz_coef(int n, int np, const double* __restrict__ d, double* __restrict__ coef,
+                          double* __restrict__ alpha, int acol) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    coef[(int64_t)r * (np + 1)] = 1.0;
+    for (int q = 0; q < np; q++) coef[(int64_t)r * (np + 1) + 1 + q] = -d[(int64_t)r * np + q];
+    if (alpha && acol >= 0) alpha[r] = d[(int64_t)r * np + acol];
+  }
+}
+
+__global__ void k_lz_beta(int n, const double* __restrict__ d, double* __restrict__ beta, double* __restrict__ coef) {
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const double b = sqrt(fmax(d[r], 0.0));
+    beta[r] = b;
+    coef[r] = b > 0.0 ? 1.0 / b : 0.0;
+  }
+}
+
 }  // namespace blml
 
 using namespace blml;
@@ -893,4 +913,20 @@ int blml_seg_append_mode(int dtype, int F, const blml_seg* old_segs, const blml_
   return BLML_OK;
 }
 
+int blml_lanczos_coef(int n, int np, const double* dots, double* coef, double* alpha, int alpha_col, void* stream) {
+  if (n < 1 || np < 1 || np > 47 || !dots || !coef || alpha_col >= np) {
+    set_error("blml_lanczos_coef: n >= 1 rows of 1..47 inner products"); return BLML_ERR_ARG;
+  }
+  k_lz_coef<<<(n + 127) / 128, 128, 0, SST>>>(n, np, dots, coef, alpha, alpha_col);
+  BLML_CHECK_LAUNCH("blml_lanczos_coef");
+  return BLML_OK;
 }
+
+int blml_lanczos_beta(int n, const double* dots, double* beta, double* coef, void* stream) {
+  if (n < 1 || !dots || !beta || !coef) { set_error("blml_lanczos_beta: bad arguments"); return BLML_ERR_ARG; }
+  k_lz_beta<<<(n + 127) / 128, 128, 0, SST>>>(n, dots, beta, coef);
+  BLML_CHECK_LAUNCH("blml_lanczos_beta");
+  return BLML_OK;
+}
+
+}  // extern "C"

@@ -282,6 +282,12 @@ int blml_seg_cert_weights(int dtype, int F, const blml_seg* segs, const void* E,
  * (v: float64 per bin, boff layout; scale: F device doubles). No single reference function does this step. */
 int blml_seg_append_mode(int dtype, int F, const blml_seg* old_segs, const blml_seg* new_segs, const void* E,
                          const double* dh, const double* v, const double* scale, void* E_new, void* stream);
+/* Lanczos steps of the batched certificate (blml_binned.py:501-518, ARPACK there) with no host round trip: from n
+   rows of np <= 47 inner products (the layout blml_seg_dots writes), coef rows [1, -c] for w -= V c, and alpha[r]
+   = c[r][alpha_col] when alpha is given (alpha_col < 0: none); and beta[r] = sqrt(max(d[r], 0)) with coef[r] =
+   1 / beta (0 when beta is 0) for the next basis vector. */
+int blml_lanczos_coef(int n, int np, const double* dots, double* coef, double* alpha, int alpha_col, void* stream);
+int blml_lanczos_beta(int n, const double* dots, double* beta, double* coef, void* stream);
 
 /* ---- batched solver phases with device-side control: the per-fit decisions of every
  *      iteration run as kernels, a ring of iterations is one CUDA graph replayed until every fit has stopped, the
