@@ -682,7 +682,7 @@ class BLMLBinnedBatch:
         return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
 
     def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300,
-                      grow_margin=1.0, history_f32=True):
+                      grow_margin=1.0, history_f32=True, ll_tol=None):
         """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
         batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
         mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
@@ -694,14 +694,20 @@ class BLMLBinnedBatch:
         (the reference computes the certificate, blml_binned.py:501-518; the rank growth is this engine's). Results
         carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...].
         history_f32: the L-BFGS history of every round in complex64 storage (the iterate, gradient and line search
-        stay float64): the certified optimum does not depend on the path the solver takes to it."""
+        stay float64): the certified optimum does not depend on the path the solver takes to it. ll_tol: the rounds'
+        L-BFGS stop on the gain of L / n over 10 iterations (None: the batch's own, 1e-11 by default)."""
         F = len(counts_list)
         first_caps = np.full(F, grow_iters if max_rank > 1 else -1, np.int64)
         self._history_f32 = bool(history_f32)
+        own_ll_tol = self.ll_tol
+        if ll_tol is not None:
+            self.ll_tol = ll_tol
         try:
             self.fit(counts_list, modes_list, init=init, caps=first_caps)
         finally:
             self._history_f32 = False
+            self.ll_tol = own_ll_tol
+        round_ll_tol = own_ll_tol if ll_tol is None else ll_tol
         final = [None] * F
         paths = [[] for _ in range(F)]
         cur, idx, capped = self, np.arange(F), first_caps >= 0
@@ -737,7 +743,7 @@ class BLMLBinnedBatch:
             grown = dict(zip(grow, cur._grown_starts(grow, dh, v, step))) if grow else {}
             starts = [grown[j] if j in grown else cur.e_hat(j) for j, _, _ in nxt_fits]
             nxt = BLMLBinnedBatch(tol=self.tol, max_sweeps=self.max_sweeps, anderson=self.anderson, dtype=self.dtype,
-                                  phase_noise=self.phase_noise, seed=self.seed, stall=self.stall, ll_tol=self.ll_tol,
+                                  phase_noise=self.phase_noise, seed=self.seed, stall=self.stall, ll_tol=round_ll_tol,
                                   ll_window=self.ll_window, lbfgs_m=self.lbfgs_m, device=self.device,
                                   verbose=self.verbose, control=self.control)
             mds = [[modes_list[i][0]] * K1 for _, i, K1 in nxt_fits]

@@ -48,6 +48,7 @@ REF_SAMPLE = 8                       # fits of the sweep in the reference arm's 
 LBFGS_M = 20                         # L-BFGS memory of the certified rounds (the certified optimum does not depend on it)
 HISTORY_F32 = True                   # their L-BFGS history in complex64 storage (likewise path only)
 PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certifies
+ROUND_LL_TOL = None                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (None: 1e-11)
 
 
 def workload(seed=0):
@@ -284,7 +285,8 @@ def certified_sweep(dev, train, val, modes, init=None):
     """One step: the sweep's certified fits (rank growth) and their held-out scores."""
     from blml_b200.sweep import BLMLBinnedBatch, certified_log_density
     b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev, lbfgs_m=LBFGS_M)
-    res = b.fit_certified(train, modes, cert_tol=CERT_TOL, max_rank=MAX_RANK, init=init, history_f32=HISTORY_F32)
+    res = b.fit_certified(train, modes, cert_tol=CERT_TOL, max_rank=MAX_RANK, init=init, history_f32=HISTORY_F32,
+                          ll_tol=ROUND_LL_TOL)
     return b, res, certified_log_density(res, val)
 
 
@@ -691,7 +693,7 @@ def flush_l2(buf):
 
 
 def main():
-    global LBFGS_M, MAX_RANK, HISTORY_F32
+    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=3)
@@ -718,11 +720,14 @@ def main():
     ap.add_argument('--lbfgs-m', type=int, default=20, help='L-BFGS memory of the certified rounds (1..20)')
     ap.add_argument('--max-rank', type=int, default=MAX_RANK, help='most shared modes a certified fit grows to')
     ap.add_argument('--history-f64', action='store_true', help='certified rounds keep a complex128 L-BFGS history')
+    ap.add_argument('--round-ll-tol', type=float, default=None,
+                    help="the certified rounds' L-BFGS stop on L / n gained over 10 iterations (default 1e-11)")
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")
     args = ap.parse_args()
     LBFGS_M, MAX_RANK, HISTORY_F32 = args.lbfgs_m, args.max_rank, not args.history_f64
+    ROUND_LL_TOL = args.round_ll_tol
     rank, ws, local = dist_init()
     if args.impl == 'reference':
         return reference_arm(args, rank, ws)
