@@ -11,8 +11,9 @@ certified fit of the same counts (oracle/sweep64_certified.json): the convex lif
 unique. Where the oracle's rank growth stops at 8 modes with its certificate above 1 + 1e-4, its loglik is only a lower
 bound of the optimum, and the fit may not fall more than 1e-6 below it. value = certified fits/s with the counts in device memory; e2e = the same through the public API from host
 counts (host->device copy of the counts, device->host read of every density and score inside each timed step).
-plain_gpu = the same certification with one fit at a time (no batching, cold starts); learned = the learned warm
-start's rank-1 starts, then the same certification.
+plain_gpu = the same certification with one fit at a time (no batching, cold starts, every 4th fit); learned = the
+learned warm start's rank-1 starts, then the same certification; same_sample_gpu = the reference arm's 8-fit sample
+certified here in one batch (the same work as the reference arm's step).
 
 Multi-GPU: the fits are independent (no exchange step): N ranks run N replicas of the sweep; value is all ranks'
 certified fits over the slowest rank's time.
