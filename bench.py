@@ -41,7 +41,8 @@ CONFIG = {'workload': '64-fit batched 2-D complex pball cut-off sweep: sides {64
                       'certified by rank growth',
           'fits': N_FITS, 'solver': 'lbfgs', 'state': 'float64',
           'certification': 'certificate lambda_max(D^1/2 S D^1/2)/n by batched float64 Lanczos; while > 1 + 1e-3 one '
-                           'more shared mode along its top eigenvector and a refit, at most 8 modes',
+                           'more shared mode along its top eigenvector and a refit, at most 8 modes; the rounds\' '
+                           'L-BFGS stops when L / n gains < 1e-9 over 10 iterations',
           'engine': 'batched lockstep, device-side control in CUDA-graph rings, grouped FFT mat-vecs; the certified '
                     'rounds keep their L-BFGS history (step and gradient-difference vectors) in complex64 storage',
           'l2': 'flushed between steps (256 MiB write)'}
@@ -49,7 +50,7 @@ REF_SAMPLE = 8                       # fits of the sweep in the reference arm's 
 LBFGS_M = 20                         # L-BFGS memory of the certified rounds (the certified optimum does not depend on it)
 HISTORY_F32 = True                   # their L-BFGS history in complex64 storage (likewise path only)
 PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certifies
-ROUND_LL_TOL = None                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (None: 1e-11)
+ROUND_LL_TOL = 1e-9                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (plain fits: 1e-11)
 
 
 def workload(seed=0):
@@ -215,7 +216,8 @@ def _port_certified_fit(i):
     sys.path.insert(0, os.path.join(ROOT, 'oracle'))
     import blml_oracle as bo
     sweep, modes = workload(0)
-    _, path = bo.certified_fit(sweep[i]['train'], modes[i][0], tol=TOL, cert_tol=CERT_TOL, max_rank=MAX_RANK)
+    _, path = bo.certified_fit(sweep[i]['train'], modes[i][0], tol=TOL, cert_tol=CERT_TOL, max_rank=MAX_RANK,
+                               ll_tol=ROUND_LL_TOL)
     return path[-1][1], path[-1][2]
 
 
@@ -721,8 +723,8 @@ def main():
     ap.add_argument('--lbfgs-m', type=int, default=20, help='L-BFGS memory of the certified rounds (1..20)')
     ap.add_argument('--max-rank', type=int, default=MAX_RANK, help='most shared modes a certified fit grows to')
     ap.add_argument('--history-f64', action='store_true', help='certified rounds keep a complex128 L-BFGS history')
-    ap.add_argument('--round-ll-tol', type=float, default=None,
-                    help="the certified rounds' L-BFGS stop on L / n gained over 10 iterations (default 1e-11)")
+    ap.add_argument('--round-ll-tol', type=float, default=ROUND_LL_TOL,
+                    help="the certified rounds' L-BFGS stop on L / n gained over 10 iterations")
     ap.add_argument('--matvec', action='store_true',
                     help="only the grouped mat-vec chain over the sweep's 64 lattices, 3 warm-up + 20 timed chains "
                          "(profiling runs)")

@@ -605,16 +605,18 @@ class _Start:
         self.e_hat, self.shape = e_hat, shape
 
 
-def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-3, max_rank=8, grow_iters=300, step=0.1, grow_margin=1.0):
+def certified_fit(counts, spec, tol=1e-6, cert_tol=1e-3, max_rank=8, grow_iters=300, step=0.1, grow_margin=1.0,
+                  ll_tol=None):
     """A certified fit of one shared kernel: the complex L-BFGS fit at rank K = 1, 2, ... until the certificate
     lambda_max(D^1/2 S D^1/2) / n <= 1 + cert_tol (blml_binned.py:501-518), each rank started from the previous fit's
     modes plus a new mode step * (rms mode norm) along d = D^1/2 v, v the certificate's top eigenvector (an ascent
     direction of the convex lift while the certificate exceeds 1). Ranks below max_rank run at most grow_iters
     L-BFGS iterations (at too low a rank the solver crawls); a capped fit within grow_margin cert_tol of the bar, and
     the fit at max_rank, run on to tol at their rank before anything else. The lift is convex, so the certified loglik is that of its unique optimum, whatever the
-    path. Returns (fit, [(K, loglik, certificate, iterations, capped), ...])."""
+    path. ll_tol: the L-BFGS stop on L / n gained over 10 iterations (None: 1e-11). Returns (fit, [(K, loglik,
+    certificate, iterations, capped), ...])."""
     def run(K, cap, init=None):
-        f = BinnedFit(tol=tol, solver='lbfgs')
+        f = BinnedFit(tol=tol, solver='lbfgs', ll_tol=ll_tol)
         f.lbfgs_cap = cap
         return f.fit(counts, [spec] * K, complex_g=True, init=init)
 
