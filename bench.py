@@ -51,6 +51,7 @@ LBFGS_M = 20                         # L-BFGS memory of the certified rounds (th
 HISTORY_F32 = True                   # their L-BFGS history in complex64 storage (likewise path only)
 PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certifies
 ROUND_LL_TOL = 1e-9                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (plain fits: 1e-11)
+GROW_ITERS, GROW_STEP = 300, 0.1     # L-BFGS cap of the rounds below the last rank; size of a new mode (x rms mode)
 
 
 def workload(seed=0):
@@ -217,7 +218,7 @@ def _port_certified_fit(i):
     import blml_oracle as bo
     sweep, modes = workload(0)
     _, path = bo.certified_fit(sweep[i]['train'], modes[i][0], tol=TOL, cert_tol=CERT_TOL, max_rank=MAX_RANK,
-                               ll_tol=ROUND_LL_TOL)
+                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP)
     return path[-1][1], path[-1][2]
 
 
@@ -289,7 +290,7 @@ def certified_sweep(dev, train, val, modes, init=None):
     from blml_b200.sweep import BLMLBinnedBatch, certified_log_density
     b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev, lbfgs_m=LBFGS_M)
     res = b.fit_certified(train, modes, cert_tol=CERT_TOL, max_rank=MAX_RANK, init=init, history_f32=HISTORY_F32,
-                          ll_tol=ROUND_LL_TOL)
+                          ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP)
     return b, res, certified_log_density(res, val)
 
 
@@ -696,7 +697,7 @@ def flush_l2(buf):
 
 
 def main():
-    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL
+    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL, GROW_ITERS, GROW_STEP
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=3)
@@ -723,6 +724,8 @@ def main():
     ap.add_argument('--lbfgs-m', type=int, default=20, help='L-BFGS memory of the certified rounds (1..20)')
     ap.add_argument('--max-rank', type=int, default=MAX_RANK, help='most shared modes a certified fit grows to')
     ap.add_argument('--history-f64', action='store_true', help='certified rounds keep a complex128 L-BFGS history')
+    ap.add_argument('--grow-iters', type=int, default=GROW_ITERS, help='L-BFGS cap of the rounds below the last rank')
+    ap.add_argument('--grow-step', type=float, default=GROW_STEP, help='size of a new mode (x the rms mode)')
     ap.add_argument('--round-ll-tol', type=float, default=ROUND_LL_TOL,
                     help="the certified rounds' L-BFGS stop on L / n gained over 10 iterations")
     ap.add_argument('--matvec', action='store_true',
@@ -730,7 +733,7 @@ def main():
                          "(profiling runs)")
     args = ap.parse_args()
     LBFGS_M, MAX_RANK, HISTORY_F32 = args.lbfgs_m, args.max_rank, not args.history_f64
-    ROUND_LL_TOL = args.round_ll_tol
+    ROUND_LL_TOL, GROW_ITERS, GROW_STEP = args.round_ll_tol, args.grow_iters, args.grow_step
     rank, ws, local = dist_init()
     if args.impl == 'reference':
         return reference_arm(args, rank, ws)
