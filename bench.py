@@ -42,7 +42,8 @@ CONFIG = {'workload': '64-fit batched 2-D complex pball cut-off sweep: sides {64
           'fits': N_FITS, 'solver': 'lbfgs', 'state': 'float64',
           'certification': 'certificate lambda_max(D^1/2 S D^1/2)/n by batched float64 Lanczos; while > 1 + 1e-3 one '
                            'more shared mode along its top eigenvector and a refit, at most 8 modes; the rounds\' '
-                           'L-BFGS stops when L / n gains < 1e-9 over 10 iterations',
+                           'L-BFGS stops when L / n gains < 1e-9 over 10 iterations; rounds below the last rank '
+                           'capped at 150 iterations',
           'engine': 'batched lockstep, device-side control in CUDA-graph rings, grouped FFT mat-vecs; the certified '
                     'rounds keep their L-BFGS history (step and gradient-difference vectors) in complex64 storage',
           'l2': 'flushed between steps (256 MiB write)'}
@@ -51,7 +52,7 @@ LBFGS_M = 20                         # L-BFGS memory of the certified rounds (th
 HISTORY_F32 = True                   # their L-BFGS history in complex64 storage (likewise path only)
 PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certifies
 ROUND_LL_TOL = 1e-9                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (plain fits: 1e-11)
-GROW_ITERS, GROW_STEP = 300, 0.1     # L-BFGS cap of the rounds below the last rank; size of a new mode (x rms mode)
+GROW_ITERS, GROW_STEP = 150, 0.1     # L-BFGS cap of the rounds below the last rank; size of a new mode (x rms mode)
 
 
 def workload(seed=0):
