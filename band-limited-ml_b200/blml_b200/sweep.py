@@ -643,15 +643,17 @@ class BLMLBinnedBatch:
         return self.dens_t[a:b].cpu().numpy().reshape(self.shapes[f])
 
     # ---------------------------------------------------------------- certificate and certified fits
-    def certificate(self, tol=1e-6, vectors=False, decide_above=None):
+    def certificate(self, tol=1e-6, vectors=False, decide_above=None, max_basis=64):
         """lambda_max(D^1/2 S D^1/2) / n of every fit (blml_binned.py:501-518; D = sum_k |e_k|^2 / w on occupied
         bins), by float64 Lanczos over all fits at once. <= 1 (up to the solver's tolerance) when the fit is the
         optimum of the convex lift. With vectors: (certificates, dh, v), v the top eigenvectors (per bin).
         decide_above: a level (e.g. 1 + cert_tol) past which a fit's value need not be refined -- the Lanczos value is
-        a lower bound, so the returned value is then a lower bound above that level."""
+        a lower bound, so the returned value is then a lower bound above that level. max_basis: the Lanczos basis
+        before a restart."""
         from .certificate import lanczos_max_batched
         above = None if decide_above is None else decide_above * self.n
-        theta, dh, v = lanczos_max_batched(self, tol=tol, seed=self.seed, vectors=vectors, above=above)
+        theta, dh, v = lanczos_max_batched(self, tol=tol, seed=self.seed, vectors=vectors, above=above,
+                                           max_basis=max_basis)
         cert = theta / self.n
         return (cert, dh, v) if vectors else cert
 
@@ -682,7 +684,7 @@ class BLMLBinnedBatch:
         return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
 
     def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300,
-                      grow_margin=1.0, history_f32=True, ll_tol=None):
+                      grow_margin=1.0, history_f32=True, ll_tol=None, lanczos_basis=64):
         """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
         batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
         mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
@@ -695,7 +697,8 @@ class BLMLBinnedBatch:
         carry rank_, certificate_ and rank_path_ [(K, loglik, certificate, iterations, capped), ...].
         history_f32: the L-BFGS history of every round in complex64 storage (the iterate, gradient and line search
         stay float64): the certified optimum does not depend on the path the solver takes to it. ll_tol: the rounds'
-        L-BFGS stop on the gain of L / n over 10 iterations (None: the batch's own, 1e-11 by default)."""
+        L-BFGS stop on the gain of L / n over 10 iterations (None: the batch's own, 1e-11 by default). lanczos_basis:
+        the certificate's Lanczos basis before a restart."""
         F = len(counts_list)
         first_caps = np.full(F, grow_iters if max_rank > 1 else -1, np.int64)
         self._history_f32 = bool(history_f32)
@@ -715,7 +718,7 @@ class BLMLBinnedBatch:
         while True:
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record()
-            cert, dh, v = cur.certificate(vectors=True, decide_above=1.0 + cert_tol)
+            cert, dh, v = cur.certificate(vectors=True, decide_above=1.0 + cert_tol, max_basis=lanczos_basis)
             ev[1].record(); ev[1].synchronize()
             st = self.certify_stats_
             st['seconds_certificate'] += ev[0].elapsed_time(ev[1]) / 1e3

@@ -53,6 +53,7 @@ HISTORY_F32 = True                   # their L-BFGS history in complex64 storage
 PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certifies
 ROUND_LL_TOL = 1e-9                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (plain fits: 1e-11)
 GROW_ITERS, GROW_STEP = 150, 0.1     # L-BFGS cap of the rounds below the last rank; size of a new mode (x rms mode)
+LANCZOS_BASIS = 64                   # the certificate's Lanczos basis before a restart
 
 
 def workload(seed=0):
@@ -219,7 +220,7 @@ def _port_certified_fit(i):
     import blml_oracle as bo
     sweep, modes = workload(0)
     _, path = bo.certified_fit(sweep[i]['train'], modes[i][0], tol=TOL, cert_tol=CERT_TOL, max_rank=MAX_RANK,
-                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP)
+                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS)
     return path[-1][1], path[-1][2]
 
 
@@ -291,7 +292,7 @@ def certified_sweep(dev, train, val, modes, init=None):
     from blml_b200.sweep import BLMLBinnedBatch, certified_log_density
     b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev, lbfgs_m=LBFGS_M)
     res = b.fit_certified(train, modes, cert_tol=CERT_TOL, max_rank=MAX_RANK, init=init, history_f32=HISTORY_F32,
-                          ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP)
+                          ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS)
     return b, res, certified_log_density(res, val)
 
 
@@ -698,7 +699,7 @@ def flush_l2(buf):
 
 
 def main():
-    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL, GROW_ITERS, GROW_STEP
+    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL, GROW_ITERS, GROW_STEP, LANCZOS_BASIS
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=3)
@@ -727,6 +728,7 @@ def main():
     ap.add_argument('--history-f64', action='store_true', help='certified rounds keep a complex128 L-BFGS history')
     ap.add_argument('--grow-iters', type=int, default=GROW_ITERS, help='L-BFGS cap of the rounds below the last rank')
     ap.add_argument('--grow-step', type=float, default=GROW_STEP, help='size of a new mode (x the rms mode)')
+    ap.add_argument('--lanczos-basis', type=int, default=LANCZOS_BASIS, help="the certificate's Lanczos basis")
     ap.add_argument('--round-ll-tol', type=float, default=ROUND_LL_TOL,
                     help="the certified rounds' L-BFGS stop on L / n gained over 10 iterations")
     ap.add_argument('--matvec', action='store_true',
@@ -735,6 +737,7 @@ def main():
     args = ap.parse_args()
     LBFGS_M, MAX_RANK, HISTORY_F32 = args.lbfgs_m, args.max_rank, not args.history_f64
     ROUND_LL_TOL, GROW_ITERS, GROW_STEP = args.round_ll_tol, args.grow_iters, args.grow_step
+    LANCZOS_BASIS = args.lanczos_basis
     rank, ws, local = dist_init()
     if args.impl == 'reference':
         return reference_arm(args, rank, ws)
