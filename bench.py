@@ -53,7 +53,7 @@ HISTORY_F32 = True                   # their L-BFGS history in complex64 storage
 PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certifies
 ROUND_LL_TOL = 1e-9                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (plain fits: 1e-11)
 GROW_ITERS, GROW_STEP = 150, 0.1     # L-BFGS cap of the rounds below the last rank; size of a new mode (x rms mode)
-LANCZOS_BASIS = 64                   # the certificate's Lanczos basis before a restart
+LANCZOS_BASIS = 32                   # the certificate's Lanczos basis before a restart
 
 
 def workload(seed=0):
