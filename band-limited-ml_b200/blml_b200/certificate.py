@@ -72,7 +72,8 @@ def lanczos_max(plan, dh, red, stream, tol=1e-6, seed=0, max_basis=96, max_resta
     return theta
 
 
-def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, vectors=False, above=None):
+def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, vectors=False, above=None,
+                        second=False):
     """The certificate of every fit of a fitted BLMLBinnedBatch at once: lambda_max(D^1/2 S D^1/2) per fit
     (blml_binned.py:501-518), D = sum_k |e_k|^2 / w on occupied bins, by float64 Lanczos with full
     reorthogonalisation, all fits in lockstep: one grouped mat-vec, segmented inner products and linear combinations
@@ -86,7 +87,8 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     still open only: when they fall to 3/4 of the fits the steps cover, the segment list and the grouped mat-vec are
     rebuilt over them (a fit's arithmetic does not depend on which other fits share the launch). Returns (theta (F,),
     dh, v): dh the per-bin scaling and v the top Ritz vectors (float64 per bin over all fits, None unless vectors)
-    -- d = dh v is the direction of a new mode."""
+    -- d = dh v is the direction of a new mode. second (with vectors): v is a pair (top, next) -- the Ritz vector of
+    each fit's second Ritz value from the same Krylov basis, a second ascent direction while that value is above n."""
     from .sweep import _Group, _Seg
     clock = {'wait_s': 0.0, 'host_s': 0.0}
     F, dev, st, B = batch.F, batch.device, batch.st, batch.Btot
@@ -150,10 +152,12 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     V[0].copy_(torch.as_tensor(np.random.default_rng(seed).standard_normal(B)))
     nrm = dots(every, [(V[0], V[0])])[:, 0]
     lin(every, V[0], (1.0 / np.sqrt(np.maximum(nrm, 1e-300)))[:, None], [V[0]])
-    theta = np.zeros(F); done = np.zeros(F, bool); prev = np.full(F, np.nan)
+    theta = np.zeros(F); done = np.zeros(F, bool); prev = np.full(F, np.nan); theta2 = np.full(F, np.nan)
     above = np.full(F, np.inf) if above is None else np.asarray(above, float)
     wv = torch.empty(B, dtype=torch.float64, device=dev)
     vec = torch.zeros(B, dtype=torch.float64, device=dev) if vectors else None
+    vec2 = torch.zeros(B, dtype=torch.float64, device=dev) if (vectors and second) else None
+    R2 = torch.empty(B, dtype=torch.float64, device=dev) if vec2 is not None else None
     R = torch.empty(B, dtype=torch.float64, device=dev)
     # the steps themselves make no host round trip: the reorthogonalisation's coefficients and alpha / beta come from
     # the inner products on the device (blml_lanczos_coef / _beta); the host reads alpha and beta at the checks
@@ -173,7 +177,7 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     steps = 0
     for rnd in range(max_restarts + 1):
         alphas = np.zeros((F, nb)); betas = np.zeros((F, nb))
-        conv = np.zeros(F, bool); yr = [None] * F
+        conv = np.zeros(F, bool); yr = [None] * F; yr2 = [None] * F
         S = every if not done.any() else Subset(np.where(~done)[0])
         j_end = nb
         fetched = 0                                   # steps whose alpha / beta the host holds
@@ -215,6 +219,8 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                 for t_, f in enumerate(of):
                     th = float(ev_all[t_, -1]); y = evec_all[t_, :, -1].copy()
                     theta[f] = th; yr[f] = y
+                    if j > 0:
+                        yr2[f] = evec_all[t_, :, -2].copy(); theta2[f] = float(ev_all[t_, -2])
                     if (abs(beta[f] * y[-1]) <= tol * max(abs(th), 1e-300) or beta[f] <= 1e-14 * max(abs(th), 1e-300)
                             or th > above[f] or abs(th - prev[f]) <= 1e-8 * abs(th)):
                         conv[f] = True
@@ -243,9 +249,24 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
                     if i < len(y):
                         cf[f, 1 + t] = y[i]
             lin(SA, R, cf, [R] + [V[i] for i in idx])
+        if vec2 is not None:                                      # the second Ritz vectors the same way
+            R2.zero_()
+            for c0 in range(0, j_end, 47):
+                idx = list(range(c0, min(j_end, c0 + 47)))
+                cf = np.zeros((F, 1 + len(idx))); cf[:, 0] = 1.0
+                for f in np.where(act)[0]:
+                    y = yr2[f]
+                    if y is None:
+                        continue
+                    for t, i in enumerate(idx):
+                        if i < len(y):
+                            cf[f, 1 + t] = y[i]
+                lin(SA, R2, cf, [R2] + [V[i] for i in idx])
         if vectors:                                               # keep the vectors of the fits converging now
             keep = (act & conv).astype(float)
             lin(SA, vec, np.stack([keep, 1.0 - keep], 1), [R, vec])
+            if vec2 is not None:
+                lin(SA, vec2, np.stack([keep, 1.0 - keep], 1), [R2, vec2])
         done |= conv
         if np.all(done):
             break
@@ -255,6 +276,11 @@ def lanczos_max_batched(batch, tol=1e-6, seed=0, max_basis=64, max_restarts=12, 
     if vectors:
         nv = dots(every, [(vec, vec)])[:, 0]
         lin(every, vec, (1.0 / np.sqrt(np.maximum(nv, 1e-300)))[:, None], [vec])
+        if vec2 is not None:
+            nv2 = dots(every, [(vec2, vec2)])[:, 0]
+            lin(every, vec2, np.where(nv2 > 0, 1.0 / np.sqrt(np.maximum(nv2, 1e-300)), 0.0)[:, None], [vec2])
+            vec = (vec, vec2)
+    batch.theta2_ = theta2                                        # the second Ritz values (NaN: none)
     batch.lanczos_stats_ = dict(steps=steps, restarts=rnd, converged=int(done.sum()), wait_s=round(clock['wait_s'], 4),
                                 host_s=round(clock['host_s'], 4))
     return theta, dh, vec

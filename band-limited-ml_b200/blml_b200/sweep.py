@@ -643,48 +643,73 @@ class BLMLBinnedBatch:
         return self.dens_t[a:b].cpu().numpy().reshape(self.shapes[f])
 
     # ---------------------------------------------------------------- certificate and certified fits
-    def certificate(self, tol=1e-6, vectors=False, decide_above=None, max_basis=64):
+    def certificate(self, tol=1e-6, vectors=False, decide_above=None, max_basis=64, second=False):
         """lambda_max(D^1/2 S D^1/2) / n of every fit (blml_binned.py:501-518; D = sum_k |e_k|^2 / w on occupied
         bins), by float64 Lanczos over all fits at once. <= 1 (up to the solver's tolerance) when the fit is the
         optimum of the convex lift. With vectors: (certificates, dh, v), v the top eigenvectors (per bin).
         decide_above: a level (e.g. 1 + cert_tol) past which a fit's value need not be refined -- the Lanczos value is
         a lower bound, so the returned value is then a lower bound above that level. max_basis: the Lanczos basis
-        before a restart."""
+        before a restart. second (with vectors): v is a pair (top, second Ritz vectors), the second Ritz values in
+        theta2_ (divided by n they compare with the certificate)."""
         from .certificate import lanczos_max_batched
         above = None if decide_above is None else decide_above * self.n
         theta, dh, v = lanczos_max_batched(self, tol=tol, seed=self.seed, vectors=vectors, above=above,
-                                           max_basis=max_basis)
+                                           max_basis=max_basis, second=second)
         cert = theta / self.n
         return (cert, dh, v) if vectors else cert
 
-    def _grown_starts(self, grow, dh, v, step):
+    def _grown_starts(self, grow, dh, v, step, v2=None, two=()):
         """Starts of rank K_f + 1 for the fits `grow` (indices into this batch): the K_f modes, then
-        step * sqrt(sum |e|^2 / K_f) / |d| * d with d = dh v (device tensors, one (K_f + 1, M1, M2) start per fit)."""
+        step * sqrt(sum |e|^2 / K_f) / |d| * d with d = dh v (device tensors, one (K_f + 1, M1, M2) start per fit).
+        The fits in `two` take a second new mode the same way along d2 = dh v2 (rank K_f + 2)."""
         F, code, dev = self.F, self.code, self.device
         ee = self._dots(code, True, [(self.E_t, self.E_t)])[:, 0]
-        d = torch.empty(self.Btot, dtype=torch.float64, device=dev)
-        call('blml_mul_bins', _lib.F64, 1, self.Btot, 0, v.data_ptr(), dh.data_ptr(), d.data_ptr(), self.st)
         segs1 = (_Seg * F)(*[_Seg(int(self.boff[f]), int(self.boff[f]), int(self.B[f]), 1, 0) for f in range(F)])
         s1 = torch.frombuffer(bytearray(segs1), dtype=torch.uint8).to(dev)
-        call('blml_seg_dots', _lib.F64, F, s1.data_ptr(), 0, 1, ptrs([d]), ptrs([d]), self.part.data_ptr(),
-             self.out.data_ptr(), self.st)
-        dd = self._read(1)[:, 0]
-        scale = step * np.sqrt(ee / self.Kf) / np.sqrt(np.maximum(dd, 1e-300))
+
+        def scales(vv):                                   # step * sqrt(sum |e|^2 / K) / |dh vv| per fit
+            d = torch.empty(self.Btot, dtype=torch.float64, device=dev)
+            call('blml_mul_bins', _lib.F64, 1, self.Btot, 0, vv.data_ptr(), dh.data_ptr(), d.data_ptr(), self.st)
+            call('blml_seg_dots', _lib.F64, F, s1.data_ptr(), 0, 1, ptrs([d]), ptrs([d]), self.part.data_ptr(),
+                 self.out.data_ptr(), self.st)
+            dd = self._read(1)[:, 0]
+            return step * np.sqrt(ee / self.Kf) / np.sqrt(np.maximum(dd, 1e-300))
+
+        def append(old, add_v, sc):                       # old: [(seg into src)], returns (new segs, En)
+            G = len(old)
+            nB = np.array([o.B for o in old], np.int64); nK = np.array([o.K + 1 for o in old], np.int64)
+            noff = np.concatenate([[0], np.cumsum(nB * nK)])
+            new = [_Seg(int(noff[t]), int(old[t].boff), int(nB[t]), int(nK[t]), 0) for t in range(G)]
+            return new, noff
+
+        scale = scales(v)
         G = len(grow)
         old = [self.segs_all[j] for j in grow]
-        nB = np.array([self.B[j] for j in grow], np.int64); nK = np.array([self.Kf[j] + 1 for j in grow], np.int64)
-        noff = np.concatenate([[0], np.cumsum(nB * nK)])
-        new = [_Seg(int(noff[t]), int(old[t].boff), int(nB[t]), int(nK[t]), 0) for t in range(G)]
+        new, noff = append(old, v, scale)
         o_t = torch.frombuffer(bytearray((_Seg * G)(*old)), dtype=torch.uint8).to(dev)
         n_t = torch.frombuffer(bytearray((_Seg * G)(*new)), dtype=torch.uint8).to(dev)
         En = torch.empty(int(noff[-1]), dtype=self.ct, device=dev)
         sc = self._dev(scale[np.asarray(grow)])
         call('blml_seg_append_mode', code, G, o_t.data_ptr(), n_t.data_ptr(), self.E_t.data_ptr(), dh.data_ptr(),
              v.data_ptr(), sc.data_ptr(), En.data_ptr(), self.st)
-        return [En[noff[t]:noff[t + 1]].reshape((int(nK[t]),) + self.shapes[grow[t]]) for t in range(G)]
+        starts = [En[noff[t]:noff[t + 1]].reshape((int(new[t].K),) + self.shapes[grow[t]]) for t in range(G)]
+        sel = [t for t in range(G) if grow[t] in set(two)]
+        if v2 is not None and sel:
+            scale2 = scales(v2)
+            old2 = [new[t] for t in sel]
+            new2, noff2 = append(old2, v2, scale2)
+            o2 = torch.frombuffer(bytearray((_Seg * len(sel))(*old2)), dtype=torch.uint8).to(dev)
+            n2 = torch.frombuffer(bytearray((_Seg * len(sel))(*new2)), dtype=torch.uint8).to(dev)
+            En2 = torch.empty(int(noff2[-1]), dtype=self.ct, device=dev)
+            sc2 = self._dev(scale2[np.asarray([grow[t] for t in sel])])
+            call('blml_seg_append_mode', code, len(sel), o2.data_ptr(), n2.data_ptr(), En.data_ptr(), dh.data_ptr(),
+                 v2.data_ptr(), sc2.data_ptr(), En2.data_ptr(), self.st)
+            for u, t in enumerate(sel):
+                starts[t] = En2[noff2[u]:noff2[u + 1]].reshape((int(new2[u].K),) + self.shapes[grow[t]])
+        return starts
 
     def fit_certified(self, counts_list, modes_list, cert_tol=1e-3, max_rank=8, step=0.1, init=None, grow_iters=300,
-                      grow_margin=1.0, history_f32=True, ll_tol=None, lanczos_basis=64):
+                      grow_margin=1.0, history_f32=True, ll_tol=None, lanczos_basis=64, grow_two_above=None):
         """Certified fits: each fit's one-mode kernel at rank K = 1 (the seeded start, or init), then rounds in one
         batch each: a fit whose certificate lambda_max(D^1/2 S D^1/2) / n exceeds 1 + cert_tol gets one more shared
         mode started along the certificate's top eigenvector, and a fit that meets it after a capped round is run on
@@ -698,7 +723,8 @@ class BLMLBinnedBatch:
         history_f32: the L-BFGS history of every round in complex64 storage (the iterate, gradient and line search
         stay float64): the certified optimum does not depend on the path the solver takes to it. ll_tol: the rounds'
         L-BFGS stop on the gain of L / n over 10 iterations (None: the batch's own, 1e-11 by default). lanczos_basis:
-        the certificate's Lanczos basis before a restart."""
+        the certificate's Lanczos basis before a restart. grow_two_above: a fit whose certificate exceeds this level,
+        and whose second Ritz value is above the bar too, takes two new modes at once (the top two Ritz vectors)."""
         F = len(counts_list)
         first_caps = np.full(F, grow_iters if max_rank > 1 else -1, np.int64)
         self._history_f32 = bool(history_f32)
@@ -718,7 +744,13 @@ class BLMLBinnedBatch:
         while True:
             ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
             ev[0].record()
-            cert, dh, v = cur.certificate(vectors=True, decide_above=1.0 + cert_tol, max_basis=lanczos_basis)
+            two_ok = grow_two_above is not None
+            cert, dh, v = cur.certificate(vectors=True, decide_above=1.0 + cert_tol, max_basis=lanczos_basis,
+                                          second=two_ok)
+            v2 = None
+            if two_ok:
+                v, v2 = v
+                th2 = cur.theta2_ / cur.n
             ev[1].record(); ev[1].synchronize()
             st = self.certify_stats_
             st['seconds_certificate'] += ev[0].elapsed_time(ev[1]) / 1e3
@@ -739,11 +771,15 @@ class BLMLBinnedBatch:
                 if was_capped and (near or K >= max_rank):
                     nxt_fits.append((j, i, K)); nxt_caps.append(-1)            # run on to tol at this rank
                 elif not ok and K < max_rank:
-                    nxt_fits.append((j, i, K + 1)); nxt_caps.append(grow_iters if K + 1 < max_rank else -1)
+                    add = 2 if (two_ok and cert[j] > grow_two_above and th2[j] > 1.0 + cert_tol and
+                                K + 2 <= max_rank) else 1
+                    nxt_fits.append((j, i, K + add)); nxt_caps.append(grow_iters if K + add < max_rank else -1)
             if not nxt_fits:
                 return final
             grow = [j for j, _, K1 in nxt_fits if K1 > int(cur.Kf[j])]
-            grown = dict(zip(grow, cur._grown_starts(grow, dh, v, step))) if grow else {}
+            two = [j for j, _, K1 in nxt_fits if K1 > int(cur.Kf[j]) + 1]
+            st['two_mode_growths'] = st.get('two_mode_growths', 0) + len(two)
+            grown = dict(zip(grow, cur._grown_starts(grow, dh, v, step, v2=v2, two=two))) if grow else {}
             starts = [grown[j] if j in grown else cur.e_hat(j) for j, _, _ in nxt_fits]
             nxt = BLMLBinnedBatch(tol=self.tol, max_sweeps=self.max_sweeps, anderson=self.anderson, dtype=self.dtype,
                                   phase_noise=self.phase_noise, seed=self.seed, stall=self.stall, ll_tol=round_ll_tol,

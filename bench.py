@@ -54,6 +54,7 @@ PLAIN_SAMPLE = range(0, 64, 4)       # the fits the one-fit-at-a-time arm certif
 ROUND_LL_TOL = 1e-9                  # the certified rounds' L-BFGS stop on L / n gained over 10 iterations (plain fits: 1e-11)
 GROW_ITERS, GROW_STEP = 150, 0.1     # L-BFGS cap of the rounds below the last rank; size of a new mode (x rms mode)
 LANCZOS_BASIS = 32                   # the certificate's Lanczos basis before a restart
+GROW_TWO_ABOVE = None                # a certificate above this level (and a second Ritz value above the bar): two modes
 
 
 def workload(seed=0):
@@ -220,7 +221,8 @@ def _port_certified_fit(i):
     import blml_oracle as bo
     sweep, modes = workload(0)
     _, path = bo.certified_fit(sweep[i]['train'], modes[i][0], tol=TOL, cert_tol=CERT_TOL, max_rank=MAX_RANK,
-                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS)
+                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS,
+                          grow_two_above=GROW_TWO_ABOVE)
     return path[-1][1], path[-1][2]
 
 
@@ -292,7 +294,8 @@ def certified_sweep(dev, train, val, modes, init=None):
     from blml_b200.sweep import BLMLBinnedBatch, certified_log_density
     b = BLMLBinnedBatch(tol=TOL, dtype=np.float64, device=dev, lbfgs_m=LBFGS_M)
     res = b.fit_certified(train, modes, cert_tol=CERT_TOL, max_rank=MAX_RANK, init=init, history_f32=HISTORY_F32,
-                          ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS)
+                          ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS,
+                          grow_two_above=GROW_TWO_ABOVE)
     return b, res, certified_log_density(res, val)
 
 
@@ -699,7 +702,7 @@ def flush_l2(buf):
 
 
 def main():
-    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL, GROW_ITERS, GROW_STEP, LANCZOS_BASIS
+    global LBFGS_M, MAX_RANK, HISTORY_F32, ROUND_LL_TOL, GROW_ITERS, GROW_STEP, LANCZOS_BASIS, GROW_TWO_ABOVE
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
     ap.add_argument('--steps', type=int, default=3)
@@ -729,6 +732,8 @@ def main():
     ap.add_argument('--grow-iters', type=int, default=GROW_ITERS, help='L-BFGS cap of the rounds below the last rank')
     ap.add_argument('--grow-step', type=float, default=GROW_STEP, help='size of a new mode (x the rms mode)')
     ap.add_argument('--lanczos-basis', type=int, default=LANCZOS_BASIS, help="the certificate's Lanczos basis")
+    ap.add_argument('--grow-two-above', type=float, default=GROW_TWO_ABOVE,
+                    help='a certificate above this level grows two modes at once')
     ap.add_argument('--round-ll-tol', type=float, default=ROUND_LL_TOL,
                     help="the certified rounds' L-BFGS stop on L / n gained over 10 iterations")
     ap.add_argument('--matvec', action='store_true',
@@ -737,7 +742,7 @@ def main():
     args = ap.parse_args()
     LBFGS_M, MAX_RANK, HISTORY_F32 = args.lbfgs_m, args.max_rank, not args.history_f64
     ROUND_LL_TOL, GROW_ITERS, GROW_STEP = args.round_ll_tol, args.grow_iters, args.grow_step
-    LANCZOS_BASIS = args.lanczos_basis
+    LANCZOS_BASIS, GROW_TWO_ABOVE = args.lanczos_basis, args.grow_two_above
     rank, ws, local = dist_init()
     if args.impl == 'reference':
         return reference_arm(args, rank, ws)

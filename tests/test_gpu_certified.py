@@ -80,3 +80,18 @@ def test_float32_history_reaches_the_same_certified_optimum(cuda_device):
         assert r32[f].certificate_ <= 1 + 1e-4 and r64[f].certificate_ <= 1 + 1e-4
         assert abs(r32[f].loglik_ - r64[f].loglik_) <= 1e-6 * abs(r64[f].loglik_), (f, r32[f].rank_path_,
                                                                                       r64[f].rank_path_)
+
+
+def test_two_mode_growth_reaches_the_oracle_optimum(cuda_device):
+    """Growing two modes at once (the top two Ritz vectors) changes the path, not the certified optimum."""
+    import blml_oracle as bo
+    from blml_b200.sweep import BLMLBinnedBatch
+    fits = _fits()
+    b = BLMLBinnedBatch(tol=1e-6, device='cuda')
+    res = b.fit_certified([c for c, _ in fits], [m for _, m in fits], cert_tol=1e-4, grow_two_above=1.0)
+    assert b.certify_stats_.get('two_mode_growths', 0) > 0
+    for f, (counts, modes) in enumerate(fits):
+        r = res[f]
+        assert r.certificate_ <= 1 + 1e-4, (f, r.rank_path_)
+        _, path = bo.certified_fit(counts, modes[0], cert_tol=1e-4)
+        assert abs(r.loglik_ - path[-1][1]) <= 1e-6 * abs(path[-1][1]), (f, r.rank_path_, path)
