@@ -139,6 +139,7 @@ _SIGS = {
     'blml_fill_modes': (_I, [_I, _I, _L, _I, _I, _I, _D, _P, _P, _P]),
     'blml_cert_weights': (_I, [_I, _I, _L, _I, _P, _P, _P, _P]),
     'blml_rows': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P, _P, _P]),
+    'blml_rows_multi': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P, _P, _P]),
     'blml_cols': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _P, _I, _P]),
     'blml_cols_dep': (_I, [C.POINTER(Tables), _P, _L, _P, _L, _L, _P, _P, _I, _P]),
     'blml_lattice_coords': (_I, [_P, _L, _I, _P, _P, _P]),

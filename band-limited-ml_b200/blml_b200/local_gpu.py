@@ -8,6 +8,8 @@
 
 Tables are assembled on the host in float64 (their size is the lattice span, not the number of pairs) and copied
 to the device once per table dict; rows and cols run in libblml_b200 (csrc/pairs.cu)."""
+import ctypes as C
+
 import numpy as np
 import torch
 
@@ -240,6 +242,31 @@ def rows(ZA, ZB, w, tab, grad=False, f32=False, device=None):
         w.to(device=device, dtype=torch.float64).contiguous()
     s, ds = rows_dev(A, Bz, wt, tab, grad, f32)
     return s.cpu().numpy(), ds.cpu().numpy()
+
+
+def rows_multi(ZA, ZB, Wt, tab, umask, grad=False, f32=False, device=None):
+    """Fused rows of several densities (blml_local.py:282-286, FusedFit's joint and marginals): s (R, M) with
+    s[r, m] = sum_j S_m(ZA_r, ZB_j) Wt[j, m], S_m the product over the units with umask[m, u] = 1, the unit factors
+    computed once per pair; ds zeros (R, M, 1) -- values only (grad=True raises). NumPy results."""
+    if grad:
+        raise NotImplementedError("rows_multi: derivative rows are not available")
+    device = torch.device(device or 'cuda')
+    um = np.asarray(umask, np.int64)
+    Wn = np.ascontiguousarray(Wt, np.float64)
+    if Wn.ndim != 2 or um.ndim != 2 or um.shape[0] != Wn.shape[1]:
+        raise ValueError("rows_multi: Wt (M bins, densities) and umask (densities, units)")
+    bits = np.array([int(sum(1 << u for u in range(um.shape[1]) if um[m, u])) for m in range(um.shape[0])], np.uint32)
+    A = _coords_dev(ZA, tab, device); Bz = _coords_dev(ZB, tab, device)
+    R, Mm = A.shape[0], Wn.shape[1]
+    if Wn.shape[0] != Bz.shape[0]:
+        raise ValueError("rows_multi: one weight row per ZB bin")
+    t = dev_tab(tab, device)
+    st = _struct(tab, t, False, f32)
+    W = torch.as_tensor(Wn).to(device)
+    s = torch.empty((R, Mm), dtype=torch.float64, device=device)
+    call('blml_rows_multi', st, A.data_ptr(), R, Bz.data_ptr(), Bz.shape[0], W.data_ptr(), Mm,
+         bits.ctypes.data_as(C.c_void_p), s.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
+    return s.cpu().numpy(), np.zeros((R, Mm, 1))
 
 
 def cols(ZA_dev, ZB_dev, tab, out, out_m=None, depmask=0, f32=False):

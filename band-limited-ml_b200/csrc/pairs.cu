@@ -137,6 +137,50 @@ __global__ void __launch_bounds__(PR_THREADS) k_rows_general(ColMeta cm, const R
     for (int q = 0; q < cm.nW; q++) dpart[((int64_t)blockIdx.y * R + r) * cm.nW + q] = dacc[q];
 }
 
+// Fused rows of several densities over the same pairs (blml_local.py:213-286, rows_multi): s[r][m] = sum_j W[j][m]
+// prod_u (bit u of umask[m] ? fac_u : 1), the unit factors computed once per pair and each density multiplying the
+// units its mask keeps, in unit order (the joint: every unit; a marginal: the units of its columns). part[slice][r][m].
+constexpr int MAXM = 8;
+struct DensMasks { unsigned bits[MAXM]; };
+
+template <typename REAL>
+__global__ void __launch_bounds__(PR_THREADS) k_rows_multi(ColMeta cm, const REAL* Tg, const REAL* RTg,
+                                                           const int64_t* ZA, int64_t R, const int64_t* ZB,
+                                                           const double* W, int Mm, DensMasks dm, int64_t slice,
+                                                           int64_t M, double* part) {
+  extern __shared__ unsigned char smem_raw[];
+  REAL* Ts = reinterpret_cast<REAL*>(smem_raw);
+  REAL* RTs = Ts + cm.Tn;
+  const int64_t nRT = (int64_t)cm.G * cm.LR;
+  for (int64_t i = threadIdx.x; i < cm.Tn; i += blockDim.x) Ts[i] = Tg[i];
+  for (int64_t i = threadIdx.x; i < nRT; i += blockDim.x) RTs[i] = RTg[i];
+  __syncthreads();
+  const int64_t r = (int64_t)blockIdx.x * PR_THREADS + threadIdx.x;
+  const int64_t j0 = (int64_t)blockIdx.y * slice, j1 = min(M, j0 + slice);
+  int64_t za[MAXD];
+  const bool live = r < R;
+  for (int k = 0; k < cm.d; k++) za[k] = live ? ZA[r * cm.d + k] : 0;
+  double acc[MAXM];
+  for (int m = 0; m < MAXM; m++) acc[m] = 0.0;
+  REAL fac[MAXU + 1];
+  for (int u = 0; u < MAXU; u++) fac[u] = REAL(1);
+  int64_t r2[MAXG]; bool tor[MAXG];
+  for (int64_t j = j0; j < j1 && live; j++) {
+    int64_t zb[MAXD];
+    for (int k = 0; k < cm.d; k++) zb[k] = ZB[j * cm.d + k];
+    pair_factors<REAL>(cm, Ts, RTs, za, zb, fac, r2, tor);
+    for (int m = 0; m < Mm; m++) {
+      const double wj = W[j * Mm + m];
+      if (wj == 0.0) continue;
+      REAL p = REAL(1);
+      for (int u = 0; u < cm.U; u++) p = p * (((dm.bits[m] >> u) & 1u) ? fac[u] : REAL(1));
+      acc[m] += (double)p * wj;
+    }
+  }
+  if (!live) return;
+  for (int m = 0; m < Mm; m++) part[((int64_t)blockIdx.y * R + r) * Mm + m] = acc[m];
+}
+
 // shared-memory layout of k_rows_offset (the host sizes the launch with the same functions): the table, then the
 // chunk's column coordinates (int32, D per column), then its weights, each part 16-byte aligned
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
@@ -492,6 +536,60 @@ int blml_rows(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t
   }
   if (!tb->T || (cm.G && !tb->RT) || (grad && (!tb->dT || !tb->dR))) { set_error("blml_rows: tables missing"); return BLML_ERR_ARG; }
   return rows_impl<double>(tb, cm, tb->T, tb->RT, tb->dT, tb->dR, ZA, R, ZB, M, w, grad, s, ds, st);
+}
+
+}  // extern "C"
+
+template <typename REAL>
+static int rows_multi_impl(const ColMeta& cm, const REAL* T, const REAL* RT, const int64_t* ZA, int64_t R,
+                           const int64_t* ZB, int64_t M, const double* W, int Mm, const DensMasks& dm, double* s,
+                           cudaStream_t st) {
+  const int64_t rblocks = (R + PR_THREADS - 1) / PR_THREADS;
+  int64_t nsl, slice;
+  rows_slices(R, M, nsl, slice);
+  double* part = nullptr;
+  int e = cuda_status(cudaMallocAsync((void**)&part, std::max<size_t>((size_t)nsl * R * Mm * sizeof(double), 8), st),
+                      "blml_rows_multi workspace");
+  if (e) return e;
+  const size_t sm = (size_t)cm.Tn * sizeof(REAL) + (size_t)cm.G * cm.LR * sizeof(REAL);
+  if (sm > 200 * 1024) { cudaFreeAsync(part, st); set_error("blml_rows_multi: tables too large for shared memory"); return BLML_ERR_UNSUPPORTED; }
+  cudaFuncSetAttribute(k_rows_multi<REAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+  k_rows_multi<REAL><<<dim3((unsigned)rblocks, (unsigned)nsl), PR_THREADS, sm, st>>>(cm, T, RT, ZA, R, ZB, W, Mm, dm,
+                                                                                   slice, M, part);
+  e = cuda_status(cudaGetLastError(), "blml_rows_multi");
+  if (!e) {
+    count_launches(2);
+    k_sum_slices<<<std::min<int64_t>((R * Mm + 255) / 256, 4096), 256, 0, st>>>(part, (int)nsl, R * Mm, s);
+    e = cuda_status(cudaGetLastError(), "blml_rows_multi finish");
+  }
+  cudaFreeAsync(part, st);
+  return e;
+}
+
+extern "C" {
+
+int blml_rows_multi(const blml_tables* tb, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                    const double* W, int Mm, const unsigned* umask, double* s, void* stream) {
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (Mm < 1 || Mm > MAXM || !umask) { set_error("blml_rows_multi: 1 to %d densities with a unit mask each", MAXM); return BLML_ERR_ARG; }
+  ColMeta cm;
+  int e = read_meta(tb, cm, st);
+  if (e) return e;
+  DensMasks dm;
+  for (int m = 0; m < MAXM; m++) dm.bits[m] = m < Mm ? umask[m] : 0u;
+  for (int m = 0; m < Mm; m++)
+    if (dm.bits[m] >> cm.U) { set_error("blml_rows_multi: density %d masks a unit beyond the tables' %d", m, cm.U); return BLML_ERR_ARG; }
+  if (R == 0) return BLML_OK;
+  if (M == 0) return cuda_status(cudaMemsetAsync(s, 0, R * Mm * sizeof(double), st), "blml_rows_multi");
+  if (!ZA || !ZB || !W || !s) { set_error("blml_rows_multi: null pointer"); return BLML_ERR_ARG; }
+  e = check_extents(cm, ZA, R, ZB, M, st);
+  if (e) return e;
+  if (tb->f32) {
+    if (!tb->T32 || (cm.G && !tb->RT32)) { set_error("blml_rows_multi: float32 tables missing"); return BLML_ERR_ARG; }
+    return rows_multi_impl<float>(cm, tb->T32, tb->RT32, ZA, R, ZB, M, W, Mm, dm, s, st);
+  }
+  if (!tb->T || (cm.G && !tb->RT)) { set_error("blml_rows_multi: tables missing"); return BLML_ERR_ARG; }
+  return rows_multi_impl<double>(cm, tb->T, tb->RT, ZA, R, ZB, M, W, Mm, dm, s, st);
 }
 
 }  // extern "C"

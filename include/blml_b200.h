@@ -399,6 +399,11 @@ typedef struct {
 } blml_tables;
 int blml_rows(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M, const double* w,
               int grad, double* s, double* ds, void* stream);
+/* ---- fused rows of several densities (blml_local.py:213-286 rows_multi, FusedFit's joint and marginals; K9 of
+ *      blml_local_gpu.py:107-180): s[r * Mm + m] = sum_j W[j * Mm + m] prod_u (bit u of umask[m] ? T_u : 1), the unit
+ *      factors of a pair computed once; 1 <= Mm <= 8 densities, values only (no derivative rows) ---- */
+int blml_rows_multi(const blml_tables* tab, const int64_t* ZA, int64_t R, const int64_t* ZB, int64_t M,
+                    const double* W, int Mm, const unsigned* umask, double* s, void* stream);
 /* ---- value rows over one coordinate set, validated once (the block coordinate descent of BLMLQuick,
  *      blml_trivial.py:2860-3035 / blml_gpu.py:340-373, whose passes run every bin against a block of bins) ----
  * plan_create reads the tables' metadata and checks that every pair of rows of Z (n x d rank coordinates, device)

@@ -129,3 +129,29 @@ def test_rows_plan_equals_rows(cuda_device):
             assert torch.equal(out, ref)
     finally:
         _lib.lib().blml_rows_plan_destroy(plan)
+
+
+@pytest.mark.parametrize('case', ['p5', 'pt'])
+@pytest.mark.parametrize('f32', [False, True])
+def test_rows_multi_matches_reference(cuda_device, case, f32):
+    """The fused rows of several densities (blml_local.py:282-286, FusedFit's joint and marginals in one pass) against
+    the reference's own values (tests/golden/rows_multi.npz): the 5-D sinc bins with two marginals, the pball torus
+    group with a sinc column and each unit alone. float64 tables to 1e-12 of the largest row, float32 to 2e-4; and the
+    joint density equals the single-density rows kernel."""
+    from blml_b200.local_gpu import ProductKernel, rows_multi, rows
+    g = golden('rows_multi.npz')[case]
+    if case == 'p5':
+        p = golden('pairs.npz')['p5']
+        kinds, per, fc, h = ['sinc'] * 5, [None] * 5, p['fc'], p['h']
+        tab = ProductKernel(kinds, per).tables(fc, per, h, g['ZB'])
+    else:
+        kinds, per = ['pball:0-1', 'pball:0-1', 'sinc'], [31.0, 31.0, None]
+        fc, h = np.array([0.33, 0.33, 0.2]), np.array([1.0, 1.0, 0.7])
+        tab = ProductKernel(kinds, per, fold=[True] * 3).tables(fc, per, h, np.r_[g['ZA'], g['ZB']])
+    s, _ = rows_multi(g['ZA'], g['ZB'], g['W'], tab, g['umask'], f32=f32)
+    ref = g['s']
+    tol = 2e-4 if f32 else 1e-12
+    assert s.shape == ref.shape
+    assert np.abs(s - ref).max() <= tol * np.abs(ref).max(), np.abs(s - ref).max() / np.abs(ref).max()
+    joint, _ = rows(g['ZA'], g['ZB'], g['W'][:, 0], tab, f32=f32)
+    assert np.abs(joint - s[:, 0]).max() <= tol * np.abs(joint).max()
