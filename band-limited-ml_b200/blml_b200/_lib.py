@@ -128,6 +128,7 @@ _SIGS = {
     'blml_new_bins': (_I, [_I, _I, _L, _I, _P, _P, _P, _P, _P]),
     'blml_gain_sums': (_I, [_I, _L, _P, _D, _P, _D, _P, _D, _P, _P, _P]),
     'blml_point_rows': (_I, [_L, _I, _P, _L, _P, _P, _P, _P, _P]),
+    'blml_point_rows_multi': (_I, [_L, _I, _P, _L, _P, _P, _I, _P, _P, _I, _P, _P, _P]),
     'blml_block_root': (_I, [_I, _P, _L, _P, _P, _P, _D, _P, _P]),
     'blml_block_search': (_I, [_I, _P, _L, _P, _P, _P, _P, _P, _P, _P]),
     'blml_block_apply': (_I, [_I, _P, _L, _P, _D, _P, _P]),

@@ -269,6 +269,39 @@ def rows_multi(ZA, ZB, Wt, tab, umask, grad=False, f32=False, device=None):
     return s.cpu().numpy(), np.zeros((R, Mm, 1))
 
 
+def point_rows_multi(A, Bp, Wt, kinds, fc, periods, umask, want=(), grad=False, device=None):
+    """Point sums of several densities (blml_local.py:555-560, FusedFit's joint and marginals at points): s (m, M)
+    with s[i, q] = sum_j K_q(A_i - Bp_j) Wt[j, q], K_q the continuous product kernel over the units with
+    umask[q, u] = 1 (units in kernel-unit order: one-column units first, then groups); sinc, slits, dirichlet and
+    ball units. ds zeros (m, M, 1) -- values only (want / grad raise). NumPy results."""
+    if grad or len(want):
+        raise NotImplementedError("point_rows_multi: derivatives are not available")
+    from .binned import point_cols
+    device = torch.device(device or 'cuda')
+    A = np.ascontiguousarray(np.atleast_2d(A), np.float64); Bp = np.ascontiguousarray(np.atleast_2d(Bp), np.float64)
+    d = A.shape[1]
+    Wn = np.ascontiguousarray(Wt, np.float64)
+    um = np.asarray(umask, np.int64)
+    units = units_of(list(kinds))
+    if Wn.ndim != 2 or Wn.shape[0] != Bp.shape[0] or um.shape != (Wn.shape[1], len(units)) or Bp.shape[1] != d:
+        raise ValueError("point_rows_multi: Wt (bins, densities), umask (densities, units), A and Bp with d columns")
+    sp = {'kinds': list(kinds), 'fc': np.asarray(fc, float),
+          'periods': [None if p is None else float(p) for p in (periods if periods is not None else [None] * d)]}
+    cols = point_cols(sp, d)
+    unit_of = np.zeros(d, np.int32)
+    for u, (_, dims) in enumerate(units):
+        for c in dims:
+            unit_of[c] = u
+    masks = np.array([int(sum(1 << u for u in range(len(units)) if um[q, u])) for q in range(um.shape[0])], np.uint32)
+    Mm = Wn.shape[1]
+    X, Z, W = (torch.as_tensor(v).to(device) for v in (A, Bp, Wn))
+    g = torch.empty((A.shape[0], Mm), dtype=torch.float64, device=device)
+    call('blml_point_rows_multi', A.shape[0], d, X.data_ptr(), Bp.shape[0], Z.data_ptr(), W.data_ptr(), Mm,
+         C.cast(cols, C.c_void_p), unit_of.ctypes.data_as(C.c_void_p), len(units), masks.ctypes.data_as(C.c_void_p),
+         g.data_ptr(), torch.cuda.current_stream(device).cuda_stream)
+    return g.cpu().numpy(), np.zeros((A.shape[0], Mm, 1))
+
+
 def cols(ZA_dev, ZB_dev, tab, out, out_m=None, depmask=0, f32=False):
     """The explicit block S(ZA_r, ZB_j) into out (R, M) on the device; ZA_dev, ZB_dev are rank coordinates (torch
     int64 on the device). out float64 or float32. With depmask (a bit per column), out_m receives the marginal: the

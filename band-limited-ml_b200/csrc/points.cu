@@ -104,31 +104,77 @@ __global__ void __launch_bounds__(kPtThreads) k_point_rows(int64_t m, int d, con
   if (i < m) g[i] = acc;
 }
 
+// Point sums of several densities (blml_local.py:555-560, point_rows_multi: FusedFit's joint and marginals at
+// points): g[i][m] = sum_b W[b][m] prod_u (bit u of masks[m] ? K_u(x_i - z_b) : 1), every unit's value computed once
+// per (point, bin) pair; unit_of[c] is the unit of column c (a ball group's value sits on its first column).
+constexpr int kPtMaxM = 8;
+struct PtMulti { int unit_of[kPtMaxD]; unsigned masks[kPtMaxM]; };
+
+__global__ void __launch_bounds__(kPtThreads) k_point_rows_multi(int64_t m, int d, int U, const double* __restrict__ X,
+                                                                int64_t B, const double* __restrict__ Z,
+                                                                const double* __restrict__ W, int Mm,
+                                                                blml_point_cols cols, PtMulti pm,
+                                                                double* __restrict__ g) {
+  __shared__ double zs[kPtTile * kPtMaxD];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double x[kPtMaxD];
+  for (int c = 0; c < d; c++) x[c] = i < m ? X[i * d + c] : 0.0;
+  double acc[kPtMaxM];
+  for (int q = 0; q < kPtMaxM; q++) acc[q] = 0.0;
+  for (int64_t b0 = 0; b0 < B; b0 += kPtTile) {
+    const int nt = (int)(B - b0 < kPtTile ? B - b0 : kPtTile);
+    __syncthreads();
+    for (int j = threadIdx.x; j < nt * d; j += blockDim.x) zs[j] = Z[b0 * d + j];
+    __syncthreads();
+    if (i < m) {
+      for (int j = 0; j < nt; j++) {
+        double fac[kPtMaxD];
+        for (int u = 0; u < U; u++) fac[u] = 1.0;
+        for (int c = 0; c < d; c++) {
+          const blml_point_col& cc = cols.c[c];
+          if (cc.kind == BLML_PT_BALL) {
+            if (cc.fi == 0.0) continue;
+            double s2 = 0.0;
+            for (int c2 = 0; c2 < d; c2++)
+              if ((cc.M >> c2) & 1) {
+                const double t = cols.c[c2].f * (x[c2] - zs[j * d + c2]);
+                s2 += t * t;
+              }
+            fac[pm.unit_of[c]] = cc.fi * ball_profile(sqrt(s2), cc.Mi, cc.P);
+          } else {
+            fac[pm.unit_of[c]] = point_unit(cc, x[c] - zs[j * d + c]);
+          }
+        }
+        const int64_t b = b0 + j;
+        for (int q = 0; q < Mm; q++) {
+          double p = W[b * Mm + q];
+          for (int u = 0; u < U; u++)
+            if ((pm.masks[q] >> u) & 1u) p *= fac[u];
+          acc[q] += p;
+        }
+      }
+    }
+  }
+  if (i < m)
+    for (int q = 0; q < Mm; q++) g[i * Mm + q] = acc[q];
+}
+
 }  // namespace blml
 
 using namespace blml;
 
-extern "C" {
-
-int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* e,
-                    const blml_point_col* cols, double* g, void* stream) {
-  if (m < 0 || B < 0 || d < 1 || d > kPtMaxD || !cols) {
-    set_error("blml_point_rows: 1 <= d <= %d columns, m, B >= 0", kPtMaxD);
-    return BLML_ERR_ARG;
-  }
-  if (m == 0) return BLML_OK;
-  if (!X || !g || (B > 0 && (!Z || !e))) { set_error("blml_point_rows: null pointer"); return BLML_ERR_ARG; }
-  blml_point_cols cc;
+// the columns' kinds and ball groups checked, copied into cc; nonzero (with the error set) when they are not valid
+static int check_point_cols(int d, const blml_point_col* cols, blml_point_cols& cc, const char* who) {
   for (int c = 0; c < d; c++) {
     cc.c[c] = cols[c];
     const int k = cols[c].kind;
     if (k != BLML_PT_SINC && k != BLML_PT_SLITS && k != BLML_PT_DIRICHLET && k != BLML_PT_BALL) {
-      set_error("blml_point_rows: column %d: kind %d (sinc, slits, dirichlet or ball)", c, k);
-      return BLML_ERR_ARG;
+      set_error("%s: column %d: kind %d (sinc, slits, dirichlet or ball)", who, c, k);
+      return 1;
     }
     if (k == BLML_PT_DIRICHLET && !(cols[c].P > 0)) {
-      set_error("blml_point_rows: column %d: dirichlet period must be positive", c);
-      return BLML_ERR_ARG;
+      set_error("%s: column %d: dirichlet period must be positive", who, c);
+      return 1;
     }
     if (k == BLML_PT_BALL) {
       // the group mask holds this column and only ball columns; the first column of the group carries prod fc (fi),
@@ -143,14 +189,58 @@ int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* 
       if (ok && c == lead) ok = cols[c].Mi == size && cols[c].fi > 0 && cols[c].P > 0;
       if (ok && c != lead) ok = cols[c].fi == 0.0;
       if (!ok) {
-        set_error("blml_point_rows: column %d: inconsistent ball group (mask %d)", c, mask);
-        return BLML_ERR_ARG;
+        set_error("%s: column %d: inconsistent ball group (mask %d)", who, c, mask);
+        return 1;
       }
     }
   }
+  return 0;
+}
+
+extern "C" {
+
+int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* e,
+                    const blml_point_col* cols, double* g, void* stream) {
+  if (m < 0 || B < 0 || d < 1 || d > kPtMaxD || !cols) {
+    set_error("blml_point_rows: 1 <= d <= %d columns, m, B >= 0", kPtMaxD);
+    return BLML_ERR_ARG;
+  }
+  if (m == 0) return BLML_OK;
+  if (!X || !g || (B > 0 && (!Z || !e))) { set_error("blml_point_rows: null pointer"); return BLML_ERR_ARG; }
+  blml_point_cols cc;
+  if (check_point_cols(d, cols, cc, "blml_point_rows")) return BLML_ERR_ARG;
   const int64_t blocks = (m + kPtThreads - 1) / kPtThreads;
   k_point_rows<<<(unsigned)blocks, kPtThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(m, d, X, B, Z, e, cc, g);
   BLML_CHECK_LAUNCH("blml_point_rows");
+  return BLML_OK;
+}
+
+int blml_point_rows_multi(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* W, int Mm,
+                          const blml_point_col* cols, const int* unit_of, int U, const unsigned* masks, double* g,
+                          void* stream) {
+  if (m < 0 || B < 0 || d < 1 || d > kPtMaxD || !cols || !unit_of || !masks || Mm < 1 || Mm > kPtMaxM || U < 1 ||
+      U > d) {
+    set_error("blml_point_rows_multi: 1 <= d <= %d columns, 1 <= U <= d units, 1 <= Mm <= %d densities", kPtMaxD,
+              kPtMaxM);
+    return BLML_ERR_ARG;
+  }
+  if (m == 0) return BLML_OK;
+  if (!X || !g || (B > 0 && (!Z || !W))) { set_error("blml_point_rows_multi: null pointer"); return BLML_ERR_ARG; }
+  blml_point_cols cc;
+  if (check_point_cols(d, cols, cc, "blml_point_rows_multi")) return BLML_ERR_ARG;
+  PtMulti pm;
+  for (int c = 0; c < kPtMaxD; c++) pm.unit_of[c] = 0;
+  for (int c = 0; c < d; c++) {
+    if (unit_of[c] < 0 || unit_of[c] >= U) { set_error("blml_point_rows_multi: column %d: unit %d of %d", c, unit_of[c], U); return BLML_ERR_ARG; }
+    pm.unit_of[c] = unit_of[c];
+  }
+  for (int q = 0; q < kPtMaxM; q++) pm.masks[q] = q < Mm ? masks[q] : 0u;
+  for (int q = 0; q < Mm; q++)
+    if (pm.masks[q] >> U) { set_error("blml_point_rows_multi: density %d masks a unit beyond %d", q, U); return BLML_ERR_ARG; }
+  const int64_t blocks = (m + kPtThreads - 1) / kPtThreads;
+  k_point_rows_multi<<<(unsigned)blocks, kPtThreads, 0, reinterpret_cast<cudaStream_t>(stream)>>>(m, d, U, X, B, Z, W,
+                                                                                                 Mm, cc, pm, g);
+  BLML_CHECK_LAUNCH("blml_point_rows_multi");
   return BLML_OK;
 }
 

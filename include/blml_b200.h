@@ -179,6 +179,12 @@ typedef struct { int kind; int M, Mi; double f, fi, P; } blml_point_col;
 typedef struct { blml_point_col c[8]; } blml_point_cols;
 int blml_point_rows(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* e,
                     const blml_point_col* cols, double* g, void* stream);
+/* ---- point sums of several densities (blml_local.py:555-560 point_rows_multi: FusedFit's joint and marginals at
+ *      points, K10 of blml_local_gpu.py): g[i * Mm + q] = sum_b W[b * Mm + q] prod_u (bit u of masks[q] ? K_u : 1),
+ *      unit_of[c] the kernel unit of column c (one-column units first, then groups), U units, 1 <= Mm <= 8 ---- */
+int blml_point_rows_multi(int64_t m, int d, const double* X, int64_t B, const double* Z, const double* W, int Mm,
+                          const blml_point_col* cols, const int* unit_of, int U, const unsigned* masks, double* g,
+                          void* stream);
 
 /* ---- the binned fit at arbitrary points for harmonic kernels (BLMLBinned.sqrt_density / predict / predict_grid,
  *      blml_binned.py:451-500) ----
