@@ -221,8 +221,7 @@ def _port_certified_fit(i):
     import blml_oracle as bo
     sweep, modes = workload(0)
     _, path = bo.certified_fit(sweep[i]['train'], modes[i][0], tol=TOL, cert_tol=CERT_TOL, max_rank=MAX_RANK,
-                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP, lanczos_basis=LANCZOS_BASIS,
-                          grow_two_above=GROW_TWO_ABOVE)
+                               ll_tol=ROUND_LL_TOL, grow_iters=GROW_ITERS, step=GROW_STEP)
     return path[-1][1], path[-1][2]
 
 

@@ -21,3 +21,11 @@ def test_certified_mask():
     ok, rel = bench.certified_mask(ll, cert, ref)
     assert ok.tolist() == [True, False, False, True, False, False]
     assert np.allclose(rel, (ll + 5.0) / 5.0)
+
+
+def test_reference_arm_certifies_its_cheapest_fit():
+    """The reference arm's worker (the port's certified fit of one sweep fit, with the main arm's procedure settings)
+    runs on the host: sweep fit 34, the one the port certifies fastest."""
+    import bench
+    ll, cert = bench._port_certified_fit(34)
+    assert cert <= 1 + bench.CERT_TOL and ll < 0
