@@ -100,6 +100,7 @@ _SIGS = {
     'blml_lbfgs_batch_create': (_I, [_I, _I, _P, _P, _I, _D, _D, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     'blml_lbfgs_batch_set_caps': (_I, [_P, _P]),
     'blml_lbfgs_batch_set_history': (_I, [_P, _I]),
+    'blml_seg_dots2_h32': (_I, [_I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_lanczos_coef': (_I, [_I, _I, _P, _P, _P, _I, _P]),
     'blml_lanczos_beta': (_I, [_I, _P, _P, _P, _P]),
     'blml_lbfgs_batch_run': (_I, [_P, _P]),

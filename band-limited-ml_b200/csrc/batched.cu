@@ -929,4 +929,10 @@ int blml_lanczos_beta(int n, const double* dots, double* beta, double* coef, voi
   return BLML_OK;
 }
 
+int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
+                       const void* x, double* part, double* out, void* stream) {
+  if (F < 1 || !segs || !a) { set_error("blml_seg_dots2_h32: bad arguments"); return BLML_ERR_ARG; }
+  return seg_dots2_h32(F, segs, np, a, b0, b1, x, part, out, SST);
+}
+
 }  // extern "C"

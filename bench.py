@@ -203,12 +203,14 @@ def traffic_from_profiles():
         return None
 
 
-def scan_traffic(K):
+def scan_traffic(K, variant='c128'):
     """DRAM bytes of one history-scan launch at K modes per fit: the committed ncu capture (K = 1, the same 64 lattices)
-    scaled by K -- the scan streams K-times-longer vectors, so its traffic grows in proportion."""
+    scaled by K -- the scan streams K-times-longer vectors, so its traffic grows in proportion. variant 'h32': the
+    complex64-history scan."""
     try:
         t = json.load(open(os.path.join(ROOT, 'profiles', 'history_scan_sweep64_traffic.json')))
-        return t['dram_bytes_per_launch'] * K / t['K']
+        b = t['dram_bytes_per_launch'] if variant == 'c128' else t['h32_dram_bytes_per_launch']
+        return b * K / t['K']
     except Exception:
         return None
 
@@ -401,8 +403,14 @@ def segscan_bench(dev, K=4, m=20, reps=20):
     def lincomb():
         call('blml_seg_lincomb', _lib.F64, F, st_t.data_ptr(), 1, q.data_ptr(), 1 + 2 * m, cf.data_ptr(),
              ptrs([vecs[2 * m]] + vecs[:2 * m]), st)
+    hist32 = [v.to(torch.complex64) for v in vecs[:m + 1]]          # the certified rounds' complex64 history
+
+    def dots2_h32():
+        call('blml_seg_dots2_h32', F, st_t.data_ptr(), m, ptrs(hist32[:m]), hist32[m].data_ptr(),
+             vecs[2 * m + 1].data_ptr(), vecs[2 * m + 2].data_ptr(), part.data_ptr(), out.data_ptr(), st)
     res = {'elements': n, 'vector_MB': vb / 1e6, 'K': K, 'm': m}
-    for name, fn, nbytes in (('dots2', dots2, (m + 3) * vb), ('lincomb', lincomb, (2 * m + 2) * vb)):
+    for name, fn, nbytes in (('dots2', dots2, (m + 3) * vb), ('lincomb', lincomb, (2 * m + 2) * vb),
+                             ('dots2_h32', dots2_h32, (m + 1) * vb // 2 + 2 * vb)):
         for _ in range(3):
             fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -901,15 +909,19 @@ def main():
                        'h2d_bytes_per_step': int(sum(c.nbytes for c in train) + sum(c.nbytes for c in val)),
                        'd2h_bytes_per_step': d2h},
                'gpu_launches': int(launches),
-               'roofline': {'bound': 'hbm', 'achieved': scan['dots2']['GB/s'], 'peak': peak, 'unit': 'GB/s',
-                            'frac': scan['dots2']['GB/s'] / peak, 'traffic': scan_traffic(4),
-                            'kernel': f"k_seg_dots2_c128, the L-BFGS history scan (with the direction's linear "
-                                      f"combination, two thirds of the certified sweep's GPU time): the 20 stored "
-                                      f"vectors and 2 shared ones over the 64 sweep lattices at K = 4 modes, "
-                                      f"complex128, {scan['elements']} elements: "
-                                      f"{23 * 16 * scan['elements']} algorithmic bytes, {scan['dots2']['us']:.1f} us "
-                                      f"per launch",
+               'roofline': {'bound': 'hbm', 'achieved': scan['dots2_h32']['GB/s'], 'peak': peak, 'unit': 'GB/s',
+                            'frac': scan['dots2_h32']['GB/s'] / peak, 'traffic': scan_traffic(4, 'h32'),
+                            'kernel': f"k_seg_dots2_c128<float2, float2>, the certified rounds' L-BFGS history scan "
+                                      f"(with the direction's linear combination, the largest share of the certified "
+                                      f"sweep's GPU time): the 20 stored complex64 vectors and the shared complex64 "
+                                      f"y and complex128 g and E over the 64 sweep lattices at K = 4 modes, "
+                                      f"{scan['elements']} elements: {21 * 8 * scan['elements'] + 32 * scan['elements']} "
+                                      f"algorithmic bytes, {scan['dots2_h32']['us']:.1f} us per launch",
                             'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if pk else 'fallback'},
+               'roofline_scan_c128': {'bound': 'hbm', 'achieved': scan['dots2']['GB/s'], 'peak': peak, 'unit': 'GB/s',
+                                      'frac': scan['dots2']['GB/s'] / peak, 'traffic': scan_traffic(4),
+                                      'kernel': f"k_seg_dots2_c128<double2, double2>, the complex128 history scan of "
+                                                f"plain fits, {scan['dots2']['us']:.1f} us per launch"},
                'roofline_lincomb': {'bound': 'hbm', 'achieved': scan['lincomb']['GB/s'], 'peak': peak,
                                     'unit': 'GB/s', 'frac': scan['lincomb']['GB/s'] / peak,
                                     'kernel': f"k_seg_lincomb<double, double2>, the direction (41 vectors in, 1 out), "

@@ -318,6 +318,10 @@ int blml_lbfgs_batch_set_caps(blml_lbfgs_batch runner, const int64_t* caps);
    and line search stay float64. No counterpart in the reference (its history is float64); for runs whose answer does
    not depend on the path, e.g. certified fits. Call before the first run. */
 int blml_lbfgs_batch_set_history(blml_lbfgs_batch runner, int f32);
+/* The history scan of such a runner (blml_seg_dots2's quantities, complex): the np stored vectors a and the first
+   shared vector b0 complex64, b1 and x complex128; float64 sums. */
+int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
+                       const void* x, double* part, double* out, void* stream);
 int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);
 /* per fit (host arrays of F, any may be null): iterations, stop code, L, Q, max|rho| */
 int blml_lbfgs_batch_result(blml_lbfgs_batch runner, int64_t* iters, int32_t* stop, double* L, double* Q,
