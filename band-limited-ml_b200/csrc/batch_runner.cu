@@ -834,6 +834,7 @@ struct blml_lbfgs_batch_s : Runner {
   double *cq = nullptr, *tA = nullptr, *cS = nullptr, *cY = nullptr, *cG = nullptr, *nqA = nullptr, *scrA = nullptr,
          *ones = nullptr, *sc = nullptr;
   int* need2 = nullptr;
+  int* split = nullptr;                  // the block split of the float32 history's scan (seg_split)
   LbState s{};
   long long* d_caps = nullptr;
 
@@ -841,10 +842,10 @@ struct blml_lbfgs_batch_s : Runner {
   int hist(int Fa_, const blml_seg* S, int p) {
     const void* a[LB_MMAX];
     for (int i = 0; i < m; i++) a[i] = Sh[i];
-    if (h32) RC(seg_dots2_h32(Fa_, S, m, a, Yh[p], g, E, part, H1, st));
+    if (h32) RC(seg_dots2_h32(Fa_, S, split, m, a, Yh[p], g, E, part, H1, st));
     else RC(blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, E, part, H1, st));
     for (int i = 0; i < m; i++) a[i] = Yh[i];
-    if (h32) return seg_dots2_h32(Fa_, S, m, a, Yh[p], g, nullptr, part, H2, st);
+    if (h32) return seg_dots2_h32(Fa_, S, split, m, a, Yh[p], g, nullptr, part, H2, st);
     return blml_seg_dots2(dtype, Fa_, S, 1, m, a, Yh[p], g, nullptr, part, H2, st);
   }
 
@@ -881,6 +882,8 @@ struct blml_lbfgs_batch_s : Runner {
     const int dt = dtype, Fa_ = Fa;
     const blml_seg* S = d_segs_eff;
     void* sv = st;
+    // the block split of this iteration's compact set (a fit that converges at its end keeps its blocks, idle)
+    if (h32) RC(seg_split(Fa_, S, split, st));
     // direction from the previous iteration's history scan
     k_lb_dir<<<Fa_, 32, 0, st>>>(m, d_fid, d_live, H1, H2, s, cq);
     KCHECK("lbfgs direction");
@@ -938,6 +941,7 @@ struct blml_lbfgs_batch_s : Runner {
     t1[0] = gn;
     RC(blml_seg_lincomb(dt, F, S, 1, g, 1, ones, t1, sv));
     RC(blml_seg_resid(dt, F, S, 1, E, U, c, scrA, part, outE, sv));
+    if (h32) RC(seg_split(F, S, split, st));
     RC(hist(F, S, 0));                                  // empty history: g . g and E . E for the first direction
     k_lbi_state<<<nblk(F, 128), 128, 0, st>>>(F, m, tol, cap, d_fid, d_live, d_segs_c, d_segs_eff, outD, outE, s);
     KCHECK("lbfgs set-up");
@@ -1111,7 +1115,8 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
     }
     cudaMemsetAsync(vec, 0, 6 * tot * esz, r->st);
     cudaMemsetAsync(hv, 0, 2 * (size_t)m * tot * esz, r->st);
-    const size_t pw = (size_t)SEG_PART_WIDTH(F);   // >= Fa * seg_blocks_for(Fa) for every Fa <= F
+    // >= Fa * seg_blocks_for(Fa) for every Fa <= F, and 48 pw >= 43 (SEG_SPLIT_BLOCKS(Fa) + Fa) for the split scan
+    const size_t pw = (size_t)SEG_PART_WIDTH(F);
     const int nq = 48;                    // the widest reduction: blml_seg_dots' 48 accumulators
     const int hs = 2 * m + 3;
     double* scr = (double*)r->dalloc(sizeof(double) * (nq * pw + (size_t)F * (2 * hs + (LB_T1 + 4) + LB_T2 + 1 + 2 + 2 +
@@ -1119,7 +1124,8 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
                                                                              1)));
     double* stt = (double*)r->dalloc(sizeof(double) * (size_t)F * (7 + (LB_FWIN + 1) + 2 * (size_t)m * m));
     int* ist = (int*)r->dalloc(sizeof(int) * ((size_t)F * (8 + m) + 1));
-    if (!scr || !stt || !ist) { set_error("blml_lbfgs_batch_create: allocation"); rc = BLML_ERR_CUDA; }
+    r->split = (int*)r->dalloc(sizeof(int) * (size_t)seg_split_ints(F));   // >= seg_split_ints(Fa) for Fa <= F
+    if (!scr || !stt || !ist || !r->split) { set_error("blml_lbfgs_batch_create: allocation"); rc = BLML_ERR_CUDA; }
     else {
       r->part = scr;
       double* x = scr + nq * pw;

@@ -275,6 +275,196 @@ __global__ void k_seg_finish_dots2(const double* part, int np, int nblk, double*
   }
 }
 
+// The block split of segmented.cuh (one block of 1024 threads): N = sum_f K_f B_f, fit f with n_f elements gets
+// nb_f = min(ceil(G n_f / N), ceil(n_f / SEG_SPLIT_MIN_ELEMS)) blocks (0 when n_f = 0), so sum_f nb_f <= G + F; then
+// bstart by an exclusive scan and fit_of by a binary search per block.
+__global__ void __launch_bounds__(1024) k_seg_split(int F, const blml_seg* segs, int G, int* split) {
+  __shared__ long long sh[1024];
+  __shared__ long long total;
+  const int tid = threadIdx.x, chunk = (F + 1023) / 1024, f0 = tid * chunk, f1 = min(F, f0 + chunk);
+  long long nsum = 0;
+  for (int f = f0; f < f1; f++) nsum += (long long)segs[f].K * segs[f].B;
+  sh[tid] = nsum;
+  __syncthreads();
+  for (int s = 512; s > 0; s >>= 1) {
+    if (tid < s) sh[tid] += sh[tid + s];
+    __syncthreads();
+  }
+  if (tid == 0) total = sh[0];
+  __syncthreads();
+  const long long N = total;
+  long long mine = 0;
+  for (int f = f0; f < f1; f++) {
+    const long long n = (long long)segs[f].K * segs[f].B;
+    if (n > 0) {
+      const long long a = (G * n + N - 1) / N, b = (n + SEG_SPLIT_MIN_ELEMS - 1) / SEG_SPLIT_MIN_ELEMS;
+      mine += a < b ? a : b;
+    }
+  }
+  __syncthreads();
+  sh[tid] = mine;
+  __syncthreads();
+  for (int s = 1; s < 1024; s <<= 1) {            // inclusive scan of the per-thread block counts
+    const long long v = tid >= s ? sh[tid - s] : 0;
+    __syncthreads();
+    sh[tid] += v;
+    __syncthreads();
+  }
+  long long at = sh[tid] - mine;
+  for (int f = f0; f < f1; f++) {
+    split[f] = (int)at;
+    const long long n = (long long)segs[f].K * segs[f].B;
+    if (n > 0) {
+      const long long a = (G * n + N - 1) / N, b = (n + SEG_SPLIT_MIN_ELEMS - 1) / SEG_SPLIT_MIN_ELEMS;
+      at += a < b ? a : b;
+    }
+  }
+  if (tid == 1023) split[F] = (int)sh[1023];
+  __syncthreads();
+  const int used = (int)sh[1023];
+  int* fit_of = split + F + 1;
+  for (int b = tid; b < G + F; b += 1024) {
+    int f = -1;
+    if (b < used) {                                 // the last f with bstart[f] <= b (empty fits share a start)
+      int lo = 0, hi = F - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (split[mid] <= b) lo = mid; else hi = mid - 1;
+      }
+      f = lo;
+    }
+    fit_of[b] = f;
+  }
+}
+
+// The complex64-history scan over a block split: the stored vectors a_q and b0 complex64, b1 and x complex128, the
+// quantities of k_seg_dots2_c128 (same warp roles: warp w takes q = w, w + 8, w + 16, the last warp the norms). Each
+// thread loads 4 elements per tile (128-element tiles), twice the complex128 kernel's 2 at half the bytes each, so as
+// many bytes are in flight per thread; full tiles take unchecked loads at fixed offsets from one base, the fit's last
+// tile the checked ones. Two blocks per SM leave the registers for that without spills.
+template <bool CHECK>
+__device__ __forceinline__ void h32_tile(int64_t t, int64_t n, int lane, const float2* const* A, int na,
+                                         const float2* B0, const double2* B1, const double2* X, bool norms,
+                                         double* a0, double* a1, double& n0, double& n1, double& nx) {
+  constexpr int EL = 4;
+  const double2 zero = make_double2(0.0, 0.0);
+  float2 ra[3][EL], r0[EL];
+  double2 y1[EL], z[EL];
+  bool v[EL];
+  if (CHECK) {
+    int64_t j[EL];
+#pragma unroll
+    for (int e = 0; e < EL; e++) { const int64_t i = t + 32 * e + lane; v[e] = i < n; j[e] = v[e] ? i : 0; }
+#pragma unroll
+    for (int e = 0; e < EL; e++) { r0[e] = __ldg(B0 + j[e]); y1[e] = __ldg(B1 + j[e]); z[e] = zero; }
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      if (q < na) {
+#pragma unroll
+        for (int e = 0; e < EL; e++) ra[q][e] = __ldg(A[q] + j[e]);
+      }
+    if (norms && X) {
+#pragma unroll
+      for (int e = 0; e < EL; e++) z[e] = __ldg(X + j[e]);
+    }
+  } else {
+    const int64_t base = t + lane;
+#pragma unroll
+    for (int e = 0; e < EL; e++) {
+      v[e] = true; r0[e] = __ldg(B0 + base + 32 * e); y1[e] = __ldg(B1 + base + 32 * e); z[e] = zero;
+    }
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      if (q < na) {
+        const float2* p = A[q] + base;
+#pragma unroll
+        for (int e = 0; e < EL; e++) ra[q][e] = __ldg(p + 32 * e);
+      }
+    if (norms && X) {
+#pragma unroll
+      for (int e = 0; e < EL; e++) z[e] = __ldg(X + base + 32 * e);
+    }
+  }
+  double2 y0[EL];
+#pragma unroll
+  for (int e = 0; e < EL; e++) {
+    y0[e] = make_double2((double)r0[e].x, (double)r0[e].y);
+    if (CHECK && !v[e]) { y0[e] = zero; y1[e] = zero; z[e] = zero; }
+  }
+#pragma unroll
+  for (int q = 0; q < 3; q++)
+    if (q < na) {
+#pragma unroll
+      for (int e = 0; e < EL; e++) {
+        const double ax = (double)ra[q][e].x, ay = (double)ra[q][e].y;
+        a0[q] += ax * y0[e].x + ay * y0[e].y;
+        a1[q] += ax * y1[e].x + ay * y1[e].y;
+      }
+    }
+  if (norms) {
+#pragma unroll
+    for (int e = 0; e < EL; e++) {
+      n0 += y0[e].x * y0[e].x + y0[e].y * y0[e].y; n1 += y1[e].x * y1[e].x + y1[e].y * y1[e].y;
+      nx += z[e].x * z[e].x + z[e].y * z[e].y;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256, 2) k_seg_dots2_h32(const blml_seg* segs, const int* split, int F, int np,
+                                                          SegList al, const float2* b0, const double2* b1,
+                                                          const double2* x, double* part) {
+  const int b = blockIdx.x, W = gridDim.x, f = split[F + 1 + b];
+  if (f < 0) return;
+  const int lb = b - split[f], nb = split[f + 1] - split[f];
+  const blml_seg S = segs[f];
+  const int64_t o = S.off, n = (int64_t)S.K * S.B;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const float2* B0 = b0 + o;
+  const double2* B1 = b1 + o;
+  const double2* X = x ? x + o : nullptr;
+  const float2* A[3];
+  int na = 0;
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const int q = warp + nw * j;
+    A[j] = q < np ? reinterpret_cast<const float2*>(al.a[q]) + o : nullptr;
+    na += q < np;
+  }
+  const bool norms = warp == nw - 1;
+  double a0[3] = {0.0, 0.0, 0.0}, a1[3] = {0.0, 0.0, 0.0}, n0 = 0.0, n1 = 0.0, nx = 0.0;
+  constexpr int64_t T = 128;
+  const int64_t stride = (int64_t)nb * T;
+  int64_t t = (int64_t)lb * T;
+  for (; t + T <= n; t += stride) h32_tile<false>(t, n, lane, A, na, B0, B1, X, norms, a0, a1, n0, n1, nx);
+  for (; t < n; t += stride) h32_tile<true>(t, n, lane, A, na, B0, B1, X, norms, a0, a1, n0, n1, nx);
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const double s0 = warp_sum(a0[j]), s1 = warp_sum(a1[j]);
+    if (j < na && lane == 0) {
+      const int q = warp + nw * j;
+      part[(int64_t)q * W + b] = s0; part[(int64_t)(20 + q) * W + b] = s1;
+    }
+  }
+  if (norms) {
+    n0 = warp_sum(n0); n1 = warp_sum(n1); nx = warp_sum(nx);
+    if (lane == 0) { part[40LL * W + b] = n0; part[41LL * W + b] = n1; part[42LL * W + b] = nx; }
+  }
+}
+
+// out[f * (2 np + 3) + q] from a split scan's partials: fit f's blocks [bstart[f], bstart[f + 1]), fixed order
+__global__ void k_seg_finish_dots2_split(const double* part, int W, const int* split, int np, double* out) {
+  const int f = blockIdx.x, nq = 2 * np + 3;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int b0 = split[f], b1 = split[f + 1];
+  for (int q = wid; q < nq; q += nw) {
+    const int src = q < np ? q : (q < 2 * np ? 20 + (q - np) : 40 + (q - 2 * np));
+    double acc = 0.0;
+    for (int i = b0 + lane; i < b1; i += 32) acc += part[(int64_t)src * W + i];
+    acc = warp_sum(acc);
+    if (lane == 0) out[(int64_t)f * nq + q] = acc;
+  }
+}
+
 struct SegTerms { const void* v[48]; };
 
 // out = sum_i coef[f * nt + i] v_i over each fit's slice. The block lists the fit's nonzero terms (pointer, coefficient)
@@ -647,15 +837,22 @@ using namespace blml;
 namespace blml {
 // the L-BFGS runner's history with float32 storage (internal to the library): the scan over complex64 stored vectors
 // and a complex64 first shared vector, and linear combinations over complex128 / complex64 terms
-int seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
-                  const void* x, double* part, double* out, cudaStream_t st) {
+int seg_split(int F, const blml_seg* segs, int* split, cudaStream_t st) {
+  k_seg_split<<<1, 1024, 0, st>>>(F, segs, SEG_SPLIT_BLOCKS(F), split);
+  BLML_CHECK_LAUNCH("segment block split");
+  return BLML_OK;
+}
+
+int seg_dots2_h32(int F, const blml_seg* segs, const int* split, int np, const void* const* a, const void* b0,
+                  const void* b1, const void* x, double* part, double* out, cudaStream_t st) {
   if (np < 1 || np > 20 || !a || !b0 || !b1) { set_error("history scan: 1..20 vectors, b0 and b1"); return BLML_ERR_ARG; }
   SegList al;
   for (int q = 0; q < 20; q++) al.a[q] = q < np ? a[q] : nullptr;
-  k_seg_dots2_c128<float2, float2><<<dim3((unsigned)seg_blocks_for(F), (unsigned)F), 256, 0, st>>>(segs, np, al, b0,
-                                                                                                 b1, x, part);
+  const int W = SEG_SPLIT_BLOCKS(F) + F;
+  k_seg_dots2_h32<<<W, 256, 0, st>>>(segs, split, F, np, al, (const float2*)b0, (const double2*)b1,
+                                     (const double2*)x, part);
   BLML_CHECK_LAUNCH("history scan (float32 history)");
-  k_seg_finish_dots2<<<F, 256, 0, st>>>(part, np, seg_blocks_for(F), out);
+  k_seg_finish_dots2_split<<<F, 256, 0, st>>>(part, W, split, np, out);
   BLML_CHECK_LAUNCH("history scan finish");
   return BLML_OK;
 }
@@ -931,8 +1128,11 @@ int blml_lanczos_beta(int n, const double* dots, double* beta, double* coef, voi
 
 int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
                        const void* x, double* part, double* out, void* stream) {
-  if (F < 1 || !segs || !a) { set_error("blml_seg_dots2_h32: bad arguments"); return BLML_ERR_ARG; }
-  return seg_dots2_h32(F, segs, np, a, b0, b1, x, part, out, SST);
+  if (F < 1 || F > 65535 || !segs || !a || !part) { set_error("blml_seg_dots2_h32: bad arguments"); return BLML_ERR_ARG; }
+  // the split after the partials (43 (G + F) doubles), inside the documented F * 43 * blml_seg_blocks() doubles
+  int* split = reinterpret_cast<int*>(part + 43 * ((int64_t)SEG_SPLIT_BLOCKS(F) + F));
+  if (seg_split(F, segs, split, SST)) return BLML_ERR_CUDA;
+  return seg_dots2_h32(F, segs, split, np, a, b0, b1, x, part, out, SST);
 }
 
 }  // extern "C"

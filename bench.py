@@ -911,12 +911,13 @@ def main():
                'gpu_launches': int(launches),
                'roofline': {'bound': 'hbm', 'achieved': scan['dots2_h32']['GB/s'], 'peak': peak, 'unit': 'GB/s',
                             'frac': scan['dots2_h32']['GB/s'] / peak, 'traffic': scan_traffic(4, 'h32'),
-                            'kernel': f"k_seg_dots2_c128<float2, float2>, the certified rounds' L-BFGS history scan "
-                                      f"(with the direction's linear combination, the largest share of the certified "
-                                      f"sweep's GPU time): the 20 stored complex64 vectors and the shared complex64 "
-                                      f"y and complex128 g and E over the 64 sweep lattices at K = 4 modes, "
+                            'kernel': f"k_seg_dots2_h32, the certified rounds' L-BFGS history scan (with the "
+                                      f"direction's linear combination, the largest share of the certified sweep's "
+                                      f"GPU time): the 20 stored complex64 vectors and the shared complex64 y and "
+                                      f"complex128 g and E over the 64 sweep lattices at K = 4 modes, "
                                       f"{scan['elements']} elements: {21 * 8 * scan['elements'] + 32 * scan['elements']} "
-                                      f"algorithmic bytes, {scan['dots2_h32']['us']:.1f} us per launch",
+                                      f"algorithmic bytes, {scan['dots2_h32']['us']:.1f} us per call (its block split, "
+                                      f"the scan and the partials' sum: 3 launches)",
                             'peak_source': 'MEASURED_PEAKS.json hbm_gbs (of measured)' if pk else 'fallback'},
                'roofline_scan_c128': {'bound': 'hbm', 'achieved': scan['dots2']['GB/s'], 'peak': peak, 'unit': 'GB/s',
                                       'frac': scan['dots2']['GB/s'] / peak, 'traffic': scan_traffic(4),

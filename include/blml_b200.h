@@ -232,7 +232,7 @@ int blml_cert_weights(int dtype, int K, int64_t B, int cplx, const void* E, cons
  * Fit f owns elements [off, off + K B) of every flat mode array (its (K, B) block) and [boff, boff + B) of every flat
  * bin array (counts, signs); `segs` is a device array of F entries. Per-fit scalars are device arrays of F doubles
  * (coefficient tables: F x nterms). Reductions give out[f * nq + q] (part: F * nq * blml_seg_blocks() doubles, an
- * upper bound: a launch over F fits uses min(256, max(16, 4096 / F)) blocks per fit; blml_seg_dots takes nq = 48,
+ * upper bound: a launch over F fits uses min(256, max(16, 16384 / F)) blocks per fit; blml_seg_dots takes nq = 48,
  * blml_seg_dots2 nq = 43).
  * These are the reference's single-fit operations (blml_binned.py:171-220, 278-355, 415-445, 630-645) applied to a
  * sweep of fits at once, as selector._search / the cut-off sweeps run them one after another. */
@@ -319,7 +319,9 @@ int blml_lbfgs_batch_set_caps(blml_lbfgs_batch runner, const int64_t* caps);
    not depend on the path, e.g. certified fits. Call before the first run. */
 int blml_lbfgs_batch_set_history(blml_lbfgs_batch runner, int f32);
 /* The history scan of such a runner (blml_seg_dots2's quantities, complex): the np stored vectors a and the first
-   shared vector b0 complex64, b1 and x complex128; float64 sums. */
+   shared vector b0 complex64, b1 and x complex128; float64 sums. Its blocks are shared out among the fits in
+   proportion to their sizes K B (the split is computed on the device, from segs, into the tail of part: part takes
+   the same F * 43 * blml_seg_blocks() doubles as blml_seg_dots2). */
 int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
                        const void* x, double* part, double* out, void* stream);
 int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);

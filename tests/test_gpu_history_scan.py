@@ -1,0 +1,82 @@
+"""The complex64-history scan (blml_seg_dots2_h32: the certified rounds' L-BFGS history products, the quantities the
+reference reads pair by pair at blml_binned.py:297-313) against float64 sums of the same stored values on the host.
+Its blocks are shared out among the fits in proportion to their sizes (a split computed on the device), so the cases
+cover what that split must get right: an empty fit (B = 0), fits smaller than one 128-element tile, sizes that are not
+multiples of a tile, fits hundreds of times larger than the others, one fit alone, more fits than the split has
+blocks to share, fewer than 20 stored vectors and no third vector."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _scan(dev, B, K, np_, with_x, seed):
+    import torch
+    from blml_b200 import _lib
+    from blml_b200._lib import call, ptrs
+    from blml_b200.sweep import _Seg
+    rng = np.random.default_rng(seed)
+    B = np.asarray(B, np.int64)
+    F = len(B)
+    n_f = K * B
+    off = np.concatenate([[0], np.cumsum(n_f)])
+    boff = np.concatenate([[0], np.cumsum(B)])
+    segs = (_Seg * F)(*[_Seg(int(off[f]), int(boff[f]), int(B[f]), int(K[f]), 0) for f in range(F)])
+    st_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
+    n = max(int(off[-1]), 1)
+
+    def c64():
+        return (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+
+    def c128():
+        return rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    a = [c64() for _ in range(np_)]
+    b0, b1, x = c64(), c128(), c128()
+    da = [torch.from_numpy(v).to(dev) for v in a]
+    db0, db1, dx = (torch.from_numpy(v).to(dev) for v in (b0, b1, x))
+    part = torch.full((F * 43 * _lib.lib().blml_seg_blocks(),), np.nan, dtype=torch.float64, device=dev)
+    out = torch.full((F * (2 * np_ + 3),), np.nan, dtype=torch.float64, device=dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    call('blml_seg_dots2_h32', F, st_t.data_ptr(), np_, ptrs(da), db0.data_ptr(), db1.data_ptr(),
+         dx.data_ptr() if with_x else C.c_void_p(0), part.data_ptr(), out.data_ptr(), st)
+    torch.cuda.synchronize(dev)
+    got = out.cpu().numpy().reshape(F, 2 * np_ + 3)
+
+    def rdot(u, v):                         # Re(conj(u) v) summed in float64: the scan's real inner product
+        u = u.astype(np.complex128)
+        return float(np.sum(u.real * v.real + u.imag * v.imag))
+    want = np.zeros_like(got)
+    for f in range(F):
+        s = slice(int(off[f]), int(off[f + 1]))
+        y0 = b0[s].astype(np.complex128)
+        for q in range(np_):
+            want[f, q] = rdot(a[q][s], y0)
+            want[f, np_ + q] = rdot(a[q][s], b1[s])
+        want[f, 2 * np_] = rdot(y0, y0)
+        want[f, 2 * np_ + 1] = rdot(b1[s], b1[s])
+        want[f, 2 * np_ + 2] = rdot(x[s], x[s]) if with_x else 0.0
+    return got, want, n_f
+
+
+CASES = {
+    # the sweep's spread: small and large lattices, one empty fit, ragged sizes
+    'mixed': ([4096, 0, 147456, 37, 1, 9000, 128, 129, 65536, 4097], [4, 2, 4, 1, 3, 2, 1, 1, 2, 4], 20, True),
+    'one_fit': ([300001], [1], 20, True),
+    'tiny_only': ([1, 2, 127, 128, 5], [1, 1, 1, 1, 3], 7, False),
+    # more fits than the split's 2048 blocks: every fit with work still gets one
+    'many_fits': (list(np.random.default_rng(3).integers(0, 600, 2500)), [1] * 2500, 3, True),
+}
+
+
+@pytest.mark.parametrize('case', sorted(CASES))
+def test_history_scan_matches_host_sums(cuda_device, case):
+    B, K, np_, with_x = CASES[case]
+    got, want, n_f = _scan(cuda_device, B, np.asarray(K, np.int64), np_, with_x, seed=len(B))
+    assert np.all(np.isfinite(got))
+    # float64 sums of up to ~6e5 products in another order: a few 1e-16 relative to the sum of |products|
+    scale = np.maximum(np.abs(want), np.sqrt(np.maximum(n_f, 1))[:, None])
+    err = np.abs(got - want) / scale
+    assert err.max() < 1e-12, (case, err.max())
+    assert np.all(got[n_f == 0] == 0.0)
