@@ -101,6 +101,8 @@ _SIGS = {
     'blml_lbfgs_batch_set_caps': (_I, [_P, _P]),
     'blml_lbfgs_batch_set_history': (_I, [_P, _I]),
     'blml_seg_dots2_h32': (_I, [_I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_split_ints': (_L, [_I]),
+    'blml_seg_lincomb_h32': (_I, [_I, _P, _P, _P, _I, _I, _P, _P, C.c_uint64, _P]),
     'blml_lanczos_coef': (_I, [_I, _I, _P, _P, _P, _I, _P]),
     'blml_lanczos_beta': (_I, [_I, _P, _P, _P, _P]),
     'blml_lbfgs_batch_run': (_I, [_P, _P]),

@@ -834,7 +834,7 @@ struct blml_lbfgs_batch_s : Runner {
   double *cq = nullptr, *tA = nullptr, *cS = nullptr, *cY = nullptr, *cG = nullptr, *nqA = nullptr, *scrA = nullptr,
          *ones = nullptr, *sc = nullptr;
   int* need2 = nullptr;
-  int* split = nullptr;                  // the block split of the float32 history's scan (seg_split)
+  int* split = nullptr;                  // the block split of the float32 history's kernels (seg_split)
   LbState s{};
   long long* d_caps = nullptr;
 
@@ -882,7 +882,8 @@ struct blml_lbfgs_batch_s : Runner {
     const int dt = dtype, Fa_ = Fa;
     const blml_seg* S = d_segs_eff;
     void* sv = st;
-    // the block split of this iteration's compact set (a fit that converges at its end keeps its blocks, idle)
+    // the block split of this iteration's compact set, for the float32 history's kernels (a fit that converges at the
+    // iteration's end keeps its blocks, idle)
     if (h32) RC(seg_split(Fa_, S, split, st));
     // direction from the previous iteration's history scan
     k_lb_dir<<<Fa_, 32, 0, st>>>(m, d_fid, d_live, H1, H2, s, cq);
@@ -890,7 +891,7 @@ struct blml_lbfgs_batch_s : Runner {
     const void* terms[48];
     terms[0] = g;
     for (int i = 0; i < m; i++) { terms[1 + i] = Sh[i]; terms[1 + m + i] = Yh[i]; }
-    if (h32) RC(seg_lincomb_mixed(Fa_, S, q, 0, 1 + 2 * m, cq, terms, ((1ull << (2 * m)) - 1ull) << 1, st));
+    if (h32) RC(seg_lincomb_mixed(Fa_, S, split, q, 0, 1 + 2 * m, cq, terms, ((1ull << (2 * m)) - 1ull) << 1, st));
     else RC(blml_seg_lincomb(dt, Fa_, S, 1, q, 1 + 2 * m, cq, terms, sv));
     RC(blml_group_matvec_masked(gq, d_fid, Fa_, d_live, sv));
     // every fit's Armijo search (8 trials, then 32 more for the fits that need them), the accepted steps, U = S E
@@ -906,10 +907,10 @@ struct blml_lbfgs_batch_s : Runner {
     RC(blml_group_matvec_masked(gV, d_fid, Fa_, d_live, sv));
     RC(blml_seg_lgrad_finish(dt, Fa_, S, 1, SV, U, w, nqA, gn, sv));
     terms[0] = q; terms[1] = Sh[p];
-    if (h32) RC(seg_lincomb_mixed(Fa_, S, Sh[p], 1, 2, cS, terms, 2ull, st));
+    if (h32) RC(seg_lincomb_mixed(Fa_, S, split, Sh[p], 1, 2, cS, terms, 2ull, st));
     else RC(blml_seg_lincomb(dt, Fa_, S, 1, Sh[p], 2, cS, terms, sv));
     terms[0] = g; terms[1] = gn; terms[2] = Yh[p];
-    if (h32) RC(seg_lincomb_mixed(Fa_, S, Yh[p], 1, 3, cY, terms, 4ull, st));
+    if (h32) RC(seg_lincomb_mixed(Fa_, S, split, Yh[p], 1, 3, cY, terms, 4ull, st));
     else RC(blml_seg_lincomb(dt, Fa_, S, 1, Yh[p], 3, cY, terms, sv));
     terms[0] = gn; terms[1] = g;
     RC(blml_seg_lincomb(dt, Fa_, S, 1, g, 2, cG, terms, sv));

@@ -539,68 +539,91 @@ __global__ void __launch_bounds__(256) k_seg_lincomb(const blml_seg* segs, int c
 
 // out = sum_i coef[f * nt + i] v_i for complex float64 arithmetic over terms of two storage types: bit i of f32mask
 // marks term i as complex64 (a float32 history vector), the others complex128; out is complex64 (VO = float2) or
-// complex128. Same term order, listing and load batching as k_seg_lincomb.
+// complex128. The block lists the fit's nonzero terms by storage type (the complex128 ones, then the complex64 ones,
+// each in term order) and sums them in that order, so that no load waits behind a branch on its term's type: four
+// terms' loads of four elements per thread are issued together. Blocks follow a block split (segmented.cuh) with
+// 1024-element tiles (256 threads x 4 elements). out may be one of the terms: each thread reads its elements of
+// every term before it writes them.
 template <typename VO>
-__global__ void __launch_bounds__(256) k_seg_lincomb_mixed(const blml_seg* segs, VO* out, int nt, const double* coef,
-                                                           SegTerms t, unsigned long long f32mask) {
+__global__ void __launch_bounds__(256) k_seg_lincomb_mixed(const blml_seg* segs, const int* split, int F, VO* out,
+                                                           int nt, const double* coef, SegTerms t,
+                                                           unsigned long long f32mask) {
+  constexpr int EL = 4, TB = 4;
   __shared__ const void* sp[48];
   __shared__ double sc[48];
-  __shared__ int s32[48];
-  __shared__ int snz;
-  const blml_seg S = segs[blockIdx.y];
-  const double* cf = coef + (int64_t)blockIdx.y * nt;
+  __shared__ int sn[2];
+  const int f = split[F + 1 + blockIdx.x];
+  if (f < 0) return;
+  const int lb = blockIdx.x - split[f], nb = split[f + 1] - split[f];
+  const blml_seg S = segs[f];
+  const double* cf = coef + (int64_t)f * nt;
   if (threadIdx.x == 0) {
     int c = 0;
-    for (int q = 0; q < nt; q++) {
-      const double v = cf[q];
-      if (v != 0.0) { sp[c] = t.v[q]; sc[c] = v; s32[c] = (int)((f32mask >> q) & 1ull); c++; }
+    for (int pass = 0; pass < 2; pass++) {
+      for (int q = 0; q < nt; q++) {
+        const double v = cf[q];
+        if (v != 0.0 && (int)((f32mask >> q) & 1ull) == pass) { sp[c] = t.v[q]; sc[c] = v; c++; }
+      }
+      sn[pass] = c;
     }
-    snz = c;
   }
   __syncthreads();
   const int64_t o = S.off, n = (int64_t)S.K * S.B;
-  const int nz = snz;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
-    const int64_t i2 = i + stride;
-    const bool two = i2 < n;
-    const int64_t j2 = two ? i2 : i;
-    double r0x = 0.0, r0y = 0.0, r1x = 0.0, r1y = 0.0;
-    int k = 0;
-    for (; k + 4 <= nz; k += 4) {
-      double2 v0[4], v1[4];
+  const int n64 = sn[0], nz = sn[1];
+  constexpr int64_t T = 256 * EL;
+  const int64_t stride = (int64_t)nb * T;
+  for (int64_t t0 = (int64_t)lb * T; t0 < n; t0 += stride) {
+    int64_t j[EL];
+    bool ok[EL];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        if (s32[k + j]) {
-          const float2* p = reinterpret_cast<const float2*>(sp[k + j]) + o;
-          v0[j] = ld_c2(p + i); v1[j] = ld_c2(p + j2);
-        } else {
-          const double2* p = reinterpret_cast<const double2*>(sp[k + j]) + o;
-          v0[j] = ld_c2(p + i); v1[j] = ld_c2(p + j2);
-        }
+    for (int e = 0; e < EL; e++) {
+      const int64_t i = t0 + 256 * e + threadIdx.x;
+      ok[e] = i < n; j[e] = o + (ok[e] ? i : 0);
+    }
+    double rx[EL], ry[EL];
+#pragma unroll
+    for (int e = 0; e < EL; e++) { rx[e] = 0.0; ry[e] = 0.0; }
+    int k = 0;
+    for (; k < n64; k++) {
+      const double2* p = reinterpret_cast<const double2*>(sp[k]);
+      const double c = sc[k];
+      double2 v[EL];
+#pragma unroll
+      for (int e = 0; e < EL; e++) v[e] = __ldg(p + j[e]);
+#pragma unroll
+      for (int e = 0; e < EL; e++) { rx[e] += c * v[e].x; ry[e] += c * v[e].y; }
+    }
+    for (; k + TB <= nz; k += TB) {
+      float2 v[TB][EL];
+#pragma unroll
+      for (int q = 0; q < TB; q++) {
+        const float2* p = reinterpret_cast<const float2*>(sp[k + q]);
+#pragma unroll
+        for (int e = 0; e < EL; e++) v[q][e] = __ldg(p + j[e]);
       }
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const double c = sc[k + j];
-        r0x += c * v0[j].x; r0y += c * v0[j].y; r1x += c * v1[j].x; r1y += c * v1[j].y;
+      for (int q = 0; q < TB; q++) {
+        const double c = sc[k + q];
+#pragma unroll
+        for (int e = 0; e < EL; e++) { rx[e] += c * (double)v[q][e].x; ry[e] += c * (double)v[q][e].y; }
       }
     }
     for (; k < nz; k++) {
-      double2 v0, v1;
-      if (s32[k]) {
-        const float2* p = reinterpret_cast<const float2*>(sp[k]) + o;
-        v0 = ld_c2(p + i); v1 = ld_c2(p + j2);
-      } else {
-        const double2* p = reinterpret_cast<const double2*>(sp[k]) + o;
-        v0 = ld_c2(p + i); v1 = ld_c2(p + j2);
-      }
+      const float2* p = reinterpret_cast<const float2*>(sp[k]);
       const double c = sc[k];
-      r0x += c * v0.x; r0y += c * v0.y; r1x += c * v1.x; r1y += c * v1.y;
+      float2 v[EL];
+#pragma unroll
+      for (int e = 0; e < EL; e++) v[e] = __ldg(p + j[e]);
+#pragma unroll
+      for (int e = 0; e < EL; e++) { rx[e] += c * (double)v[e].x; ry[e] += c * (double)v[e].y; }
     }
-    VO y0, y1;
-    y0.x = r0x; y0.y = r0y; y1.x = r1x; y1.y = r1y;
-    out[o + i] = y0;
-    if (two) out[o + i2] = y1;
+#pragma unroll
+    for (int e = 0; e < EL; e++)
+      if (ok[e]) {
+        VO y;
+        y.x = rx[e]; y.y = ry[e];
+        out[j[e]] = y;
+      }
   }
 }
 
@@ -857,14 +880,14 @@ int seg_dots2_h32(int F, const blml_seg* segs, const int* split, int np, const v
   return BLML_OK;
 }
 
-int seg_lincomb_mixed(int F, const blml_seg* segs, void* out, int out_f32, int nterms, const double* coef,
-                      const void* const* v, unsigned long long f32mask, cudaStream_t st) {
+int seg_lincomb_mixed(int F, const blml_seg* segs, const int* split, void* out, int out_f32, int nterms,
+                      const double* coef, const void* const* v, unsigned long long f32mask, cudaStream_t st) {
   if (nterms < 1 || nterms > 48) { set_error("linear combination: 1..48 terms"); return BLML_ERR_ARG; }
   SegTerms t;
   for (int q = 0; q < 48; q++) t.v[q] = q < nterms ? v[q] : nullptr;
-  const dim3 grid((unsigned)seg_blocks_for(F), (unsigned)F);
-  if (out_f32) k_seg_lincomb_mixed<float2><<<grid, 256, 0, st>>>(segs, (float2*)out, nterms, coef, t, f32mask);
-  else k_seg_lincomb_mixed<double2><<<grid, 256, 0, st>>>(segs, (double2*)out, nterms, coef, t, f32mask);
+  const unsigned W = (unsigned)(SEG_SPLIT_BLOCKS(F) + F);
+  if (out_f32) k_seg_lincomb_mixed<float2><<<W, 256, 0, st>>>(segs, split, F, (float2*)out, nterms, coef, t, f32mask);
+  else k_seg_lincomb_mixed<double2><<<W, 256, 0, st>>>(segs, split, F, (double2*)out, nterms, coef, t, f32mask);
   BLML_CHECK_LAUNCH("linear combination (mixed storage)");
   return BLML_OK;
 }
@@ -1133,6 +1156,17 @@ int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a
   int* split = reinterpret_cast<int*>(part + 43 * ((int64_t)SEG_SPLIT_BLOCKS(F) + F));
   if (seg_split(F, segs, split, SST)) return BLML_ERR_CUDA;
   return seg_dots2_h32(F, segs, split, np, a, b0, b1, x, part, out, SST);
+}
+
+int64_t blml_seg_split_ints(int F) { return F < 1 ? 0 : seg_split_ints(F); }
+
+int blml_seg_lincomb_h32(int F, const blml_seg* segs, int* split, void* out, int out_f32, int nterms,
+                         const double* coef, const void* const* v, unsigned long long f32mask, void* stream) {
+  if (F < 1 || F > 65535 || !segs || !split || !out || !coef || !v) {
+    set_error("blml_seg_lincomb_h32: bad arguments"); return BLML_ERR_ARG;
+  }
+  if (seg_split(F, segs, split, SST)) return BLML_ERR_CUDA;
+  return seg_lincomb_mixed(F, segs, split, out, out_f32, nterms, coef, v, f32mask, SST);
 }
 
 }  // extern "C"

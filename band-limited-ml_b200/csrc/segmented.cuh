@@ -27,7 +27,7 @@ __host__ __device__ inline int seg_blocks_for(int F) {
 // changes (a converged fit's B set to 0). Its ints: bstart[F + 1] (fit f owns split blocks
 // [bstart[f], bstart[f + 1])), then fit_of[G + F] (the fit of each block of a launch of G + F blocks, -1 for blocks
 // past the last fit's). Partials of a split reduction: quantity q of block b at part[q * (G + F) + b].
-constexpr int SEG_SPLIT_MAX = 2048, SEG_SPLIT_MIN_ELEMS = 512;
+constexpr int SEG_SPLIT_MAX = 2048, SEG_SPLIT_MIN_ELEMS = 1024;
 __host__ __device__ inline int SEG_SPLIT_BLOCKS(int F) { return 200 * F < SEG_SPLIT_MAX ? 200 * F : SEG_SPLIT_MAX; }
 __host__ __device__ inline int64_t seg_split_ints(int F) { return 2 * (int64_t)F + 1 + SEG_SPLIT_BLOCKS(F); }
 int seg_split(int F, const blml_seg* segs, int* split, cudaStream_t st);
@@ -35,8 +35,8 @@ int seg_split(int F, const blml_seg* segs, int* split, cudaStream_t st);
 // the L-BFGS runner's float32 history (batched.cu); split: seg_split's output for these segments
 int seg_dots2_h32(int F, const blml_seg* segs, const int* split, int np, const void* const* a, const void* b0,
                   const void* b1, const void* x, double* part, double* out, cudaStream_t st);
-int seg_lincomb_mixed(int F, const blml_seg* segs, void* out, int out_f32, int nterms, const double* coef,
-                      const void* const* v, unsigned long long f32mask, cudaStream_t st);
+int seg_lincomb_mixed(int F, const blml_seg* segs, const int* split, void* out, int out_f32, int nterms,
+                      const double* coef, const void* const* v, unsigned long long f32mask, cudaStream_t st);
 
 template <typename T, bool CPLX>
 struct SAcc {

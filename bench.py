@@ -373,8 +373,9 @@ def pairs_bench(dev, reps=3):
 def segscan_bench(dev, K=4, m=20, reps=20):
     """The L-BFGS history kernels that dominate the certified sweep's GPU time, at its size: every sweep fit at K
     shared modes (complex128 vectors of sum K B elements), the history scan (blml_seg_dots2: m stored vectors against
-    two shared ones) and the direction's linear combination (blml_seg_lincomb of 1 + 2 m vectors). CUDA events;
-    GB/s of the algorithmic bytes (each vector read once, the output written once)."""
+    two shared ones) and the direction's linear combination (blml_seg_lincomb of 1 + 2 m vectors), and both with the
+    certified rounds' complex64 history (blml_seg_dots2_h32, blml_seg_lincomb_h32). CUDA events; GB/s of the
+    algorithmic bytes (each vector read once, the output written once)."""
     import ctypes as C
     import torch
     from blml_b200 import _lib
@@ -408,9 +409,16 @@ def segscan_bench(dev, K=4, m=20, reps=20):
     def dots2_h32():
         call('blml_seg_dots2_h32', F, st_t.data_ptr(), m, ptrs(hist32[:m]), hist32[m].data_ptr(),
              vecs[2 * m + 1].data_ptr(), vecs[2 * m + 2].data_ptr(), part.data_ptr(), out.data_ptr(), st)
+    hist32 += [v.to(torch.complex64) for v in vecs[m + 1:2 * m]]    # 2 m complex64 history vectors in all
+    split = torch.empty(int(_lib.lib().blml_seg_split_ints(F)), dtype=torch.int32, device=dev)
+
+    def lincomb_h32():                  # the certified rounds' direction: complex128 g and 2 m complex64 vectors
+        call('blml_seg_lincomb_h32', F, st_t.data_ptr(), split.data_ptr(), q.data_ptr(), 0, 1 + 2 * m,
+             cf.data_ptr(), ptrs([vecs[2 * m]] + hist32[:2 * m]), ((1 << (2 * m)) - 1) << 1, st)
     res = {'elements': n, 'vector_MB': vb / 1e6, 'K': K, 'm': m}
     for name, fn, nbytes in (('dots2', dots2, (m + 3) * vb), ('lincomb', lincomb, (2 * m + 2) * vb),
-                             ('dots2_h32', dots2_h32, (m + 1) * vb // 2 + 2 * vb)):
+                             ('dots2_h32', dots2_h32, (m + 1) * vb // 2 + 2 * vb),
+                             ('lincomb_h32', lincomb_h32, m * vb + 2 * vb)):
         for _ in range(3):
             fn()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -927,6 +935,12 @@ def main():
                                     'unit': 'GB/s', 'frac': scan['lincomb']['GB/s'] / peak,
                                     'kernel': f"k_seg_lincomb<double, double2>, the direction (41 vectors in, 1 out), "
                                               f"{scan['lincomb']['us']:.1f} us per launch"},
+               'roofline_lincomb_h32': {'bound': 'hbm', 'achieved': scan['lincomb_h32']['GB/s'], 'peak': peak,
+                                        'unit': 'GB/s', 'frac': scan['lincomb_h32']['GB/s'] / peak,
+                                        'kernel': f"k_seg_lincomb_mixed<double2>, the certified rounds' direction "
+                                                  f"(complex128 g and 40 complex64 vectors in, complex128 out), "
+                                                  f"{scan['lincomb_h32']['us']:.1f} us per call (its block split and "
+                                                  f"the combination: 2 launches)"},
                'roofline_matvec': {'bound': 'hbm', 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                                    'frac': achieved / peak, 'traffic': traffic_from_profiles(),
                                    'kernel': f'grouped mat-vec over the 64 fits (FFT route: 3 grouped launches, '

@@ -324,6 +324,13 @@ int blml_lbfgs_batch_set_history(blml_lbfgs_batch runner, int f32);
    the same F * 43 * blml_seg_blocks() doubles as blml_seg_dots2). */
 int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
                        const void* x, double* part, double* out, void* stream);
+/* The direction's linear combination of such a runner (blml_seg_lincomb, complex): out = sum_i coef[f * nterms + i]
+   v_i, bit i of f32mask marking v_i complex64, the others complex128; out complex64 (out_f32) or complex128; float64
+   arithmetic, the complex128 terms summed first, then the complex64 ones, each in term order. Blocks are shared out
+   among the fits in proportion to their sizes: split is device scratch of blml_seg_split_ints(F) ints. */
+int64_t blml_seg_split_ints(int F);
+int blml_seg_lincomb_h32(int F, const blml_seg* segs, int* split, void* out, int out_f32, int nterms,
+                         const double* coef, const void* const* v, unsigned long long f32mask, void* stream);
 int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);
 /* per fit (host arrays of F, any may be null): iterations, stop code, L, Q, max|rho| */
 int blml_lbfgs_batch_result(blml_lbfgs_batch runner, int64_t* iters, int32_t* stop, double* L, double* Q,

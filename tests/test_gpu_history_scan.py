@@ -80,3 +80,65 @@ def test_history_scan_matches_host_sums(cuda_device, case):
     err = np.abs(got - want) / scale
     assert err.max() < 1e-12, (case, err.max())
     assert np.all(got[n_f == 0] == 0.0)
+
+
+def _lincomb(dev, B, K, nt, f32mask, out_f32, inplace, seed):
+    import torch
+    from blml_b200 import _lib
+    from blml_b200._lib import call, ptrs
+    from blml_b200.sweep import _Seg
+    rng = np.random.default_rng(seed)
+    B = np.asarray(B, np.int64)
+    F = len(B)
+    n_f = K * B
+    off = np.concatenate([[0], np.cumsum(n_f)])
+    boff = np.concatenate([[0], np.cumsum(B)])
+    segs = (_Seg * F)(*[_Seg(int(off[f]), int(boff[f]), int(B[f]), int(K[f]), 0) for f in range(F)])
+    st_t = torch.frombuffer(bytearray(segs), dtype=torch.uint8).to(dev)
+    n = max(int(off[-1]), 1)
+    is32 = [bool((f32mask >> q) & 1) for q in range(nt)]
+    v = [(rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64 if w else np.complex128)
+         for w in is32]
+    coef = rng.standard_normal((F, nt))
+    coef[rng.random((F, nt)) < 0.2] = 0.0                # skipped terms
+    dv = [torch.from_numpy(x).to(dev) for x in v]
+    if inplace:                                          # out is the last term (complex64 when out_f32)
+        assert is32[-1] == out_f32
+        dout = dv[-1]
+    else:
+        dout = torch.full((n,), np.nan, dtype=torch.complex64 if out_f32 else torch.complex128, device=dev)
+    split = torch.empty(int(_lib.lib().blml_seg_split_ints(F)), dtype=torch.int32, device=dev)
+    dcoef = torch.from_numpy(coef.ravel()).to(dev)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    call('blml_seg_lincomb_h32', F, st_t.data_ptr(), split.data_ptr(), dout.data_ptr(), int(out_f32), nt,
+         dcoef.data_ptr(), ptrs(dv), f32mask, st)
+    torch.cuda.synchronize(dev)
+    got = dout.cpu().numpy().astype(np.complex128)
+    want = np.zeros(n, np.complex128)
+    for f in range(F):
+        s = slice(int(off[f]), int(off[f + 1]))
+        for q in range(nt):
+            want[s] += coef[f, q] * v[q][s].astype(np.complex128)
+    scale = sum(np.abs(x.astype(np.complex128)) for x in v) * np.abs(coef).max() + 1e-300
+    return got[:int(off[-1])], want[:int(off[-1])], scale[:int(off[-1])]
+
+
+LINCOMB = {
+    # the direction: one complex128 gradient and 40 complex64 history vectors into complex128
+    'direction': ('mixed', 41, ((1 << 40) - 1) << 1, False, False),
+    # the history update in place: complex128 q and the complex64 slot itself into that slot
+    'slot_inplace': ('mixed', 2, 0b10, True, True),
+    # complex128 terms after complex64 ones in the term list
+    'interleaved': ('tiny_only', 6, 0b010101, False, False),
+    'many_fits': ('many_fits', 5, 0b11110, False, False),
+}
+
+
+@pytest.mark.parametrize('case', sorted(LINCOMB))
+def test_history_lincomb_matches_host_sums(cuda_device, case):
+    geo, nt, mask, out_f32, inplace = LINCOMB[case]
+    B, K, _, _ = CASES[geo]
+    got, want, scale = _lincomb(cuda_device, B, np.asarray(K, np.int64), nt, mask, out_f32, inplace, seed=nt)
+    err = np.abs(got - want) / scale
+    # float64 sums of nt terms (complex64 output rounds to float32: 2^-24 of the terms' scale)
+    assert err.max() < (1e-7 if out_f32 else 1e-14), (case, err.max())
