@@ -37,6 +37,7 @@ class PointCol(C.Structure):
 
 
 PT_SINC, PT_SLITS, PT_DIRICHLET, PT_BALL = 0, 1, 2, 3
+SEG_SPLIT_BLOCKS = 2048                 # BLML_SEG_SPLIT_BLOCKS: the history kernels' blocks, shared out by fit size
 
 _P, _I, _L, _D = C.c_void_p, C.c_int, C.c_int64, C.c_double
 _SIGS = {
@@ -100,7 +101,7 @@ _SIGS = {
     'blml_lbfgs_batch_create': (_I, [_I, _I, _P, _P, _I, _D, _D, _L, _P, _P, _P, _P, _P, C.POINTER(_P)]),
     'blml_lbfgs_batch_set_caps': (_I, [_P, _P]),
     'blml_lbfgs_batch_set_history': (_I, [_P, _I]),
-    'blml_seg_dots2_h32': (_I, [_I, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
+    'blml_seg_dots2_h32': (_I, [_I, _P, _P, _I, _P, _P, _P, _P, _P, _P, _P]),
     'blml_seg_split_ints': (_L, [_I]),
     'blml_seg_lincomb_h32': (_I, [_I, _P, _P, _P, _I, _I, _P, _P, C.c_uint64, _P]),
     'blml_lanczos_coef': (_I, [_I, _I, _P, _P, _P, _I, _P]),

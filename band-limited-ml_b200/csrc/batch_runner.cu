@@ -1116,7 +1116,7 @@ int blml_lbfgs_batch_create(int dtype, int F, const blml_seg* segs, const blml_p
     }
     cudaMemsetAsync(vec, 0, 6 * tot * esz, r->st);
     cudaMemsetAsync(hv, 0, 2 * (size_t)m * tot * esz, r->st);
-    // >= Fa * seg_blocks_for(Fa) for every Fa <= F, and 48 pw >= 43 (SEG_SPLIT_BLOCKS(Fa) + Fa) for the split scan
+    // >= Fa * seg_blocks_for(Fa) for every Fa <= F, and 48 pw >= 43 (SEG_SPLIT_BLOCKS + Fa) for the split scan
     const size_t pw = (size_t)SEG_PART_WIDTH(F);
     const int nq = 48;                    // the widest reduction: blml_seg_dots' 48 accumulators
     const int hs = 2 * m + 3;

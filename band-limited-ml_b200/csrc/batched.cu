@@ -861,7 +861,7 @@ namespace blml {
 // the L-BFGS runner's history with float32 storage (internal to the library): the scan over complex64 stored vectors
 // and a complex64 first shared vector, and linear combinations over complex128 / complex64 terms
 int seg_split(int F, const blml_seg* segs, int* split, cudaStream_t st) {
-  k_seg_split<<<1, 1024, 0, st>>>(F, segs, SEG_SPLIT_BLOCKS(F), split);
+  k_seg_split<<<1, 1024, 0, st>>>(F, segs, SEG_SPLIT_BLOCKS, split);
   BLML_CHECK_LAUNCH("segment block split");
   return BLML_OK;
 }
@@ -871,7 +871,7 @@ int seg_dots2_h32(int F, const blml_seg* segs, const int* split, int np, const v
   if (np < 1 || np > 20 || !a || !b0 || !b1) { set_error("history scan: 1..20 vectors, b0 and b1"); return BLML_ERR_ARG; }
   SegList al;
   for (int q = 0; q < 20; q++) al.a[q] = q < np ? a[q] : nullptr;
-  const int W = SEG_SPLIT_BLOCKS(F) + F;
+  const int W = SEG_SPLIT_BLOCKS + F;
   k_seg_dots2_h32<<<W, 256, 0, st>>>(segs, split, F, np, al, (const float2*)b0, (const double2*)b1,
                                      (const double2*)x, part);
   BLML_CHECK_LAUNCH("history scan (float32 history)");
@@ -885,7 +885,7 @@ int seg_lincomb_mixed(int F, const blml_seg* segs, const int* split, void* out, 
   if (nterms < 1 || nterms > 48) { set_error("linear combination: 1..48 terms"); return BLML_ERR_ARG; }
   SegTerms t;
   for (int q = 0; q < 48; q++) t.v[q] = q < nterms ? v[q] : nullptr;
-  const unsigned W = (unsigned)(SEG_SPLIT_BLOCKS(F) + F);
+  const unsigned W = (unsigned)(SEG_SPLIT_BLOCKS + F);
   if (out_f32) k_seg_lincomb_mixed<float2><<<W, 256, 0, st>>>(segs, split, F, (float2*)out, nterms, coef, t, f32mask);
   else k_seg_lincomb_mixed<double2><<<W, 256, 0, st>>>(segs, split, F, (double2*)out, nterms, coef, t, f32mask);
   BLML_CHECK_LAUNCH("linear combination (mixed storage)");
@@ -1149,11 +1149,11 @@ int blml_lanczos_beta(int n, const double* dots, double* beta, double* coef, voi
   return BLML_OK;
 }
 
-int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
-                       const void* x, double* part, double* out, void* stream) {
-  if (F < 1 || F > 65535 || !segs || !a || !part) { set_error("blml_seg_dots2_h32: bad arguments"); return BLML_ERR_ARG; }
-  // the split after the partials (43 (G + F) doubles), inside the documented F * 43 * blml_seg_blocks() doubles
-  int* split = reinterpret_cast<int*>(part + 43 * ((int64_t)SEG_SPLIT_BLOCKS(F) + F));
+int blml_seg_dots2_h32(int F, const blml_seg* segs, int* split, int np, const void* const* a, const void* b0,
+                       const void* b1, const void* x, double* part, double* out, void* stream) {
+  if (F < 1 || F > 65535 || !segs || !split || !a || !part) {
+    set_error("blml_seg_dots2_h32: bad arguments"); return BLML_ERR_ARG;
+  }
   if (seg_split(F, segs, split, SST)) return BLML_ERR_CUDA;
   return seg_dots2_h32(F, segs, split, np, a, b0, b1, x, part, out, SST);
 }

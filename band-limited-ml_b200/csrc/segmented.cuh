@@ -20,16 +20,15 @@ __host__ __device__ inline int seg_blocks_for(int F) {
   return x < SEG_BLOCKS_MIN ? SEG_BLOCKS_MIN : (x > SEG_BLOCKS_MAX ? SEG_BLOCKS_MAX : x);
 }
 
-// A block split: SEG_SPLIT_BLOCKS(F) blocks in all, shared out among the fits in proportion to their element counts
+// A block split: SEG_SPLIT_BLOCKS blocks in all, shared out among the fits in proportion to their element counts
 // K B (at least one block per fit with work, none per fit without, and no more blocks than SEG_SPLIT_MIN_ELEMS-element
 // chunks), so that big and small fits finish together and every block has several tiles to stream. The split is
 // computed on the device from the segment table itself (k_seg_split), so it follows fits whose table entry the device
 // changes (a converged fit's B set to 0). Its ints: bstart[F + 1] (fit f owns split blocks
 // [bstart[f], bstart[f + 1])), then fit_of[G + F] (the fit of each block of a launch of G + F blocks, -1 for blocks
 // past the last fit's). Partials of a split reduction: quantity q of block b at part[q * (G + F) + b].
-constexpr int SEG_SPLIT_MAX = 2048, SEG_SPLIT_MIN_ELEMS = 1024;
-__host__ __device__ inline int SEG_SPLIT_BLOCKS(int F) { return 200 * F < SEG_SPLIT_MAX ? 200 * F : SEG_SPLIT_MAX; }
-__host__ __device__ inline int64_t seg_split_ints(int F) { return 2 * (int64_t)F + 1 + SEG_SPLIT_BLOCKS(F); }
+constexpr int SEG_SPLIT_BLOCKS = BLML_SEG_SPLIT_BLOCKS, SEG_SPLIT_MIN_ELEMS = 1024;
+__host__ __device__ inline int64_t seg_split_ints(int F) { return 2 * (int64_t)F + 1 + SEG_SPLIT_BLOCKS; }
 int seg_split(int F, const blml_seg* segs, int* split, cudaStream_t st);
 
 // the L-BFGS runner's float32 history (batched.cu); split: seg_split's output for these segments

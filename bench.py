@@ -390,7 +390,8 @@ def segscan_bench(dev, K=4, m=20, reps=20):
     n = int(off[-1])
     g = torch.Generator(device=dev).manual_seed(0)
     vecs = [torch.randn(n, dtype=torch.complex128, device=dev, generator=g) for _ in range(2 * m + 3)]
-    part = torch.empty(48 * F * _lib.lib().blml_seg_blocks() + 64, dtype=torch.float64, device=dev)
+    part = torch.empty(max(48 * F * _lib.lib().blml_seg_blocks(), 43 * (_lib.SEG_SPLIT_BLOCKS + F)) + 64,
+                       dtype=torch.float64, device=dev)
     out = torch.empty(48 * F + 64, dtype=torch.float64, device=dev)
     q = torch.empty_like(vecs[0])
     cf = torch.full((F, 1 + 2 * m), 0.5, dtype=torch.float64, device=dev)
@@ -406,11 +407,12 @@ def segscan_bench(dev, K=4, m=20, reps=20):
              ptrs([vecs[2 * m]] + vecs[:2 * m]), st)
     hist32 = [v.to(torch.complex64) for v in vecs[:m + 1]]          # the certified rounds' complex64 history
 
+    split = torch.empty(int(_lib.lib().blml_seg_split_ints(F)), dtype=torch.int32, device=dev)
+
     def dots2_h32():
-        call('blml_seg_dots2_h32', F, st_t.data_ptr(), m, ptrs(hist32[:m]), hist32[m].data_ptr(),
+        call('blml_seg_dots2_h32', F, st_t.data_ptr(), split.data_ptr(), m, ptrs(hist32[:m]), hist32[m].data_ptr(),
              vecs[2 * m + 1].data_ptr(), vecs[2 * m + 2].data_ptr(), part.data_ptr(), out.data_ptr(), st)
     hist32 += [v.to(torch.complex64) for v in vecs[m + 1:2 * m]]    # 2 m complex64 history vectors in all
-    split = torch.empty(int(_lib.lib().blml_seg_split_ints(F)), dtype=torch.int32, device=dev)
 
     def lincomb_h32():                  # the certified rounds' direction: complex128 g and 2 m complex64 vectors
         call('blml_seg_lincomb_h32', F, st_t.data_ptr(), split.data_ptr(), q.data_ptr(), 0, 1 + 2 * m,

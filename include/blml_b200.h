@@ -318,17 +318,18 @@ int blml_lbfgs_batch_set_caps(blml_lbfgs_batch runner, const int64_t* caps);
    and line search stay float64. No counterpart in the reference (its history is float64); for runs whose answer does
    not depend on the path, e.g. certified fits. Call before the first run. */
 int blml_lbfgs_batch_set_history(blml_lbfgs_batch runner, int f32);
-/* The history scan of such a runner (blml_seg_dots2's quantities, complex): the np stored vectors a and the first
-   shared vector b0 complex64, b1 and x complex128; float64 sums. Its blocks are shared out among the fits in
-   proportion to their sizes K B (the split is computed on the device, from segs, into the tail of part: part takes
-   the same F * 43 * blml_seg_blocks() doubles as blml_seg_dots2). */
-int blml_seg_dots2_h32(int F, const blml_seg* segs, int np, const void* const* a, const void* b0, const void* b1,
-                       const void* x, double* part, double* out, void* stream);
-/* The direction's linear combination of such a runner (blml_seg_lincomb, complex): out = sum_i coef[f * nterms + i]
-   v_i, bit i of f32mask marking v_i complex64, the others complex128; out complex64 (out_f32) or complex128; float64
-   arithmetic, the complex128 terms summed first, then the complex64 ones, each in term order. Blocks are shared out
-   among the fits in proportion to their sizes: split is device scratch of blml_seg_split_ints(F) ints. */
+/* The history kernels of such a runner share their blocks out among the fits in proportion to the fits' sizes K B:
+   BLML_SEG_SPLIT_BLOCKS blocks in all (at most one per 1024 elements of a fit), the split computed on the device from
+   segs into `split`, device scratch of blml_seg_split_ints(F) ints. */
+#define BLML_SEG_SPLIT_BLOCKS 2048
 int64_t blml_seg_split_ints(int F);
+/* The history scan (blml_seg_dots2's quantities, complex): the np stored vectors a and the first shared vector b0
+   complex64, b1 and x complex128; float64 sums. part: 43 * (BLML_SEG_SPLIT_BLOCKS + F) doubles. */
+int blml_seg_dots2_h32(int F, const blml_seg* segs, int* split, int np, const void* const* a, const void* b0,
+                       const void* b1, const void* x, double* part, double* out, void* stream);
+/* The direction's linear combination (blml_seg_lincomb, complex): out = sum_i coef[f * nterms + i] v_i, bit i of
+   f32mask marking v_i complex64, the others complex128; out complex64 (out_f32) or complex128; float64 arithmetic,
+   the complex128 terms summed first, then the complex64 ones, each in term order. */
 int blml_seg_lincomb_h32(int F, const blml_seg* segs, int* split, void* out, int out_f32, int nterms,
                          const double* coef, const void* const* v, unsigned long long f32mask, void* stream);
 int blml_lbfgs_batch_run(blml_lbfgs_batch runner, void* stream);

@@ -38,3 +38,10 @@ def test_load_and_query_without_gpu():
     assert L.blml_abi_version() == 1
     assert L.blml_reduce_blocks() > 0
     assert L.blml_last_error() is not None
+
+
+def test_split_constant_matches_header():
+    """The host's copy of BLML_SEG_SPLIT_BLOCKS (the history kernels' block count, used to size their partials)."""
+    from blml_b200 import _lib
+    hdr = open(os.path.join(ROOT, 'include', 'blml_b200.h')).read()
+    assert int(re.search(r'#define BLML_SEG_SPLIT_BLOCKS (\d+)', hdr).group(1)) == _lib.SEG_SPLIT_BLOCKS

@@ -36,10 +36,11 @@ def _scan(dev, B, K, np_, with_x, seed):
     b0, b1, x = c64(), c128(), c128()
     da = [torch.from_numpy(v).to(dev) for v in a]
     db0, db1, dx = (torch.from_numpy(v).to(dev) for v in (b0, b1, x))
-    part = torch.full((F * 43 * _lib.lib().blml_seg_blocks(),), np.nan, dtype=torch.float64, device=dev)
+    part = torch.full((43 * (_lib.SEG_SPLIT_BLOCKS + F),), np.nan, dtype=torch.float64, device=dev)
+    split = torch.empty(int(_lib.lib().blml_seg_split_ints(F)), dtype=torch.int32, device=dev)
     out = torch.full((F * (2 * np_ + 3),), np.nan, dtype=torch.float64, device=dev)
     st = torch.cuda.current_stream(dev).cuda_stream
-    call('blml_seg_dots2_h32', F, st_t.data_ptr(), np_, ptrs(da), db0.data_ptr(), db1.data_ptr(),
+    call('blml_seg_dots2_h32', F, st_t.data_ptr(), split.data_ptr(), np_, ptrs(da), db0.data_ptr(), db1.data_ptr(),
          dx.data_ptr() if with_x else C.c_void_p(0), part.data_ptr(), out.data_ptr(), st)
     torch.cuda.synchronize(dev)
     got = out.cpu().numpy().reshape(F, 2 * np_ + 3)
