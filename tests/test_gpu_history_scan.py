@@ -43,6 +43,7 @@ def _scan(dev, B, K, np_, with_x, seed):
     call('blml_seg_dots2_h32', F, st_t.data_ptr(), split.data_ptr(), np_, ptrs(da), db0.data_ptr(), db1.data_ptr(),
          dx.data_ptr() if with_x else C.c_void_p(0), part.data_ptr(), out.data_ptr(), st)
     torch.cuda.synchronize(dev)
+    _check_split(split.cpu().numpy(), n_f)
     got = out.cpu().numpy().reshape(F, 2 * np_ + 3)
 
     def rdot(u, v):                         # Re(conj(u) v) summed in float64: the scan's real inner product
@@ -59,6 +60,22 @@ def _scan(dev, B, K, np_, with_x, seed):
         want[f, 2 * np_ + 1] = rdot(b1[s], b1[s])
         want[f, 2 * np_ + 2] = rdot(x[s], x[s]) if with_x else 0.0
     return got, want, n_f
+
+
+def _check_split(split, n_f):
+    """The device's block split against its rule: fit f gets min(ceil(G n_f / N), ceil(n_f / 1024)) of the G blocks
+    (none without elements), bstart is their exclusive prefix sum and fit_of names each block's fit (-1 past the
+    last); integer work, so exact."""
+    from blml_b200 import _lib
+    G, F = _lib.SEG_SPLIT_BLOCKS, len(n_f)
+    N = int(n_f.sum())
+    nb = np.array([0 if n == 0 else min(-(-G * int(n) // N), -(-int(n) // 1024)) for n in n_f], np.int64)
+    bstart = np.concatenate([[0], np.cumsum(nb)])
+    fit_of = np.full(G + F, -1, np.int64)
+    fit_of[:bstart[-1]] = np.repeat(np.arange(F), nb)
+    assert len(split) == 2 * F + 1 + G
+    np.testing.assert_array_equal(split[:F + 1], bstart)
+    np.testing.assert_array_equal(split[F + 1:], fit_of)
 
 
 CASES = {
