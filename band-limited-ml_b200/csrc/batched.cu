@@ -189,17 +189,14 @@ __global__ void __launch_bounds__(256) k_seg_dots2(const blml_seg* segs, int cpl
 }
 
 // the same scan for float64 complex vectors, one (re, im) load per element and vector -- the stored vectors (TA)
-// and the first shared one (TB0) complex128, or complex64 when the history is kept in float32. The block's 8 warps
+// and the first shared one (TB0) complex128 (the plain fits' history; the float32 history has its own scan,
+// k_seg_dots2_h32, with twice the elements per thread and a block split by fit size). The block's 8 warps
 // split the stored vectors (warp w takes q = w, w + 8, w + 16) and walk the same 64-element tiles, so each thread
 // holds at most 6 accumulators (full occupancy, many loads in flight) and the two shared vectors are read from HBM
 // once per tile and from L1 by the other warps; the last warp also sums the three squared norms. Each quantity's
 // block partial comes from one warp (warp_sum, fixed order), in seg_partials' layout.
-// one complex element as (re, im) in float64, from complex128 or complex64 storage
+// one complex128 element as (re, im)
 __device__ __forceinline__ double2 ld_c2(const double2* p) { return __ldg(p); }
-__device__ __forceinline__ double2 ld_c2(const float2* p) {
-  const float2 v = __ldg(p);
-  return make_double2((double)v.x, (double)v.y);
-}
 
 template <typename TA, typename TB0>
 __global__ void __launch_bounds__(256, 3) k_seg_dots2_c128(const blml_seg* segs, int np, SegList al, const void* b0,
