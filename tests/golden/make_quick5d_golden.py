@@ -5,7 +5,7 @@ the reference's own binning, sinc columns at fc = 0.1 cycles per bin, float64, t
 convex (real rank 1), so its optimum is unique. Stored: the bin count, the counts' checksum, the loglik, sweeps and
 seconds, and the coefficients and densities at 2,000 sampled bins of the fit (their lattice coordinates with them).
 
-    python tests/golden/make_quick5d_golden.py <reference checkout>      (about an hour or more on 8 cores)
+    python tests/golden/make_quick5d_golden.py <reference checkout>      (about four hours on 8 cores: the fit 2.2 h)
 """
 import os
 import sys
